@@ -1,0 +1,788 @@
+/* On-device binned-SAH BVH build.
+ *
+ * The reference builds its binary SAH BVH on one CPU thread (aggregate/native/BvhBuilder.cpp:48-253,
+ * four candidate planes per axis, one O(n) pass per candidate) and its OptiX path hands the
+ * build to the driver (aggregate/api/optix/host.cpp:440-480).  Here the build runs on the GPU,
+ * top-down and breadth-first, with centroid binning:
+ *
+ *   large nodes (> kSmallTask primitives), one level per host iteration:
+ *     k_init_level   reset per-node centroid bounds and bins
+ *     k_cbounds      centroid bounds, one CTA per chunk of 4096 primitives, merged with atomics
+ *     k_bin          centroid bins per axis in shared memory, merged into the node's global bins
+ *     k_split        one CTA per node: SAH over bins*3 candidate planes, node allocation, children
+ *     k_partition    primitive ids scattered to the children's ranges of the other id buffer
+ *   small nodes (<= kSmallTask): k_build_small, one CTA per node builds its whole subtree with a
+ *     CTA-local task stack, shared-memory bins and a stable block-scan partition.
+ *
+ * Leaves list their primitives in a contiguous range of `order`; each leaf's range is finally
+ * sorted by primitive index so the layout is deterministic (atomics only reorder primitives
+ * inside a node's range, and SAH decisions depend on the set of primitives, not their order).
+ * Child boxes are padded outwards by 2^-20 relative so transformed-instance boxes stay
+ * conservative.  Below depth kMedianDepth nodes are split at their median position, which bounds
+ * the depth (and the traversal stack) for any input.
+ */
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <vector>
+
+#include "bvh_build.cuh"
+#include "traverse.cuh"
+
+namespace nb {
+namespace {
+
+constexpr int kMaxBins = 32;
+constexpr uint32_t kSmallTask = 4096;
+constexpr uint32_t kChunk = 4096;
+constexpr int kMedianDepth = 40;
+constexpr int kBlock = 256;
+constexpr int kHardLeaf = 16;
+constexpr int kSmallStack = 64;
+
+struct Task {
+  uint32_t begin, end;
+  int32_t parent, slot, depth, buf;
+  float lo[3], hi[3];
+};
+
+struct Bins {
+  unsigned cnt[3][kMaxBins];
+  float lo[3][kMaxBins][3];
+  float hi[3][kMaxBins][3];
+};
+
+struct SplitInfo {
+  int axis, bin, median;
+  uint32_t mid;
+  unsigned left_ptr, right_ptr;
+  float cmin[3], scale[3];
+};
+
+struct Chunk {
+  uint32_t task, begin, end;
+};
+
+struct Shared {
+  const float4 *lo, *hi;
+  uint32_t *ids0, *ids1;
+  float4 *nodes;
+  uint32_t *order;
+  unsigned *node_counter;
+  Task *large_next;
+  unsigned *large_next_count;
+  Task *small;
+  unsigned *small_count;
+  uint2 *leaves;
+  unsigned *leaf_count;
+  int *max_depth;
+  int bins, max_leaf;
+  float cost_trav;
+};
+
+__device__ __forceinline__ uint32_t *ids_of(const Shared &s, int buf) { return buf ? s.ids1 : s.ids0; }
+
+__device__ __forceinline__ void atomic_min_f(float *a, float v) {
+  if (v >= 0.f)
+    atomicMin(reinterpret_cast<int *>(a), __float_as_int(v));
+  else
+    atomicMax(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f(float *a, float v) {
+  if (v >= 0.f)
+    atomicMax(reinterpret_cast<int *>(a), __float_as_int(v));
+  else
+    atomicMin(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+
+__device__ __forceinline__ float3 centroid(const Shared &s, uint32_t i) {
+  float4 a = __ldg(s.lo + i), b = __ldg(s.hi + i);
+  return make_float3((a.x + b.x) * 0.5f, (a.y + b.y) * 0.5f, (a.z + b.z) * 0.5f);
+}
+__device__ __forceinline__ float comp(float3 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ float half_area(const float lo[3], const float hi[3]) {
+  float dx = fmaxf(hi[0] - lo[0], 0.f), dy = fmaxf(hi[1] - lo[1], 0.f), dz = fmaxf(hi[2] - lo[2], 0.f);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+/* Bin mapping shared by binning and partitioning (identical inputs give identical bins). */
+__device__ __forceinline__ float bin_scale(float cmin, float cmax, int nb) {
+  float ext = cmax - cmin;
+  return ext > 0.f ? (float)nb * (1.f - 1e-6f) / ext : 0.f;
+}
+__device__ __forceinline__ int bin_of(float c, float cmin, float scale, int nb) {
+  int b = (int)((c - cmin) * scale);
+  return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+}
+
+__device__ __forceinline__ float pad_lo(float x) { return x - (fabsf(x) * 9.5367431640625e-07f + 1e-30f); }
+__device__ __forceinline__ float pad_hi(float x) { return x + (fabsf(x) * 9.5367431640625e-07f + 1e-30f); }
+
+__device__ void write_child(float4 *nodes, int node, int slot, const float lo[3], const float hi[3]) {
+  float *n = reinterpret_cast<float *>(nodes + 4 * node);
+  const float lx = pad_lo(lo[0]), ly = pad_lo(lo[1]), lz = pad_lo(lo[2]);
+  const float hx = pad_hi(hi[0]), hy = pad_hi(hi[1]), hz = pad_hi(hi[2]);
+  if (slot == 0) {
+    n[0] = lx, n[1] = hx, n[2] = ly, n[3] = hy;
+    n[8] = lz, n[9] = hz;
+  } else {
+    n[4] = lx, n[5] = hx, n[6] = ly, n[7] = hy;
+    n[10] = lz, n[11] = hz;
+  }
+}
+__device__ void write_ref(float4 *nodes, int node, int slot, int32_t ref) {
+  int32_t *n = reinterpret_cast<int32_t *>(nodes + 4 * node);
+  n[12 + slot] = ref;
+  n[14 + slot] = 0;
+}
+
+/* Thread 0 only: records a finished leaf (ids already copied into order[begin, end)). */
+__device__ void finish_leaf(const Shared &s, const Task &t) {
+  const uint32_t n = t.end - t.begin;
+  const int32_t ref = leaf_ref(t.begin, n);
+  if (t.parent < 0) { /* whole scene in one leaf: root with an empty second child */
+    const float elo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, ehi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    const int node = (int)atomicAdd(s.node_counter, 1u);
+    write_child(s.nodes, node, 0, t.lo, t.hi);
+    write_child(s.nodes, node, 1, elo, ehi);
+    write_ref(s.nodes, node, 0, ref);
+    write_ref(s.nodes, node, 1, ref);
+  } else {
+    write_ref(s.nodes, t.parent, t.slot, ref);
+  }
+  unsigned li = atomicAdd(s.leaf_count, 1u);
+  s.leaves[li] = make_uint2(t.begin, n);
+  atomicMax(s.max_depth, t.depth);
+}
+
+__device__ __forceinline__ void push_task(const Shared &s, const Task &t) {
+  if (t.end - t.begin > kSmallTask) {
+    unsigned i = atomicAdd(s.large_next_count, 1u);
+    s.large_next[i] = t;
+  } else {
+    unsigned i = atomicAdd(s.small_count, 1u);
+    s.small[i] = t;
+  }
+}
+
+/* ------------------------------------------------------------------ whole-scene box */
+
+__global__ void k_scene_box(const float4 *lo, const float4 *hi, uint32_t n, float *out /* 6 */) {
+  float l[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, h[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 a = lo[i], b = hi[i];
+    l[0] = fminf(l[0], a.x), l[1] = fminf(l[1], a.y), l[2] = fminf(l[2], a.z);
+    h[0] = fmaxf(h[0], b.x), h[1] = fmaxf(h[1], b.y), h[2] = fmaxf(h[2], b.z);
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; k++) {
+      l[k] = fminf(l[k], __shfl_xor_sync(0xffffffffu, l[k], o));
+      h[k] = fmaxf(h[k], __shfl_xor_sync(0xffffffffu, h[k], o));
+    }
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; k++) {
+      atomic_min_f(out + k, l[k]);
+      atomic_max_f(out + 3 + k, h[k]);
+    }
+}
+
+__global__ void k_iota(uint32_t *ids, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ids[i] = i;
+}
+
+/* ------------------------------------------------------------------ large nodes */
+
+__global__ void k_init_level(Bins *bins, float *cb, uint32_t n_tasks, int nb) {
+  uint32_t t = blockIdx.x;
+  if (t >= n_tasks) return;
+  for (int i = threadIdx.x; i < 3 * nb; i += blockDim.x) {
+    int a = i / nb, b = i % nb;
+    bins[t].cnt[a][b] = 0u;
+    for (int k = 0; k < 3; k++) {
+      bins[t].lo[a][b][k] = FLT_MAX;
+      bins[t].hi[a][b][k] = -FLT_MAX;
+    }
+  }
+  if (threadIdx.x < 3) {
+    cb[6 * t + threadIdx.x] = FLT_MAX;
+    cb[6 * t + 3 + threadIdx.x] = -FLT_MAX;
+  }
+}
+
+__device__ __forceinline__ void block_minmax3(float l[3], float h[3], float *sh /* 6 * 32 */) {
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; k++) {
+      l[k] = fminf(l[k], __shfl_xor_sync(0xffffffffu, l[k], o));
+      h[k] = fmaxf(h[k], __shfl_xor_sync(0xffffffffu, h[k], o));
+    }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+    for (int k = 0; k < 3; k++) {
+      sh[k * 32 + w] = l[k];
+      sh[(3 + k) * 32 + w] = h[k];
+    }
+  __syncthreads();
+  for (int k = 0; k < 3; k++) {
+    float a = FLT_MAX, b = -FLT_MAX;
+    for (int j = 0; j < nw; j++) {
+      a = fminf(a, sh[k * 32 + j]);
+      b = fmaxf(b, sh[(3 + k) * 32 + j]);
+    }
+    l[k] = a;
+    h[k] = b;
+  }
+  __syncthreads();
+}
+
+__global__ void k_cbounds(Shared s, const Task *tasks, const Chunk *chunks, float *cb) {
+  __shared__ float sh[6 * 32];
+  const Chunk c = chunks[blockIdx.x];
+  const Task &t = tasks[c.task];
+  const uint32_t *src = ids_of(s, t.buf);
+  float l[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, h[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (uint32_t i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) {
+    float3 p = centroid(s, src[i]);
+    l[0] = fminf(l[0], p.x), l[1] = fminf(l[1], p.y), l[2] = fminf(l[2], p.z);
+    h[0] = fmaxf(h[0], p.x), h[1] = fmaxf(h[1], p.y), h[2] = fmaxf(h[2], p.z);
+  }
+  block_minmax3(l, h, sh);
+  if (threadIdx.x < 3) {
+    atomic_min_f(cb + 6 * c.task + threadIdx.x, l[threadIdx.x]);
+    atomic_max_f(cb + 6 * c.task + 3 + threadIdx.x, h[threadIdx.x]);
+  }
+}
+
+__global__ void k_bin(Shared s, const Task *tasks, const Chunk *chunks, const float *cb, Bins *bins) {
+  __shared__ unsigned scnt[3][kMaxBins];
+  __shared__ float slo[3][kMaxBins][3], shi[3][kMaxBins][3];
+  const int nb = s.bins;
+  const Chunk c = chunks[blockIdx.x];
+  const Task &t = tasks[c.task];
+  const uint32_t *src = ids_of(s, t.buf);
+  for (int i = threadIdx.x; i < 3 * nb; i += blockDim.x) {
+    int a = i / nb, b = i % nb;
+    scnt[a][b] = 0u;
+    for (int k = 0; k < 3; k++) slo[a][b][k] = FLT_MAX, shi[a][b][k] = -FLT_MAX;
+  }
+  float cmin[3], scale[3];
+  for (int a = 0; a < 3; a++) {
+    cmin[a] = cb[6 * c.task + a];
+    scale[a] = bin_scale(cmin[a], cb[6 * c.task + 3 + a], nb);
+  }
+  __syncthreads();
+  for (uint32_t i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) {
+    const uint32_t id = src[i];
+    const float4 bl = __ldg(s.lo + id), bh = __ldg(s.hi + id);
+    const float3 p = make_float3((bl.x + bh.x) * 0.5f, (bl.y + bh.y) * 0.5f, (bl.z + bh.z) * 0.5f);
+    for (int a = 0; a < 3; a++) {
+      const int b = bin_of(comp(p, a), cmin[a], scale[a], nb);
+      atomicAdd(&scnt[a][b], 1u);
+      atomic_min_f(&slo[a][b][0], bl.x), atomic_min_f(&slo[a][b][1], bl.y), atomic_min_f(&slo[a][b][2], bl.z);
+      atomic_max_f(&shi[a][b][0], bh.x), atomic_max_f(&shi[a][b][1], bh.y), atomic_max_f(&shi[a][b][2], bh.z);
+    }
+  }
+  __syncthreads();
+  Bins &g = bins[c.task];
+  for (int i = threadIdx.x; i < 3 * nb; i += blockDim.x) {
+    int a = i / nb, b = i % nb;
+    if (scnt[a][b] == 0u) continue;
+    atomicAdd(&g.cnt[a][b], scnt[a][b]);
+    for (int k = 0; k < 3; k++) {
+      atomic_min_f(&g.lo[a][b][k], slo[a][b][k]);
+      atomic_max_f(&g.hi[a][b][k], shi[a][b][k]);
+    }
+  }
+}
+
+/* SAH sweep over bins: best (cost, axis, plane) with a deterministic tie order. */
+struct Best {
+  float cost;
+  int key; /* axis * kMaxBins + plane; planes 1..nb-1 */
+};
+__device__ __forceinline__ bool better(const Best &a, const Best &b) {
+  return a.cost < b.cost || (a.cost == b.cost && a.key < b.key);
+}
+
+template <class CntF, class LoF, class HiF>
+__device__ Best sah_best(int nb, float parent_area, float cost_trav, CntF cnt, LoF blo, HiF bhi) {
+  Best best{FLT_MAX, 0x7fffffff};
+  for (int cand = threadIdx.x; cand < 3 * (nb - 1); cand += blockDim.x) {
+    const int a = cand / (nb - 1), plane = cand % (nb - 1) + 1;
+    unsigned nl = 0, nr = 0;
+    float ll[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, lh[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float rl[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, rh[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int b = 0; b < nb; b++) {
+      unsigned c = cnt(a, b);
+      if (!c) continue;
+      if (b < plane) {
+        nl += c;
+        for (int k = 0; k < 3; k++) ll[k] = fminf(ll[k], blo(a, b, k)), lh[k] = fmaxf(lh[k], bhi(a, b, k));
+      } else {
+        nr += c;
+        for (int k = 0; k < 3; k++) rl[k] = fminf(rl[k], blo(a, b, k)), rh[k] = fmaxf(rh[k], bhi(a, b, k));
+      }
+    }
+    if (nl == 0 || nr == 0) continue;
+    const float cost = cost_trav + (half_area(ll, lh) * (float)nl + half_area(rl, rh) * (float)nr) / parent_area;
+    Best c{cost, a * kMaxBins + plane};
+    if (better(c, best)) best = c;
+  }
+  return best;
+}
+
+__device__ Best block_best(Best b, Best *sh) {
+  for (int o = 16; o > 0; o >>= 1) {
+    Best q{__shfl_xor_sync(0xffffffffu, b.cost, o), __shfl_xor_sync(0xffffffffu, b.key, o)};
+    if (better(q, b)) b = q;
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = b;
+  __syncthreads();
+  Best r = sh[0];
+  for (int j = 1; j < (int)(blockDim.x >> 5); j++)
+    if (better(sh[j], r)) r = sh[j];
+  __syncthreads();
+  return r;
+}
+
+__global__ void k_split(Shared s, const Task *tasks, const float *cb, const Bins *bins, SplitInfo *splits) {
+  __shared__ Best sh[kBlock / 32];
+  const Task t = tasks[blockIdx.x];
+  const Bins &B = bins[blockIdx.x];
+  const int nb = s.bins;
+  const float area = half_area(t.lo, t.hi);
+  Best best{FLT_MAX, 0x7fffffff};
+  if (area > 0.f && t.depth < kMedianDepth)
+    best = sah_best(
+        nb, area, s.cost_trav, [&](int a, int b) { return B.cnt[a][b]; },
+        [&](int a, int b, int k) { return B.lo[a][b][k]; }, [&](int a, int b, int k) { return B.hi[a][b][k]; });
+  best = block_best(best, sh);
+  if (threadIdx.x != 0) return;
+  SplitInfo sp;
+  for (int a = 0; a < 3; a++) {
+    sp.cmin[a] = cb[6 * blockIdx.x + a];
+    sp.scale[a] = bin_scale(sp.cmin[a], cb[6 * blockIdx.x + 3 + a], nb);
+  }
+  float llo[3], lhi[3], rlo[3], rhi[3];
+  const uint32_t n = t.end - t.begin;
+  if (best.key != 0x7fffffff) {
+    sp.median = 0;
+    sp.axis = best.key / kMaxBins;
+    sp.bin = best.key % kMaxBins - 1; /* left side: bins <= sp.bin */
+    unsigned nl = 0;
+    for (int k = 0; k < 3; k++) llo[k] = rlo[k] = FLT_MAX, lhi[k] = rhi[k] = -FLT_MAX;
+    for (int b = 0; b < nb; b++) {
+      const unsigned c = B.cnt[sp.axis][b];
+      if (!c) continue;
+      float *l = b <= sp.bin ? llo : rlo, *h = b <= sp.bin ? lhi : rhi;
+      if (b <= sp.bin) nl += c;
+      for (int k = 0; k < 3; k++) l[k] = fminf(l[k], B.lo[sp.axis][b][k]), h[k] = fmaxf(h[k], B.hi[sp.axis][b][k]);
+    }
+    sp.mid = t.begin + nl;
+  } else {
+    sp.median = 1;
+    sp.axis = 0;
+    sp.bin = 0;
+    sp.mid = t.begin + n / 2;
+    for (int k = 0; k < 3; k++) llo[k] = rlo[k] = t.lo[k], lhi[k] = rhi[k] = t.hi[k];
+  }
+  sp.left_ptr = t.begin;
+  sp.right_ptr = sp.mid;
+  splits[blockIdx.x] = sp;
+  const int node = (int)atomicAdd(s.node_counter, 1u);
+  if (t.parent >= 0) write_ref(s.nodes, t.parent, t.slot, node);
+  write_child(s.nodes, node, 0, llo, lhi);
+  write_child(s.nodes, node, 1, rlo, rhi);
+  Task L{t.begin, sp.mid, node, 0, t.depth + 1, 1 - t.buf, {llo[0], llo[1], llo[2]}, {lhi[0], lhi[1], lhi[2]}};
+  Task R{sp.mid, t.end, node, 1, t.depth + 1, 1 - t.buf, {rlo[0], rlo[1], rlo[2]}, {rhi[0], rhi[1], rhi[2]}};
+  push_task(s, L);
+  push_task(s, R);
+}
+
+__global__ void k_partition(Shared s, const Task *tasks, const Chunk *chunks, SplitInfo *splits) {
+  __shared__ unsigned warp_l[kBlock / 32], warp_r[kBlock / 32];
+  __shared__ unsigned base_l, base_r;
+  const Chunk c = chunks[blockIdx.x];
+  const Task &t = tasks[c.task];
+  SplitInfo &sp = splits[c.task];
+  const uint32_t *src = ids_of(s, t.buf);
+  uint32_t *dst = ids_of(s, 1 - t.buf);
+  const int nb = s.bins;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t r0 = c.begin; r0 < c.end; r0 += blockDim.x) {
+    const uint32_t i = r0 + threadIdx.x;
+    const bool valid = i < c.end;
+    uint32_t id = 0;
+    bool left = false;
+    if (valid) {
+      id = src[i];
+      if (sp.median)
+        left = i < sp.mid;
+      else
+        left = bin_of(comp(centroid(s, id), sp.axis), sp.cmin[sp.axis], sp.scale[sp.axis], nb) <= sp.bin;
+    }
+    const unsigned ml = __ballot_sync(0xffffffffu, valid && left), mr = __ballot_sync(0xffffffffu, valid && !left);
+    if (lane == 0) warp_l[w] = __popc(ml), warp_r[w] = __popc(mr);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tl = 0, tr = 0;
+      for (int j = 0; j < (int)(blockDim.x >> 5); j++) {
+        unsigned a = warp_l[j], b = warp_r[j];
+        warp_l[j] = tl, warp_r[j] = tr;
+        tl += a, tr += b;
+      }
+      base_l = atomicAdd(&sp.left_ptr, tl);
+      base_r = atomicAdd(&sp.right_ptr, tr);
+    }
+    __syncthreads();
+    const unsigned below = (1u << lane) - 1u;
+    if (valid) {
+      if (left)
+        dst[base_l + warp_l[w] + __popc(ml & below)] = id;
+      else
+        dst[base_r + warp_r[w] + __popc(mr & below)] = id;
+    }
+    __syncthreads();
+  }
+}
+
+/* ------------------------------------------------------------------ small nodes */
+
+__device__ unsigned block_exclusive_scan(unsigned v, unsigned *sh /* 32 */, unsigned *total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned run = 0;
+    for (int j = 0; j < nw; j++) {
+      unsigned a = sh[j];
+      sh[j] = run;
+      run += a;
+    }
+    sh[31] = run;
+  }
+  __syncthreads();
+  const unsigned r = sh[w] + x - v;
+  *total = sh[31];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kBlock) k_build_small(Shared s, const Task *small_tasks) {
+  __shared__ Task stack[kSmallStack];
+  __shared__ int sp, have;
+  __shared__ unsigned scnt[3][kMaxBins];
+  __shared__ float slo[3][kMaxBins][3], shi[3][kMaxBins][3];
+  __shared__ float red[6 * 32];
+  __shared__ unsigned scan_sh[32];
+  __shared__ Best best_sh[kBlock / 32];
+  __shared__ Task cur;
+  __shared__ float cmin_s[3], scale_s[3];
+  const int nb = s.bins;
+  if (threadIdx.x == 0) {
+    stack[0] = small_tasks[blockIdx.x];
+    sp = 1;
+  }
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      have = sp > 0;
+      if (have) cur = stack[--sp];
+    }
+    __syncthreads();
+    if (!have) break;
+    const Task t = cur;
+    const uint32_t n = t.end - t.begin;
+    const uint32_t *src = ids_of(s, t.buf);
+    uint32_t *dst = ids_of(s, 1 - t.buf);
+    bool make_leaf = n <= 1;
+    /* centroid bounds */
+    float l[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, h[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
+      float3 p = centroid(s, src[i]);
+      l[0] = fminf(l[0], p.x), l[1] = fminf(l[1], p.y), l[2] = fminf(l[2], p.z);
+      h[0] = fmaxf(h[0], p.x), h[1] = fmaxf(h[1], p.y), h[2] = fmaxf(h[2], p.z);
+    }
+    block_minmax3(l, h, red);
+    if (threadIdx.x < 3) {
+      cmin_s[threadIdx.x] = l[threadIdx.x];
+      scale_s[threadIdx.x] = bin_scale(l[threadIdx.x], h[threadIdx.x], nb);
+    }
+    for (int i = threadIdx.x; i < 3 * nb; i += blockDim.x) {
+      int a = i / nb, b = i % nb;
+      scnt[a][b] = 0u;
+      for (int k = 0; k < 3; k++) slo[a][b][k] = FLT_MAX, shi[a][b][k] = -FLT_MAX;
+    }
+    __syncthreads();
+    Best best{FLT_MAX, 0x7fffffff};
+    const float area = half_area(t.lo, t.hi);
+    if (!make_leaf) {
+      for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
+        const uint32_t id = src[i];
+        const float4 bl = __ldg(s.lo + id), bh = __ldg(s.hi + id);
+        const float3 p = make_float3((bl.x + bh.x) * 0.5f, (bl.y + bh.y) * 0.5f, (bl.z + bh.z) * 0.5f);
+        for (int a = 0; a < 3; a++) {
+          const int b = bin_of(comp(p, a), cmin_s[a], scale_s[a], nb);
+          atomicAdd(&scnt[a][b], 1u);
+          atomic_min_f(&slo[a][b][0], bl.x), atomic_min_f(&slo[a][b][1], bl.y), atomic_min_f(&slo[a][b][2], bl.z);
+          atomic_max_f(&shi[a][b][0], bh.x), atomic_max_f(&shi[a][b][1], bh.y), atomic_max_f(&shi[a][b][2], bh.z);
+        }
+      }
+      __syncthreads();
+      if (area > 0.f && t.depth < kMedianDepth)
+        best = sah_best(
+            nb, area, s.cost_trav, [&](int a, int b) { return scnt[a][b]; },
+            [&](int a, int b, int k) { return slo[a][b][k]; }, [&](int a, int b, int k) { return shi[a][b][k]; });
+    }
+    best = block_best(best, best_sh);
+    const bool has_split = best.key != 0x7fffffff;
+    if (!make_leaf) {
+      const float leaf_cost = (float)n;
+      if ((int)n <= s.max_leaf && (!has_split || leaf_cost <= best.cost)) make_leaf = true;
+      if ((int)n <= kHardLeaf && !has_split) make_leaf = true;
+    }
+    if (make_leaf) {
+      for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) s.order[i] = src[i];
+      if (threadIdx.x == 0) finish_leaf(s, t);
+      continue;
+    }
+    /* partition into dst (stable), then child boxes */
+    const int axis = has_split ? best.key / kMaxBins : 0;
+    const int split_bin = has_split ? best.key % kMaxBins - 1 : 0;
+    const uint32_t mid_med = t.begin + n / 2;
+    unsigned left_total = 0;
+    {
+      /* count left first */
+      unsigned cnt = 0;
+      for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
+        bool left = has_split ? bin_of(comp(centroid(s, src[i]), axis), cmin_s[axis], scale_s[axis], nb) <= split_bin
+                              : i < mid_med;
+        cnt += left;
+      }
+      unsigned tot;
+      block_exclusive_scan(cnt, scan_sh, &tot);
+      left_total = tot;
+    }
+    const uint32_t mid = t.begin + left_total;
+    unsigned run_l = 0, run_r = 0;
+    for (uint32_t r0 = t.begin; r0 < t.end; r0 += blockDim.x) {
+      const uint32_t i = r0 + threadIdx.x;
+      const bool valid = i < t.end;
+      uint32_t id = 0;
+      bool left = false;
+      if (valid) {
+        id = src[i];
+        left = has_split ? bin_of(comp(centroid(s, id), axis), cmin_s[axis], scale_s[axis], nb) <= split_bin
+                         : i < mid_med;
+      }
+      unsigned tl, tr;
+      const unsigned pl = block_exclusive_scan(valid && left, scan_sh, &tl);
+      const unsigned pr = block_exclusive_scan(valid && !left, scan_sh, &tr);
+      if (valid) {
+        if (left)
+          dst[t.begin + run_l + pl] = id;
+        else
+          dst[mid + run_r + pr] = id;
+      }
+      run_l += tl;
+      run_r += tr;
+    }
+    __syncthreads();
+    /* exact child boxes */
+    float cl[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, ch[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float dl[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, dh[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
+      const uint32_t id = dst[i];
+      const float4 bl = __ldg(s.lo + id), bh = __ldg(s.hi + id);
+      float *ol = i < mid ? cl : dl, *oh = i < mid ? ch : dh;
+      ol[0] = fminf(ol[0], bl.x), ol[1] = fminf(ol[1], bl.y), ol[2] = fminf(ol[2], bl.z);
+      oh[0] = fmaxf(oh[0], bh.x), oh[1] = fmaxf(oh[1], bh.y), oh[2] = fmaxf(oh[2], bh.z);
+    }
+    block_minmax3(cl, ch, red);
+    block_minmax3(dl, dh, red);
+    if (threadIdx.x == 0) {
+      const int node = (int)atomicAdd(s.node_counter, 1u);
+      if (t.parent >= 0) write_ref(s.nodes, t.parent, t.slot, node);
+      write_child(s.nodes, node, 0, cl, ch);
+      write_child(s.nodes, node, 1, dl, dh);
+      Task L{t.begin, mid, node, 0, t.depth + 1, 1 - t.buf, {cl[0], cl[1], cl[2]}, {ch[0], ch[1], ch[2]}};
+      Task R{mid, t.end, node, 1, t.depth + 1, 1 - t.buf, {dl[0], dl[1], dl[2]}, {dh[0], dh[1], dh[2]}};
+      if (sp + 2 <= kSmallStack) { /* depth-first: at most one pending sibling per level */
+        stack[sp++] = R;
+        stack[sp++] = L;
+      }
+    }
+  }
+}
+
+__global__ void k_sort_leaves(const uint2 *leaves, unsigned n, uint32_t *order) {
+  unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint2 L = leaves[i];
+  uint32_t *o = order + L.x;
+  for (uint32_t a = 1; a < L.y; a++) {
+    uint32_t v = o[a];
+    int b = (int)a - 1;
+    while (b >= 0 && o[b] > v) {
+      o[b + 1] = o[b];
+      b--;
+    }
+    o[b + 1] = v;
+  }
+}
+
+}  // namespace
+
+cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhBuildParams &p, float4 *nodes,
+                      uint32_t *order, cudaStream_t stream, BvhBuildResult *res) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (n == 0) return cudaErrorInvalidValue;
+  const int nb = std::max(4, std::min(kMaxBins, p.bins > 0 ? p.bins : 16));
+  const int max_leaf = std::max(1, std::min(kHardLeaf, p.max_leaf > 0 ? p.max_leaf : 8));
+  const size_t max_large = n / kSmallTask + 2;
+  const size_t max_small = n + 1;
+  /* scratch */
+  uint32_t *ids0 = nullptr, *ids1 = nullptr;
+  Task *large_a = nullptr, *large_b = nullptr, *small = nullptr;
+  unsigned *counters = nullptr; /* node, large_next, small, leaf */
+  uint2 *leaves = nullptr;
+  int *maxdepth = nullptr;
+  float *scene = nullptr, *cb = nullptr;
+  Bins *bins = nullptr;
+  SplitInfo *splits = nullptr;
+  Chunk *chunks = nullptr;
+  const size_t max_chunks = n / kChunk + max_large + 2;
+  cudaError_t err = cudaSuccess;
+#define NB_TRY(x)                        \
+  do {                                   \
+    err = (x);                           \
+    if (err != cudaSuccess) goto cleanup; \
+  } while (0)
+  {
+    NB_TRY(cudaMallocAsync(&ids0, sizeof(uint32_t) * n, stream));
+    NB_TRY(cudaMallocAsync(&ids1, sizeof(uint32_t) * n, stream));
+    NB_TRY(cudaMallocAsync(&large_a, sizeof(Task) * max_large, stream));
+    NB_TRY(cudaMallocAsync(&large_b, sizeof(Task) * max_large, stream));
+    NB_TRY(cudaMallocAsync(&small, sizeof(Task) * max_small, stream));
+    NB_TRY(cudaMallocAsync(&counters, sizeof(unsigned) * 4, stream));
+    NB_TRY(cudaMallocAsync(&leaves, sizeof(uint2) * n, stream));
+    NB_TRY(cudaMallocAsync(&maxdepth, sizeof(int), stream));
+    NB_TRY(cudaMallocAsync(&scene, sizeof(float) * 6, stream));
+    NB_TRY(cudaMallocAsync(&cb, sizeof(float) * 6 * max_large, stream));
+    NB_TRY(cudaMallocAsync(&bins, sizeof(Bins) * max_large, stream));
+    NB_TRY(cudaMallocAsync(&splits, sizeof(SplitInfo) * max_large, stream));
+    NB_TRY(cudaMallocAsync(&chunks, sizeof(Chunk) * max_chunks, stream));
+    NB_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * 4, stream));
+    NB_TRY(cudaMemsetAsync(maxdepth, 0, sizeof(int), stream));
+    {
+      const float init[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+      NB_TRY(cudaMemcpyAsync(scene, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    }
+    k_scene_box<<<std::min<uint32_t>(1024, (n + 255) / 256), 256, 0, stream>>>(lo, hi, n, scene);
+    k_iota<<<(n + 255) / 256, 256, 0, stream>>>(ids0, n);
+    NB_TRY(cudaGetLastError());
+    float hscene[6];
+    NB_TRY(cudaMemcpyAsync(hscene, scene, sizeof(hscene), cudaMemcpyDeviceToHost, stream));
+    NB_TRY(cudaStreamSynchronize(stream));
+
+    Shared sh;
+    sh.lo = lo;
+    sh.hi = hi;
+    sh.ids0 = ids0;
+    sh.ids1 = ids1;
+    sh.nodes = nodes;
+    sh.order = order;
+    sh.node_counter = counters + 0;
+    sh.large_next_count = counters + 1;
+    sh.small_count = counters + 2;
+    sh.leaf_count = counters + 3;
+    sh.small = small;
+    sh.leaves = leaves;
+    sh.max_depth = maxdepth;
+    sh.bins = nb;
+    sh.max_leaf = max_leaf;
+    sh.cost_trav = p.cost_trav > 0.f ? p.cost_trav : 1.0f;
+
+    Task root{0u, n, -1, 0, 0, 0, {hscene[0], hscene[1], hscene[2]}, {hscene[3], hscene[4], hscene[5]}};
+    std::vector<Task> level;
+    if (n > kSmallTask) {
+      level.push_back(root);
+    } else {
+      NB_TRY(cudaMemcpyAsync(small, &root, sizeof(Task), cudaMemcpyHostToDevice, stream));
+      const unsigned one = 1;
+      NB_TRY(cudaMemcpyAsync(counters + 2, &one, sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+    }
+    Task *cur = large_a, *next = large_b;
+    while (!level.empty()) {
+      std::vector<Chunk> ch;
+      for (uint32_t ti = 0; ti < level.size(); ti++)
+        for (uint32_t b = level[ti].begin; b < level[ti].end; b += kChunk)
+          ch.push_back(Chunk{ti, b, std::min(level[ti].end, b + kChunk)});
+      const uint32_t nt = (uint32_t)level.size(), nc = (uint32_t)ch.size();
+      NB_TRY(cudaMemcpyAsync(cur, level.data(), sizeof(Task) * nt, cudaMemcpyHostToDevice, stream));
+      NB_TRY(cudaMemcpyAsync(chunks, ch.data(), sizeof(Chunk) * nc, cudaMemcpyHostToDevice, stream));
+      NB_TRY(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned), stream));
+      sh.large_next = next;
+      k_init_level<<<nt, 128, 0, stream>>>(bins, cb, nt, nb);
+      k_cbounds<<<nc, kBlock, 0, stream>>>(sh, cur, chunks, cb);
+      k_bin<<<nc, kBlock, 0, stream>>>(sh, cur, chunks, cb, bins);
+      k_split<<<nt, kBlock, 0, stream>>>(sh, cur, cb, bins, splits);
+      k_partition<<<nc, kBlock, 0, stream>>>(sh, cur, chunks, splits);
+      NB_TRY(cudaGetLastError());
+      unsigned n_next = 0;
+      NB_TRY(cudaMemcpyAsync(&n_next, counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+      NB_TRY(cudaStreamSynchronize(stream));
+      level.resize(n_next);
+      if (n_next) NB_TRY(cudaMemcpyAsync(level.data(), next, sizeof(Task) * n_next, cudaMemcpyDeviceToHost, stream));
+      NB_TRY(cudaStreamSynchronize(stream));
+      std::swap(cur, next);
+    }
+    unsigned n_small = 0;
+    NB_TRY(cudaMemcpyAsync(&n_small, counters + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    NB_TRY(cudaStreamSynchronize(stream));
+    if (n_small) k_build_small<<<n_small, kBlock, 0, stream>>>(sh, small);
+    NB_TRY(cudaGetLastError());
+    unsigned hc[4];
+    int hdepth = 0;
+    NB_TRY(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+    NB_TRY(cudaMemcpyAsync(&hdepth, maxdepth, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    NB_TRY(cudaStreamSynchronize(stream));
+    if (hc[3]) k_sort_leaves<<<(hc[3] + 255) / 256, 256, 0, stream>>>(leaves, hc[3], order);
+    NB_TRY(cudaGetLastError());
+    NB_TRY(cudaStreamSynchronize(stream));
+    if (res) {
+      res->n_nodes = hc[0];
+      res->n_leaves = hc[3];
+      res->max_depth = hdepth;
+    }
+  }
+cleanup:
+  cudaFreeAsync(ids0, stream);
+  cudaFreeAsync(ids1, stream);
+  cudaFreeAsync(large_a, stream);
+  cudaFreeAsync(large_b, stream);
+  cudaFreeAsync(small, stream);
+  cudaFreeAsync(counters, stream);
+  cudaFreeAsync(leaves, stream);
+  cudaFreeAsync(maxdepth, stream);
+  cudaFreeAsync(scene, stream);
+  cudaFreeAsync(cb, stream);
+  cudaFreeAsync(bins, stream);
+  cudaFreeAsync(splits, stream);
+  cudaFreeAsync(chunks, stream);
+  cudaStreamSynchronize(stream);
+#undef NB_TRY
+  if (res) res->ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return err;
+}
+
+}  // namespace nb

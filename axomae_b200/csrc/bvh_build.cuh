@@ -1,0 +1,28 @@
+/* On-device binned-SAH BVH build (declarations).  See bvh_build.cu. */
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nb {
+
+struct BvhBuildParams {
+  int max_leaf;     /* preferred maximum leaf size (SAH may stop earlier); hard cap 16 */
+  int bins;         /* SAH bins per axis (<= 32) */
+  float cost_trav;  /* SAH cost of one inner-node visit relative to one triangle test */
+};
+
+struct BvhBuildResult {
+  uint32_t n_nodes;
+  uint32_t n_leaves;
+  int max_depth;
+  double ms;
+};
+
+/* Builds a binary BVH over n primitive boxes (lo/hi: world-space, float4 with w unused).
+ * nodes: room for max(2n, 2) nodes (4 float4 each, layout in device_scene.cuh).
+ * order: receives, for every leaf slot, the index (into lo/hi) of the primitive stored there.
+ * Returns a CUDA error code (cudaSuccess on success). */
+cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhBuildParams &p, float4 *nodes,
+                      uint32_t *order, cudaStream_t stream, BvhBuildResult *res);
+
+}  // namespace nb

@@ -1,0 +1,449 @@
+/* C-ABI entry points: context lifecycle, scene upload, BVH build, queries.
+ *
+ * Upload (Engine::buildScene, api/engine.cpp:201-233): mesh attribute spans, instances with their
+ * transform records, materials and textures are validated on the host and copied to device
+ * memory; the global primitive order is the reference's (instance by instance, triangle by
+ * triangle, api/engine.cpp:159-175).  Triangles whose indices repeat are never hit by the
+ * reference (Triangle::isDegenerate, shape/Triangle.h:127-132) and are left out of the BVH.
+ *
+ * Build (Engine::buildAcceleration, api/engine.cpp:235): world boxes of the valid triangles
+ * (transform.m * vertex, Triangle::computeAABB, Triangle.h:99-109) -> device binned SAH
+ * (bvh_build.cu) -> structural validation (every inner reference points to a later node, every
+ * leaf range is in bounds, so traversal always terminates) -> triangle records in leaf order.
+ */
+#include <cmath>
+#include <cstring>
+
+#include "bvh_build.cuh"
+#include "context.cuh"
+#include "traverse.cuh"
+
+namespace {
+
+struct JoeKuoRow {
+  int d, s, a;
+  int m[12];
+};
+const JoeKuoRow kJoeKuo[255] = {
+#include "joe_kuo_params.inc"
+};
+
+/* Direction numbers V_i = m_i << (32 - i) from the Joe & Kuo recurrence
+ * m_k = (m_{k-s} << s) ^ m_{k-s} ^ XOR_{j=1..s-1} a_j (m_{k-j} << j), a_1 the most significant
+ * of the s - 1 coefficient bits (the reference's scripts/generate_luts_sobol.py:51-95). */
+void sobol_table(std::vector<uint32_t> &t) {
+  t.assign(256 * 32, 0u);
+  for (int d = 0; d < 255; d++) {
+    const JoeKuoRow &r = kJoeKuo[d];
+    uint64_t m[32];
+    for (int k = 0; k < 32; k++) {
+      if (k < r.s) {
+        m[k] = (uint64_t)r.m[k];
+        continue;
+      }
+      uint64_t v = (m[k - r.s] << r.s) ^ m[k - r.s];
+      for (int j = 1; j < r.s; j++)
+        if ((r.a >> (r.s - 1 - j)) & 1) v ^= m[k - j] << j;
+      m[k] = v;
+    }
+    for (int i = 0; i < 32; i++) t[d * 32 + i] = (uint32_t)(m[i] << (31 - i));
+  }
+}
+
+/* acos table f(i) = acos(2 i / P - 1), P = 500000, rounded to float
+ * (scripts/generate_luts_trigonometrics.py:11-18, looked up by math_acos_lt.cpp:37-40). */
+void acos_table(std::vector<float> &t) {
+  t.resize(nb::kAcosPrecision);
+  for (int i = 0; i < nb::kAcosPrecision; i++)
+    t[i] = (float)std::acos(((double)i / (double)nb::kAcosPrecision) * 2.0 - 1.0);
+}
+
+bool is_identity(const float *m) {
+  for (int c = 0; c < 4; c++)
+    for (int r = 0; r < 4; r++)
+      if (m[4 * c + r] != (c == r ? 1.f : 0.f)) return false;
+  return true;
+}
+
+template <class T>
+nova_b200_status upload(nova_b200_ctx *c, const T *src, size_t n, T **dst) {
+  *dst = nullptr;
+  if (n == 0) return NOVA_B200_SUCCESS;
+  void *p = nullptr;
+  NB_CUDA(c, cudaMalloc(&p, sizeof(T) * n), "cudaMalloc(scene)");
+  c->scene_allocs.push_back(p);
+  c->scene_bytes += sizeof(T) * n;
+  NB_CUDA(c, cudaMemcpyAsync(p, src, sizeof(T) * n, cudaMemcpyHostToDevice, c->stream), "cudaMemcpy(scene)");
+  *dst = static_cast<T *>(p);
+  return NOVA_B200_SUCCESS;
+}
+
+void free_scene(nova_b200_ctx *c) {
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void *p : c->scene_allocs) cudaFree(p);
+  c->scene_allocs.clear();
+  cudaFree(c->d_nodes);
+  cudaFree(c->d_tris);
+  c->d_nodes = nullptr;
+  c->d_tris = nullptr;
+  c->scene = nb::DevScene{};
+  c->h_instances.clear();
+  c->h_valid.clear();
+  c->scene_ready = c->bvh_ready = false;
+  c->scene_bytes = 0;
+  c->n_nodes = c->n_leaves = 0;
+}
+
+/* ------------------------------------------------------------------ build kernels */
+
+__global__ void k_prim_boxes(nb::DevScene sc, const uint32_t *valid, uint32_t n, float4 *lo, float4 *hi) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t prim = valid[i];
+  const uint32_t inst = sc.prim_inst[prim];
+  const nb::DevInstance &I = sc.instances[inst];
+  const nb::DevMesh &m = sc.meshes[I.mesh];
+  const uint32_t tri = prim - I.prim_offset;
+  nb::V3 w[3];
+  for (int k = 0; k < 3; k++) {
+    const uint32_t vi = m.idx[3 * tri + k];
+    nb::V3 v{m.v[3 * vi], m.v[3 * vi + 1], m.v[3 * vi + 2]};
+    w[k] = I.identity ? v : nb::xform_point(I.m, v);
+  }
+  lo[i] = make_float4(fminf(w[0].x, fminf(w[1].x, w[2].x)), fminf(w[0].y, fminf(w[1].y, w[2].y)),
+                      fminf(w[0].z, fminf(w[1].z, w[2].z)), 0.f);
+  hi[i] = make_float4(fmaxf(w[0].x, fmaxf(w[1].x, w[2].x)), fmaxf(w[0].y, fmaxf(w[1].y, w[2].y)),
+                      fmaxf(w[0].z, fmaxf(w[1].z, w[2].z)), 0.f);
+}
+
+/* Triangle records in leaf order: (v0, prim id), (v1 - v0, instance), (v2 - v0, 0), object space. */
+__global__ void k_write_tris(nb::DevScene sc, const uint32_t *valid, const uint32_t *order, uint32_t n, float4 *tris) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t prim = valid[order[k]];
+  const uint32_t inst = sc.prim_inst[prim];
+  const nb::DevInstance &I = sc.instances[inst];
+  const nb::DevMesh &m = sc.meshes[I.mesh];
+  const uint32_t tri = prim - I.prim_offset;
+  const uint32_t a = m.idx[3 * tri], b = m.idx[3 * tri + 1], cc = m.idx[3 * tri + 2];
+  const nb::V3 v0{m.v[3 * a], m.v[3 * a + 1], m.v[3 * a + 2]};
+  const nb::V3 v1{m.v[3 * b], m.v[3 * b + 1], m.v[3 * b + 2]};
+  const nb::V3 v2{m.v[3 * cc], m.v[3 * cc + 1], m.v[3 * cc + 2]};
+  const nb::V3 e1 = v1 - v0, e2 = v2 - v0;
+  tris[3 * k + 0] = make_float4(v0.x, v0.y, v0.z, __int_as_float((int)prim));
+  tris[3 * k + 1] = make_float4(e1.x, e1.y, e1.z, __int_as_float((int)inst));
+  tris[3 * k + 2] = make_float4(e2.x, e2.y, e2.z, 0.f);
+}
+
+__global__ void k_validate(const float4 *nodes, uint32_t n_nodes, uint32_t n_tris, unsigned *bad) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_nodes) return;
+  const float4 n3 = nodes[4 * i + 3];
+  const int32_t r[2] = {__float_as_int(n3.x), __float_as_int(n3.y)};
+  for (int s = 0; s < 2; s++) {
+    if (r[s] >= 0) {
+      if ((uint32_t)r[s] <= i || (uint32_t)r[s] >= n_nodes) atomicAdd(bad, 1u);
+    } else {
+      const uint32_t f = nb::leaf_first(r[s]), cnt = nb::leaf_count(r[s]);
+      if (f + cnt > n_tris) atomicAdd(bad, 1u);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+nova_b200_status nova_b200_create(nova_b200_ctx **out, int32_t device) {
+  if (!out) return NOVA_B200_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return NOVA_B200_NOT_GPU_BUILD;
+  if (device < 0 || device >= count) return NOVA_B200_INVALID_ARGUMENT;
+  nova_b200_ctx *c = new nova_b200_ctx();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev_begin) != cudaSuccess || cudaEventCreate(&c->ev_end) != cudaSuccess ||
+      cudaEventCreate(&c->ev_a) != cudaSuccess || cudaEventCreate(&c->ev_b) != cudaSuccess) {
+    delete c;
+    return NOVA_B200_RENDER_ENGINE_NOT_INITIALIZED;
+  }
+  std::vector<uint32_t> sob;
+  std::vector<float> ac;
+  sobol_table(sob);
+  acos_table(ac);
+  if (cudaMalloc(&c->d_sobol, sob.size() * 4) != cudaSuccess || cudaMalloc(&c->d_acos, ac.size() * 4) != cudaSuccess ||
+      cudaMalloc(&c->d_counters, 64) != cudaSuccess || cudaMallocHost(&c->h_counters, 64) != cudaSuccess) {
+    nova_b200_destroy(c);
+    return NOVA_B200_OUT_OF_MEMORY;
+  }
+  cudaMemcpy(c->d_sobol, sob.data(), sob.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->d_acos, ac.data(), ac.size() * 4, cudaMemcpyHostToDevice);
+  *out = c;
+  return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nova_b200_destroy(nova_b200_ctx *c) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  free_scene(c);
+  cudaFree(c->d_sobol);
+  cudaFree(c->d_acos);
+  cudaFree(c->d_counters);
+  cudaFree(c->d_film_acc);
+  cudaFree(c->d_queue);
+  cudaFree(c->d_radiance);
+  cudaFree(c->d_film_out);
+  if (c->h_counters) cudaFreeHost(c->h_counters);
+  if (c->ev_begin) cudaEventDestroy(c->ev_begin);
+  if (c->ev_end) cudaEventDestroy(c->ev_end);
+  if (c->ev_a) cudaEventDestroy(c->ev_a);
+  if (c->ev_b) cudaEventDestroy(c->ev_b);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_desc *d) {
+  using namespace nbctx;
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  if (!d) return fail(c, NOVA_B200_INVALID_ARGUMENT, "scene descriptor is null%s");
+  cudaSetDevice(c->device);
+  free_scene(c);
+  if (d->n_instances == 0 || !d->instances || !d->meshes || d->n_meshes == 0)
+    return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "scene has no meshes or instances%s");
+  if (d->envmap < 0 || (uint32_t)d->envmap >= d->n_textures || !d->textures[d->envmap].f32_pixels ||
+      d->textures[d->envmap].channels != 4)
+    return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "environment map must be a 4-channel float texture%s");
+  /* textures */
+  std::vector<nb::DevTexture> tex(d->n_textures);
+  for (uint32_t i = 0; i < d->n_textures; i++) {
+    const nova_b200_texture &t = d->textures[i];
+    if ((!t.u8_pixels) == (!t.f32_pixels) || t.width < 2 || t.height < 2 || t.channels < 1 || t.channels > 4)
+      return fail(c, NOVA_B200_INVALID_CHANNEL_DESCRIPTOR, "texture needs exactly one pixel buffer, >= 2x2 texels%s");
+    nb::DevTexture &o = tex[i];
+    o.w = t.width, o.h = t.height, o.ch = t.channels;
+    o.is_rgba = t.is_rgba, o.invert_u = t.invert_u, o.invert_v = t.invert_v;
+    const size_t px = (size_t)t.width * t.height;
+    nova_b200_status st;
+    if (t.u8_pixels) {
+      uint32_t *p;
+      if ((st = upload(c, t.u8_pixels, px, &p)) != NOVA_B200_SUCCESS) return st;
+      o.u8 = p;
+      o.f32 = nullptr;
+    } else {
+      float *p;
+      if ((st = upload(c, t.f32_pixels, px * t.channels, &p)) != NOVA_B200_SUCCESS) return st;
+      o.f32 = p;
+      o.u8 = nullptr;
+    }
+  }
+  /* materials */
+  std::vector<nb::DevMaterial> mats(d->n_materials);
+  bool emissive = false;
+  for (uint32_t i = 0; i < d->n_materials; i++) {
+    const nova_b200_material &m = d->materials[i];
+    const int32_t slots[4] = {m.albedo, m.metallic, m.normalmap, m.emissive};
+    for (int32_t s : slots)
+      if (s >= (int32_t)d->n_textures || (s >= 0 && !d->textures[s].u8_pixels))
+        return fail(c, NOVA_B200_INVALID_ARGUMENT, "material texture slot must name an 8-bit texture or be -1%s");
+    mats[i].albedo = m.albedo, mats[i].metallic = m.metallic, mats[i].normalmap = m.normalmap;
+    mats[i].emissive = m.emissive;
+    for (int k = 0; k < 3; k++) mats[i].eta[k] = m.eta[k], mats[i].k[k] = m.k[k];
+    mats[i].anisotropy = m.anisotropy;
+    emissive |= m.emissive >= 0;
+  }
+  /* meshes */
+  std::vector<nb::DevMesh> meshes(d->n_meshes);
+  for (uint32_t i = 0; i < d->n_meshes; i++) {
+    const nova_b200_mesh &m = d->meshes[i];
+    if (!m.vertices || !m.normals || !m.tangents || !m.bitangents || !m.uv || !m.indices || m.n_tris == 0)
+      return fail(c, NOVA_B200_INVALID_ARGUMENT, "mesh needs vertices, normals, tangents, bitangents, uv, indices%s");
+    for (uint64_t k = 0; k < 3ull * m.n_tris; k++)
+      if (m.indices[k] >= m.n_verts) return fail(c, NOVA_B200_INVALID_ARGUMENT, "mesh index out of range%s");
+    nb::DevMesh &o = meshes[i];
+    o.n_verts = m.n_verts, o.n_tris = m.n_tris;
+    nova_b200_status st;
+    const size_t nv = m.n_verts;
+    float *p;
+    uint32_t *q;
+    if ((st = upload(c, m.vertices, 3 * nv, &p))) return st;
+    o.v = p;
+    if ((st = upload(c, m.normals, 3 * nv, &p))) return st;
+    o.n = p;
+    if ((st = upload(c, m.tangents, 3 * nv, &p))) return st;
+    o.t = p;
+    if ((st = upload(c, m.bitangents, 3 * nv, &p))) return st;
+    o.b = p;
+    if ((st = upload(c, m.uv, 2 * nv, &p))) return st;
+    o.uv = p;
+    if ((st = upload(c, m.indices, 3ull * m.n_tris, &q))) return st;
+    o.idx = q;
+  }
+  /* instances + primitive tables */
+  c->h_instances.resize(d->n_instances);
+  uint64_t offset = 0;
+  for (uint32_t i = 0; i < d->n_instances; i++) {
+    const nova_b200_instance &x = d->instances[i];
+    if (x.mesh >= d->n_meshes || x.material >= d->n_materials)
+      return fail(c, NOVA_B200_INVALID_ARGUMENT, "instance references a missing mesh or material%s");
+    nb::DevInstance &o = c->h_instances[i];
+    std::memcpy(o.m, x.m, sizeof(o.m));
+    std::memcpy(o.inv, x.inv, sizeof(o.inv));
+    std::memcpy(o.n, x.n, sizeof(o.n));
+    o.mesh = x.mesh;
+    o.material = x.material;
+    o.prim_offset = (uint32_t)offset;
+    o.identity = is_identity(x.m) && is_identity(x.inv);
+    offset += d->meshes[x.mesh].n_tris;
+  }
+  if (offset >= (1ull << 27))
+    return fail(c, NOVA_B200_OUT_OF_MEMORY, "more than 2^27 triangles are not supported by the leaf encoding%s");
+  c->n_prims = offset;
+  std::vector<uint32_t> prim_inst(offset);
+  c->h_valid.clear();
+  c->h_valid.reserve(offset);
+  for (uint32_t i = 0; i < d->n_instances; i++) {
+    const nova_b200_mesh &m = d->meshes[d->instances[i].mesh];
+    const uint32_t base = c->h_instances[i].prim_offset;
+    for (uint32_t t = 0; t < m.n_tris; t++) {
+      prim_inst[base + t] = i;
+      const uint32_t *id = m.indices + 3ull * t;
+      if (!(id[0] == id[1] || id[2] == id[1] || id[2] == id[0])) c->h_valid.push_back(base + t);
+    }
+  }
+  if (c->h_valid.empty()) return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "scene has no non-degenerate triangle%s");
+  nova_b200_status st;
+  nb::DevTexture *dt;
+  nb::DevMaterial *dm;
+  nb::DevMesh *dme;
+  nb::DevInstance *di;
+  uint32_t *dpi;
+  if ((st = upload(c, tex.data(), tex.size(), &dt))) return st;
+  if ((st = upload(c, mats.data(), mats.size(), &dm))) return st;
+  if ((st = upload(c, meshes.data(), meshes.size(), &dme))) return st;
+  if ((st = upload(c, c->h_instances.data(), c->h_instances.size(), &di))) return st;
+  if ((st = upload(c, prim_inst.data(), prim_inst.size(), &dpi))) return st;
+  c->scene.textures = dt;
+  c->scene.materials = dm;
+  c->scene.meshes = dme;
+  c->scene.instances = di;
+  c->scene.prim_inst = dpi;
+  c->scene.sobol_dv = c->d_sobol;
+  c->scene.acos_lut = c->d_acos;
+  c->scene.envmap = d->envmap;
+  c->scene.n_prims = (uint32_t)offset;
+  c->scene.has_emissive = emissive ? 1u : 0u;
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "upload_scene");
+  c->scene_ready = true;
+  return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_options *opts) {
+  using namespace nbctx;
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  if (!c->scene_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "upload a scene before building%s");
+  cudaSetDevice(c->device);
+  const uint32_t n = (uint32_t)c->h_valid.size();
+  nb::BvhBuildParams p;
+  p.max_leaf = opts && opts->max_leaf_size > 0 ? opts->max_leaf_size : 8;
+  p.bins = opts && opts->bins > 0 ? opts->bins : 16;
+  p.cost_trav = 1.0f;
+  if (p.max_leaf > 16 || p.bins < 4 || p.bins > 32)
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "max_leaf_size must be 1..16 and bins 4..32%s");
+  cudaFree(c->d_nodes);
+  cudaFree(c->d_tris);
+  c->d_nodes = nullptr;
+  c->d_tris = nullptr;
+  c->bvh_ready = false;
+  uint32_t *d_valid = nullptr, *d_order = nullptr;
+  float4 *d_lo = nullptr, *d_hi = nullptr;
+  const size_t max_nodes = std::max<size_t>(2 * (size_t)n, 2);
+  NB_CUDA(c, cudaMalloc(&c->d_nodes, sizeof(float4) * 4 * max_nodes), "cudaMalloc(nodes)");
+  NB_CUDA(c, cudaMalloc(&c->d_tris, sizeof(float4) * 3 * (size_t)n), "cudaMalloc(tris)");
+  NB_CUDA(c, cudaMemsetAsync(c->d_nodes, 0, sizeof(float4) * 4 * max_nodes, c->stream), "memset(nodes)");
+  NB_CUDA(c, cudaMallocAsync(&d_valid, sizeof(uint32_t) * n, c->stream), "cudaMalloc(valid)");
+  NB_CUDA(c, cudaMallocAsync(&d_order, sizeof(uint32_t) * n, c->stream), "cudaMalloc(order)");
+  NB_CUDA(c, cudaMallocAsync(&d_lo, sizeof(float4) * n, c->stream), "cudaMalloc(lo)");
+  NB_CUDA(c, cudaMallocAsync(&d_hi, sizeof(float4) * n, c->stream), "cudaMalloc(hi)");
+  NB_CUDA(c, cudaMemcpyAsync(d_valid, c->h_valid.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream),
+          "upload(valid)");
+  k_prim_boxes<<<(n + 255) / 256, 256, 0, c->stream>>>(c->scene, d_valid, n, d_lo, d_hi);
+  NB_CUDA(c, cudaGetLastError(), "k_prim_boxes");
+  nb::BvhBuildResult r{};
+  cudaError_t e = nb::build_bvh(d_lo, d_hi, n, p, c->d_nodes, d_order, c->stream, &r);
+  if (e != cudaSuccess) return cuda_fail(c, e, "build_bvh");
+  k_write_tris<<<(n + 255) / 256, 256, 0, c->stream>>>(c->scene, d_valid, d_order, n, c->d_tris);
+  NB_CUDA(c, cudaMemsetAsync(c->d_counters, 0, 4, c->stream), "memset");
+  k_validate<<<(r.n_nodes + 255) / 256, 256, 0, c->stream>>>(c->d_nodes, r.n_nodes, n, c->d_counters);
+  NB_CUDA(c, cudaMemcpyAsync(c->h_counters, c->d_counters, 4, cudaMemcpyDeviceToHost, c->stream), "readback");
+  cudaFreeAsync(d_valid, c->stream);
+  cudaFreeAsync(d_order, c->stream);
+  cudaFreeAsync(d_lo, c->stream);
+  cudaFreeAsync(d_hi, c->stream);
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "build_bvh");
+  if (c->h_counters[0] != 0 || r.n_nodes == 0 || r.n_nodes > max_nodes || r.max_depth >= nb::kTraversalStack)
+    return fail(c, NOVA_B200_RENDERER_EXCEPTION, "BVH validation failed%s");
+  c->scene.nodes = c->d_nodes;
+  c->scene.tris = c->d_tris;
+  c->n_nodes = r.n_nodes;
+  c->n_leaves = r.n_leaves;
+  c->bvh_depth = r.max_depth;
+  c->bvh_ms = r.ms;
+  c->bvh_ready = true;
+  return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nova_b200_render(nova_b200_ctx *c, const nova_b200_frame *f, float *film_host, float *film_device,
+                                  nova_b200_render_stats *stats) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  return nb_render(c, f, film_host, film_device, stats);
+}
+
+nova_b200_status nova_b200_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,
+                                 float *u, float *v) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  return nb_trace(c, n, o, d, prim, t, u, v);
+}
+
+nova_b200_status nova_b200_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *idx, const uint32_t *dim, uint32_t seed,
+                                 float *out) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  return nb_sobol(c, n, idx, dim, seed, out);
+}
+
+nova_b200_status nova_b200_bake_irradiance(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh, int32_t ch,
+                                           int32_t ow, int32_t oh, int32_t samples, float *out) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  return nb_bake(c, src, sw, sh, ch, ow, oh, samples, out);
+}
+
+void nova_b200_get_error(nova_b200_ctx *c, char buf[1024], size_t *size) {
+  if (!buf) return;
+  const std::string &e = c ? c->error : std::string("null context");
+  size_t n = std::min<size_t>(e.size(), 1023);
+  std::memcpy(buf, e.data(), n);
+  buf[n] = 0;
+  if (size) *size = n;
+}
+
+nova_b200_status nova_b200_scene_info(nova_b200_ctx *c, uint64_t *tris, uint64_t *insts, uint64_t *nodes,
+                                      uint64_t *leaves, uint64_t *bytes) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  if (tris) *tris = c->n_prims;
+  if (insts) *insts = c->h_instances.size();
+  if (nodes) *nodes = c->n_nodes;
+  if (leaves) *leaves = c->n_leaves;
+  if (bytes)
+    *bytes = c->scene_bytes + (uint64_t)c->n_nodes * 64 + (uint64_t)c->h_valid.size() * 48 + c->queue_bytes +
+             c->radiance_cap * 16;
+  return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nova_b200_synchronize(nova_b200_ctx *c) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "synchronize");
+  return NOVA_B200_SUCCESS;
+}
+
+}  // extern "C"

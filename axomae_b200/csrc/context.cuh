@@ -1,0 +1,86 @@
+/* The C-ABI context: owns the device, stream, scene buffers, BVH and render buffers. */
+#pragma once
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/nova_b200.h"
+#include "device_scene.cuh"
+
+struct nova_b200_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_a = nullptr, ev_b = nullptr;
+  std::string error;
+
+  /* tables (allocated once) */
+  uint32_t *d_sobol = nullptr;
+  float *d_acos = nullptr;
+
+  /* scene */
+  std::vector<void *> scene_allocs;
+  nb::DevScene scene{};
+  std::vector<nb::DevInstance> h_instances;
+  std::vector<uint32_t> h_valid; /* global primitive ids that can be hit */
+  uint64_t n_prims = 0;
+  bool scene_ready = false;
+  bool bvh_ready = false;
+  uint32_t n_nodes = 0, n_leaves = 0;
+  int bvh_depth = 0;
+  double bvh_ms = 0.0;
+  uint64_t scene_bytes = 0;
+
+  /* BVH buffers */
+  float4 *d_nodes = nullptr;
+  float4 *d_tris = nullptr;
+
+  /* render buffers */
+  float4 *d_film_acc = nullptr; /* running sum, row-major */
+  int film_w = 0, film_h = 0;
+  uint64_t film_samples = 0;
+  void *d_queue = nullptr;
+  size_t queue_bytes = 0;
+  uint32_t queue_cap = 0;
+  float4 *d_radiance = nullptr;
+  size_t radiance_cap = 0; /* float4 entries */
+  unsigned *d_counters = nullptr;
+  unsigned *h_counters = nullptr; /* pinned */
+  float *d_film_out = nullptr;
+  size_t film_out_cap = 0;
+};
+
+namespace nbctx {
+
+inline nova_b200_status fail(nova_b200_ctx *c, nova_b200_status st, const char *fmt, const char *detail = "") {
+  if (c) {
+    char buf[1024];
+    std::snprintf(buf, sizeof(buf), fmt, detail);
+    c->error = buf;
+  }
+  return st;
+}
+
+inline nova_b200_status cuda_fail(nova_b200_ctx *c, cudaError_t e, const char *where) {
+  char buf[1024];
+  std::snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+  if (c) c->error = buf;
+  return e == cudaErrorMemoryAllocation ? NOVA_B200_OUT_OF_MEMORY : NOVA_B200_RENDERER_EXCEPTION;
+}
+
+}  // namespace nbctx
+
+#define NB_CUDA(ctx, call, where)                                       \
+  do {                                                                  \
+    cudaError_t nb_e_ = (call);                                         \
+    if (nb_e_ != cudaSuccess) return nbctx::cuda_fail((ctx), nb_e_, where); \
+  } while (0)
+
+/* Defined in integrator.cu / bake.cu, called by the C-ABI entry points in context.cu. */
+nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *film_host, float *film_device,
+                           nova_b200_render_stats *stats);
+nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,
+                          float *u, float *v);
+nova_b200_status nb_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *idx, const uint32_t *dim, uint32_t seed,
+                          float *out);
+nova_b200_status nb_bake(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh, int32_t ch, int32_t ow,
+                         int32_t oh, int32_t samples, float *out);

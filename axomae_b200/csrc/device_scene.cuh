@@ -1,0 +1,68 @@
+/* Device-resident scene layout.
+ *
+ * HBM layout (all arrays are owned by the context, see context.cu):
+ *   tris       3 float4 per triangle in BVH leaf order: (v0.xyz, prim id), (e1.xyz, instance id), (e2.xyz, 0)
+ *              with object-space v0 and edges e1 = v1 - v0, e2 = v2 - v0 (Triangle.h:154-156 computes the
+ *              same edges), 48 B per triangle.
+ *   nodes      binary BVH, 4 float4 per node (64 B): both children's boxes and references
+ *                n0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)   n1 = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+ *                n2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)   n3 = (ref0, ref1, count0, count1)
+ *              ref >= 0: inner node index; ref < 0: leaf whose triangles start at ~ref (count in n3.z/w).
+ *   prim_inst  instance index of every global primitive (primitive order of the reference:
+ *              instance by instance, triangle by triangle; api/engine.cpp:159-175).
+ *   meshes / instances / materials / textures: shading data, object-space vertex attributes gathered
+ *              through the index buffer at hit time.
+ */
+#pragma once
+#include "dmath.cuh"
+
+namespace nb {
+
+struct DevTexture {
+  const uint32_t *u8;
+  const float *f32;
+  int32_t w, h, ch;
+  int32_t is_rgba, invert_u, invert_v;
+};
+
+struct DevMaterial {
+  int32_t albedo, metallic, normalmap, emissive;
+  float eta[3];
+  float k[3];
+  float anisotropy;
+};
+
+struct DevMesh {
+  const float *v, *n, *t, *b, *uv;
+  const uint32_t *idx;
+  uint32_t n_verts, n_tris;
+};
+
+struct DevInstance {
+  float m[16];
+  float inv[16];
+  float n[9];
+  uint32_t mesh;
+  uint32_t material;
+  uint32_t prim_offset; /* global id of this instance's first triangle */
+  int32_t identity;     /* m == inv == identity: the object-space ray is the world ray bit for bit */
+};
+
+struct DevScene {
+  const float4 *nodes;
+  const float4 *tris;
+  const uint32_t *prim_inst;
+  const DevMesh *meshes;
+  const DevInstance *instances;
+  const DevMaterial *materials;
+  const DevTexture *textures;
+  const uint32_t *sobol_dv;  /* 256 x 32 direction vectors */
+  const float *acos_lut;     /* 500000 entries */
+  int32_t envmap;
+  uint32_t n_prims;
+  uint32_t has_emissive;
+};
+
+constexpr int kAcosPrecision = 500000;
+
+}  // namespace nb

@@ -1,0 +1,148 @@
+/* Closest-hit traversal of the device BVH.
+ *
+ * Semantics follow the reference's native accelerator (aggregate/native/native.cpp:56-114): the
+ * nearer child is visited first, a box is skipped when its entry distance exceeds the current
+ * closest hit, and a triangle replaces the current hit when its distance is <= the current one.
+ * The triangle test is the reference's Moller-Trumbore (shape/Triangle.h:146-177) evaluated in
+ * the same order (no fused multiply-add), in object space: the ray is brought into the instance's
+ * space with the instance's inverse transform exactly as Triangle::hit does, and identity
+ * instances skip the (bit-exact no-op) transform.
+ *
+ * Box tests only prune: each slab distance is (plane - origin) * rcp(direction), and the exit
+ * distance is widened by 2^-21 relative, so rounding never prunes a box whose triangles the
+ * Moller-Trumbore test would hit.
+ *
+ * Node layout and leaf encoding: see device_scene.cuh.  Leaf reference = ~((first << 4) | (count - 1)).
+ */
+#pragma once
+#include <cfloat>
+#include "device_scene.cuh"
+
+namespace nb {
+
+constexpr int kTraversalStack = 64;
+constexpr float kRayTNear = 0.000001f; /* Ray::tnear, ray/Ray.h:14 */
+constexpr float kFarScale = 1.000000477f; /* 1 + 2^-21: covers the rounding of the slab distances */
+
+NB_HD int32_t leaf_ref(uint32_t first, uint32_t count) { return ~(int32_t)((first << 4) | (count - 1)); }
+NB_HD uint32_t leaf_first(int32_t ref) { return ((uint32_t)~ref) >> 4; }
+NB_HD uint32_t leaf_count(int32_t ref) { return (((uint32_t)~ref) & 15u) + 1u; }
+
+/* Triangle::hit, Triangle.h:154-177 (inv_det before the det == 0 test, inclusive edges). */
+NB_D bool mt_hit(V3 o, V3 d, V3 v0, V3 e1, V3 e2, float tmin, float tmax, float &t, float &u, float &v) {
+  const V3 P = cross(d, e2);
+  const float det = dot(P, e1);
+  const float inv_det = 1.f / det;
+  if (det == 0.f) return false;
+  const V3 T = o - v0;
+  const float uu = dot(P, T) * inv_det;
+  if (uu < 0 || uu > 1.f) return false;
+  const V3 Q = cross(T, e1);
+  const float vv = dot(Q, d) * inv_det;
+  if (vv < 0.f || (uu + vv) > 1.f) return false;
+  const float tt = dot(Q, e2) * inv_det;
+  if (tt < tmin || tt > tmax) return false;
+  t = tt;
+  u = uu;
+  v = vv;
+  return true;
+}
+
+struct TraceResult {
+  int32_t prim;
+  float t, u, v;
+};
+
+NB_D float safe_rcp(float d) {
+  /* reciprocal for the slab test; zero components get a huge finite value of the right sign */
+  const float big = 1e30f;
+  return fabsf(d) > 1e-30f ? __frcp_rn(d) : copysignf(big, d);
+}
+
+/* Closest hit of one world-space ray. */
+NB_D TraceResult trace_closest(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
+                               uint64_t *tri_tests = nullptr) {
+  TraceResult r{-1, 0.f, 0.f, 0.f};
+  float tmax = FLT_MAX; /* native.cpp:57 starts from MAXFLOAT */
+  const float ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
+  int32_t stack[kTraversalStack];
+  int sp = 0;
+  int32_t cur = 0; /* the root is always an inner node (a one-leaf scene gets an empty sibling) */
+  int32_t cached_inst = -1;
+  V3 lo_o = o, lo_d = d;
+  uint64_t nv = 0, tt = 0;
+  for (;;) {
+    if (cur >= 0) {
+      nv++;
+      const float4 n0 = __ldg(&sc.nodes[4 * cur + 0]);
+      const float4 n1 = __ldg(&sc.nodes[4 * cur + 1]);
+      const float4 n2 = __ldg(&sc.nodes[4 * cur + 2]);
+      const float4 n3 = __ldg(&sc.nodes[4 * cur + 3]);
+      /* slabs as (plane - origin) * rcp(dir): two roundings per distance, far end widened by 2^-21 */
+      float a0 = (n0.x - o.x) * ix, b0 = (n0.y - o.x) * ix;
+      float a1 = (n0.z - o.y) * iy, b1 = (n0.w - o.y) * iy;
+      float a2 = (n2.x - o.z) * iz, b2 = (n2.y - o.z) * iz;
+      float c0n = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), 0.f));
+      float c0f = fminf(fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fmaxf(a2, b2)) * kFarScale, tmax);
+      float d0 = (n1.x - o.x) * ix, e0 = (n1.y - o.x) * ix;
+      float d1 = (n1.z - o.y) * iy, e1 = (n1.w - o.y) * iy;
+      float d2 = (n2.z - o.z) * iz, e2 = (n2.w - o.z) * iz;
+      float c1n = fmaxf(fmaxf(fminf(d0, e0), fminf(d1, e1)), fmaxf(fminf(d2, e2), 0.f));
+      float c1f = fminf(fminf(fminf(fmaxf(d0, e0), fmaxf(d1, e1)), fmaxf(d2, e2)) * kFarScale, tmax);
+      const bool h0 = c0n <= c0f, h1 = c1n <= c1f;
+      const int32_t r0 = __float_as_int(n3.x), r1 = __float_as_int(n3.y);
+      if (h0 && h1) {
+        int32_t first = r0, second = r1;
+        if (c1n < c0n) {
+          first = r1;
+          second = r0;
+        }
+        if (sp < kTraversalStack) stack[sp++] = second;
+        cur = first;
+        continue;
+      } else if (h0) {
+        cur = r0;
+        continue;
+      } else if (h1) {
+        cur = r1;
+        continue;
+      }
+    } else {
+      const uint32_t first = leaf_first(cur), count = leaf_count(cur);
+      for (uint32_t k = first; k < first + count; k++) {
+        const float4 t0 = __ldg(&sc.tris[3 * k + 0]);
+        const float4 t1 = __ldg(&sc.tris[3 * k + 1]);
+        const float4 t2 = __ldg(&sc.tris[3 * k + 2]);
+        const int32_t inst = __float_as_int(t1.w);
+        if (inst != cached_inst) {
+          cached_inst = inst;
+          const DevInstance &I = sc.instances[inst];
+          if (I.identity) {
+            lo_o = o;
+            lo_d = d;
+          } else {
+            lo_o = xform_point(I.inv, o);
+            lo_d = xform_dir(I.inv, d);
+          }
+        }
+        tt++;
+        float ht, hu, hv;
+        if (mt_hit(lo_o, lo_d, V3{t0.x, t0.y, t0.z}, V3{t1.x, t1.y, t1.z}, V3{t2.x, t2.y, t2.z}, kRayTNear, tmax, ht,
+                   hu, hv)) {
+          tmax = ht;
+          r.prim = __float_as_int(t0.w);
+          r.t = ht;
+          r.u = hu;
+          r.v = hv;
+        }
+      }
+    }
+    if (sp == 0) break;
+    cur = stack[--sp];
+  }
+  if (node_visits) *node_visits += nv;
+  if (tri_tests) *tri_tests += tt;
+  return r;
+}
+
+}  // namespace nb

@@ -1,0 +1,228 @@
+"""ctypes binding of the C ABI in include/nova_b200.h (libnova_b200.so, built in-tree).
+
+The library is the product: a Python caller (tests, bench.py, the smoke check) talks to it only
+through the C entry points, exactly as a C++ Nova render call would.  There is no CPU fallback:
+importing this module on a machine without the built library, or creating a context without a
+GPU, raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnova_b200.so")
+
+f32p = C.POINTER(C.c_float)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+
+STATUS = ["SUCCESS", "INVALID_ENGINE_STATE", "INVALID_BUFFER_STATE", "INVALID_CHANNEL_DESCRIPTOR", "INVALID_SCENE_TYPE",
+          "INVALID_TRANSFORM_TYPE", "RENDER_BUFFER_NOT_INITIALIZED", "RENDER_OPTIONS_NOT_INITIALIZED",
+          "RENDER_ENGINE_NOT_INITIALIZED", "SCENE_NOT_PROCESSED", "NOT_GPU_BUILD", "OUT_OF_MEMORY",
+          "MULTIPLE_INTEGRATORS_NOT_SUPPORTED", "THREADPOOL_CREATION_ERROR", "THREADPOOL_NOT_INITIALIZED",
+          "INVALID_ARGUMENT", "RENDERER_EXCEPTION"]
+
+
+class NovaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        name = STATUS[status] if 0 <= status < len(STATUS) else str(status)
+        super().__init__("%s: %s" % (name, message))
+
+
+class Mesh(C.Structure):
+    _fields_ = [("vertices", f32p), ("normals", f32p), ("tangents", f32p), ("bitangents", f32p), ("uv", f32p),
+                ("indices", u32p), ("n_verts", C.c_uint32), ("n_tris", C.c_uint32)]
+
+
+class Instance(C.Structure):
+    _fields_ = [("mesh", C.c_uint32), ("material", C.c_uint32), ("m", C.c_float * 16), ("inv", C.c_float * 16),
+                ("n", C.c_float * 9)]
+
+
+class Material(C.Structure):
+    _fields_ = [("albedo", C.c_int32), ("metallic", C.c_int32), ("normalmap", C.c_int32), ("emissive", C.c_int32),
+                ("eta", C.c_float * 3), ("k", C.c_float * 3), ("anisotropy", C.c_float)]
+
+
+class Texture(C.Structure):
+    _fields_ = [("u8_pixels", u32p), ("f32_pixels", f32p), ("width", C.c_int32), ("height", C.c_int32),
+                ("channels", C.c_int32), ("is_rgba", C.c_int32), ("invert_u", C.c_int32), ("invert_v", C.c_int32)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("meshes", C.POINTER(Mesh)), ("n_meshes", C.c_uint32), ("instances", C.POINTER(Instance)),
+                ("n_instances", C.c_uint32), ("materials", C.POINTER(Material)), ("n_materials", C.c_uint32),
+                ("textures", C.POINTER(Texture)), ("n_textures", C.c_uint32), ("envmap", C.c_int32)]
+
+
+class BvhOptions(C.Structure):
+    _fields_ = [("max_leaf_size", C.c_int32), ("bins", C.c_int32)]
+
+
+class Frame(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp_total", C.c_int32), ("sample_begin", C.c_int32),
+                ("sample_count", C.c_int32), ("max_depth", C.c_int32), ("seed", C.c_uint32), ("rr_start", C.c_int32),
+                ("reset", C.c_int32), ("vertical_invert", C.c_int32), ("inv_P", C.c_float * 16),
+                ("inv_V", C.c_float * 16)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("traced", C.c_uint64), ("waves", C.c_uint64),
+                ("device_ms", C.c_double), ("trace_ms", C.c_double), ("shade_ms", C.c_double),
+                ("kernels", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "nova_b200_build_bvh",
+           "nova_b200_render", "nova_b200_trace", "nova_b200_sobol", "nova_b200_bake_irradiance",
+           "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize"]
+
+
+def lib():
+    """Loads libnova_b200.so; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libnova_b200.so is not built (run __graft_entry__.build() or make -C axomae_b200/csrc)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.nova_b200_create.argtypes = [C.POINTER(vp), C.c_int32]
+        L.nova_b200_destroy.argtypes = [vp]
+        L.nova_b200_upload_scene.argtypes = [vp, C.POINTER(SceneDesc)]
+        L.nova_b200_build_bvh.argtypes = [vp, C.POINTER(BvhOptions)]
+        L.nova_b200_render.argtypes = [vp, C.POINTER(Frame), vp, vp, C.POINTER(RenderStats)]
+        L.nova_b200_trace.argtypes = [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]
+        L.nova_b200_sobol.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, vp]
+        L.nova_b200_bake_irradiance.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                                C.c_int32, vp]
+        L.nova_b200_get_error.argtypes = [vp, C.c_char_p, C.POINTER(C.c_size_t)]
+        L.nova_b200_get_error.restype = None
+        L.nova_b200_scene_info.argtypes = [vp] + [C.POINTER(C.c_uint64)] * 5
+        L.nova_b200_synchronize.argtypes = [vp]
+        for name in EXPORTS:
+            if name != "nova_b200_get_error":
+                getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def make_scene_desc(scene: dict):
+    """Builds the C scene descriptor for a scene dictionary (axomae_b200.scenes layout).
+    Returns (desc, keepalive) — keep `keepalive` referenced until the upload call returns."""
+    keep = []
+    meshes = (Mesh * len(scene["meshes"]))()
+    for i, m in enumerate(scene["meshes"]):
+        arrs = [np.ascontiguousarray(m[k], np.float32) for k in ("vertices", "normals", "tangents", "bitangents", "uv")]
+        idx = np.ascontiguousarray(m["indices"], np.uint32)
+        keep += arrs + [idx]
+        meshes[i] = Mesh(*[_p(a, f32p) for a in arrs], _p(idx, u32p), arrs[0].size // 3, idx.size // 3)
+    insts = (Instance * len(scene["instances"]))()
+    for i, x in enumerate(scene["instances"]):
+        insts[i] = Instance(x["mesh"], x["material"], (C.c_float * 16)(*np.asarray(x["m"], np.float32).reshape(16)),
+                            (C.c_float * 16)(*np.asarray(x["inv"], np.float32).reshape(16)),
+                            (C.c_float * 9)(*np.asarray(x["n"], np.float32).reshape(9)))
+    mats = (Material * len(scene["materials"]))()
+    for i, m in enumerate(scene["materials"]):
+        mats[i] = Material(m.get("albedo", -1), m.get("metallic", -1), m.get("normalmap", -1), m.get("emissive", -1),
+                           (C.c_float * 3)(*m.get("eta", (0, 0, 0))), (C.c_float * 3)(*m.get("k", (0, 0, 0))),
+                           m.get("anisotropy", 0.0))
+    texs = (Texture * len(scene["textures"]))()
+    for i, t in enumerate(scene["textures"]):
+        if t["format"] == "u8":
+            px = np.ascontiguousarray(t["pixels"], np.uint32)
+            texs[i] = Texture(_p(px, u32p), None, t["width"], t["height"], t.get("channels", 4), int(t.get("is_rgba", 1)),
+                              int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+        else:
+            px = np.ascontiguousarray(t["pixels"], np.float32)
+            texs[i] = Texture(None, _p(px, f32p), t["width"], t["height"], t.get("channels", 4), int(t.get("is_rgba", 1)),
+                              int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+        keep.append(px)
+    desc = SceneDesc(meshes, len(scene["meshes"]), insts, len(scene["instances"]), mats, len(scene["materials"]), texs,
+                     len(scene["textures"]), scene["envmap"])
+    keep += [meshes, insts, mats, texs]
+    return desc, keep
+
+
+def make_frame(scene: dict, width, height, spp_total, max_depth, seed=0, sample_begin=0, sample_count=None,
+               rr_start=-1, reset=1, vertical_invert=0) -> Frame:
+    return Frame(width, height, spp_total, sample_begin, spp_total if sample_count is None else sample_count,
+                 max_depth, seed, rr_start, reset, vertical_invert,
+                 (C.c_float * 16)(*np.asarray(scene["inv_P"], np.float32).reshape(16)),
+                 (C.c_float * 16)(*np.asarray(scene["inv_V"], np.float32).reshape(16)))
+
+
+class Context:
+    """One device context: scene upload, BVH build, render, queries."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        st = lib().nova_b200_create(C.byref(self.h), device)
+        if st != 0:
+            raise NovaError(st, "nova_b200_create failed")
+
+    def close(self):
+        if self.h:
+            lib().nova_b200_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def error(self) -> str:
+        buf = C.create_string_buffer(1024)
+        n = C.c_size_t()
+        lib().nova_b200_get_error(self.h, buf, C.byref(n))
+        return buf.value.decode()
+
+    def _check(self, st):
+        if st != 0:
+            raise NovaError(st, self.error())
+
+    def upload(self, scene: dict):
+        desc, keep = make_scene_desc(scene)
+        self._check(lib().nova_b200_upload_scene(self.h, C.byref(desc)))
+        del keep
+
+    def build(self, max_leaf=0, bins=0):
+        self._check(lib().nova_b200_build_bvh(self.h, C.byref(BvhOptions(max_leaf, bins))))
+
+    def info(self) -> dict:
+        vals = [C.c_uint64() for _ in range(5)]
+        self._check(lib().nova_b200_scene_info(self.h, *[C.byref(v) for v in vals]))
+        return dict(zip(["triangles", "instances", "nodes", "leaves", "device_bytes"], [v.value for v in vals]))
+
+    def render(self, frame: Frame, film_host: np.ndarray = None, film_device_ptr: int = None) -> RenderStats:
+        st = RenderStats()
+        host = None if film_host is None else film_host.ctypes.data_as(C.c_void_p)
+        dev = None if film_device_ptr is None else C.c_void_p(film_device_ptr)
+        self._check(lib().nova_b200_render(self.h, C.byref(frame), host, dev, C.byref(st)))
+        return st
+
+    def trace(self, orig_ptr, dir_ptr, n, prim_ptr, t_ptr, u_ptr, v_ptr):
+        """Device pointers (e.g. torch CUDA tensors' data_ptr())."""
+        self._check(lib().nova_b200_trace(self.h, n, C.c_void_p(orig_ptr), C.c_void_p(dir_ptr), C.c_void_p(prim_ptr),
+                                          C.c_void_p(t_ptr), C.c_void_p(u_ptr), C.c_void_p(v_ptr)))
+
+    def sobol(self, idx_ptr, dim_ptr, n, seed, out_ptr):
+        self._check(lib().nova_b200_sobol(self.h, n, C.c_void_p(idx_ptr), C.c_void_p(dim_ptr), seed,
+                                          C.c_void_p(out_ptr)))
+
+    def bake_irradiance(self, src_ptr, sw, sh, ch, ow, oh, samples, out_ptr):
+        self._check(lib().nova_b200_bake_irradiance(self.h, C.c_void_p(src_ptr), sw, sh, ch, ow, oh, samples,
+                                                    C.c_void_p(out_ptr)))
+
+    def synchronize(self):
+        self._check(lib().nova_b200_synchronize(self.h))

@@ -1,0 +1,192 @@
+/* nova_b200.h — C ABI of the B200 (sm_100a) implementation of the Nova path-tracing hot path.
+ *
+ * This is the boundary a Nova render call binds to.  It replaces the reference's GPU backend
+ * plug-in point and the render dispatch that drives it (HamilcarR/Axomae, corelib/nova):
+ *
+ *   DeviceAcceleratorInterface::make / build / cleanup / copyParamsToDevice / getIntersectorObject
+ *       aggregate/device_acceleration_interface.h:20-36, factory api/device_accelerator_factory.cpp:9-18
+ *   DeviceIntersectorInterface::traverse        aggregate/device_acceleration_interface.h:11-15
+ *   Engine::buildScene / buildAcceleration      api_engine.h:68-82, api/engine.cpp:201,235
+ *   NvEngineInstance::renderGpu + writeFramebuffer (progressive running-mean film)
+ *                                               api/engine.cpp:457-496, :351-363
+ *   Engine::getRenderEngineError                api_engine.h:185
+ *   TextureOperations<float>::computeDiffuseIrradiance (irradiance bake)
+ *                                               sources/processing/TextureProcessing.cpp:10-64,
+ *                                               sources/processing/cuda/CubemapProcessing.cu:244-284
+ *
+ * Conventions: plain C types only; every call returns a status whose values are the reference's
+ * nova::ERROR_STATE enumerators (api_common.h:7-27); no exception crosses the ABI.  A context owns
+ * all device memory it allocates and one CUDA stream; it is not thread-safe (one caller thread).
+ * Scene data is copied to the device by nova_b200_upload_scene, so caller buffers may be released
+ * afterwards (the reference keeps non-owning spans; api/geometry.cpp:17-70).
+ */
+#ifndef NOVA_B200_H
+#define NOVA_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: identical numbering to nova::ERROR_STATE (api_common.h:7-27). */
+typedef enum {
+  NOVA_B200_SUCCESS = 0,
+  NOVA_B200_INVALID_ENGINE_STATE = 1,
+  NOVA_B200_INVALID_BUFFER_STATE = 2,
+  NOVA_B200_INVALID_CHANNEL_DESCRIPTOR = 3,
+  NOVA_B200_INVALID_SCENE_TYPE = 4,
+  NOVA_B200_INVALID_TRANSFORM_TYPE = 5,
+  NOVA_B200_RENDER_BUFFER_NOT_INITIALIZED = 6,
+  NOVA_B200_RENDER_OPTIONS_NOT_INITIALIZED = 7,
+  NOVA_B200_RENDER_ENGINE_NOT_INITIALIZED = 8,
+  NOVA_B200_SCENE_NOT_PROCESSED = 9,
+  NOVA_B200_NOT_GPU_BUILD = 10,
+  NOVA_B200_OUT_OF_MEMORY = 11,
+  NOVA_B200_MULTIPLE_INTEGRATORS_NOT_SUPPORTED = 12,
+  NOVA_B200_THREADPOOL_CREATION_ERROR = 13,
+  NOVA_B200_THREADPOOL_NOT_INITIALIZED = 14,
+  NOVA_B200_INVALID_ARGUMENT = 15,
+  NOVA_B200_RENDERER_EXCEPTION = 16
+} nova_b200_status;
+
+typedef struct nova_b200_ctx nova_b200_ctx;
+
+/* Triangle mesh in object space: the reference's Object3D spans (internal/geometry/Object3D.h:384-394).
+ * positions / normals / tangents / bitangents: 3 floats per vertex; uv: 2; indices: 3 per triangle. */
+typedef struct {
+  const float *vertices;
+  const float *normals;
+  const float *tangents;
+  const float *bitangents;
+  const float *uv;
+  const uint32_t *indices;
+  uint32_t n_verts;
+  uint32_t n_tris;
+} nova_b200_mesh;
+
+/* One placed mesh with its transform record transform4x4_t {m, inv, n} (internal/common/math/utils_3D.h:84-96),
+ * column-major like glm, and its material (one material per mesh, api/engine.cpp:177-184). */
+typedef struct {
+  uint32_t mesh;
+  uint32_t material;
+  float m[16];
+  float inv[16];
+  float n[9];
+} nova_b200_instance;
+
+/* PrincipledMaterial inputs (material/NovaMaterials.h:45-137): u8 texture indices or -1, eta, k. */
+typedef struct {
+  int32_t albedo;
+  int32_t metallic; /* roughness = green, metal = blue (NovaMaterials.h:116-117) */
+  int32_t normalmap;
+  int32_t emissive;
+  float eta[3];
+  float k[3];
+  float anisotropy;
+} nova_b200_material;
+
+/* Texture: exactly one of u8_pixels (32-bit packed 8-bit RGBA/BGRA texels) or f32_pixels. */
+typedef struct {
+  const uint32_t *u8_pixels;
+  const float *f32_pixels;
+  int32_t width, height, channels;
+  int32_t is_rgba, invert_u, invert_v;
+} nova_b200_texture;
+
+typedef struct {
+  const nova_b200_mesh *meshes;
+  uint32_t n_meshes;
+  const nova_b200_instance *instances;
+  uint32_t n_instances;
+  const nova_b200_material *materials;
+  uint32_t n_materials;
+  const nova_b200_texture *textures;
+  uint32_t n_textures;
+  int32_t envmap; /* index of a 4-channel f32 texture (api/engine.cpp:273-290) */
+} nova_b200_scene_desc;
+
+/* Acceleration-structure build options. */
+typedef struct {
+  int32_t max_leaf_size; /* 1..16; 0 = default (8) */
+  int32_t bins;          /* SAH bins per axis, 4..64; 0 = default (16) */
+} nova_b200_bvh_options;
+
+/* One render call.  Samples [sample_begin, sample_begin + sample_count) of every pixel are traced and
+ * added to the context's accumulation film; the returned image is the running mean over all samples
+ * accumulated since the last reset (writeFramebuffer, api/engine.cpp:351-363).  The sample index of
+ * pixel (x, y), sample s is (x * height + y) * spp_total + s (integrator_optix.cu:43). */
+typedef struct {
+  int32_t width, height;
+  int32_t spp_total;    /* samples per pixel of the whole render (index mapping) */
+  int32_t sample_begin;
+  int32_t sample_count;
+  int32_t max_depth;    /* scatter events per path = max_depth + 1 (integrator/Integrator.cpp:71) */
+  uint32_t seed;        /* Sobol / Owen scrambling seed */
+  int32_t rr_start;     /* Russian roulette from this bounce on; -1 = off (the reference has none) */
+  int32_t reset;        /* 1: clear the accumulation film first */
+  int32_t vertical_invert;
+  float inv_P[16];      /* camera inverse projection / view, column-major (camera/nova_camera.h) */
+  float inv_V[16];
+} nova_b200_frame;
+
+/* Counters of the last render call. */
+typedef struct {
+  uint64_t paths;      /* camera paths traced */
+  uint64_t segments;   /* ray segments of the reference estimator (Li evaluations) */
+  uint64_t traced;     /* closest-hit queries issued on the device */
+  uint64_t waves;      /* wavefront iterations */
+  double device_ms;    /* device time of the render (CUDA events) */
+  double trace_ms;     /* device time inside the closest-hit kernel */
+  double shade_ms;     /* device time inside the shading kernel */
+  uint64_t kernels;    /* kernels launched */
+} nova_b200_render_stats;
+
+/* Context lifecycle: DeviceAcceleratorInterface::make (api/device_accelerator_factory.cpp:9) and cleanup. */
+nova_b200_status nova_b200_create(nova_b200_ctx **ctx, int32_t device);
+nova_b200_status nova_b200_destroy(nova_b200_ctx *ctx);
+
+/* Copies a scene to device memory: Engine::buildScene (api/engine.cpp:201-233). */
+nova_b200_status nova_b200_upload_scene(nova_b200_ctx *ctx, const nova_b200_scene_desc *scene);
+
+/* Builds the device BVH (binned SAH on the GPU): Engine::buildAcceleration (api/engine.cpp:235)
+ * and DeviceAcceleratorInterface::build (aggregate/device_acceleration_interface.h:25). */
+nova_b200_status nova_b200_build_bvh(nova_b200_ctx *ctx, const nova_b200_bvh_options *opts);
+
+/* Renders one frame batch (renderGpu, api/engine.cpp:457-496).  film_host (width*height*4 floats,
+ * pageable or pinned) and/or film_device (a device pointer) receive the running-mean RGBA image;
+ * either may be NULL.  stats may be NULL. */
+nova_b200_status nova_b200_render(nova_b200_ctx *ctx, const nova_b200_frame *frame, float *film_host,
+                                  float *film_device, nova_b200_render_stats *stats);
+
+/* Closest-hit queries for n world-space rays held in DEVICE memory (3 floats each): the intersector
+ * of DeviceIntersectorInterface::traverse / GenericHostAccelerator::hit (aggregate/acceleration_interface.h).
+ * prim = global primitive index (-1 on miss), t / u / v = Moller-Trumbore distance and barycentrics. */
+nova_b200_status nova_b200_trace(nova_b200_ctx *ctx, uint64_t n, const float *orig_dev, const float *dir_dev,
+                                 int32_t *prim_dev, float *t_dev, float *u_dev, float *v_dev);
+
+/* Sobol + Owen samples (math_random.h:73-98 SobolGenerator::generate) for n (index, dimension)
+ * pairs in device memory. */
+nova_b200_status nova_b200_sobol(nova_b200_ctx *ctx, uint64_t n, const uint32_t *index_dev, const uint32_t *dim_dev,
+                                 uint32_t seed, float *out_dev);
+
+/* Diffuse irradiance bake of an equirectangular f32 map (TextureProcessing.cpp:10-64 semantics).
+ * src_dev: src_w*src_h*channels floats; out_dev: out_w*out_h*channels floats (power-of-two sizes). */
+nova_b200_status nova_b200_bake_irradiance(nova_b200_ctx *ctx, const float *src_dev, int32_t src_w, int32_t src_h,
+                                           int32_t channels, int32_t out_w, int32_t out_h, int32_t samples,
+                                           float *out_dev);
+
+/* Last error message: Engine::getRenderEngineError (api_engine.h:185).  buf holds 1024 chars. */
+void nova_b200_get_error(nova_b200_ctx *ctx, char buf[1024], size_t *size);
+
+/* Scene / BVH statistics: triangles, instances, BVH nodes, BVH leaves, device bytes held. */
+nova_b200_status nova_b200_scene_info(nova_b200_ctx *ctx, uint64_t *triangles, uint64_t *instances, uint64_t *nodes,
+                                      uint64_t *leaves, uint64_t *device_bytes);
+
+/* Waits for all work of the context's stream. */
+nova_b200_status nova_b200_synchronize(nova_b200_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NOVA_B200_H */

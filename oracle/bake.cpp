@@ -1,0 +1,171 @@
+/* ORACLE — test infrastructure only (see oracle.h).
+ *
+ * Diffuse irradiance bake, CPU path of the reference:
+ *   TextureOperations<float>::computeDiffuseIrradiance   sources/processing/TextureProcessing.cpp:10-64
+ *   launchAsyncDiffuseIrradianceCompute / computeIrradianceImportanceSampling /
+ *   computeIrradianceSingleTexel / uvSample / bilinearInterpolate / wrapAround*
+ *                                                       sources/processing/TextureProcessing.h:174-303
+ *   pgc3d                                                corelib/internal/common/math/math_importance_sampling.h:7-22
+ * The spherical mapping uses the reference's fast approximations (atan2 polynomial, acos table).
+ */
+#include "oracle_internal.h"
+#include <algorithm>
+#include <cmath>
+#include <thread>
+#include <vector>
+
+namespace orc {
+namespace {
+
+constexpr double PI_D = M_PI;
+
+/* uvToPixel(coord, dim) = static_cast<unsigned>(coord * dim).  A negative coordinate is converted
+ * the way x86-64 GCC code does it (truncate to a 64-bit integer, keep the low 32 bits). */
+inline unsigned to_pixel(float coord, unsigned dim) { return (unsigned)(int64_t)(coord * (float)dim); }
+
+inline void pgc3d(unsigned x, unsigned y, unsigned z, float out[3]) {
+  x = x * 1664525u + 1013904223u;
+  y = y * 1664525u + 1013904223u;
+  z = z * 1664525u + 1013904223u;
+  x += y * z;
+  y += z * x;
+  z += x * y;
+  x ^= x >> 16u;
+  y ^= y >> 16u;
+  z ^= z >> 16u;
+  x += y * z;
+  y += z * x;
+  z += x * y;
+  const float k = 1.f / float(0xFFFFFFFFu);
+  out[0] = (float)x * k;
+  out[1] = (float)y * k;
+  out[2] = (float)z * k;
+}
+
+inline float horner(float x) {
+  float x_sq = x * x;
+  return x * (0.99997726f + x_sq * (-0.33262347f + x_sq * (0.19354346f + x_sq * (-0.11643287f +
+                                                                          x_sq * (0.05265332f + x_sq * -0.01172120f)))));
+}
+inline float atan2_approx(float y, float x) {
+  bool swap = std::fabs(x) < std::fabs(y);
+  float in = (swap ? x : y) / (swap ? y : x);
+  float res = horner(in);
+  res = swap ? (in >= 0.0f ? (float)M_PI_2 : -(float)M_PI_2) - res : res;
+  if (x >= 0.0f && y >= 0.0f) {
+  } else if (x < 0.0f && y >= 0.0f) {
+    res = (float)M_PI + res;
+  } else if (x < 0.0f && y < 0.0f) {
+    res = -(float)M_PI + res;
+  }
+  return res;
+}
+inline float acos_lt(float a) {
+  int scaled = std::clamp((int)((a + 1.f) * kAcosPrecision * 0.5f), 0, kAcosPrecision - 1);
+  return acos_lut()[scaled];
+}
+inline void to_uv(float x, float y, float z, float &u, float &v) { /* sphericalToUv(cartesianToSpherical()) */
+  float phi = atan2_approx(y, x);
+  float theta = acos_lt(z);
+  u = (float)(phi * (1.f / (2.f * PI_D)));
+  v = (float)(theta * (1.f / PI_D));
+}
+
+struct Src {
+  const float *data;
+  int w, h, ch;
+  V3 texel(int x, int y) const { /* discreteSample + wrapAroundPixelCoords */
+    int xc, yc;
+    if (x >= w)
+      xc = x % w;
+    else if (x < 0)
+      xc = w + (x % w);
+    else
+      xc = x;
+    if (y >= h)
+      yc = y % h;
+    else if (y < 0)
+      yc = h + (y % h);
+    else
+      yc = y;
+    size_t i = ((size_t)yc * w + xc) * ch;
+    return {data[i], data[i + 1], data[i + 2]};
+  }
+  V3 uv_sample(float u, float v) const { /* uvSample + wrapAroundTexCoords + bilinearInterpolate */
+    float ui = std::floor(u), vi = std::floor(v);
+    float uw = (u > 1. || u < 0.) ? u - ui : u;
+    float vw = (v > 1. || v < 0.) ? v - vi : v;
+    float px = (float)(double)to_pixel(uw, (unsigned)w);
+    float py = (float)(double)to_pixel(vw, (unsigned)h);
+    float tlx = std::floor(px), tly = std::floor(py);
+    float trx = std::floor(px) + 1, blY = std::floor(py) + 1;
+    const float fu = (px - tlx) / (trx - tlx);
+    const float fv = (py - tly) / (blY - tly);
+    const float hd = (1 - fu);
+    V3 tl = texel((int)tlx, (int)tly), tr = texel((int)trx, (int)tly);
+    V3 bl = texel((int)tlx, (int)blY), br = texel((int)trx, (int)blY);
+    V3 top = hd * tl + fu * tr;
+    V3 bot = hd * bl + fu * br;
+    return (1 - fv) * top + fv * bot;
+  }
+};
+
+V3 texel_irradiance(const Src &src, float x, float y, float z, unsigned W, unsigned H, unsigned total) {
+  V3 irr{0, 0, 0};
+  V3 normal{x, y, z};
+  V3 right{1.f, 0.f, 0.f};
+  float u, v;
+  to_uv(x, y, z, u, v);
+  const unsigned px = to_pixel(u, W), py = to_pixel(v, H);
+  float dd = dot(right, normal);
+  V3 tangent{0.f, 1.f, 0.f};
+  if (1.0 - std::fabs(dd) > 1e-6) tangent = normalize(cross(right, normal));
+  V3 bitangent = cross(normal, tangent);
+  for (unsigned s = 0; s < total; s++) {
+    float r[3];
+    pgc3d(px, py, s, r);
+    float phi = (float)(2 * PI_D * r[0]);
+    float theta = std::asin(std::sqrt(r[1]));
+    V3 c{std::sin(theta) * std::cos(phi), std::sin(theta) * std::sin(phi), std::cos(theta)};
+    c = c.x * tangent + c.y * bitangent + c.z * normal;
+    float su, sv;
+    to_uv(c.x, c.y, c.z, su, sv);
+    irr = irr + src.uv_sample(su, sv);
+  }
+  return irr / (float)total;
+}
+
+}  // namespace
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" int32_t orc_bake_irradiance(const float *src, int32_t src_w, int32_t src_h, int32_t channels, int32_t out_w,
+                                       int32_t out_h, int32_t samples, int32_t threads, float *out) {
+  auto pow2 = [](int32_t v) { return v > 0 && (v & (v - 1)) == 0; };
+  if (!pow2(out_w) || !pow2(out_h) || channels < 3 || samples <= 0) return 1;
+  (void)acos_lut();
+  Src s{src, src_w, src_h, channels};
+  const unsigned W = (unsigned)out_w, H = (unsigned)out_h;
+  const unsigned MAX_THREADS = threads > 0 ? (unsigned)threads : 8u; /* TextureProcessing.h:45 */
+  std::vector<std::thread> pool;
+  for (unsigned i = 1; i <= MAX_THREADS; i++) {
+    unsigned wmax = (W / MAX_THREADS) * i, wmin = wmax - (W / MAX_THREADS);
+    if (i == MAX_THREADS) wmax += W % MAX_THREADS - 1;
+    pool.emplace_back([=, &s] {
+      for (unsigned x = wmin; x <= wmax && x < W; x++)
+        for (unsigned y = 0; y < H; y++) {
+          float u = (float)((double)x / (double)W), v = (float)((double)y / (double)H);
+          float phi = (float)(2 * PI_D * u), theta = (float)(PI_D * v);
+          float cz = std::cos(theta), cx = std::sin(theta) * std::cos(phi), cy = std::sin(theta) * std::sin(phi);
+          V3 irr = texel_irradiance(s, cx, cy, cz, W, H, (unsigned)samples);
+          size_t idx = ((size_t)y * W + x) * channels;
+          out[idx] = irr.x;
+          out[idx + 1] = irr.y;
+          out[idx + 2] = irr.z;
+        }
+    });
+  }
+  for (auto &t : pool) t.join();
+  return 0;
+}

@@ -1,0 +1,129 @@
+/* ORACLE — test infrastructure only.  A CPU restatement of the reference's Nova path-tracing hot
+ * path (HamilcarR/Axomae, corelib/nova), used as the parity checker for the CUDA path and as the
+ * timed CPU baseline.  Nothing in the product links or loads this library; only tests/, the smoke
+ * check and bench.py's CPU-baseline leg do.
+ *
+ * Parity status: the Sobol direction vectors, the Sobol/Owen sample values and the acos lookup
+ * table are pinned against fixtures produced by the reference's own generator scripts
+ * (tests/golden/).  Everything downstream (camera, BVH, triangle test, hit record, BSDFs,
+ * envmap, integrator) is a restatement of the reference sources cited per function; the
+ * reference itself cannot be built here (glm/boost/Embree are empty submodules), so those parts
+ * are pinned only by the reference's own property tests and are otherwise "parity unpinned".
+ */
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One triangle mesh in object space (reference Object3D spans, corelib/internal/geometry/Object3D.h:384-394).
+ * All attribute arrays are required: positions/normals/tangents/bitangents 3 floats per vertex, uv 2. */
+typedef struct {
+  const float *vertices;
+  const float *normals;
+  const float *tangents;
+  const float *bitangents;
+  const float *uv;
+  const uint32_t *indices; /* 3 per triangle */
+  uint32_t n_verts;
+  uint32_t n_tris;
+} orc_mesh;
+
+/* One placed mesh: the reference's per-mesh transform record transform4x4_t {m, inv, t, n}
+ * (corelib/internal/common/math/utils_3D.h:84-96), column-major, and its material. */
+typedef struct {
+  uint32_t mesh;
+  uint32_t material;
+  float m[16];
+  float inv[16];
+  float n[9];
+} orc_instance;
+
+/* PrincipledMaterial inputs (corelib/nova/material/NovaMaterials.h:45-137, api/material.cpp:212-226):
+ * u8 texture indices (-1 = absent) and the refractive indices eta, k. */
+typedef struct {
+  int32_t albedo;
+  int32_t metallic; /* roughness = .g, metal = .b (NovaMaterials.h:116-117) */
+  int32_t normalmap;
+  int32_t emissive;
+  float eta[3];
+  float k[3];
+  float anisotropy;
+} orc_material;
+
+/* A texture: exactly one of u8_pixels (packed 8-bit RGBA or BGRA words) / f32_pixels is set. */
+typedef struct {
+  const uint32_t *u8_pixels;
+  const float *f32_pixels;
+  int32_t width, height, channels;
+  int32_t is_rgba, invert_u, invert_v;
+} orc_texture;
+
+typedef struct {
+  const orc_mesh *meshes;
+  uint32_t n_meshes;
+  const orc_instance *instances;
+  uint32_t n_instances;
+  const orc_material *materials;
+  uint32_t n_materials;
+  const orc_texture *textures;
+  uint32_t n_textures;
+  int32_t envmap; /* index of a 4-channel f32 texture */
+  float inv_P[16];
+  float inv_V[16];
+} orc_scene;
+
+typedef struct {
+  int32_t width, height, spp, max_depth;
+  uint32_t seed;       /* Sobol/Owen seed */
+  int32_t index_mode;  /* 0: (x*H+y)*spp+s (integrator_optix.cu:43); 1: 4*pixel*frame (Integrator.h:80) */
+  int32_t rr_start;    /* Russian roulette from this bounce; -1 = off (the reference has none) */
+  int32_t threads;     /* tile workers; 0 = hardware concurrency */
+  int32_t tile;        /* tile edge in pixels (editor default 20, NovaRenderer_draw.cpp:14) */
+  int32_t vertical_invert;
+} orc_options;
+
+typedef struct {
+  uint64_t segments;   /* Li evaluations (one ray segment each) */
+  uint64_t traced;     /* BVH queries issued */
+  uint64_t node_visits;
+  uint64_t tri_tests;
+  double seconds;      /* wall time of the frame loop */
+} orc_stats;
+
+/* Sampler (math_random.h:29-120). */
+void orc_sobol_table(uint32_t out[256 * 32]);
+void orc_sobol_samples(const uint32_t *index, const uint32_t *dim, uint64_t n, uint32_t seed, float *out);
+void orc_acos_lut(float *out, int32_t precision);
+
+/* Scene + native SAH BVH (aggregate/native/BvhBuilder.cpp). Returns NULL on bad input. */
+void *orc_build(const orc_scene *scene);
+void orc_free(void *h);
+void orc_bvh_info(void *h, int64_t *nodes, int64_t *leaves, int64_t *max_leaf);
+
+/* Closest hit of n world-space rays (tnear 1e-6, tfar MAXFLOAT as Ray.h:14 / native.cpp:57).
+ * prim = global primitive id or -1, t/u/v = Moller-Trumbore distance and barycentrics. */
+void orc_trace(void *h, uint64_t n, const float *orig, const float *dir, int32_t *prim, float *t, float *u,
+               float *v, orc_stats *stats);
+
+/* Camera ray of pixel (x, y), sample s (Integrator.h:66-85 with the chosen index mapping). */
+void orc_camera_rays(void *h, const orc_options *opt, uint64_t n, const int32_t *px, const int32_t *py,
+                     const int32_t *s, float *orig, float *dir);
+
+/* Full progressive render: frames of 1 spp over 20x20 tiles on a worker pool, running-mean film.
+ * out_rgba = W*H*4 floats.  If pixel_ids != NULL only those pixels (y*W+x) are rendered. */
+int32_t orc_render(void *h, const orc_options *opt, float *out_rgba, const int32_t *pixel_ids, int64_t n_pixels,
+                   orc_stats *stats);
+
+/* Radiance of single samples (pixel x, y, sample s), RGB into out (3 per sample). */
+void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int32_t *px, const int32_t *py,
+                         const int32_t *s, float *out);
+
+/* Diffuse irradiance bake, CPU path (sources/processing/TextureProcessing.cpp:10-64). */
+int32_t orc_bake_irradiance(const float *src, int32_t src_w, int32_t src_h, int32_t channels, int32_t out_w,
+                            int32_t out_h, int32_t samples, int32_t threads, float *out);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,223 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+Test infrastructure: the oracle is the parity checker for the CUDA path and the timed CPU
+baseline.  Only tests/, the smoke check and bench.py's CPU-baseline leg load it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+
+f32p = C.POINTER(C.c_float)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+
+
+class OrcMesh(C.Structure):
+    _fields_ = [("vertices", f32p), ("normals", f32p), ("tangents", f32p), ("bitangents", f32p), ("uv", f32p),
+                ("indices", u32p), ("n_verts", C.c_uint32), ("n_tris", C.c_uint32)]
+
+
+class OrcInstance(C.Structure):
+    _fields_ = [("mesh", C.c_uint32), ("material", C.c_uint32), ("m", C.c_float * 16), ("inv", C.c_float * 16),
+                ("n", C.c_float * 9)]
+
+
+class OrcMaterial(C.Structure):
+    _fields_ = [("albedo", C.c_int32), ("metallic", C.c_int32), ("normalmap", C.c_int32), ("emissive", C.c_int32),
+                ("eta", C.c_float * 3), ("k", C.c_float * 3), ("anisotropy", C.c_float)]
+
+
+class OrcTexture(C.Structure):
+    _fields_ = [("u8_pixels", u32p), ("f32_pixels", f32p), ("width", C.c_int32), ("height", C.c_int32),
+                ("channels", C.c_int32), ("is_rgba", C.c_int32), ("invert_u", C.c_int32), ("invert_v", C.c_int32)]
+
+
+class OrcScene(C.Structure):
+    _fields_ = [("meshes", C.POINTER(OrcMesh)), ("n_meshes", C.c_uint32),
+                ("instances", C.POINTER(OrcInstance)), ("n_instances", C.c_uint32),
+                ("materials", C.POINTER(OrcMaterial)), ("n_materials", C.c_uint32),
+                ("textures", C.POINTER(OrcTexture)), ("n_textures", C.c_uint32),
+                ("envmap", C.c_int32), ("inv_P", C.c_float * 16), ("inv_V", C.c_float * 16)]
+
+
+class OrcOptions(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
+                ("seed", C.c_uint32), ("index_mode", C.c_int32), ("rr_start", C.c_int32), ("threads", C.c_int32),
+                ("tile", C.c_int32), ("vertical_invert", C.c_int32)]
+
+
+class OrcStats(C.Structure):
+    _fields_ = [("segments", C.c_uint64), ("traced", C.c_uint64), ("node_visits", C.c_uint64),
+                ("tri_tests", C.c_uint64), ("seconds", C.c_double)]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.orc_sobol_table.argtypes = [u32p]
+        L.orc_sobol_samples.argtypes = [u32p, u32p, C.c_uint64, C.c_uint32, f32p]
+        L.orc_acos_lut.argtypes = [f32p, C.c_int32]
+        L.orc_build.argtypes = [C.POINTER(OrcScene)]
+        L.orc_build.restype = C.c_void_p
+        L.orc_free.argtypes = [C.c_void_p]
+        L.orc_bvh_info.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_trace.argtypes = [C.c_void_p, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, C.POINTER(OrcStats)]
+        L.orc_camera_rays.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_uint64, i32p, i32p, i32p, f32p, f32p]
+        L.orc_render.argtypes = [C.c_void_p, C.POINTER(OrcOptions), f32p, i32p, C.c_int64, C.POINTER(OrcStats)]
+        L.orc_render.restype = C.c_int32
+        L.orc_sample_radiance.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_uint64, i32p, i32p, i32p, f32p]
+        L.orc_bake_irradiance.argtypes = [f32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                          C.c_int32, f32p]
+        L.orc_bake_irradiance.restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def sobol_table() -> np.ndarray:
+    out = np.zeros((256, 32), np.uint32)
+    lib().orc_sobol_table(_p(out, u32p))
+    return out
+
+
+def sobol_samples(index, dim, seed: int) -> np.ndarray:
+    index = np.ascontiguousarray(index, np.uint32)
+    dim = np.ascontiguousarray(dim, np.uint32)
+    out = np.zeros(index.shape, np.float32)
+    lib().orc_sobol_samples(_p(index, u32p), _p(dim, u32p), index.size, seed, _p(out, f32p))
+    return out
+
+
+def acos_lut(precision: int = 500000) -> np.ndarray:
+    out = np.zeros(precision, np.float32)
+    lib().orc_acos_lut(_p(out, f32p), precision)
+    return out
+
+
+def options(width, height, spp, max_depth, seed=0, index_mode=0, rr_start=-1, threads=0, tile=20, vertical_invert=0):
+    return OrcOptions(width, height, spp, max_depth, seed, index_mode, rr_start, threads, tile, vertical_invert)
+
+
+class OracleScene:
+    """Builds the oracle's scene + reference binary SAH BVH from a scene dictionary
+    (see axomae_b200.scenes for the layout)."""
+
+    def __init__(self, scene: dict):
+        self._keep = []
+        meshes = (OrcMesh * len(scene["meshes"]))()
+        for i, m in enumerate(scene["meshes"]):
+            arrs = [np.ascontiguousarray(m[k], np.float32) for k in ("vertices", "normals", "tangents", "bitangents",
+                                                                      "uv")]
+            idx = np.ascontiguousarray(m["indices"], np.uint32)
+            self._keep += arrs + [idx]
+            meshes[i] = OrcMesh(*[_p(a, f32p) for a in arrs], _p(idx, u32p), arrs[0].size // 3, idx.size // 3)
+        insts = (OrcInstance * len(scene["instances"]))()
+        for i, x in enumerate(scene["instances"]):
+            m = np.asarray(x["m"], np.float32).reshape(16)
+            inv = np.asarray(x["inv"], np.float32).reshape(16)
+            n = np.asarray(x["n"], np.float32).reshape(9)
+            insts[i] = OrcInstance(x["mesh"], x["material"], (C.c_float * 16)(*m), (C.c_float * 16)(*inv),
+                                   (C.c_float * 9)(*n))
+        mats = (OrcMaterial * len(scene["materials"]))()
+        for i, m in enumerate(scene["materials"]):
+            mats[i] = OrcMaterial(m.get("albedo", -1), m.get("metallic", -1), m.get("normalmap", -1),
+                                  m.get("emissive", -1), (C.c_float * 3)(*m.get("eta", (0, 0, 0))),
+                                  (C.c_float * 3)(*m.get("k", (0, 0, 0))), m.get("anisotropy", 0.0))
+        texs = (OrcTexture * len(scene["textures"]))()
+        for i, t in enumerate(scene["textures"]):
+            if t["format"] == "u8":
+                px = np.ascontiguousarray(t["pixels"], np.uint32)
+                texs[i] = OrcTexture(_p(px, u32p), None, t["width"], t["height"], t.get("channels", 4),
+                                     int(t.get("is_rgba", 1)), int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+            else:
+                px = np.ascontiguousarray(t["pixels"], np.float32)
+                texs[i] = OrcTexture(None, _p(px, f32p), t["width"], t["height"], t.get("channels", 4),
+                                     int(t.get("is_rgba", 1)), int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+            self._keep.append(px)
+        sc = OrcScene(meshes, len(scene["meshes"]), insts, len(scene["instances"]), mats, len(scene["materials"]),
+                      texs, len(scene["textures"]), scene["envmap"],
+                      (C.c_float * 16)(*np.asarray(scene["inv_P"], np.float32).reshape(16)),
+                      (C.c_float * 16)(*np.asarray(scene["inv_V"], np.float32).reshape(16)))
+        self._keep += [meshes, insts, mats, texs, sc]
+        self.h = lib().orc_build(C.byref(sc))
+        if not self.h:
+            raise ValueError("oracle rejected the scene")
+        self._keep = []  # the oracle copied everything it needs
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_free(self.h)
+            self.h = None
+
+    def bvh_info(self):
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        lib().orc_bvh_info(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+    def trace(self, orig, dirs):
+        orig = np.ascontiguousarray(orig, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        n = orig.shape[0]
+        prim = np.zeros(n, np.int32)
+        t, u, v = (np.zeros(n, np.float32) for _ in range(3))
+        st = OrcStats()
+        lib().orc_trace(self.h, n, _p(orig, f32p), _p(dirs, f32p), _p(prim, i32p), _p(t, f32p), _p(u, f32p),
+                        _p(v, f32p), C.byref(st))
+        return prim, t, u, v, st
+
+    def camera_rays(self, opt, px, py, ps):
+        px, py, ps = (np.ascontiguousarray(a, np.int32) for a in (px, py, ps))
+        n = px.size
+        o = np.zeros((n, 3), np.float32)
+        d = np.zeros((n, 3), np.float32)
+        lib().orc_camera_rays(self.h, C.byref(opt), n, _p(px, i32p), _p(py, i32p), _p(ps, i32p), _p(o, f32p),
+                              _p(d, f32p))
+        return o, d
+
+    def render(self, opt, pixel_ids=None):
+        out = np.zeros((opt.height, opt.width, 4), np.float32)
+        st = OrcStats()
+        if pixel_ids is None:
+            rc = lib().orc_render(self.h, C.byref(opt), _p(out, f32p), None, 0, C.byref(st))
+        else:
+            ids = np.ascontiguousarray(pixel_ids, np.int32)
+            rc = lib().orc_render(self.h, C.byref(opt), _p(out, f32p), _p(ids, i32p), ids.size, C.byref(st))
+        if rc != 0:
+            raise ValueError("oracle render failed: %d" % rc)
+        return out, st
+
+    def sample_radiance(self, opt, px, py, ps):
+        px, py, ps = (np.ascontiguousarray(a, np.int32) for a in (px, py, ps))
+        out = np.zeros((px.size, 3), np.float32)
+        lib().orc_sample_radiance(self.h, C.byref(opt), px.size, _p(px, i32p), _p(py, i32p), _p(ps, i32p),
+                                  _p(out, f32p))
+        return out
+
+
+def bake_irradiance(src: np.ndarray, out_w: int, out_h: int, samples: int, threads: int = 8) -> np.ndarray:
+    src = np.ascontiguousarray(src, np.float32)
+    h, w, ch = src.shape
+    out = np.zeros((out_h, out_w, ch), np.float32)
+    rc = lib().orc_bake_irradiance(_p(src, f32p), w, h, ch, out_w, out_h, samples, threads, _p(out, f32p))
+    if rc != 0:
+        raise ValueError("bake rejected")
+    return out
