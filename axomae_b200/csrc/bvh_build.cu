@@ -440,10 +440,13 @@ __global__ void k_partition(Shared s, const Task *tasks, const Chunk *chunks, Sp
     __syncthreads();
     const unsigned below = (1u << lane) - 1u;
     if (valid) {
-      if (left)
-        dst[base_l + warp_l[w] + __popc(ml & below)] = id;
+      /* positions stay inside [begin, mid) / [mid, end) because partition and binning share
+       * bin_of(); the guard keeps a bookkeeping error from ever writing outside the node */
+      const unsigned pos = left ? base_l + warp_l[w] + __popc(ml & below) : base_r + warp_r[w] + __popc(mr & below);
+      if (left ? (pos < sp.mid) : (pos < t.end))
+        dst[pos] = id;
       else
-        dst[base_r + warp_r[w] + __popc(mr & below)] = id;
+        atomicAdd(s.leaf_count + 1, 1u);
     }
     __syncthreads();
   }
@@ -588,10 +591,11 @@ __global__ void __launch_bounds__(kBlock) k_build_small(Shared s, const Task *sm
       const unsigned pl = block_exclusive_scan(valid && left, scan_sh, &tl);
       const unsigned pr = block_exclusive_scan(valid && !left, scan_sh, &tr);
       if (valid) {
-        if (left)
-          dst[t.begin + run_l + pl] = id;
+        const uint32_t pos = left ? t.begin + run_l + pl : mid + run_r + pr;
+        if (left ? (pos < mid) : (pos < t.end))
+          dst[pos] = id;
         else
-          dst[mid + run_r + pr] = id;
+          atomicAdd(s.leaf_count + 1, 1u);
       }
       run_l += tl;
       run_r += tr;
@@ -653,7 +657,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
   /* scratch */
   uint32_t *ids0 = nullptr, *ids1 = nullptr;
   Task *large_a = nullptr, *large_b = nullptr, *small = nullptr;
-  unsigned *counters = nullptr; /* node, large_next, small, leaf */
+  unsigned *counters = nullptr; /* node, large_next, small, leaf, partition errors */
   uint2 *leaves = nullptr;
   int *maxdepth = nullptr;
   float *scene = nullptr, *cb = nullptr;
@@ -673,7 +677,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     NB_TRY(cudaMallocAsync(&large_a, sizeof(Task) * max_large, stream));
     NB_TRY(cudaMallocAsync(&large_b, sizeof(Task) * max_large, stream));
     NB_TRY(cudaMallocAsync(&small, sizeof(Task) * max_small, stream));
-    NB_TRY(cudaMallocAsync(&counters, sizeof(unsigned) * 4, stream));
+    NB_TRY(cudaMallocAsync(&counters, sizeof(unsigned) * 5, stream));
     NB_TRY(cudaMallocAsync(&leaves, sizeof(uint2) * n, stream));
     NB_TRY(cudaMallocAsync(&maxdepth, sizeof(int), stream));
     NB_TRY(cudaMallocAsync(&scene, sizeof(float) * 6, stream));
@@ -681,7 +685,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     NB_TRY(cudaMallocAsync(&bins, sizeof(Bins) * max_large, stream));
     NB_TRY(cudaMallocAsync(&splits, sizeof(SplitInfo) * max_large, stream));
     NB_TRY(cudaMallocAsync(&chunks, sizeof(Chunk) * max_chunks, stream));
-    NB_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * 4, stream));
+    NB_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * 5, stream));
     NB_TRY(cudaMemsetAsync(maxdepth, 0, sizeof(int), stream));
     {
       const float init[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -751,7 +755,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     NB_TRY(cudaStreamSynchronize(stream));
     if (n_small) k_build_small<<<n_small, kBlock, 0, stream>>>(sh, small);
     NB_TRY(cudaGetLastError());
-    unsigned hc[4];
+    unsigned hc[5];
     int hdepth = 0;
     NB_TRY(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, stream));
     NB_TRY(cudaMemcpyAsync(&hdepth, maxdepth, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -759,6 +763,10 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     if (hc[3]) k_sort_leaves<<<(hc[3] + 255) / 256, 256, 0, stream>>>(leaves, hc[3], order);
     NB_TRY(cudaGetLastError());
     NB_TRY(cudaStreamSynchronize(stream));
+    if (hc[4] != 0) {
+      err = cudaErrorUnknown; /* partition inconsistency: never expected, reported as a build failure */
+      goto cleanup;
+    }
     if (res) {
       res->n_nodes = hc[0];
       res->n_leaves = hc[3];

@@ -191,6 +191,7 @@ def run_ours(args, rank, world, local_rank):
     traced = 0
     dev_ms = 0.0
     trace_ms = 0.0
+    shade_ms = 0.0
     kernels = 0
     waves = 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -201,6 +202,7 @@ def run_ours(args, rank, world, local_rank):
             traced += st.traced
             dev_ms += st.device_ms
             trace_ms += st.trace_ms
+            shade_ms += st.shade_ms
             kernels += st.kernels
             waves += st.waves
         ev1.record()
@@ -281,6 +283,7 @@ def run_ours(args, rank, world, local_rank):
                     os.environ.get("NOVA_BENCH_CPU_STRIDE", "64"), cpu["pixels"], cpu["seconds"])},
             "clocks": clk.summary(), "gpu_launches": kernels,
             "extra": {"waves_per_step": waves / args.steps, "traced_per_step": traced / args.steps,
+                      "trace_ms_per_step": trace_ms / args.steps, "shade_ms_per_step": shade_ms / args.steps,
                       "bvh_build_s": build_s, "upload_s": upload_s, "bvh_nodes": info["nodes"],
                       "device_bytes": info["device_bytes"]}}
     print(json.dumps(line), flush=True)
@@ -293,12 +296,18 @@ def pin_scene(scene):
     import torch
 
     def pin(a):
-        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-        return t.numpy()
+        a = np.ascontiguousarray(a)
+        raw = a.view(np.int32) if a.dtype == np.uint32 else a
+        t = torch.from_numpy(raw).pin_memory()
+        keep.append(t)
+        return t.numpy().view(a.dtype)
+
+    keep = []
 
     out = dict(scene)
     out["meshes"] = [{k: pin(v) for k, v in m.items()} for m in scene["meshes"]]
     out["textures"] = [dict(t, pixels=pin(t["pixels"])) for t in scene["textures"]]
+    out["_pinned"] = keep
     return out
 
 
@@ -310,7 +319,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="override the frame size (profiling)")
+    ap.add_argument("--spp", type=int, help="override samples per pixel (profiling)")
     args = ap.parse_args()
+    if args.frame:
+        CFG["width"], CFG["height"] = args.frame
+    if args.spp:
+        CFG["spp"] = args.spp
+    if args.frame or args.spp:
+        global WORKLOAD
+        WORKLOAD = WORKLOAD.replace("1920x1080, 64 spp", "%dx%d, %d spp" % (CFG["width"], CFG["height"], CFG["spp"]))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus else 1)))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
