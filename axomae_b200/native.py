@@ -81,7 +81,7 @@ _lib = None
 
 EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "nova_b200_build_bvh",
            "nova_b200_render", "nova_b200_trace", "nova_b200_sobol", "nova_b200_bake_irradiance",
-           "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize"]
+           "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc"]
 
 
 def lib():
@@ -105,6 +105,7 @@ def lib():
         L.nova_b200_get_error.restype = None
         L.nova_b200_scene_info.argtypes = [vp] + [C.POINTER(C.c_uint64)] * 5
         L.nova_b200_synchronize.argtypes = [vp]
+        L.nova_b200_render_noalloc.argtypes = [vp, C.POINTER(Frame), vp]
         for name in EXPORTS:
             if name != "nova_b200_get_error":
                 getattr(L, name).restype = C.c_int
@@ -210,6 +211,10 @@ class Context:
         dev = None if film_device_ptr is None else C.c_void_p(film_device_ptr)
         self._check(lib().nova_b200_render(self.h, C.byref(frame), host, dev, C.byref(st)))
         return st
+
+    def render_noalloc(self, frame: Frame, film_device_ptr: int):
+        """Allocation-free render into a device film (mean of the frame's sample range)."""
+        self._check(lib().nova_b200_render_noalloc(self.h, C.byref(frame), C.c_void_p(film_device_ptr)))
 
     def trace(self, orig_ptr, dir_ptr, n, prim_ptr, t_ptr, u_ptr, v_ptr):
         """Device pointers (e.g. torch CUDA tensors' data_ptr())."""

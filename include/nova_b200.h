@@ -159,6 +159,16 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *ctx, const nova_b200_bvh_opt
 nova_b200_status nova_b200_render(nova_b200_ctx *ctx, const nova_b200_frame *frame, float *film_host,
                                   float *film_device, nova_b200_render_stats *stats);
 
+/* Allocation-free variant of nova_b200_render, for callers that cannot call cudaMalloc during a
+ * frame (device memory fully reserved by another allocator, or a real-time loop that must not risk
+ * an allocation or a device-wide synchronisation).  No counterpart in the reference.  Renders
+ * samples [sample_begin, sample_begin + sample_count) of every pixel and writes their mean RGBA
+ * to film_device (width*height*4 floats, device memory); the context's accumulation film and
+ * frame->reset are not used.  Its only scratch is a static 32 MiB device array shared by every
+ * call, so calls that overlap on the GPU race.  sample_count is limited to 2097152.  The first
+ * call on a device looks up the array's address; make it before any stream capture. */
+nova_b200_status nova_b200_render_noalloc(nova_b200_ctx *ctx, const nova_b200_frame *frame, float *film_device);
+
 /* Closest-hit queries for n world-space rays held in DEVICE memory (3 floats each): the intersector
  * of DeviceIntersectorInterface::traverse / GenericHostAccelerator::hit (aggregate/acceleration_interface.h).
  * prim = global primitive index (-1 on miss), t / u / v = Moller-Trumbore distance and barycentrics. */
