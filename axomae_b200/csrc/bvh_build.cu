@@ -76,7 +76,7 @@ struct Shared {
   uint2 *leaves;
   unsigned *leaf_count;
   int *max_depth;
-  int bins, max_leaf;
+  int bins, max_leaf, hard_leaf;
   float cost_trav;
 };
 
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(kBlock) k_build_small(Shared s, const Task *sm
     if (!make_leaf) {
       const float leaf_cost = (float)n;
       if ((int)n <= s.max_leaf && (!has_split || leaf_cost <= best.cost)) make_leaf = true;
-      if ((int)n <= kHardLeaf && !has_split) make_leaf = true;
+      if ((int)n <= s.hard_leaf && !has_split) make_leaf = true;
     }
     if (make_leaf) {
       for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) s.order[i] = src[i];
@@ -651,7 +651,8 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
   auto t0 = std::chrono::steady_clock::now();
   if (n == 0) return cudaErrorInvalidValue;
   const int nb = std::max(4, std::min(kMaxBins, p.bins > 0 ? p.bins : 16));
-  const int max_leaf = std::max(1, std::min(kHardLeaf, p.max_leaf > 0 ? p.max_leaf : 8));
+  const int hard_leaf = std::max(1, std::min(kHardLeaf, p.hard_leaf > 0 ? p.hard_leaf : kHardLeaf));
+  const int max_leaf = std::max(1, std::min(hard_leaf, p.max_leaf > 0 ? p.max_leaf : 8));
   const size_t max_large = n / kSmallTask + 2;
   const size_t max_small = n + 1;
   /* scratch */
@@ -714,6 +715,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     sh.max_depth = maxdepth;
     sh.bins = nb;
     sh.max_leaf = max_leaf;
+    sh.hard_leaf = hard_leaf;
     sh.cost_trav = p.cost_trav > 0.f ? p.cost_trav : 1.0f;
 
     Task root{0u, n, -1, 0, 0, 0, {hscene[0], hscene[1], hscene[2]}, {hscene[3], hscene[4], hscene[5]}};

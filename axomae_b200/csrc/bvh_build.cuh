@@ -7,6 +7,7 @@ namespace nb {
 
 struct BvhBuildParams {
   int max_leaf;     /* preferred maximum leaf size (SAH may stop earlier); hard cap 16 */
+  int hard_leaf;    /* nodes with more primitives are always split (median when SAH finds no plane) */
   int bins;         /* SAH bins per axis (<= 32) */
   float cost_trav;  /* SAH cost of one inner-node visit relative to one triangle test */
 };

@@ -15,6 +15,7 @@
 #include <cstring>
 
 #include "bvh_build.cuh"
+#include "bvh_wide.cuh"
 #include "context.cuh"
 #include "traverse.cuh"
 
@@ -106,8 +107,7 @@ __global__ void k_prim_boxes(nb::DevScene sc, const uint32_t *valid, uint32_t n,
   const uint32_t tri = prim - I.prim_offset;
   nb::V3 w[3];
   for (int k = 0; k < 3; k++) {
-    const uint32_t vi = m.idx[3 * tri + k];
-    nb::V3 v{m.v[3 * vi], m.v[3 * vi + 1], m.v[3 * vi + 2]};
+    const nb::V3 v = nb::vertex_position(m, m.idx[3 * tri + k]);
     w[k] = I.identity ? v : nb::xform_point(I.m, v);
   }
   lo[i] = make_float4(fminf(w[0].x, fminf(w[1].x, w[2].x)), fminf(w[0].y, fminf(w[1].y, w[2].y)),
@@ -126,13 +126,22 @@ __global__ void k_write_tris(nb::DevScene sc, const uint32_t *valid, const uint3
   const nb::DevMesh &m = sc.meshes[I.mesh];
   const uint32_t tri = prim - I.prim_offset;
   const uint32_t a = m.idx[3 * tri], b = m.idx[3 * tri + 1], cc = m.idx[3 * tri + 2];
-  const nb::V3 v0{m.v[3 * a], m.v[3 * a + 1], m.v[3 * a + 2]};
-  const nb::V3 v1{m.v[3 * b], m.v[3 * b + 1], m.v[3 * b + 2]};
-  const nb::V3 v2{m.v[3 * cc], m.v[3 * cc + 1], m.v[3 * cc + 2]};
+  const nb::V3 v0 = nb::vertex_position(m, a), v1 = nb::vertex_position(m, b), v2 = nb::vertex_position(m, cc);
   const nb::V3 e1 = v1 - v0, e2 = v2 - v0;
   tris[3 * k + 0] = make_float4(v0.x, v0.y, v0.z, __int_as_float((int)prim));
   tris[3 * k + 1] = make_float4(e1.x, e1.y, e1.z, __int_as_float((int)inst));
   tris[3 * k + 2] = make_float4(e2.x, e2.y, e2.z, 0.f);
+}
+
+/* Interleaves the SoA vertex attributes of one mesh into 64 B records (layout in device_scene.cuh). */
+__global__ void k_interleave(const float *v, const float *n, const float *t, const float *b, const float *uv,
+                             uint32_t nv, float4 *attr) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  attr[4 * (size_t)i + 0] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], n[3 * i]);
+  attr[4 * (size_t)i + 1] = make_float4(n[3 * i + 1], n[3 * i + 2], t[3 * i], t[3 * i + 1]);
+  attr[4 * (size_t)i + 2] = make_float4(t[3 * i + 2], b[3 * i], b[3 * i + 1], b[3 * i + 2]);
+  attr[4 * (size_t)i + 3] = make_float4(uv[2 * i], uv[2 * i + 1], 0.f, 0.f);
 }
 
 __global__ void k_validate(const float4 *nodes, uint32_t n_nodes, uint32_t n_tris, unsigned *bad) {
@@ -265,20 +274,27 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     o.n_verts = m.n_verts, o.n_tris = m.n_tris;
     nova_b200_status st;
     const size_t nv = m.n_verts;
-    float *p;
     uint32_t *q;
-    if ((st = upload(c, m.vertices, 3 * nv, &p))) return st;
-    o.v = p;
-    if ((st = upload(c, m.normals, 3 * nv, &p))) return st;
-    o.n = p;
-    if ((st = upload(c, m.tangents, 3 * nv, &p))) return st;
-    o.t = p;
-    if ((st = upload(c, m.bitangents, 3 * nv, &p))) return st;
-    o.b = p;
-    if ((st = upload(c, m.uv, 2 * nv, &p))) return st;
-    o.uv = p;
     if ((st = upload(c, m.indices, 3ull * m.n_tris, &q))) return st;
     o.idx = q;
+    /* attributes: SoA staging on the stream, interleaved into the persistent 64 B records */
+    void *attr = nullptr;
+    NB_CUDA(c, cudaMalloc(&attr, nv * 64), "cudaMalloc(attributes)");
+    c->scene_allocs.push_back(attr);
+    c->scene_bytes += nv * 64;
+    float *stage = nullptr;
+    NB_CUDA(c, cudaMallocAsync(&stage, nv * 14 * sizeof(float), c->stream), "cudaMalloc(staging)");
+    float *sv = stage, *sn = stage + 3 * nv, *st_ = stage + 6 * nv, *sb = stage + 9 * nv, *suv = stage + 12 * nv;
+    NB_CUDA(c, cudaMemcpyAsync(sv, m.vertices, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(vertices)");
+    NB_CUDA(c, cudaMemcpyAsync(sn, m.normals, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(normals)");
+    NB_CUDA(c, cudaMemcpyAsync(st_, m.tangents, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(tangents)");
+    NB_CUDA(c, cudaMemcpyAsync(sb, m.bitangents, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(bitangents)");
+    NB_CUDA(c, cudaMemcpyAsync(suv, m.uv, 8 * nv, cudaMemcpyHostToDevice, c->stream), "upload(uv)");
+    k_interleave<<<(unsigned)((nv + 255) / 256), 256, 0, c->stream>>>(sv, sn, st_, sb, suv, (uint32_t)nv,
+                                                                      static_cast<float4 *>(attr));
+    NB_CUDA(c, cudaGetLastError(), "k_interleave");
+    NB_CUDA(c, cudaFreeAsync(stage, c->stream), "cudaFree(staging)");
+    o.attr = static_cast<const float4 *>(attr);
   }
   /* instances + primitive tables */
   c->h_instances.resize(d->n_instances);
@@ -345,12 +361,15 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   if (!c->scene_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "upload a scene before building%s");
   cudaSetDevice(c->device);
   const uint32_t n = (uint32_t)c->h_valid.size();
+  const int width = opts && opts->width ? opts->width : 2;
+  if (width != 2 && width != 8) return fail(c, NOVA_B200_INVALID_ARGUMENT, "BVH width must be 2 or 8%s");
   nb::BvhBuildParams p;
-  p.max_leaf = opts && opts->max_leaf_size > 0 ? opts->max_leaf_size : 8;
+  p.max_leaf = opts && opts->max_leaf_size > 0 ? opts->max_leaf_size : (width == 8 ? nb::kWideLeafMax : 8);
+  p.hard_leaf = width == 8 ? nb::kWideLeafMax : 16;
   p.bins = opts && opts->bins > 0 ? opts->bins : 16;
   p.cost_trav = 1.0f;
-  if (p.max_leaf > 16 || p.bins < 4 || p.bins > 32)
-    return fail(c, NOVA_B200_INVALID_ARGUMENT, "max_leaf_size must be 1..16 and bins 4..32%s");
+  if (p.max_leaf > p.hard_leaf || p.bins < 4 || p.bins > 32)
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "max_leaf_size must be 1..16 (1..4 for width 8) and bins 4..32%s");
   cudaFree(c->d_nodes);
   cudaFree(c->d_tris);
   c->d_nodes = nullptr;
@@ -384,8 +403,34 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   NB_CUDA(c, cudaStreamSynchronize(c->stream), "build_bvh");
   if (c->h_counters[0] != 0 || r.n_nodes == 0 || r.n_nodes > max_nodes || r.max_depth >= nb::kTraversalStack)
     return fail(c, NOVA_B200_RENDERER_EXCEPTION, "BVH validation failed%s");
+  if (width == 8) {
+    float4 *wnodes = nullptr, *wtris = nullptr;
+    NB_CUDA(c, cudaMalloc(&wnodes, sizeof(float4) * 5 * ((size_t)r.n_nodes + 1)), "cudaMalloc(wide nodes)");
+    cudaError_t we = cudaMalloc(&wtris, sizeof(float4) * 3 * (size_t)n);
+    if (we != cudaSuccess) {
+      cudaFree(wnodes);
+      return cuda_fail(c, we, "cudaMalloc(wide triangles)");
+    }
+    nb::WideBuildResult wr{};
+    we = nb::build_wide_bvh(c->d_nodes, r.n_nodes, c->d_tris, n, wnodes, wtris, c->stream, &wr);
+    if (we != cudaSuccess || wr.depth >= nb::kWideStack) {
+      cudaFree(wnodes);
+      cudaFree(wtris);
+      if (we != cudaSuccess) return cuda_fail(c, we, "build_wide_bvh");
+      return fail(c, NOVA_B200_RENDERER_EXCEPTION, "wide BVH deeper than the traversal stack%s");
+    }
+    cudaFree(c->d_nodes);
+    cudaFree(c->d_tris);
+    c->d_nodes = wnodes;
+    c->d_tris = wtris;
+    r.n_nodes = wr.n_nodes;
+    r.max_depth = wr.depth;
+    r.ms += wr.ms;
+  }
   c->scene.nodes = c->d_nodes;
   c->scene.tris = c->d_tris;
+  c->scene.width = width;
+  c->bvh_width = width;
   c->n_nodes = r.n_nodes;
   c->n_leaves = r.n_leaves;
   c->bvh_depth = r.max_depth;
@@ -435,8 +480,8 @@ nova_b200_status nova_b200_scene_info(nova_b200_ctx *c, uint64_t *tris, uint64_t
   if (nodes) *nodes = c->n_nodes;
   if (leaves) *leaves = c->n_leaves;
   if (bytes)
-    *bytes = c->scene_bytes + (uint64_t)c->n_nodes * 64 + (uint64_t)c->h_valid.size() * 48 + c->queue_bytes +
-             c->radiance_cap * 16;
+    *bytes = c->scene_bytes + (uint64_t)c->n_nodes * (c->bvh_width == 8 ? 80 : 64) +
+             (uint64_t)c->h_valid.size() * 48 + c->queue_bytes + c->radiance_cap * 16;
   return NOVA_B200_SUCCESS;
 }
 

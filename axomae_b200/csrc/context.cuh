@@ -27,6 +27,7 @@ struct nova_b200_ctx {
   bool bvh_ready = false;
   uint32_t n_nodes = 0, n_leaves = 0;
   int bvh_depth = 0;
+  int bvh_width = 0;
   double bvh_ms = 0.0;
   uint64_t scene_bytes = 0;
 

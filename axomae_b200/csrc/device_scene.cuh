@@ -10,8 +10,8 @@
  *              ref >= 0: inner node index; ref < 0: leaf whose triangles start at ~ref (count in n3.z/w).
  *   prim_inst  instance index of every global primitive (primitive order of the reference:
  *              instance by instance, triangle by triangle; api/engine.cpp:159-175).
- *   meshes / instances / materials / textures: shading data, object-space vertex attributes gathered
- *              through the index buffer at hit time.
+ *   meshes / instances / materials / textures: shading data; object-space vertex attributes are
+ *              interleaved per vertex (DevMesh) and gathered through the index buffer at hit time.
  */
 #pragma once
 #include "dmath.cuh"
@@ -32,11 +32,19 @@ struct DevMaterial {
   float anisotropy;
 };
 
+/* Vertex attributes interleaved, 64 B per vertex (two 32 B sectors):
+ *   attr[4 i + 0] = (p.x, p.y, p.z, n.x)   attr[4 i + 1] = (n.y, n.z, t.x, t.y)
+ *   attr[4 i + 2] = (t.z, b.x, b.y, b.z)   attr[4 i + 3] = (u, v, 0, 0)                          */
 struct DevMesh {
-  const float *v, *n, *t, *b, *uv;
+  const float4 *attr;
   const uint32_t *idx;
   uint32_t n_verts, n_tris;
 };
+
+NB_D V3 vertex_position(const DevMesh &m, uint32_t i) {
+  const float4 a = __ldg(m.attr + 4 * (size_t)i);
+  return {a.x, a.y, a.z};
+}
 
 struct DevInstance {
   float m[16];
@@ -49,7 +57,8 @@ struct DevInstance {
 };
 
 struct DevScene {
-  const float4 *nodes;
+  const float4 *nodes;       /* binary BVH (width 2) or compressed 8-wide BVH (width 8, bvh_wide.cuh) */
+  int32_t width;
   const float4 *tris;
   const uint32_t *prim_inst;
   const DevMesh *meshes;

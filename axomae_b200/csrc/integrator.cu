@@ -3,8 +3,9 @@
  *
  *   k_raygen   camera rays for new paths (Integrator.h:66-85 with the OptiX raygen's sample index
  *              (x * H + y) * spp + s, integrator_optix.cu:43; Sobol dimensions 0 and 1 jitter NDC)
- *   k_trace    closest hit per queued ray (traverse.cuh)
- *   k_shade    miss -> environment; hit -> principled scatter (Sobol dimensions 2 + 4b .. 5 + 4b at
+ *   k_trace    closest hit per queued ray (traverse.cuh); a miss finishes its path with the
+ *              environment lookup, hits go to a compact hit list
+ *   k_shade    per hit: principled scatter (Sobol dimensions 2 + 4b .. 5 + 4b at
  *              bounce b), throughput update, spawned ray appended to the next queue with
  *              warp-aggregated atomics; after the last allowed scatter the spawned direction looks
  *              up the environment directly (the reference traces that ray but discards the hit,
@@ -15,7 +16,7 @@
  * The recursive estimator e_0 + c_0 (e_1 + c_1 (... env)) is evaluated forward as
  * sum_k beta_k e_k + beta_K env with beta_k = c_0 ... c_{k-1}; a path whose result is not finite
  * contributes 0 (DENAN, Integrator.cpp:92).  Path state: origin + path id, direction + bounce,
- * throughput (3 x 16 B); hits 16 B; per-path radiance 16 B, written once.
+ * throughput (3 x 16 B); hits 16 B + 4 B slot; per-path radiance 16 B, written once.
  */
 #include <algorithm>
 #include <cfloat>
@@ -82,27 +83,68 @@ __global__ void __launch_bounds__(256) k_raygen(Queue q, uint32_t off, uint64_t 
   if (sc.has_emissive) L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-__global__ void __launch_bounds__(128) k_trace(Queue q, uint32_t n, float4 *hits, DevScene sc) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 o = q.o[i], d = q.d[i];
-  const TraceResult r = trace_closest(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
-  hits[i] = make_float4(r.t, r.u, r.v, __int_as_float(r.prim));
-}
-
 __device__ __forceinline__ float4 finite_or_zero(V3 L, float alpha) {
   if (!finite3(L)) return make_float4(0.f, 0.f, 0.f, 0.f);
   return make_float4(L.x, L.y, L.z, alpha);
 }
 
-__global__ void __launch_bounds__(128) k_shade(Queue in, const float4 *hits, uint32_t n, Queue out, unsigned *out_count,
-                                               float4 *L, RenderParams rp, DevScene sc) {
+/* Writes a finished path's radiance (adds the emission gathered so far when the scene has any). */
+__device__ __forceinline__ void finish_path(const DevScene &sc, float4 *L, uint32_t p, float4 result) {
+  if (sc.has_emissive) {
+    const float4 acc = L[p];
+    float4 r = make_float4(acc.x + result.x, acc.y + result.y, acc.z + result.z, result.w);
+    if (!isfinite(r.x) || !isfinite(r.y) || !isfinite(r.z)) r = make_float4(0.f, 0.f, 0.f, 0.f);
+    L[p] = r;
+  } else {
+    L[p] = result;
+  }
+}
+
+/* Closest hit of every queued ray.  A miss finishes its path here (environment lookup,
+ * Integrator.cpp:94-98); hits are appended to a compact hit list (warp-aggregated atomics) so
+ * the shading kernel only runs on rays that hit. */
+template <int WIDTH>
+__global__ void __launch_bounds__(128) k_trace(Queue q, uint32_t n, float4 *hits, uint32_t *hit_slot,
+                                               unsigned *hit_count, float4 *L, DevScene sc) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = i < n;
+  bool is_hit = false;
+  TraceResult r{-1, 0.f, 0.f, 0.f};
+  if (i < n) {
+    const float4 o = q.o[i], d = q.d[i];
+    r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
+    if (r.prim < 0) {
+      const float4 b4 = q.beta[i];
+      const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
+      finish_path(sc, L, __float_as_uint(o.w),
+                  finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z}, (float)__float_as_int(d.w) + e.w));
+    } else {
+      is_hit = true;
+    }
+  }
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned m = __ballot_sync(0xffffffffu, is_hit);
+  unsigned base = 0;
+  if (m) {
+    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(hit_count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+  }
+  if (is_hit) {
+    const unsigned slot = base + __popc(m & ((1u << lane) - 1u));
+    hits[slot] = make_float4(r.t, r.u, r.v, __int_as_float(r.prim));
+    hit_slot[slot] = i;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_shade(Queue in, const float4 *hits, const uint32_t *hit_slot,
+                                               const unsigned *hit_count, Queue out, unsigned *out_count, float4 *L,
+                                               RenderParams rp, DevScene sc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < *hit_count;
   bool enq = false;
   float4 no{}, nd{}, nbeta{};
   if (live) {
-    const float4 o4 = in.o[i], d4 = in.d[i], b4 = in.beta[i], h = hits[i];
+    const uint32_t slot_in = hit_slot[i];
+    const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
     const uint32_t p = __float_as_uint(o4.w);
     const int bounce = __float_as_int(d4.w);
     const uint32_t index = sample_index(rp, p);
@@ -111,11 +153,7 @@ __global__ void __launch_bounds__(128) k_shade(Queue in, const float4 *hits, uin
     const int prim = __float_as_int(h.w);
     bool done = false;
     float4 result = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (prim < 0) {
-      const V4 e = env_sample(sc, rd);
-      result = finite_or_zero(beta * V3{e.x, e.y, e.z}, (float)bounce + e.w);
-      done = true;
-    } else {
+    {
       const uint32_t inst = __ldg(sc.prim_inst + prim);
       const DevInstance &I = sc.instances[inst];
       const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)prim - I.prim_offset, h.x, h.y, h.z);
@@ -161,16 +199,7 @@ __global__ void __launch_bounds__(128) k_shade(Queue in, const float4 *hits, uin
         }
       }
     }
-    if (done) {
-      if (sc.has_emissive) {
-        const float4 acc = L[p];
-        float4 r = make_float4(acc.x + result.x, acc.y + result.y, acc.z + result.z, result.w);
-        if (!isfinite(r.x) || !isfinite(r.y) || !isfinite(r.z)) r = make_float4(0.f, 0.f, 0.f, 0.f);
-        L[p] = r;
-      } else {
-        L[p] = result;
-      }
-    }
+    if (done) finish_path(sc, L, p, result);
   }
   const unsigned lane = threadIdx.x & 31u;
   const unsigned m = __ballot_sync(0xffffffffu, enq);
@@ -228,7 +257,7 @@ nova_b200_status ensure_buffers(nova_b200_ctx *c, uint32_t cap, size_t radiance,
     c->d_queue = nullptr;
     c->queue_cap = 0;
     c->queue_bytes = 0;
-    const size_t bytes = (size_t)cap * 16 * 7;
+    const size_t bytes = (size_t)cap * (16 * 7 + 4);
     NB_CUDA(c, cudaMalloc(&c->d_queue, bytes), "cudaMalloc(queue)");
     c->queue_cap = cap;
     c->queue_bytes = bytes;
@@ -297,6 +326,7 @@ nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *fi
   Queue qa{base, base + cap, base + 2 * (size_t)cap}, qb{base + 3 * (size_t)cap, base + 4 * (size_t)cap,
                                                          base + 5 * (size_t)cap};
   float4 *hits = base + 6 * (size_t)cap;
+  uint32_t *hit_slot = reinterpret_cast<uint32_t *>(base + 7 * (size_t)cap);
   nova_b200_render_stats s{};
   float t_trace = 0.f, t_shade = 0.f;
   NB_CUDA(c, cudaEventRecord(c->ev_begin, c->stream), "event");
@@ -317,11 +347,17 @@ nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *fi
       next += n_new;
       s.traced += n;
       s.segments += n;
+      NB_CUDA(c, cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream), "memset");
       NB_CUDA(c, cudaEventRecord(c->ev_a, c->stream), "event");
-      k_trace<<<(n + 127) / 128, 128, 0, c->stream>>>(qa, n, hits, c->scene);
+      if (c->scene.width == 8)
+        k_trace<8><<<(n + 127) / 128, 128, 0, c->stream>>>(qa, n, hits, hit_slot, c->d_counters + 1, c->d_radiance,
+                                                          c->scene);
+      else
+        k_trace<2><<<(n + 127) / 128, 128, 0, c->stream>>>(qa, n, hits, hit_slot, c->d_counters + 1, c->d_radiance,
+                                                          c->scene);
       NB_CUDA(c, cudaEventRecord(c->ev_b, c->stream), "event");
-      NB_CUDA(c, cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned), c->stream), "memset");
-      k_shade<<<(n + 127) / 128, 128, 0, c->stream>>>(qa, hits, n, qb, c->d_counters, c->d_radiance, rp, c->scene);
+      k_shade<<<(n + 127) / 128, 128, 0, c->stream>>>(qa, hits, hit_slot, c->d_counters + 1, qb, c->d_counters,
+                                                       c->d_radiance, rp, c->scene);
       NB_CUDA(c, cudaEventRecord(c->ev_end, c->stream), "event");
       s.kernels += 2;
       NB_CUDA(c, cudaMemcpyAsync(c->h_counters, c->d_counters, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream),

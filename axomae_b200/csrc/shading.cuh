@@ -160,26 +160,32 @@ NB_D void make_onb(V3 n, V3 &b1, V3 &b2) { /* utils_3D.h:74-81 */
   b2 = {b, sign + n.y * n.y * a, -n.y};
 }
 
-NB_D V3 ld3(const float *a, uint32_t i) { return {__ldg(a + 3 * i), __ldg(a + 3 * i + 1), __ldg(a + 3 * i + 2)}; }
 NB_D V3 blerp(V3 p0, V3 p1, V3 p2, float w, float u, float v) { return p0 * w + p1 * u + p2 * v; }
+
+struct VertexAttr {
+  V3 p, n, t, b;
+  float u, v;
+};
+NB_D VertexAttr load_vertex(const DevMesh &m, uint32_t i) {
+  const float4 *a = m.attr + 4 * (size_t)i;
+  const float4 a0 = __ldg(a), a1 = __ldg(a + 1), a2 = __ldg(a + 2), a3 = __ldg(a + 3);
+  return {{a0.x, a0.y, a0.z}, {a0.w, a1.x, a1.y}, {a1.z, a1.w, a2.x}, {a2.y, a2.z, a2.w}, a3.x, a3.y};
+}
 
 NB_D HitRecord make_record(const DevScene &sc, V3 ro, V3 rd, const DevInstance &I, uint32_t tri, float t, float bu,
                            float bv) {
   const DevMesh &m = sc.meshes[I.mesh];
   const uint32_t i0 = __ldg(m.idx + 3 * tri), i1 = __ldg(m.idx + 3 * tri + 1), i2 = __ldg(m.idx + 3 * tri + 2);
+  const VertexAttr A = load_vertex(m, i0), B = load_vertex(m, i1), C = load_vertex(m, i2);
   HitRecord r;
   const float w = 1 - (bu + bv);
-  const float uv0x = __ldg(m.uv + 2 * i0), uv0y = __ldg(m.uv + 2 * i0 + 1);
-  const float uv1x = __ldg(m.uv + 2 * i1), uv1y = __ldg(m.uv + 2 * i1 + 1);
-  const float uv2x = __ldg(m.uv + 2 * i2), uv2y = __ldg(m.uv + 2 * i2 + 1);
-  r.u = uv0x * w + uv1x * bu + uv2x * bv;
-  r.v = uv0y * w + uv1y * bu + uv2y * bv;
+  r.u = A.u * w + B.u * bu + C.u * bv;
+  r.v = A.v * w + B.v * bu + C.v * bv;
   const M3 l = m3_of4(I.m);
-  const float duv02x = uv0x - uv2x, duv02y = uv0y - uv2y;
-  const float duv12x = uv1x - uv2x, duv12y = uv1y - uv2y;
-  const V3 v0 = ld3(m.v, i0), v1 = ld3(m.v, i1), v2 = ld3(m.v, i2);
-  const V3 dp02 = mul(l, V3{v0.x - v2.x, v0.y - v2.y, v0.z - v2.z});
-  const V3 dp12 = mul(l, V3{v1.x - v2.x, v1.y - v2.y, v1.z - v2.z});
+  const float duv02x = A.u - C.u, duv02y = A.v - C.v;
+  const float duv12x = B.u - C.u, duv12y = B.v - C.v;
+  const V3 dp02 = mul(l, V3{A.p.x - C.p.x, A.p.y - C.p.y, A.p.z - C.p.z});
+  const V3 dp12 = mul(l, V3{B.p.x - C.p.x, B.p.y - C.p.y, B.p.z - C.p.z});
   const float det = duv02x * duv12y - duv02y * duv12x;
   const bool degen_uv = fabsf(det) < 1e-9f;
   const float invdet = 1.f / det;
@@ -196,9 +202,9 @@ NB_D HitRecord make_record(const DevScene &sc, V3 ro, V3 rd, const DevInstance &
   r.position = ro + t * rd;
   r.dpdu = dpdu;
   r.dpdv = dpdv;
-  const V3 nn = blerp(ld3(m.n, i0), ld3(m.n, i1), ld3(m.n, i2), w, bu, bv);
-  const V3 tt = blerp(ld3(m.t, i0), ld3(m.t, i1), ld3(m.t, i2), w, bu, bv);
-  const V3 bb = blerp(ld3(m.b, i0), ld3(m.b, i1), ld3(m.b, i2), w, bu, bv);
+  const V3 nn = blerp(A.n, B.n, C.n, w, bu, bv);
+  const V3 tt = blerp(A.t, B.t, C.t, w, bu, bv);
+  const V3 bb = blerp(A.b, B.b, C.b, w, bu, bv);
   const V3 tn = normalize(mul(m3_load(I.n), nn));
   const V3 tt2 = normalize(mul(l, tt));
   const V3 tb = normalize(mul(l, bb));

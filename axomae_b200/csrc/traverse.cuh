@@ -16,6 +16,7 @@
  */
 #pragma once
 #include <cfloat>
+#include "bvh_wide.cuh"
 #include "device_scene.cuh"
 
 namespace nb {
@@ -59,8 +60,8 @@ NB_D float safe_rcp(float d) {
   return fabsf(d) > 1e-30f ? __frcp_rn(d) : copysignf(big, d);
 }
 
-/* Closest hit of one world-space ray. */
-NB_D TraceResult trace_closest(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
+/* Closest hit of one world-space ray on the binary BVH. */
+NB_D TraceResult trace_closest2(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
                                uint64_t *tri_tests = nullptr) {
   TraceResult r{-1, 0.f, 0.f, 0.f};
   float tmax = FLT_MAX; /* native.cpp:57 starts from MAXFLOAT */
@@ -143,6 +144,133 @@ NB_D TraceResult trace_closest(const DevScene &sc, V3 o, V3 d, uint64_t *node_vi
   if (node_visits) *node_visits += nv;
   if (tri_tests) *tri_tests += tt;
   return r;
+}
+
+/* Triangle tests of one leaf range with the instance-transform cache (Triangle.h:146-153). */
+NB_D void test_triangles(const DevScene &sc, uint32_t first, uint32_t count, V3 o, V3 d, int32_t &cached_inst, V3 &lo_o,
+                         V3 &lo_d, float &tmax, TraceResult &r) {
+  for (uint32_t k = first; k < first + count; k++) {
+    const float4 t0 = __ldg(&sc.tris[3 * k + 0]);
+    const float4 t1 = __ldg(&sc.tris[3 * k + 1]);
+    const float4 t2 = __ldg(&sc.tris[3 * k + 2]);
+    const int32_t inst = __float_as_int(t1.w);
+    if (inst != cached_inst) {
+      cached_inst = inst;
+      const DevInstance &I = sc.instances[inst];
+      if (I.identity) {
+        lo_o = o;
+        lo_d = d;
+      } else {
+        lo_o = xform_point(I.inv, o);
+        lo_d = xform_dir(I.inv, d);
+      }
+    }
+    float ht, hu, hv;
+    if (mt_hit(lo_o, lo_d, V3{t0.x, t0.y, t0.z}, V3{t1.x, t1.y, t1.z}, V3{t2.x, t2.y, t2.z}, kRayTNear, tmax, ht, hu,
+               hv)) {
+      tmax = ht;
+      r.prim = __float_as_int(t0.w);
+      r.t = ht;
+      r.u = hu;
+      r.v = hv;
+    }
+  }
+}
+
+/* Closest hit on the compressed 8-wide BVH (layout in bvh_wide.cuh).  Every visited node tests its
+ * eight quantised child boxes, tests the triangles of hit leaf children in slot order, then
+ * descends into the first hit inner child; the other hit inner children stay on a stack as one
+ * (child_base, hit mask, inner mask) group.  Child slots are visited in increasing (slot ^ oct)
+ * order, oct being the ray's direction-sign bits, which is near-to-far for the slot assignment. */
+NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d) {
+  TraceResult r{-1, 0.f, 0.f, 0.f};
+  float tmax = FLT_MAX;
+  const float ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
+  const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+  uint2 stack[kWideStack];
+  int sp = 0;
+  uint32_t node = 0;
+  int32_t cached_inst = -1;
+  V3 lo_o = o, lo_d = d;
+  for (;;) {
+    const float4 *np = sc.nodes + 5 * (size_t)node;
+    const float4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    const uint32_t hdr = __float_as_uint(w0.w);
+    const uint32_t imask = hdr >> 24;
+    const float sx = __uint_as_float((hdr & 0xffu) << 23), sy = __uint_as_float(((hdr >> 8) & 0xffu) << 23),
+                sz = __uint_as_float(((hdr >> 16) & 0xffu) << 23);
+    /* plane distance = (p + q s - o) * idir = q (s idir) + (p - o) idir; the near plane of each
+     * axis is the low plane when the direction component is positive, the high plane otherwise */
+    const float ax = (w0.x - o.x) * ix, ay = (w0.y - o.y) * iy, az = (w0.z - o.z) * iz;
+    const float bx = sx * ix, by = sy * iy, bz = sz * iz;
+    const uint32_t child_base = __float_as_uint(w1.x), tri_base = __float_as_uint(w1.y);
+    const uint32_t meta[2] = {__float_as_uint(w1.z), __float_as_uint(w1.w)};
+    const bool px = ix >= 0.f, py = iy >= 0.f, pz = iz >= 0.f;
+    const uint32_t nx[2] = {px ? __float_as_uint(w2.x) : __float_as_uint(w3.z), px ? __float_as_uint(w2.y) : __float_as_uint(w3.w)};
+    const uint32_t fx[2] = {px ? __float_as_uint(w3.z) : __float_as_uint(w2.x), px ? __float_as_uint(w3.w) : __float_as_uint(w2.y)};
+    const uint32_t ny[2] = {py ? __float_as_uint(w2.z) : __float_as_uint(w4.x), py ? __float_as_uint(w2.w) : __float_as_uint(w4.y)};
+    const uint32_t fy[2] = {py ? __float_as_uint(w4.x) : __float_as_uint(w2.z), py ? __float_as_uint(w4.y) : __float_as_uint(w2.w)};
+    const uint32_t nz[2] = {pz ? __float_as_uint(w3.x) : __float_as_uint(w4.z), pz ? __float_as_uint(w3.y) : __float_as_uint(w4.w)};
+    const uint32_t fz[2] = {pz ? __float_as_uint(w4.z) : __float_as_uint(w3.x), pz ? __float_as_uint(w4.w) : __float_as_uint(w3.y)};
+    uint32_t inner_hits = 0, leaf_hits = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int w = i >> 2;
+      const uint32_t sel = 0x7540u + (uint32_t)(i & 3);
+      /* byte -> exact float: 0x4B0000bb is 2^23 + bb */
+      const float qnx = __uint_as_float(__byte_perm(nx[w], 0x4B000000u, sel)) - 8388608.f;
+      const float qfx = __uint_as_float(__byte_perm(fx[w], 0x4B000000u, sel)) - 8388608.f;
+      const float qny = __uint_as_float(__byte_perm(ny[w], 0x4B000000u, sel)) - 8388608.f;
+      const float qfy = __uint_as_float(__byte_perm(fy[w], 0x4B000000u, sel)) - 8388608.f;
+      const float qnz = __uint_as_float(__byte_perm(nz[w], 0x4B000000u, sel)) - 8388608.f;
+      const float qfz = __uint_as_float(__byte_perm(fz[w], 0x4B000000u, sel)) - 8388608.f;
+      const float nr = fmaxf(fmaxf(__fmaf_rn(qnx, bx, ax), __fmaf_rn(qny, by, ay)), fmaxf(__fmaf_rn(qnz, bz, az), 0.f));
+      const float fr =
+          fminf(fminf(fminf(__fmaf_rn(qfx, bx, ax), __fmaf_rn(qfy, by, ay)), __fmaf_rn(qfz, bz, az)) * kFarScale, tmax);
+      /* empty slots store qlo = 255, qhi = 0 on every axis: near > far for either ray sign */
+      if (nr <= fr) {
+        const uint32_t bit = 1u << (i ^ oct);
+        if ((imask >> i) & 1u)
+          inner_hits |= bit;
+        else
+          leaf_hits |= bit;
+      }
+    }
+    while (leaf_hits) {
+      const uint32_t slot = (uint32_t)(__ffs(leaf_hits) - 1) ^ oct;
+      leaf_hits &= leaf_hits - 1;
+      const uint32_t m = (meta[slot >> 2] >> (8 * (slot & 3))) & 0xffu;
+      test_triangles(sc, tri_base + (m & 31u), ((m >> 5) & 3u) + 1u, o, d, cached_inst, lo_o, lo_d, tmax, r);
+    }
+    if (inner_hits) {
+      const uint32_t slot = (uint32_t)(__ffs(inner_hits) - 1) ^ oct;
+      inner_hits &= inner_hits - 1;
+      if (inner_hits && sp < kWideStack) stack[sp++] = make_uint2(child_base, inner_hits | (imask << 8));
+      node = child_base + __popc(imask & ((1u << slot) - 1u));
+      continue;
+    }
+    if (sp == 0) break;
+    uint2 g = stack[--sp];
+    uint32_t hits = g.y & 0xffu;
+    const uint32_t gmask = g.y >> 8;
+    const uint32_t slot = (uint32_t)(__ffs(hits) - 1) ^ oct;
+    hits &= hits - 1;
+    if (hits) stack[sp++] = make_uint2(g.x, hits | (gmask << 8));
+    node = g.x + __popc(gmask & ((1u << slot) - 1u));
+  }
+  return r;
+}
+
+template <int WIDTH>
+NB_D TraceResult trace_closest_w(const DevScene &sc, V3 o, V3 d) {
+  if constexpr (WIDTH == 8)
+    return trace_closest8(sc, o, d);
+  else
+    return trace_closest2(sc, o, d);
+}
+
+NB_D TraceResult trace_closest(const DevScene &sc, V3 o, V3 d) {
+  return sc.width == 8 ? trace_closest8(sc, o, d) : trace_closest2(sc, o, d);
 }
 
 }  // namespace nb

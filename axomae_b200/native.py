@@ -58,7 +58,7 @@ class SceneDesc(C.Structure):
 
 
 class BvhOptions(C.Structure):
-    _fields_ = [("max_leaf_size", C.c_int32), ("bins", C.c_int32)]
+    _fields_ = [("max_leaf_size", C.c_int32), ("bins", C.c_int32), ("width", C.c_int32)]
 
 
 class Frame(C.Structure):
@@ -197,8 +197,8 @@ class Context:
         self._check(lib().nova_b200_upload_scene(self.h, C.byref(desc)))
         del keep
 
-    def build(self, max_leaf=0, bins=0):
-        self._check(lib().nova_b200_build_bvh(self.h, C.byref(BvhOptions(max_leaf, bins))))
+    def build(self, max_leaf=0, bins=0, width=0):
+        self._check(lib().nova_b200_build_bvh(self.h, C.byref(BvhOptions(max_leaf, bins, width))))
 
     def info(self) -> dict:
         vals = [C.c_uint64() for _ in range(5)]

@@ -167,7 +167,7 @@ def run_ours(args, rank, world, local_rank):
     ctx.upload(scene)
     upload_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    ctx.build()
+    ctx.build(width=args.bvh_width)
     build_s = time.perf_counter() - t0
     info = ctx.info()
     spp_total = spp * world
@@ -229,20 +229,35 @@ def run_ours(args, rank, world, local_rank):
         host_film = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
         e_steps = max(1, min(args.steps, 3))
         ectx = native.Context(local_rank)
+        eframe = native.make_frame(scene, W, H, spp, depth, seed=CFG["seed"], rr_start=CFG["rr_start"])
+
+        def e2e_step():
+            t0 = time.perf_counter()
+            ectx.upload(pinned)
+            t1 = time.perf_counter()
+            ectx.build(width=args.bvh_width)
+            t2 = time.perf_counter()
+            st = ectx.render(eframe, film_host=host_film.numpy())
+            t3 = time.perf_counter()
+            return st.traced, (t1 - t0, t2 - t1, t3 - t2)
+
+        e2e_step()  # untimed: the context's first render allocates its path queues and film
         e_traced = 0
+        stages = np.zeros(3)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e_steps):
-            ectx.upload(pinned)
-            ectx.build()
-            st = ectx.render(native.make_frame(scene, W, H, spp, depth, seed=CFG["seed"], rr_start=CFG["rr_start"]),
-                             film_host=host_film.numpy())
-            e_traced += st.traced
+            tr, st3 = e2e_step()
+            e_traced += tr
+            stages += st3
         ectx.synchronize()
         e_s = time.perf_counter() - t0
         ectx.close()
         e2e = {"value": e_traced / e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": scene_bytes(scene),
-               "d2h_bytes_per_step": W * H * 16, "steps": e_steps}
+               "d2h_bytes_per_step": W * H * 16, "steps": e_steps, "warmup": 1,
+               "upload_ms": 1e3 * stages[0] / e_steps, "build_ms": 1e3 * stages[1] / e_steps,
+               "render_ms": 1e3 * stages[2] / e_steps,
+               "timing": "host wall clock around upload (pinned H2D) + BVH build + render + film D2H"}
 
     if rank != 0:
         ctx.close()
@@ -273,7 +288,7 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded heightfield + log-normal env map)",
-            "config": {"workload": WORKLOAD, "spp_per_gpu": spp, "parallelism": "sample-range partition + NCCL film "
+            "config": {"workload": WORKLOAD, "spp_per_gpu": spp, "bvh_width": args.bvh_width or 2, "parallelism": "sample-range partition + NCCL film "
                        "all-reduce" if world > 1 else "single GPU", "l2": "working set larger than L2 (BVH %d nodes "
                        "x 64 B + %d tris x 48 B)" % (info["nodes"], info["triangles"])},
             "e2e": e2e, "roofline": roof,
@@ -321,6 +336,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="override the frame size (profiling)")
     ap.add_argument("--spp", type=int, help="override samples per pixel (profiling)")
+    ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8], help="BVH layout (0 = library default)")
     args = ap.parse_args()
     if args.frame:
         CFG["width"], CFG["height"] = args.frame

@@ -86,12 +86,18 @@ def _check_hits(ctx, torch, osc, o, d, max_mismatch_frac):
 
 
 @pytest.fixture(scope="module")
-def spheres(ctx, oracle):
+def spheres_scene(oracle):
     from axomae_b200 import scenes
     s = scenes.spheres_scene(96, 96)
-    ctx.upload(s)
-    ctx.build()
     return s, oracle.OracleScene(s)
+
+
+@pytest.fixture(params=[8, 2], ids=["bvh8", "bvh2"])
+def spheres(ctx, spheres_scene, request):
+    s, osc = spheres_scene
+    ctx.upload(s)
+    ctx.build(width=request.param)
+    return s, osc
 
 
 def test_primary_ray_hits(ctx, oracle, spheres, torch_cuda):
