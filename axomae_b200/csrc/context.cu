@@ -177,6 +177,13 @@ nova_b200_status nova_b200_create(nova_b200_ctx **out, int32_t device) {
     delete c;
     return NOVA_B200_RENDER_ENGINE_NOT_INITIALIZED;
   }
+  /* keep memory freed with cudaFreeAsync (BVH build scratch, upload staging) in the device pool
+   * instead of returning it to the driver at every synchronisation */
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   std::vector<uint32_t> sob;
   std::vector<float> ac;
   sobol_table(sob);
@@ -203,6 +210,13 @@ nova_b200_status nova_b200_destroy(nova_b200_ctx *c) {
   cudaFree(c->d_queue);
   cudaFree(c->d_radiance);
   cudaFree(c->d_film_out);
+  cudaFree(c->d_jobs);
+  cudaFree(c->d_wave);
+  if (c->h_jobs) cudaFreeHost(c->h_jobs);
+  if (c->h_wave) cudaFreeHost(c->h_wave);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  for (cudaEvent_t e : c->ev_wave)
+    if (e) cudaEventDestroy(e);
   if (c->h_counters) cudaFreeHost(c->h_counters);
   if (c->ev_begin) cudaEventDestroy(c->ev_begin);
   if (c->ev_end) cudaEventDestroy(c->ev_end);
@@ -443,6 +457,12 @@ nova_b200_status nova_b200_render(nova_b200_ctx *c, const nova_b200_frame *f, fl
                                   nova_b200_render_stats *stats) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;
   return nb_render(c, f, film_host, film_device, stats);
+}
+
+nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
+                                        float *const *films_host, float *const *films_device,
+                                        nova_b200_render_stats *stats) {
+  return nb_render_batch(ctxs, frames, n, films_host, films_device, stats);
 }
 
 nova_b200_status nova_b200_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,

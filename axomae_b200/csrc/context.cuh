@@ -48,6 +48,13 @@ struct nova_b200_ctx {
   unsigned *h_counters = nullptr; /* pinned */
   float *d_film_out = nullptr;
   size_t film_out_cap = 0;
+
+  /* device-driven wave loop (integrator.cu) */
+  void *d_jobs = nullptr, *h_jobs = nullptr; /* job table, device copy and pinned staging */
+  void *d_wave = nullptr, *h_wave = nullptr; /* wave counters, device copy and pinned read-back */
+  cudaEvent_t ev_wave[24] = {};
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_width = 0;
 };
 
 namespace nbctx {
@@ -79,6 +86,8 @@ inline nova_b200_status cuda_fail(nova_b200_ctx *c, cudaError_t e, const char *w
 /* Defined in integrator.cu / bake.cu, called by the C-ABI entry points in context.cu. */
 nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *film_host, float *film_device,
                            nova_b200_render_stats *stats);
+nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
+                                 float *const *films_host, float *const *films_device, nova_b200_render_stats *stats);
 nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,
                           float *u, float *v);
 nova_b200_status nb_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *idx, const uint32_t *dim, uint32_t seed,

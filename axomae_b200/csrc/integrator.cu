@@ -1,25 +1,41 @@
 /* Wavefront path tracer: the reference's PathIntegrator::Li (integrator/Integrator.cpp:60-99) as
- * four sm_100a kernels over a path queue in HBM.
+ * sm_100a kernels over a path queue in HBM, for one frame or a batch of frames of different scenes.
  *
- *   k_raygen   camera rays for new paths (Integrator.h:66-85 with the OptiX raygen's sample index
- *              (x * H + y) * spp + s, integrator_optix.cu:43; Sobol dimensions 0 and 1 jitter NDC)
+ *   k_refill   fills free queue slots with camera rays of new paths (Integrator.h:66-85 with the
+ *              OptiX raygen's sample index (x * H + y) * spp + s, integrator_optix.cu:43; Sobol
+ *              dimensions 0 and 1 jitter NDC)
  *   k_trace    closest hit per queued ray (traverse.cuh); a miss finishes its path with the
  *              environment lookup, hits go to a compact hit list
- *   k_shade    per hit: principled scatter (Sobol dimensions 2 + 4b .. 5 + 4b at
- *              bounce b), throughput update, spawned ray appended to the next queue with
- *              warp-aggregated atomics; after the last allowed scatter the spawned direction looks
- *              up the environment directly (the reference traces that ray but discards the hit,
+ *   k_shade    per hit: principled scatter (Sobol dimensions 2 + 4b .. 5 + 4b at bounce b),
+ *              throughput update, spawned ray appended to the next queue with warp-aggregated
+ *              atomics; after the last allowed scatter the spawned direction looks up the
+ *              environment directly (the reference traces that ray but discards the hit,
  *              Integrator.cpp:94-98)
- *   k_resolve  per pixel, adds the per-path radiance of this call's samples to the running sum in
+ *   k_wave_end advances the device-side wave counters
+ *   k_resolve  per pixel, adds the per-path radiance of the call's samples to the running sum in
  *              sample order and writes sum / samples (writeFramebuffer, api/engine.cpp:351-363)
+ *
+ * Jobs: every path carries its job index (a frame of one context: scene, BVH, camera, sample
+ * range) and every kernel reads the job table, so a batch of frames of different scenes runs as
+ * one wavefront.  A single render is a batch of one.  The per-path arithmetic does not depend on
+ * the batch, and each pixel's samples are added in sample order, so a frame rendered in a batch
+ * equals the same frame rendered alone, bit for bit.
+ *
+ * Wave loop: the counters (active paths, next path, hits, survivors) live on the device and the
+ * kernels read device-resident counts, so the host never waits between waves; it enqueues four
+ * waves at a time and checks the device's "done" flag after each group.  A chunk of one frame
+ * passes its job by value as a kernel parameter and launches directly; a batch chunk reads the job
+ * table from device memory and replays the four waves from a CUDA graph captured once (event
+ * record nodes around each trace and shade kernel time them).
  *
  * The recursive estimator e_0 + c_0 (e_1 + c_1 (... env)) is evaluated forward as
  * sum_k beta_k e_k + beta_K env with beta_k = c_0 ... c_{k-1}; a path whose result is not finite
- * contributes 0 (DENAN, Integrator.cpp:92).  Path state: origin + path id, direction + bounce,
- * throughput (3 x 16 B); hits 16 B + 4 B slot; per-path radiance 16 B, written once.
+ * contributes 0 (DENAN, Integrator.cpp:92).  Path state: origin + path id, direction + bounce +
+ * job, throughput (3 x 16 B); hits 16 B + 4 B slot; per-path radiance 16 B, written once.
  */
 #include <algorithm>
 #include <cfloat>
+#include <vector>
 
 #include "context.cuh"
 #include "shading.cuh"
@@ -33,12 +49,14 @@ constexpr uint32_t kQueueCap = 1u << 22;
 constexpr size_t kRadianceCapBytes = 4ull << 30;
 constexpr unsigned kRRDimBase = 200; /* Russian roulette decisions use Sobol dimension 200 + bounce */
 constexpr int kMaxDepth = 48;        /* 2 + 4 (depth + 1) Sobol dimensions must stay below 200 */
+constexpr int kWavesPerGraph = 4;    /* even: the queues end each graph launch where they started */
+constexpr uint32_t kMaxJobs = 4096;
 
 struct RenderParams {
   int32_t W, H;
-  uint32_t NP;       /* pixels */
-  uint32_t count;    /* samples traced by this chunk */
-  uint32_t begin;    /* first sample of this chunk */
+  uint32_t NP;    /* pixels */
+  uint32_t count; /* samples traced for this job in the current chunk */
+  uint32_t begin; /* first of those samples */
   uint32_t spp_total;
   int32_t max_depth;
   uint32_t seed;
@@ -46,9 +64,54 @@ struct RenderParams {
   float inv_P[16], inv_V[16];
 };
 
+struct Job {
+  DevScene sc;
+  RenderParams rp;
+  uint32_t path_begin; /* first path id of this job in the chunk (radiance slot of its first path) */
+  uint32_t n_paths;
+};
+
+struct WaveCounters {
+  uint32_t n_active; /* rays waiting in the input queue */
+  uint32_t next;     /* next path id to start */
+  uint32_t total;    /* paths in the chunk */
+  uint32_t cap;      /* queue capacity */
+  uint32_t hit_count, out_count;
+  uint32_t done;
+  uint32_t waves; /* waves that did work */
+  uint32_t n_jobs;
+  unsigned long long traced;
+};
+
 struct Queue {
   float4 *o, *d, *beta;
 };
+
+__device__ __forceinline__ uint32_t wave_new(const WaveCounters &wc) {
+  return min(wc.cap - wc.n_active, wc.total - wc.next);
+}
+
+__device__ __forceinline__ uint32_t job_of_path(const Job *jobs, uint32_t n_jobs, uint32_t g) {
+  uint32_t lo = 0, hi = n_jobs; /* last job with path_begin <= g */
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].path_begin <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+/* A chunk of one frame passes its job by value (kernel parameter space); a batch chunk reads the
+ * job table in global memory. */
+template <bool SINGLE>
+__device__ __forceinline__ const Job &job_at(const Job &j0, const Job *jobs, uint32_t k) {
+  if constexpr (SINGLE)
+    return j0;
+  else
+    return jobs[k];
+}
 
 __device__ __forceinline__ uint32_t sample_index(const RenderParams &rp, uint32_t p) {
   const uint32_t s_local = p / rp.NP, pix = p - s_local * rp.NP;
@@ -56,31 +119,40 @@ __device__ __forceinline__ uint32_t sample_index(const RenderParams &rp, uint32_
   return ((uint32_t)x * (uint32_t)rp.H + y) * rp.spp_total + (rp.begin + s_local);
 }
 
-__global__ void __launch_bounds__(256) k_raygen(Queue q, uint32_t off, uint64_t first, uint32_t n_new, RenderParams rp,
-                                                DevScene sc, float4 *L) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_new) return;
-  const uint32_t p = (uint32_t)(first + i);
-  const uint32_t s_local = p / rp.NP, pix = p - s_local * rp.NP;
-  const int y = (int)(pix / (uint32_t)rp.W), x = (int)(pix - (uint32_t)y * (uint32_t)rp.W);
-  const uint32_t index = ((uint32_t)x * (uint32_t)rp.H + (uint32_t)y) * rp.spp_total + (rp.begin + s_local);
-  const float r0 = sobol_sample(sc.sobol_dv, index, 0, rp.seed);
-  const float r1 = sobol_sample(sc.sobol_dv, index, 1, rp.seed);
-  const float dx = r0 * 0.0005f, dy = r1 * 0.0005f; /* RAND_DX / RAND_DY, Integrator.h:54-55 */
-  const int ys = rp.H - y;                          /* screen row, Integrator.h:84 */
-  const float ndc_x = (float)(2 * x - rp.W) / (float)rp.W;
-  const float ndc_y = (float)(rp.H - 2 * ys) / (float)rp.H;
-  const float nx = ndc_x + dx, ny = ndc_y + dy;
-  const M4 iP = m4_load(rp.inv_P), iV = m4_load(rp.inv_V);
-  V4 o = mul(iP, V4{nx, ny, -1.f, 1.f});
-  o = o / o.w;
-  o = mul(iV, V4{o.x, o.y, o.z, 1.f});
-  V4 d = mul(iP, V4{nx, ny, -1.f, 0.f});
-  d = normalize(mul(iV, V4{d.x, d.y, -1.f, 0.f}));
-  q.o[off + i] = make_float4(o.x, o.y, o.z, __uint_as_float(p));
-  q.d[off + i] = make_float4(d.x, d.y, d.z, __int_as_float(0));
-  q.beta[off + i] = make_float4(1.f, 1.f, 1.f, 0.f);
-  if (sc.has_emissive) L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+template <bool SINGLE>
+__global__ void __launch_bounds__(256) k_refill(Queue q, const WaveCounters *wcp, const Job *jobs, const Job j0,
+                                                float4 *L) {
+  const WaveCounters wc = *wcp;
+  const uint32_t n_jobs = wc.n_jobs;
+  const uint32_t n_new = wave_new(wc);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
+    const uint32_t g = wc.next + i;
+    const uint32_t job = SINGLE ? 0u : job_of_path(jobs, n_jobs, g);
+    const Job &J = job_at<SINGLE>(j0, jobs, job);
+    const RenderParams &rp = J.rp;
+    const uint32_t p = g - J.path_begin;
+    const uint32_t s_local = p / rp.NP, pix = p - s_local * rp.NP;
+    const int y = (int)(pix / (uint32_t)rp.W), x = (int)(pix - (uint32_t)y * (uint32_t)rp.W);
+    const uint32_t index = ((uint32_t)x * (uint32_t)rp.H + (uint32_t)y) * rp.spp_total + (rp.begin + s_local);
+    const float r0 = sobol_sample(J.sc.sobol_dv, index, 0, rp.seed);
+    const float r1 = sobol_sample(J.sc.sobol_dv, index, 1, rp.seed);
+    const float dx = r0 * 0.0005f, dy = r1 * 0.0005f; /* RAND_DX / RAND_DY, Integrator.h:54-55 */
+    const int ys = rp.H - y;                          /* screen row, Integrator.h:84 */
+    const float ndc_x = (float)(2 * x - rp.W) / (float)rp.W;
+    const float ndc_y = (float)(rp.H - 2 * ys) / (float)rp.H;
+    const float nx = ndc_x + dx, ny = ndc_y + dy;
+    const M4 iP = m4_load(rp.inv_P), iV = m4_load(rp.inv_V);
+    V4 o = mul(iP, V4{nx, ny, -1.f, 1.f});
+    o = o / o.w;
+    o = mul(iV, V4{o.x, o.y, o.z, 1.f});
+    V4 d = mul(iP, V4{nx, ny, -1.f, 0.f});
+    d = normalize(mul(iV, V4{d.x, d.y, -1.f, 0.f}));
+    const uint32_t slot = wc.n_active + i;
+    q.o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(g));
+    q.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(job << 8));
+    q.beta[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+    if (J.sc.has_emissive) L[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
 }
 
 __device__ __forceinline__ float4 finite_or_zero(V3 L, float alpha) {
@@ -89,79 +161,95 @@ __device__ __forceinline__ float4 finite_or_zero(V3 L, float alpha) {
 }
 
 /* Writes a finished path's radiance (adds the emission gathered so far when the scene has any). */
-__device__ __forceinline__ void finish_path(const DevScene &sc, float4 *L, uint32_t p, float4 result) {
+__device__ __forceinline__ void finish_path(const DevScene &sc, float4 *L, uint32_t g, float4 result) {
   if (sc.has_emissive) {
-    const float4 acc = L[p];
+    const float4 acc = L[g];
     float4 r = make_float4(acc.x + result.x, acc.y + result.y, acc.z + result.z, result.w);
     if (!isfinite(r.x) || !isfinite(r.y) || !isfinite(r.z)) r = make_float4(0.f, 0.f, 0.f, 0.f);
-    L[p] = r;
+    L[g] = r;
   } else {
-    L[p] = result;
+    L[g] = result;
   }
+}
+
+/* Warp-aggregated append: returns the slot of every lane with `flag` set. */
+__device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned m = __ballot_sync(0xffffffffu, flag);
+  unsigned base = 0;
+  if (m) {
+    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(counter, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+  }
+  return base + __popc(m & ((1u << lane) - 1u));
 }
 
 /* Closest hit of every queued ray.  A miss finishes its path here (environment lookup,
- * Integrator.cpp:94-98); hits are appended to a compact hit list (warp-aggregated atomics) so
- * the shading kernel only runs on rays that hit. */
-template <int WIDTH>
-__global__ void __launch_bounds__(128) k_trace(Queue q, uint32_t n, float4 *hits, uint32_t *hit_slot,
-                                               unsigned *hit_count, float4 *L, DevScene sc) {
+ * Integrator.cpp:94-98); hits are appended to a compact hit list so the shading kernel only runs
+ * on rays that hit. */
+template <int WIDTH, bool SINGLE>
+__global__ void __launch_bounds__(128) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
+                                               const Job *jobs, const Job j0) {
+  const uint32_t n = wcp->n_active + wave_new(*wcp);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool is_hit = false;
-  TraceResult r{-1, 0.f, 0.f, 0.f};
-  if (i < n) {
-    const float4 o = q.o[i], d = q.d[i];
-    r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
-    if (r.prim < 0) {
-      const float4 b4 = q.beta[i];
-      const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
-      finish_path(sc, L, __float_as_uint(o.w),
-                  finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z}, (float)__float_as_int(d.w) + e.w));
-    } else {
-      is_hit = true;
+  if ((i & ~31u) >= n) return; /* whole warps leave together (the append below is a warp ballot) */
+  {
+    bool is_hit = false;
+    TraceResult r{-1, 0.f, 0.f, 0.f};
+    if (i < n) {
+      const float4 o = q.o[i], d = q.d[i];
+      const DevScene &sc = job_at<SINGLE>(j0, jobs, __float_as_uint(d.w) >> 8).sc;
+      r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
+      if (r.prim < 0) {
+        const float4 b4 = q.beta[i];
+        const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
+        finish_path(sc, L, __float_as_uint(o.w),
+                    finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z},
+                                   (float)(__float_as_uint(d.w) & 0xffu) + e.w));
+      } else {
+        is_hit = true;
+      }
     }
-  }
-  const unsigned lane = threadIdx.x & 31u;
-  const unsigned m = __ballot_sync(0xffffffffu, is_hit);
-  unsigned base = 0;
-  if (m) {
-    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(hit_count, (unsigned)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-  }
-  if (is_hit) {
-    const unsigned slot = base + __popc(m & ((1u << lane) - 1u));
-    hits[slot] = make_float4(r.t, r.u, r.v, __int_as_float(r.prim));
-    hit_slot[slot] = i;
+    const unsigned slot = warp_append(is_hit, &wcp->hit_count);
+    if (is_hit) {
+      hits[slot] = make_float4(r.t, r.u, r.v, __int_as_float(r.prim));
+      hit_slot[slot] = i;
+    }
   }
 }
 
-__global__ void __launch_bounds__(128) k_shade(Queue in, const float4 *hits, const uint32_t *hit_slot,
-                                               const unsigned *hit_count, Queue out, unsigned *out_count, float4 *L,
-                                               RenderParams rp, DevScene sc) {
+template <bool SINGLE>
+__global__ void __launch_bounds__(128) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
+                                               const uint32_t *hit_slot, float4 *L, const Job *jobs, const Job j0) {
+  const uint32_t n = wcp->hit_count;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = i < *hit_count;
-  bool enq = false;
-  float4 no{}, nd{}, nbeta{};
-  if (live) {
-    const uint32_t slot_in = hit_slot[i];
-    const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
-    const uint32_t p = __float_as_uint(o4.w);
-    const int bounce = __float_as_int(d4.w);
-    const uint32_t index = sample_index(rp, p);
-    const V3 ro{o4.x, o4.y, o4.z}, rd{d4.x, d4.y, d4.z};
-    V3 beta{b4.x, b4.y, b4.z};
-    const int prim = __float_as_int(h.w);
-    bool done = false;
-    float4 result = make_float4(0.f, 0.f, 0.f, 0.f);
-    {
+  if ((i & ~31u) >= n) return;
+  {
+    bool enq = false;
+    float4 no{}, nd{}, nbeta{};
+    if (i < n) {
+      const uint32_t slot_in = hit_slot[i];
+      const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
+      const uint32_t g = __float_as_uint(o4.w);
+      const uint32_t tag = __float_as_uint(d4.w);
+      const int bounce = (int)(tag & 0xffu);
+      const Job &J = job_at<SINGLE>(j0, jobs, tag >> 8);
+      const DevScene &sc = J.sc;
+      const RenderParams &rp = J.rp;
+      const uint32_t index = sample_index(rp, g - J.path_begin);
+      const V3 ro{o4.x, o4.y, o4.z}, rd{d4.x, d4.y, d4.z};
+      V3 beta{b4.x, b4.y, b4.z};
+      const int prim = __float_as_int(h.w);
+      bool done = false;
+      float4 result = make_float4(0.f, 0.f, 0.f, 0.f);
       const uint32_t inst = __ldg(sc.prim_inst + prim);
       const DevInstance &I = sc.instances[inst];
       const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)prim - I.prim_offset, h.x, h.y, h.z);
       const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed);
       if (sc.has_emissive && any_nonzero(sr.emissive)) {
         const V3 em = beta * sr.emissive;
-        float4 acc = L[p];
-        L[p] = make_float4(acc.x + em.x, acc.y + em.y, acc.z + em.z, acc.w);
+        const float4 acc = L[g];
+        L[g] = make_float4(acc.x + em.x, acc.y + em.y, acc.z + em.z, acc.w);
       }
       if (!sr.valid) {
         result = make_float4(0.f, 0.f, 0.f, (float)bounce);
@@ -193,27 +281,34 @@ __global__ void __launch_bounds__(128) k_shade(Queue in, const float4 *hits, con
           } else {
             enq = true;
             no = make_float4(no3.x, no3.y, no3.z, o4.w);
-            nd = make_float4(nd3.x, nd3.y, nd3.z, __int_as_float(bounce + 1));
+            nd = make_float4(nd3.x, nd3.y, nd3.z, __uint_as_float(tag + 1u));
             nbeta = make_float4(beta.x, beta.y, beta.z, 0.f);
           }
         }
       }
+      if (done) finish_path(sc, L, g, result);
     }
-    if (done) finish_path(sc, L, p, result);
+    const unsigned slot = warp_append(enq, &wcp->out_count);
+    if (enq) {
+      out.o[slot] = no;
+      out.d[slot] = nd;
+      out.beta[slot] = nbeta;
+    }
   }
-  const unsigned lane = threadIdx.x & 31u;
-  const unsigned m = __ballot_sync(0xffffffffu, enq);
-  unsigned base = 0;
-  if (m) {
-    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(out_count, (unsigned)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+}
+
+__global__ void k_wave_end(WaveCounters *wc) {
+  const uint32_t n_new = wave_new(*wc);
+  const uint32_t n = wc->n_active + n_new;
+  if (n) {
+    wc->waves++;
+    wc->traced += n;
   }
-  if (enq) {
-    const unsigned slot = base + __popc(m & ((1u << lane) - 1u));
-    out.o[slot] = no;
-    out.d[slot] = nd;
-    out.beta[slot] = nbeta;
-  }
+  wc->next += n_new;
+  wc->n_active = wc->out_count;
+  wc->out_count = 0;
+  wc->hit_count = 0;
+  wc->done = (wc->n_active == 0 && wc->next == wc->total) ? 1u : 0u;
 }
 
 __global__ void k_resolve(const float4 *L, uint32_t NP, uint32_t count, float4 *acc, float denom, float *out, int W,
@@ -251,24 +346,9 @@ __global__ void k_sobol_api(const uint32_t *dv, uint64_t n, const uint32_t *idx,
   out[i] = dm < (uint32_t)kSobolDims ? sobol_sample(dv, idx[i], dm, seed) : __int_as_float(0x7fc00000);
 }
 
-nova_b200_status ensure_buffers(nova_b200_ctx *c, uint32_t cap, size_t radiance, int W, int H) {
-  if (c->queue_cap < cap) {
-    cudaFree(c->d_queue);
-    c->d_queue = nullptr;
-    c->queue_cap = 0;
-    c->queue_bytes = 0;
-    const size_t bytes = (size_t)cap * (16 * 7 + 4);
-    NB_CUDA(c, cudaMalloc(&c->d_queue, bytes), "cudaMalloc(queue)");
-    c->queue_cap = cap;
-    c->queue_bytes = bytes;
-  }
-  if (c->radiance_cap < radiance) {
-    cudaFree(c->d_radiance);
-    c->d_radiance = nullptr;
-    c->radiance_cap = 0;
-    NB_CUDA(c, cudaMalloc(&c->d_radiance, radiance * sizeof(float4)), "cudaMalloc(radiance)");
-    c->radiance_cap = radiance;
-  }
+/* ------------------------------------------------------------------ host side */
+
+nova_b200_status ensure_film(nova_b200_ctx *c, int W, int H) {
   const size_t npx = (size_t)W * H;
   if (c->film_w != W || c->film_h != H || !c->d_film_acc) {
     cudaFree(c->d_film_acc);
@@ -288,10 +368,130 @@ nova_b200_status ensure_buffers(nova_b200_ctx *c, uint32_t cap, size_t radiance,
   return NOVA_B200_SUCCESS;
 }
 
-}  // namespace
+nova_b200_status ensure_wave_buffers(nova_b200_ctx *c, uint32_t cap, size_t radiance) {
+  bool changed = false;
+  if (c->queue_cap < cap) {
+    cudaFree(c->d_queue);
+    c->d_queue = nullptr;
+    c->queue_cap = 0;
+    c->queue_bytes = 0;
+    const size_t bytes = (size_t)cap * (16 * 7 + 4);
+    NB_CUDA(c, cudaMalloc(&c->d_queue, bytes), "cudaMalloc(queue)");
+    c->queue_cap = cap;
+    c->queue_bytes = bytes;
+    changed = true;
+  }
+  if (c->radiance_cap < radiance) {
+    cudaFree(c->d_radiance);
+    c->d_radiance = nullptr;
+    c->radiance_cap = 0;
+    NB_CUDA(c, cudaMalloc(&c->d_radiance, radiance * sizeof(float4)), "cudaMalloc(radiance)");
+    c->radiance_cap = radiance;
+    changed = true;
+  }
+  if (!c->d_jobs) {
+    NB_CUDA(c, cudaMalloc(&c->d_jobs, sizeof(Job) * kMaxJobs), "cudaMalloc(jobs)");
+    NB_CUDA(c, cudaMalloc(&c->d_wave, sizeof(WaveCounters)), "cudaMalloc(wave counters)");
+    NB_CUDA(c, cudaMallocHost(&c->h_wave, sizeof(WaveCounters)), "cudaMallocHost(wave counters)");
+    NB_CUDA(c, cudaMallocHost(&c->h_jobs, sizeof(Job) * kMaxJobs), "cudaMallocHost(jobs)");
+    for (int k = 0; k < 3 * kWavesPerGraph; k++) NB_CUDA(c, cudaEventCreate(&c->ev_wave[k]), "cudaEventCreate");
+    changed = true;
+  }
+  if (changed && c->graph_exec) {
+    cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+  }
+  return NOVA_B200_SUCCESS;
+}
 
-nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *film_host, float *film_device,
-                           nova_b200_render_stats *stats) {
+struct WaveBuffers {
+  Queue qa, qb;
+  float4 *hits;
+  uint32_t *hit_slot;
+  WaveCounters *wc;
+  const Job *jobs;
+};
+
+WaveBuffers wave_buffers(nova_b200_ctx *c) {
+  const uint32_t cap = c->queue_cap;
+  float4 *base = static_cast<float4 *>(c->d_queue);
+  WaveBuffers b;
+  b.qa = Queue{base, base + cap, base + 2 * (size_t)cap};
+  b.qb = Queue{base + 3 * (size_t)cap, base + 4 * (size_t)cap, base + 5 * (size_t)cap};
+  b.hits = base + 6 * (size_t)cap;
+  b.hit_slot = reinterpret_cast<uint32_t *>(base + 7 * (size_t)cap);
+  b.wc = static_cast<WaveCounters *>(c->d_wave);
+  b.jobs = static_cast<const Job *>(c->d_jobs);
+  return b;
+}
+
+/* Enqueues kWavesPerGraph waves (queues alternating A -> B -> A ...), an event record around each
+ * trace and shade kernel (`external` while capturing, so they become graph event-record nodes) and
+ * the read-back of the counters into pinned memory. */
+template <bool SINGLE, int WIDTH>
+void enqueue_waves(nova_b200_ctx *c, const Job &j0, bool external) {
+  const WaveBuffers b = wave_buffers(c);
+  int dev_sms = 148, occ_r = 1;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, k_refill<SINGLE>, 256, 0);
+  /* trace and shade: one ray per thread over the whole queue capacity, so the hardware block
+   * scheduler balances rays of very different cost; blocks past the live count exit at once */
+  const unsigned g_trace = (c->queue_cap + 127) / 128, g_shade = (c->queue_cap + 127) / 128;
+  const unsigned g_refill = (unsigned)(dev_sms * std::max(1, occ_r) * 2);
+  const unsigned flags = external ? cudaEventRecordExternal : cudaEventRecordDefault;
+  for (int w = 0; w < kWavesPerGraph; w++) {
+    const Queue &in = (w & 1) ? b.qb : b.qa;
+    const Queue &out = (w & 1) ? b.qa : b.qb;
+    k_refill<SINGLE><<<g_refill, 256, 0, c->stream>>>(in, b.wc, b.jobs, j0, c->d_radiance);
+    cudaEventRecordWithFlags(c->ev_wave[3 * w + 0], c->stream, flags);
+    k_trace<WIDTH, SINGLE><<<g_trace, 128, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, b.jobs, j0);
+    cudaEventRecordWithFlags(c->ev_wave[3 * w + 1], c->stream, flags);
+    k_shade<SINGLE><<<g_shade, 128, 0, c->stream>>>(in, out, b.wc, b.hits, b.hit_slot, c->d_radiance, b.jobs, j0);
+    cudaEventRecordWithFlags(c->ev_wave[3 * w + 2], c->stream, flags);
+    k_wave_end<<<1, 1, 0, c->stream>>>(b.wc);
+  }
+  cudaMemcpyAsync(c->h_wave, b.wc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, c->stream);
+}
+
+/* Batch chunks: the waves are captured once into a CUDA graph (their arguments are buffer
+ * pointers only; the job table and counters are read from device memory). */
+nova_b200_status capture_graph(nova_b200_ctx *c, int width) {
+  if (c->graph_exec && c->graph_width == width) return NOVA_B200_SUCCESS;
+  if (c->graph_exec) {
+    cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  NB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "capture");
+  const Job unused{};
+  if (width == 8)
+    enqueue_waves<false, 8>(c, unused, true);
+  else
+    enqueue_waves<false, 2>(c, unused, true);
+  const cudaError_t e_launch = cudaGetLastError();
+  const cudaError_t e_end = cudaStreamEndCapture(c->stream, &graph);
+  if (e_launch != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return nbctx::cuda_fail(c, e_launch, "capture kernels");
+  }
+  if (e_end != cudaSuccess) return nbctx::cuda_fail(c, e_end, "cudaStreamEndCapture");
+  const cudaError_t e_inst = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e_inst != cudaSuccess) {
+    c->graph_exec = nullptr;
+    return nbctx::cuda_fail(c, e_inst, "cudaGraphInstantiate");
+  }
+  c->graph_width = width;
+  return NOVA_B200_SUCCESS;
+}
+
+struct Piece {
+  nova_b200_ctx *ctx; /* the job's context: scene, BVH, film */
+  const nova_b200_frame *f;
+  uint32_t begin, count;
+};
+
+nova_b200_status validate_frame(nova_b200_ctx *c, const nova_b200_frame *f) {
   using namespace nbctx;
   if (!f) return fail(c, NOVA_B200_INVALID_ARGUMENT, "frame is null%s");
   if (!c->bvh_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "build the acceleration structure first%s");
@@ -300,101 +500,197 @@ nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *fi
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "invalid frame size or sample range%s");
   if (f->max_depth < 0 || f->max_depth > kMaxDepth)
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "max_depth must be in 0..48 (Sobol dimensions)%s");
-  const uint64_t NP = (uint64_t)f->width * f->height;
-  if (NP * (uint64_t)f->spp_total >= (1ull << 32))
+  if ((uint64_t)f->width * f->height * (uint64_t)f->spp_total >= (1ull << 32))
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "width * height * spp must stay below 2^32 (Sobol index)%s");
-  cudaSetDevice(c->device);
-  const size_t cap_entries = kRadianceCapBytes / sizeof(float4);
-  const uint32_t chunk_samples = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(f->sample_count, cap_entries / NP));
-  const uint64_t max_paths = NP * chunk_samples;
-  const uint32_t cap = (uint32_t)std::min<uint64_t>(kQueueCap, max_paths);
-  nova_b200_status st = ensure_buffers(c, cap, max_paths, f->width, f->height);
-  if (st != NOVA_B200_SUCCESS) return st;
-  if (f->reset) {
-    NB_CUDA(c, cudaMemsetAsync(c->d_film_acc, 0, NP * sizeof(float4), c->stream), "memset(film)");
-    c->film_samples = 0;
-  }
-  RenderParams rp;
-  rp.W = f->width, rp.H = f->height, rp.NP = (uint32_t)NP;
-  rp.spp_total = (uint32_t)f->spp_total;
-  rp.max_depth = f->max_depth;
-  rp.seed = f->seed;
-  rp.rr_start = f->rr_start;
-  std::copy(f->inv_P, f->inv_P + 16, rp.inv_P);
-  std::copy(f->inv_V, f->inv_V + 16, rp.inv_V);
-  float4 *base = static_cast<float4 *>(c->d_queue);
-  Queue qa{base, base + cap, base + 2 * (size_t)cap}, qb{base + 3 * (size_t)cap, base + 4 * (size_t)cap,
-                                                         base + 5 * (size_t)cap};
-  float4 *hits = base + 6 * (size_t)cap;
-  uint32_t *hit_slot = reinterpret_cast<uint32_t *>(base + 7 * (size_t)cap);
-  nova_b200_render_stats s{};
-  float t_trace = 0.f, t_shade = 0.f;
-  NB_CUDA(c, cudaEventRecord(c->ev_begin, c->stream), "event");
-  for (uint32_t done_s = 0; done_s < (uint32_t)f->sample_count; done_s += chunk_samples) {
-    const uint32_t cs = std::min<uint32_t>(chunk_samples, (uint32_t)f->sample_count - done_s);
-    rp.begin = (uint32_t)f->sample_begin + done_s;
-    rp.count = cs;
-    const uint64_t paths = NP * cs;
-    uint64_t next = 0;
-    uint32_t n_active = 0;
-    while (next < paths || n_active > 0) {
-      const uint32_t n_new = (uint32_t)std::min<uint64_t>(cap - n_active, paths - next);
-      if (n_new) {
-        k_raygen<<<(n_new + 255) / 256, 256, 0, c->stream>>>(qa, n_active, next, n_new, rp, c->scene, c->d_radiance);
-        s.kernels++;
-      }
-      const uint32_t n = n_active + n_new;
-      next += n_new;
-      s.traced += n;
-      s.segments += n;
-      NB_CUDA(c, cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned), c->stream), "memset");
-      NB_CUDA(c, cudaEventRecord(c->ev_a, c->stream), "event");
-      if (c->scene.width == 8)
-        k_trace<8><<<(n + 127) / 128, 128, 0, c->stream>>>(qa, n, hits, hit_slot, c->d_counters + 1, c->d_radiance,
-                                                          c->scene);
-      else
-        k_trace<2><<<(n + 127) / 128, 128, 0, c->stream>>>(qa, n, hits, hit_slot, c->d_counters + 1, c->d_radiance,
-                                                          c->scene);
-      NB_CUDA(c, cudaEventRecord(c->ev_b, c->stream), "event");
-      k_shade<<<(n + 127) / 128, 128, 0, c->stream>>>(qa, hits, hit_slot, c->d_counters + 1, qb, c->d_counters,
-                                                       c->d_radiance, rp, c->scene);
-      NB_CUDA(c, cudaEventRecord(c->ev_end, c->stream), "event");
-      s.kernels += 2;
-      NB_CUDA(c, cudaMemcpyAsync(c->h_counters, c->d_counters, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream),
-              "readback");
-      NB_CUDA(c, cudaStreamSynchronize(c->stream), "wave");
-      float a = 0.f, b = 0.f;
-      cudaEventElapsedTime(&a, c->ev_a, c->ev_b);
-      cudaEventElapsedTime(&b, c->ev_b, c->ev_end);
-      t_trace += a;
-      t_shade += b;
-      n_active = c->h_counters[0];
-      std::swap(qa, qb);
-      s.waves++;
-    }
-    c->film_samples += cs;
-    k_resolve<<<(uint32_t)((NP + 255) / 256), 256, 0, c->stream>>>(c->d_radiance, (uint32_t)NP, cs, c->d_film_acc,
-                                                                   (float)c->film_samples, c->d_film_out, f->width,
-                                                                   f->height, f->vertical_invert);
-    s.kernels++;
-    s.paths += paths;
-  }
-  NB_CUDA(c, cudaGetLastError(), "render kernels");
-  NB_CUDA(c, cudaEventRecord(c->ev_end, c->stream), "event");
-  if (film_device)
-    NB_CUDA(c, cudaMemcpyAsync(film_device, c->d_film_out, NP * 4 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream),
-            "copy film");
-  if (film_host)
-    NB_CUDA(c, cudaMemcpyAsync(film_host, c->d_film_out, NP * 4 * sizeof(float), cudaMemcpyDeviceToHost, c->stream),
-            "copy film");
-  NB_CUDA(c, cudaStreamSynchronize(c->stream), "render");
-  float total = 0.f;
-  cudaEventElapsedTime(&total, c->ev_begin, c->ev_end);
-  s.device_ms = total;
-  s.trace_ms = t_trace;
-  s.shade_ms = t_shade;
-  if (stats) *stats = s;
   return NOVA_B200_SUCCESS;
+}
+
+/* Renders frames (one per job) as one wavefront on the executing context `x`.  Jobs are cut into
+ * chunks whose per-path radiance fits the radiance buffer; a job's samples stay in order. */
+nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *> &ctxs,
+                             const std::vector<const nova_b200_frame *> &frames, float *const *films_host,
+                             float *const *films_device, nova_b200_render_stats *stats) {
+  using namespace nbctx;
+  const size_t nj = ctxs.size();
+  const int width = ctxs[0]->bvh_width;
+  uint64_t max_np = 0, total = 0;
+  for (size_t j = 0; j < nj; j++) {
+    if (ctxs[j]->device != x->device)
+      return fail(x, NOVA_B200_INVALID_ARGUMENT, "all contexts of a batch must use the same device%s");
+    if (ctxs[j]->bvh_width != width)
+      return fail(x, NOVA_B200_INVALID_ARGUMENT, "all scenes of a batch must use the same BVH width%s");
+    const uint64_t np = (uint64_t)frames[j]->width * frames[j]->height;
+    max_np = std::max(max_np, np);
+    total += np * (uint64_t)frames[j]->sample_count;
+  }
+  const uint64_t cap_entries = kRadianceCapBytes / sizeof(float4);
+  const uint64_t radiance = std::max<uint64_t>(max_np, std::min<uint64_t>(total, cap_entries));
+  const uint32_t cap = (uint32_t)std::min<uint64_t>(kQueueCap, std::max<uint64_t>(radiance, 1024));
+  nova_b200_status st = ensure_wave_buffers(x, cap, radiance);
+  if (st != NOVA_B200_SUCCESS) return st;
+  for (size_t j = 0; j < nj; j++) {
+    nova_b200_ctx *c = ctxs[j];
+    if ((st = ensure_film(c, frames[j]->width, frames[j]->height)) != NOVA_B200_SUCCESS) return st;
+    if (frames[j]->reset) {
+      NB_CUDA(x, cudaMemsetAsync(c->d_film_acc, 0, (size_t)frames[j]->width * frames[j]->height * sizeof(float4),
+                                 x->stream),
+              "memset(film)");
+      c->film_samples = 0;
+    }
+  }
+  /* scene uploads and film clears of other contexts ran on their own streams */
+  for (size_t j = 0; j < nj; j++)
+    if (ctxs[j] != x) NB_CUDA(x, cudaStreamSynchronize(ctxs[j]->stream), "sync batch context");
+  /* cut the work into chunks of at most `radiance` paths */
+  std::vector<std::vector<Piece>> chunks(1);
+  uint64_t in_chunk = 0;
+  for (size_t j = 0; j < nj; j++) {
+    const nova_b200_frame *f = frames[j];
+    const uint64_t np = (uint64_t)f->width * f->height;
+    uint32_t s = 0;
+    while (s < (uint32_t)f->sample_count) {
+      uint64_t room = (radiance - in_chunk) / np;
+      if (room == 0) {
+        chunks.emplace_back();
+        in_chunk = 0;
+        room = radiance / np;
+      }
+      const uint32_t take = (uint32_t)std::min<uint64_t>(room, (uint64_t)f->sample_count - s);
+      chunks.back().push_back(Piece{ctxs[j], f, (uint32_t)f->sample_begin + s, take});
+      in_chunk += np * take;
+      s += take;
+    }
+  }
+  nova_b200_render_stats sum{};
+  float t_trace = 0.f, t_shade = 0.f;
+  NB_CUDA(x, cudaEventRecord(x->ev_begin, x->stream), "event");
+  Job *hj = static_cast<Job *>(x->h_jobs);
+  for (const auto &chunk : chunks) {
+    if (chunk.empty()) continue;
+    if (chunk.size() > kMaxJobs) return fail(x, NOVA_B200_INVALID_ARGUMENT, "more than 4096 frame pieces in a chunk%s");
+    /* the previous chunk's resolve kernels read the pinned job table: wait before rewriting it */
+    NB_CUDA(x, cudaStreamSynchronize(x->stream), "chunk");
+    uint32_t pb = 0;
+    for (size_t k = 0; k < chunk.size(); k++) {
+      const Piece &P = chunk[k];
+      Job &J = hj[k];
+      J.sc = P.ctx->scene;
+      RenderParams &rp = J.rp;
+      rp.W = P.f->width, rp.H = P.f->height, rp.NP = (uint32_t)((uint64_t)P.f->width * P.f->height);
+      rp.count = P.count;
+      rp.begin = P.begin;
+      rp.spp_total = (uint32_t)P.f->spp_total;
+      rp.max_depth = P.f->max_depth;
+      rp.seed = P.f->seed;
+      rp.rr_start = P.f->rr_start;
+      std::copy(P.f->inv_P, P.f->inv_P + 16, rp.inv_P);
+      std::copy(P.f->inv_V, P.f->inv_V + 16, rp.inv_V);
+      J.path_begin = pb;
+      J.n_paths = rp.NP * P.count;
+      pb += J.n_paths;
+    }
+    const bool single = chunk.size() == 1;
+    if (!single) {
+      if ((st = capture_graph(x, width)) != NOVA_B200_SUCCESS) return st;
+      NB_CUDA(x, cudaMemcpyAsync(x->d_jobs, hj, sizeof(Job) * chunk.size(), cudaMemcpyHostToDevice, x->stream),
+              "upload(jobs)");
+    }
+    WaveCounters *hw = static_cast<WaveCounters *>(x->h_wave);
+    *hw = WaveCounters{};
+    hw->total = pb;
+    hw->cap = x->queue_cap;
+    hw->n_jobs = (uint32_t)chunk.size();
+    NB_CUDA(x, cudaMemcpyAsync(x->d_wave, hw, sizeof(WaveCounters), cudaMemcpyHostToDevice, x->stream),
+            "upload(wave counters)");
+    NB_CUDA(x, cudaStreamSynchronize(x->stream), "upload(wave counters)");
+    for (;;) {
+      if (!single) {
+        NB_CUDA(x, cudaGraphLaunch(x->graph_exec, x->stream), "cudaGraphLaunch");
+      } else if (width == 8) {
+        enqueue_waves<true, 8>(x, hj[0], false);
+      } else {
+        enqueue_waves<true, 2>(x, hj[0], false);
+      }
+      NB_CUDA(x, cudaGetLastError(), "wave kernels");
+      NB_CUDA(x, cudaStreamSynchronize(x->stream), "waves");
+      for (int w = 0; w < kWavesPerGraph; w++) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, x->ev_wave[3 * w], x->ev_wave[3 * w + 1]);
+        cudaEventElapsedTime(&b, x->ev_wave[3 * w + 1], x->ev_wave[3 * w + 2]);
+        t_trace += a;
+        t_shade += b;
+      }
+      sum.kernels += 4 * kWavesPerGraph;
+      if (hw->done) break;
+    }
+    sum.traced += hw->traced;
+    sum.segments += hw->traced;
+    sum.waves += hw->waves;
+    sum.paths += pb;
+    for (size_t k = 0; k < chunk.size(); k++) {
+      const Piece &P = chunk[k];
+      nova_b200_ctx *c = P.ctx;
+      c->film_samples += P.count;
+      const uint32_t NP = hj[k].rp.NP;
+      k_resolve<<<(NP + 255) / 256, 256, 0, x->stream>>>(x->d_radiance + hj[k].path_begin, NP, P.count, c->d_film_acc,
+                                                         (float)c->film_samples, c->d_film_out, P.f->width,
+                                                         P.f->height, P.f->vertical_invert);
+      sum.kernels++;
+    }
+  }
+  NB_CUDA(x, cudaGetLastError(), "render kernels");
+  NB_CUDA(x, cudaEventRecord(x->ev_end, x->stream), "event");
+  for (size_t j = 0; j < nj; j++) {
+    const size_t bytes = (size_t)frames[j]->width * frames[j]->height * 4 * sizeof(float);
+    if (films_device && films_device[j])
+      NB_CUDA(x, cudaMemcpyAsync(films_device[j], ctxs[j]->d_film_out, bytes, cudaMemcpyDeviceToDevice, x->stream),
+              "copy film");
+    if (films_host && films_host[j])
+      NB_CUDA(x, cudaMemcpyAsync(films_host[j], ctxs[j]->d_film_out, bytes, cudaMemcpyDeviceToHost, x->stream),
+              "copy film");
+  }
+  NB_CUDA(x, cudaStreamSynchronize(x->stream), "render");
+  float total_ms = 0.f;
+  cudaEventElapsedTime(&total_ms, x->ev_begin, x->ev_end);
+  sum.device_ms = total_ms;
+  sum.trace_ms = t_trace;
+  sum.shade_ms = t_shade;
+  if (stats) *stats = sum;
+  return NOVA_B200_SUCCESS;
+}
+
+}  // namespace
+
+nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *film_host, float *film_device,
+                           nova_b200_render_stats *stats) {
+  nova_b200_status st = validate_frame(c, f);
+  if (st != NOVA_B200_SUCCESS) return st;
+  cudaSetDevice(c->device);
+  return render_jobs(c, {c}, {f}, &film_host, &film_device, stats);
+}
+
+nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
+                                 float *const *films_host, float *const *films_device, nova_b200_render_stats *stats) {
+  using namespace nbctx;
+  if (!ctxs || !ctxs[0]) return NOVA_B200_INVALID_ARGUMENT;
+  nova_b200_ctx *x = ctxs[0];
+  if (!frames || n == 0) return fail(x, NOVA_B200_INVALID_ARGUMENT, "empty batch%s");
+  std::vector<nova_b200_ctx *> cs(n);
+  std::vector<const nova_b200_frame *> fs(n);
+  for (uint32_t j = 0; j < n; j++) {
+    if (!ctxs[j]) return fail(x, NOVA_B200_INVALID_ARGUMENT, "null context in batch%s");
+    nova_b200_status st = validate_frame(ctxs[j], &frames[j]);
+    if (st != NOVA_B200_SUCCESS) {
+      x->error = ctxs[j]->error;
+      return st;
+    }
+    for (uint32_t k = 0; k < j; k++)
+      if (ctxs[k] == ctxs[j]) return fail(x, NOVA_B200_INVALID_ARGUMENT, "a context appears twice in a batch%s");
+    cs[j] = ctxs[j];
+    fs[j] = &frames[j];
+  }
+  cudaSetDevice(x->device);
+  return render_jobs(x, cs, fs, films_host, films_device, stats);
 }
 
 nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,

@@ -81,7 +81,7 @@ _lib = None
 
 EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "nova_b200_build_bvh",
            "nova_b200_render", "nova_b200_trace", "nova_b200_sobol", "nova_b200_bake_irradiance",
-           "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc"]
+           "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch"]
 
 
 def lib():
@@ -106,6 +106,8 @@ def lib():
         L.nova_b200_scene_info.argtypes = [vp] + [C.POINTER(C.c_uint64)] * 5
         L.nova_b200_synchronize.argtypes = [vp]
         L.nova_b200_render_noalloc.argtypes = [vp, C.POINTER(Frame), vp]
+        L.nova_b200_render_batch.argtypes = [C.POINTER(vp), C.POINTER(Frame), C.c_uint32, C.POINTER(vp),
+                                             C.POINTER(vp), C.POINTER(RenderStats)]
         for name in EXPORTS:
             if name != "nova_b200_get_error":
                 getattr(L, name).restype = C.c_int
@@ -160,6 +162,20 @@ def make_frame(scene: dict, width, height, spp_total, max_depth, seed=0, sample_
                  max_depth, seed, rr_start, reset, vertical_invert,
                  (C.c_float * 16)(*np.asarray(scene["inv_P"], np.float32).reshape(16)),
                  (C.c_float * 16)(*np.asarray(scene["inv_V"], np.float32).reshape(16)))
+
+
+def render_batch(contexts, frames, films_host=None, films_device=None) -> "RenderStats":
+    """Renders frames[j] of contexts[j] for every j in one wavefront (nova_b200_render_batch)."""
+    n = len(contexts)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    fs = (Frame * n)(*frames)
+    fh = None if films_host is None else (C.c_void_p * n)(*[None if a is None else a.ctypes.data for a in films_host])
+    fd = None if films_device is None else (C.c_void_p * n)(*films_device)
+    st = RenderStats()
+    rc = lib().nova_b200_render_batch(hs, fs, n, fh, fd, C.byref(st))
+    if rc != 0:
+        raise NovaError(rc, contexts[0].error())
+    return st
 
 
 class Context:

@@ -160,6 +160,16 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *ctx, const nova_b200_bvh_opt
 nova_b200_status nova_b200_render(nova_b200_ctx *ctx, const nova_b200_frame *frame, float *film_host,
                                   float *film_device, nova_b200_render_stats *stats);
 
+/* Renders n frames of n different contexts (scenes) as one wavefront on ctxs[0]'s device, stream
+ * and path buffers: the batched form of renderGpu for many cameras and scenes of uneven size, sample
+ * count and depth (no counterpart in the reference, which renders one engine at a time).  Every
+ * frame follows the semantics of nova_b200_render on its own context (sample range, running-mean
+ * film, reset) and produces the same film bit for bit.  films_host / films_device may be NULL or
+ * hold n pointers (entries may be NULL).  All contexts must share a device and a BVH width. */
+nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
+                                        float *const *films_host, float *const *films_device,
+                                        nova_b200_render_stats *stats);
+
 /* Allocation-free variant of nova_b200_render, for callers that cannot call cudaMalloc during a
  * frame (device memory fully reserved by another allocator, or a real-time loop that must not risk
  * an allocation or a device-wide synchronisation).  No counterpart in the reference.  Renders
