@@ -477,6 +477,14 @@ nova_b200_status nova_b200_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *i
   return nb_sobol(c, n, idx, dim, seed, out);
 }
 
+nova_b200_status nova_b200_scatter(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, const int32_t *prim,
+                                   const float *t, const float *u, const float *v, const uint32_t *index,
+                                   const int32_t *bounce, uint32_t seed, float *out_o, float *out_d, float *weight,
+                                   float *emissive, int32_t *valid) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  return nb_scatter(c, n, o, d, prim, t, u, v, index, bounce, seed, out_o, out_d, weight, emissive, valid);
+}
+
 nova_b200_status nova_b200_bake_irradiance(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh, int32_t ch,
                                            int32_t ow, int32_t oh, int32_t samples, float *out) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;

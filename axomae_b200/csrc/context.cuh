@@ -90,6 +90,10 @@ nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_fra
                                  float *const *films_host, float *const *films_device, nova_b200_render_stats *stats);
 nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,
                           float *u, float *v);
+nova_b200_status nb_scatter(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, const int32_t *prim,
+                            const float *t, const float *u, const float *v, const uint32_t *index,
+                            const int32_t *bounce, uint32_t seed, float *out_o, float *out_d, float *weight,
+                            float *emissive, int32_t *valid);
 nova_b200_status nb_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *idx, const uint32_t *dim, uint32_t seed,
                           float *out);
 nova_b200_status nb_bake(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh, int32_t ch, int32_t ow,

@@ -338,6 +338,36 @@ __global__ void k_trace_api(DevScene sc, uint64_t n, const float *o, const float
   v[i] = r.v;
 }
 
+/* One shading event per given hit: the hit record, the principled scatter with Sobol dimensions
+ * 2 + 4 * bounce .. 5 + 4 * bounce, and the spawned ray (the body of k_shade for one path). */
+__global__ void k_scatter_api(DevScene sc, uint64_t n, const float *o, const float *d, const int32_t *prim,
+                              const float *t, const float *u, const float *v, const uint32_t *index,
+                              const int32_t *bounce, uint32_t seed, float *out_o, float *out_d, float *weight,
+                              float *emissive, int32_t *valid) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t p = prim[i];
+  if (p < 0 || (uint64_t)p >= sc.n_prims || bounce[i] < 0 || bounce[i] > kMaxDepth) {
+    valid[i] = -1;
+    return;
+  }
+  const V3 ro{o[3 * i], o[3 * i + 1], o[3 * i + 2]}, rd{d[3 * i], d[3 * i + 1], d[3 * i + 2]};
+  const DevInstance &I = sc.instances[__ldg(sc.prim_inst + p)];
+  const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)p - I.prim_offset, t[i], u[i], v[i]);
+  const ScatterResult sr =
+      scatter(sc, rd, hr, sc.materials[I.material], index[i], 2u + 4u * (unsigned)bounce[i], seed);
+  const float eps = 1e-3f;
+  const V3 nd3 = normalize(sr.wi);
+  const V3 no3 = hr.position + hr.ng * (eps + eps * fsign(dot(hr.ng, sr.wi)));
+  for (int k = 0; k < 3; k++) {
+    out_o[3 * i + k] = k == 0 ? no3.x : k == 1 ? no3.y : no3.z;
+    out_d[3 * i + k] = k == 0 ? nd3.x : k == 1 ? nd3.y : nd3.z;
+    weight[3 * i + k] = k == 0 ? sr.weight.x : k == 1 ? sr.weight.y : sr.weight.z;
+    emissive[3 * i + k] = k == 0 ? sr.emissive.x : k == 1 ? sr.emissive.y : sr.emissive.z;
+  }
+  valid[i] = sr.valid ? 1 : 0;
+}
+
 __global__ void k_sobol_api(const uint32_t *dv, uint64_t n, const uint32_t *idx, const uint32_t *dim, uint32_t seed,
                             float *out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -703,6 +733,23 @@ nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const fl
   k_trace_api<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(c->scene, n, o, d, prim, t, u, v);
   NB_CUDA(c, cudaGetLastError(), "k_trace_api");
   NB_CUDA(c, cudaStreamSynchronize(c->stream), "trace");
+  return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nb_scatter(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, const int32_t *prim,
+                            const float *t, const float *u, const float *v, const uint32_t *index,
+                            const int32_t *bounce, uint32_t seed, float *out_o, float *out_d, float *weight,
+                            float *emissive, int32_t *valid) {
+  using namespace nbctx;
+  if (!c->bvh_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "build the acceleration structure first%s");
+  if (n == 0) return NOVA_B200_SUCCESS;
+  if (!o || !d || !prim || !t || !u || !v || !index || !bounce || !out_o || !out_d || !weight || !emissive || !valid)
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "null buffer%s");
+  cudaSetDevice(c->device);
+  k_scatter_api<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(c->scene, n, o, d, prim, t, u, v, index, bounce,
+                                                                     seed, out_o, out_d, weight, emissive, valid);
+  NB_CUDA(c, cudaGetLastError(), "k_scatter_api");
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "scatter");
   return NOVA_B200_SUCCESS;
 }
 

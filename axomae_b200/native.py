@@ -81,7 +81,8 @@ _lib = None
 
 EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "nova_b200_build_bvh",
            "nova_b200_render", "nova_b200_trace", "nova_b200_sobol", "nova_b200_bake_irradiance",
-           "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch"]
+           "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
+           "nova_b200_scatter"]
 
 
 def lib():
@@ -99,6 +100,7 @@ def lib():
         L.nova_b200_render.argtypes = [vp, C.POINTER(Frame), vp, vp, C.POINTER(RenderStats)]
         L.nova_b200_trace.argtypes = [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]
         L.nova_b200_sobol.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, vp]
+        L.nova_b200_scatter.argtypes = [vp, C.c_uint64] + [vp] * 8 + [C.c_uint32] + [vp] * 5
         L.nova_b200_bake_irradiance.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                 C.c_int32, vp]
         L.nova_b200_get_error.argtypes = [vp, C.c_char_p, C.POINTER(C.c_size_t)]
@@ -236,6 +238,14 @@ class Context:
         """Device pointers (e.g. torch CUDA tensors' data_ptr())."""
         self._check(lib().nova_b200_trace(self.h, n, C.c_void_p(orig_ptr), C.c_void_p(dir_ptr), C.c_void_p(prim_ptr),
                                           C.c_void_p(t_ptr), C.c_void_p(u_ptr), C.c_void_p(v_ptr)))
+
+    def scatter(self, n, o_ptr, d_ptr, prim_ptr, t_ptr, u_ptr, v_ptr, index_ptr, bounce_ptr, seed, out_o_ptr,
+                out_d_ptr, weight_ptr, emissive_ptr, valid_ptr):
+        """One shading event per hit (nova_b200_scatter); device pointers."""
+        ptrs = [o_ptr, d_ptr, prim_ptr, t_ptr, u_ptr, v_ptr, index_ptr, bounce_ptr]
+        outs = [out_o_ptr, out_d_ptr, weight_ptr, emissive_ptr, valid_ptr]
+        self._check(lib().nova_b200_scatter(self.h, n, *[C.c_void_p(p) for p in ptrs], seed,
+                                            *[C.c_void_p(p) for p in outs]))
 
     def sobol(self, idx_ptr, dim_ptr, n, seed, out_ptr):
         self._check(lib().nova_b200_sobol(self.h, n, C.c_void_p(idx_ptr), C.c_void_p(dim_ptr), seed,

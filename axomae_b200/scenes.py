@@ -140,6 +140,26 @@ def quad(size, y=0.0):
             "indices": np.array([[0, 2, 1], [0, 3, 2]], np.uint32)}
 
 
+def grid_quad(size, n, y=0.0):
+    """A size x size ground plane at height y tessellated into n x n quads (2 n^2 triangles, facing +y)."""
+    h = size / 2.0
+    c = np.arange(n + 1) / n
+    X, Z = np.meshgrid(-h + size * c, -h + size * c, indexing="xy")
+    v = np.stack([X, np.full_like(X, y), Z], -1).reshape(-1, 3).astype(np.float32)
+    k = v.shape[0]
+    nrm = np.tile([0, 1, 0], (k, 1)).astype(np.float32)
+    t = np.tile([1, 0, 0], (k, 1)).astype(np.float32)
+    b = np.cross(nrm, t).astype(np.float32)
+    U, V = np.meshgrid(c, c, indexing="xy")
+    uv = np.stack([U, V], -1).reshape(-1, 2).astype(np.float32)
+    j, i = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    a = (j * (n + 1) + i).reshape(-1)
+    bb, cc, dd = a + 1, a + n + 1, a + n + 2
+    idx = np.stack([np.stack([a, cc, dd], -1), np.stack([a, dd, bb], -1)], 1).reshape(-1, 3)
+    return {"vertices": v, "normals": nrm, "tangents": t, "bitangents": b, "uv": uv,
+            "indices": idx.astype(np.uint32)}
+
+
 def box(center, half, rot):
     """Axis box of half extents `half` rotated by `rot` (3x3), 24 vertices, 12 triangles."""
     faces = []
@@ -340,12 +360,16 @@ def heightfield_scene(n=1024, width=1920, height=1080, env_w=2048, env_h=1024, s
 
 
 def mixed_scene(target_tris=50000, width=256, height=256, seed=0, env_w=256, env_h=128) -> dict:
-    """Random spheres and boxes until `target_tris` triangles; materials 1/3 Lambert, 1/3 GGX
-    conductor, 1/3 GGX dielectric IOR 1.5."""
+    """Random spheres and boxes on a tessellated 40 x 40 ground until `target_tris` triangles;
+    materials 1/3 Lambert, 1/3 GGX conductor, 1/3 GGX dielectric IOR 1.5.  The ground is cut into
+    32 x 32 quads: two ground triangles spanning the whole scene would sit in almost every node of a
+    BVH built with node-box split candidates (aggregate/native/BvhBuilder.cpp:151-184) and leave
+    leaves of thousands of triangles there."""
     rng = np.random.default_rng(seed)
     b = _Builder()
-    b.add(quad(40.0), b.lambert((0.6, 0.6, 0.6)))
-    tris = 2
+    g = grid_quad(40.0, 32)
+    b.add(g, b.lambert((0.6, 0.6, 0.6)))
+    tris = len(g["indices"])
     while tris < target_tris:
         kind = rng.integers(3)
         if kind == 0:
@@ -408,6 +432,25 @@ def instanced_scene(n_meshes=10, n_instances=1000, tris_per_mesh=10000, width=38
     env = np.concatenate([env, np.ones((env_h, env_w, 1), np.float32)], -1)
     e = b.tex(f32_texture(env))
     return b.finish(e, camera((0.0, 0.0, box_size * 1.2), (0.0, 0.0, 0.0), width, height))
+
+
+def batch_jobs(n_jobs=32, seed=0, tris=(50000, 500000), res=(256, 2048), spp_choices=(1, 4, 16, 64),
+               depth_choices=(3, 6, 12)):
+    """The batched workload: `n_jobs` seeded jobs, each a mixed spheres + boxes scene of
+    U[tris] triangles (1/3 Lambert, 1/3 GGX conductor, 1/3 GGX dielectric IOR 1.5), a square
+    frame whose pixel count is log-uniform in [res[0]^2, res[1]^2], spp drawn from `spp_choices`
+    and max depth from `depth_choices`.  Returns a list of dicts
+    {scene, width, height, spp, depth, seed}."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(n_jobs):
+        n_tris = int(rng.integers(tris[0], tris[1] + 1))
+        side = int(round(math.exp(rng.uniform(math.log(res[0]), math.log(res[1])))))
+        spp = int(rng.choice(spp_choices))
+        depth = int(rng.choice(depth_choices))
+        scene = mixed_scene(n_tris, side, side, seed=seed * 1000 + j + 1)
+        jobs.append({"scene": scene, "width": side, "height": side, "spp": spp, "depth": depth, "seed": j})
+    return jobs
 
 
 def scene_stats(scene: dict) -> dict:

@@ -1,20 +1,29 @@
-"""Benchmark: Nova path tracing on B200, plain wavefront, heightfield workload.
+"""Benchmark: Nova path tracing on B200 — batched vs plain wavefront.
 
-Workload (one step = one full render): a 1024 x 1024 quad heightfield (2,097,152 triangles) from
-seeded 6-octave fBm (amplitude 0.3), per-quad material 50/50 Lambert / GGX conductor, a
-2048 x 1024 log-normal(0, 1.5) float environment map, 1920 x 1080 pixels, 64 spp, max depth 8,
-Russian roulette from bounce 3.  Synthetic seeded data (no dataset exists for this path).
+Default workload ("batched", one step = one render of all jobs): 32 seeded jobs, each a scene of
+50k-500k triangles (random UV spheres + boxes; 1/3 Lambert, 1/3 GGX conductor, 1/3 GGX dielectric
+IOR 1.5; 256x128 log-normal float environment), a square frame whose pixel count is log-uniform in
+[256^2, 2048^2], spp drawn from {1, 4, 16, 64}, max depth from {3, 6, 12}, Sobol seed 0.  The
+batched arm renders all 32 frames with one nova_b200_render_batch call (one device-driven
+wavefront); the plain arm renders the same frames with one nova_b200_render call each.  Both run the
+same estimator on the same sample indices, so their images are equal (checked bit for bit every
+run) and so is their RMSE against the CPU oracle (reported on a pixel sample).
+
+Second workload ("heightfield", --workload heightfield): a 1024 x 1024 quad heightfield
+(2,097,152 triangles), 50/50 Lambert / GGX conductor, 2048 x 1024 log-normal(0, 1.5) environment,
+1920 x 1080, 64 spp, depth 8, Russian roulette from bounce 3; plain wavefront only.
 
 Metric: Mrays/s = closest-hit rays traced on the device / device render time (CUDA events on the
-render stream), whole job over all ranks.  `e2e` is the same metric through the C ABI starting
-from pinned host buffers each step: scene upload + device BVH build + render + film readback.
+render stream), whole job over all ranks.  `e2e` is the same metric through the C ABI from pinned
+host buffers each step: scene upload + device BVH build + render + film readback.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload batched|heightfield]
 
-With N > 1 (torchrun, one rank per GPU) every rank renders its own 64-sample range of a 64N-spp
-image and the films are summed with one NCCL all-reduce (weak scaling).  --impl reference times
-the CPU implementation of the path (the oracle restatement of the reference's CPU Nova path; the
-reference itself cannot be built here) on the host cores on a bounded pixel sample.
+With N > 1 (torchrun, one rank per GPU) every rank renders its own sample range of every frame
+(frame spp x N in total) and the films are summed with one NCCL all-reduce (weak scaling).
+--impl reference times the CPU implementation of the path (the oracle restatement of the
+reference's CPU Nova path; the reference itself cannot be built) on the host cores on a bounded
+pixel sample of the same workload.
 """
 import argparse
 import json
@@ -29,9 +38,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-CFG = dict(n=1024, width=1920, height=1080, spp=64, depth=8, rr_start=3, env_w=2048, env_h=1024, seed=0)
-WORKLOAD = "heightfield 1024^2 quads (2,097,152 tris), env 2048x1024, 1920x1080, 64 spp, depth 8, RR from 3"
-METRIC = "Mrays/s (plain wavefront path tracing, heightfield workload)"
+HF = dict(n=1024, width=1920, height=1080, spp=64, depth=8, rr_start=3, env_w=2048, env_h=1024, seed=0)
+HF_WORKLOAD = "heightfield 1024^2 quads (2,097,152 tris), env 2048x1024, 1920x1080, 64 spp, depth 8, RR from 3"
+HF_METRIC = "Mrays/s (plain wavefront path tracing, heightfield workload)"
+BATCH_WORKLOAD = ("32 jobs: mixed spheres+boxes scenes of 50k-500k tris (Lambert / GGX conductor / GGX "
+                  "dielectric IOR 1.5), square frames log-uniform 256^2-2048^2, spp in {1,4,16,64}, "
+                  "depth in {3,6,12}, seed 0")
+BATCH_METRIC = "Mrays/s batched wavefront (32-job batch; plain wavefront on the same jobs in extra.plain)"
 
 
 def peaks():
@@ -94,10 +107,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_scene():
+# ----------------------------------------------------------------------------------------------
+# workloads: a list of jobs {scene, width, height, spp, depth, rr_start}
+
+
+def make_jobs(workload):
     from axomae_b200 import scenes
-    return scenes.heightfield_scene(n=CFG["n"], width=CFG["width"], height=CFG["height"], env_w=CFG["env_w"],
-                                    env_h=CFG["env_h"], seed=CFG["seed"])
+    if workload == "heightfield":
+        s = scenes.heightfield_scene(n=HF["n"], width=HF["width"], height=HF["height"], env_w=HF["env_w"],
+                                     env_h=HF["env_h"], seed=HF["seed"])
+        return [{"scene": s, "width": HF["width"], "height": HF["height"], "spp": HF["spp"], "depth": HF["depth"],
+                 "rr_start": HF["rr_start"]}]
+    jobs = scenes.batch_jobs(32, seed=0)
+    for j in jobs:
+        j["rr_start"] = -1
+    return jobs
 
 
 def scene_bytes(scene):
@@ -109,202 +133,97 @@ def scene_bytes(scene):
     return b
 
 
-def cpu_sample(scene, frac_stride=64, threads=0):
-    """Oracle render of every `frac_stride`-th pixel (all samples): Mrays/s on the host cores."""
+def oracle_module():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_binding as ob
     ob.build()
+    return ob
+
+
+def oracle_scenes(jobs):
+    """Oracle scenes (reference BVH builds) of all jobs, built on a thread pool (the builds run in
+    C with the GIL released)."""
+    from concurrent.futures import ThreadPoolExecutor
+    ob = oracle_module()
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+        return list(ex.map(lambda j: ob.OracleScene(j["scene"]), jobs))
+
+
+def cpu_sample(jobs, stride, threads=0, oscs=None, films=None):
+    """Oracle render of every `stride`-th pixel of every job (all samples): Mrays/s on the host
+    cores, the reference-BVH node visits / triangle tests per ray, and, when GPU films are given,
+    the relative RMSE of those films against the oracle on the sampled pixels."""
     t0 = time.perf_counter()
-    osc = ob.OracleScene(scene)
+    ob = oracle_module()
+    if oscs is None:
+        oscs = oracle_scenes(jobs)
     build_s = time.perf_counter() - t0
-    W, H = CFG["width"], CFG["height"]
-    ids = np.arange(0, W * H, frac_stride, dtype=np.int32)
-    opt = ob.options(W, H, CFG["spp"], CFG["depth"], seed=CFG["seed"], rr_start=CFG["rr_start"], threads=threads)
-    _, st = osc.render(opt, pixel_ids=ids)
+    traced = seconds = nodes = tris = 0
+    pixels = 0
+    sq, cnt = 0.0, 0
+    for k, (j, osc) in enumerate(zip(jobs, oscs)):
+        W, H = j["width"], j["height"]
+        ids = np.arange(k % stride, W * H, stride, dtype=np.int32)
+        opt = ob.options(W, H, j["spp"], j["depth"], seed=0, rr_start=j["rr_start"], threads=threads)
+        ref, st = osc.render(opt, pixel_ids=ids)
+        traced += st.traced
+        seconds += st.seconds
+        nodes += st.node_visits
+        tris += st.tri_tests
+        pixels += ids.size
+        if films is not None:
+            r = ref.reshape(-1, 4)[ids, :3].astype(np.float64)
+            g = films[k].reshape(-1, 4)[ids, :3].astype(np.float64)
+            d = (g - r) / np.maximum(r, 1e-3)
+            sq += float((d * d).sum())
+            cnt += d.size
     cores = threads if threads > 0 else os.cpu_count()
-    return {"mrays": st.traced / st.seconds / 1e6, "seconds": st.seconds, "traced": st.traced,
-            "node_visits_per_ray": st.node_visits / max(1, st.traced), "tri_tests_per_ray": st.tri_tests / max(1, st.traced),
-            "segments": st.segments, "pixels": int(ids.size), "cores": cores, "build_s": build_s}
+    return {"mrays": traced / seconds / 1e6, "seconds": seconds, "traced": traced, "pixels": pixels,
+            "node_visits_per_ray": nodes / max(1, traced), "tri_tests_per_ray": tris / max(1, traced),
+            "cores": cores, "build_s": build_s, "oscs": oscs,
+            "rel_rmse": float(np.sqrt(sq / cnt)) if cnt else None}
+
+
+def cpu_stride(workload, kind):
+    env = os.environ.get("NOVA_BENCH_CPU_STRIDE")
+    if env:
+        return int(env)
+    # baseline sample (our arm, once): about 10-30 s of oracle work on a 16-core host;
+    # reference arm: a few seconds per step
+    if workload == "heightfield":
+        return 2 if kind == "baseline" else 8
+    return 16 if kind == "baseline" else 64
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    scene = make_scene()
-    stride = int(os.environ.get("NOVA_BENCH_CPU_STRIDE", "64"))
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
-    vals = []
+    jobs = make_jobs(args.workload)
+    stride = cpu_stride(args.workload, "reference")
+    oscs = oracle_scenes(jobs)
+    for _ in range(min(args.warmup, 1)):
+        cpu_sample(jobs, stride * 4, oscs=oscs)
+    vals, secs = [], []
     last = None
     for _ in range(args.steps):
-        last = cpu_sample(scene, stride)
+        last = cpu_sample(jobs, stride, oscs=oscs)
         vals.append(last["mrays"])
+        secs.append(last["seconds"])
     v = float(np.median(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": last["seconds"] * 1000.0, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "pixel_sample": "every %dth pixel, all 64 spp" % stride},
-            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": last["cores"], "kind": "port",
-                             "sample": "oracle (CPU restatement of the reference Nova path) on every %dth pixel of "
-                                       "the 1920x1080 frame, 64 spp, %d pixels" % (stride, last["pixels"])},
+    metric = HF_METRIC if args.workload == "heightfield" else BATCH_METRIC
+    workload = HF_WORKLOAD if args.workload == "heightfield" else BATCH_WORKLOAD
+    sample = ("oracle (CPU restatement of the reference Nova path, thread pool of %d workers, 20x20 tiles) on every "
+              "%dth pixel of every frame, all samples: %d pixels" % (last["cores"], stride, last["pixels"]))
+    line = {"impl": "reference", "metric": metric, "value": v, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(secs)) * 1000.0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": {"workload": workload, "pixel_sample": sample},
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": last["cores"], "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world, local_rank):
-    import torch
-    from axomae_b200 import native
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    scene = make_scene()
-    W, H, spp, depth = CFG["width"], CFG["height"], CFG["spp"], CFG["depth"]
-    ctx = native.Context(local_rank)
-    t0 = time.perf_counter()
-    ctx.upload(scene)
-    upload_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    ctx.build(width=args.bvh_width)
-    build_s = time.perf_counter() - t0
-    info = ctx.info()
-    spp_total = spp * world
-    film = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
-    frame = native.make_frame(scene, W, H, spp_total, depth, seed=CFG["seed"], sample_begin=rank * spp,
-                              sample_count=spp, rr_start=CFG["rr_start"], reset=1)
-
-    def step():
-        st = ctx.render(frame, film_device_ptr=film.data_ptr())
-        if world > 1:
-            dist.all_reduce(film)
-            film.div_(world)
-        return st
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    traced = 0
-    dev_ms = 0.0
-    trace_ms = 0.0
-    shade_ms = 0.0
-    kernels = 0
-    waves = 0
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        ev0.record()
-        for _ in range(args.steps):
-            st = step()
-            traced += st.traced
-            dev_ms += st.device_ms
-            trace_ms += st.trace_ms
-            shade_ms += st.shade_ms
-            kernels += st.kernels
-            waves += st.waves
-        ev1.record()
-        torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    wall_ms = ev0.elapsed_time(ev1)
-    step_ms = max(dev_ms, wall_ms) / args.steps  # the render stream's events; the torch-stream bracket
-    if dist:
-        t = torch.tensor([step_ms, float(traced)], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        step_ms, traced_all = float(mx[0]), float(t[1])
-    else:
-        traced_all = float(traced)
-    value = traced_all / args.steps / (step_ms / 1e3) / 1e6
-
-    # end to end through the C ABI from pinned host buffers: upload + build + render + readback
-    e2e = None
-    if rank == 0 and not args.no_e2e:
-        pinned = pin_scene(scene)
-        host_film = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
-        e_steps = max(1, min(args.steps, 3))
-        ectx = native.Context(local_rank)
-        eframe = native.make_frame(scene, W, H, spp, depth, seed=CFG["seed"], rr_start=CFG["rr_start"])
-
-        def e2e_step():
-            t0 = time.perf_counter()
-            ectx.upload(pinned)
-            t1 = time.perf_counter()
-            ectx.build(width=args.bvh_width)
-            t2 = time.perf_counter()
-            st = ectx.render(eframe, film_host=host_film.numpy())
-            t3 = time.perf_counter()
-            return st.traced, (t1 - t0, t2 - t1, t3 - t2)
-
-        e2e_step()  # untimed: the context's first render allocates its path queues and film
-        e_traced = 0
-        stages = np.zeros(3)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e_steps):
-            tr, st3 = e2e_step()
-            e_traced += tr
-            stages += st3
-        ectx.synchronize()
-        e_s = time.perf_counter() - t0
-        ectx.close()
-        e2e = {"value": e_traced / e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": scene_bytes(scene),
-               "d2h_bytes_per_step": W * H * 16, "steps": e_steps, "warmup": 1,
-               "upload_ms": 1e3 * stages[0] / e_steps, "build_ms": 1e3 * stages[1] / e_steps,
-               "render_ms": 1e3 * stages[2] / e_steps,
-               "timing": "host wall clock around upload (pinned H2D) + BVH build + render + film D2H"}
-
-    if rank != 0:
-        ctx.close()
-        if dist:
-            dist.destroy_process_group()
-        return
-    cpu = None
-    if not args.no_cpu:
-        cpu = cpu_sample(scene, int(os.environ.get("NOVA_BENCH_CPU_STRIDE", "64")))
-    pk = peaks()
-    hbm = pk.get("hbm_gbs")
-    peak_src = "measured" if hbm else "fallback"
-    hbm = hbm or 6650.0
-    # Algorithmic bytes per traced ray (reference binary BVH node/triangle counts measured by the
-    # oracle on this workload's rays): 32 B ray + 16 B hit + 64 B per inner-node visit + 36 B per
-    # triangle test.
-    if cpu:
-        b_ray = 32 + 16 + 64 * cpu["node_visits_per_ray"] + 36 * cpu["tri_tests_per_ray"]
-    else:
-        b_ray = None
-    trace_rate = traced / (trace_ms / 1e3) if trace_ms > 0 else None
-    roof = None
-    if b_ray and trace_rate:
-        achieved = trace_rate * b_ray / 1e9
-        roof = {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": peak_src, "traffic": None,
-                "bytes_per_ray": b_ray, "trace_ms_per_step": trace_ms / args.steps}
-    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded heightfield + log-normal env map)",
-            "config": {"workload": WORKLOAD, "spp_per_gpu": spp, "bvh_width": args.bvh_width or 2, "parallelism": "sample-range partition + NCCL film "
-                       "all-reduce" if world > 1 else "single GPU", "l2": "working set larger than L2 (BVH %d nodes "
-                       "x 64 B + %d tris x 48 B)" % (info["nodes"], info["triangles"])},
-            "e2e": e2e, "roofline": roof,
-            "cpu_baseline": None if not cpu else {
-                "value": cpu["mrays"], "unit": "Mrays/s", "cores": cpu["cores"], "kind": "port",
-                "sample": "oracle on every %sth pixel of the frame, 64 spp (%d pixels, %.1f s)" % (
-                    os.environ.get("NOVA_BENCH_CPU_STRIDE", "64"), cpu["pixels"], cpu["seconds"])},
-            "clocks": clk.summary(), "gpu_launches": kernels,
-            "extra": {"waves_per_step": waves / args.steps, "traced_per_step": traced / args.steps,
-                      "trace_ms_per_step": trace_ms / args.steps, "shade_ms_per_step": shade_ms / args.steps,
-                      "bvh_build_s": build_s, "upload_s": upload_s, "bvh_nodes": info["nodes"],
-                      "device_bytes": info["device_bytes"]}}
-    print(json.dumps(line), flush=True)
-    ctx.close()
-    if dist:
-        dist.destroy_process_group()
+# ----------------------------------------------------------------------------------------------
 
 
 def pin_scene(scene):
@@ -318,12 +237,238 @@ def pin_scene(scene):
         return t.numpy().view(a.dtype)
 
     keep = []
-
     out = dict(scene)
     out["meshes"] = [{k: pin(v) for k, v in m.items()} for m in scene["meshes"]]
     out["textures"] = [dict(t, pixels=pin(t["pixels"])) for t in scene["textures"]]
     out["_pinned"] = keep
     return out
+
+
+class Acc:
+    """Sums render stats over steps."""
+
+    def __init__(self):
+        self.traced = self.paths = self.kernels = self.waves = 0
+        self.dev_ms = self.trace_ms = self.shade_ms = 0.0
+
+    def add(self, st):
+        self.traced += st.traced
+        self.paths += st.paths
+        self.kernels += st.kernels
+        self.waves += st.waves
+        self.dev_ms += st.device_ms
+        self.trace_ms += st.trace_ms
+        self.shade_ms += st.shade_ms
+
+
+def timed(step, steps, torch, dist, clock=None):
+    """Runs `steps` steps between barriers + synchronizes; returns (Acc, ms per step over the
+    render stream and the torch stream, max over ranks, traced rays summed over ranks)."""
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    acc = Acc()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(steps):
+        for st in step():
+            acc.add(st)
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = max(acc.dev_ms, ev0.elapsed_time(ev1)) / steps
+    traced = float(acc.traced)
+    if dist:
+        t = torch.tensor([step_ms, traced], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        step_ms, traced = float(mx[0]), float(t[1])
+    return acc, step_ms, traced
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from axomae_b200 import native
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    batched = args.workload == "batched"
+    jobs = make_jobs(args.workload)
+    nj = len(jobs)
+    ctxs = [native.Context(local_rank) for _ in jobs]
+    t0 = time.perf_counter()
+    for c, j in zip(ctxs, jobs):
+        c.upload(j["scene"])
+    upload_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for c in ctxs:
+        c.build(width=args.bvh_width)
+    build_s = time.perf_counter() - t0
+    infos = [c.info() for c in ctxs]
+    frames = [native.make_frame(j["scene"], j["width"], j["height"], j["spp"] * world, j["depth"], seed=0,
+                                sample_begin=rank * j["spp"], sample_count=j["spp"], rr_start=j["rr_start"], reset=1)
+              for j in jobs]
+    sizes = [j["width"] * j["height"] * 4 for j in jobs]
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    flat = torch.zeros(int(offs[-1]), dtype=torch.float32, device="cuda")
+    films = [flat[int(offs[k]):int(offs[k + 1])] for k in range(nj)]
+    plain_flat = torch.zeros_like(flat)
+    plain_films = [plain_flat[int(offs[k]):int(offs[k + 1])] for k in range(nj)]
+
+    def reduce(buf):
+        if dist:
+            dist.all_reduce(buf)
+            buf.div_(world)
+
+    def plain_step():
+        sts = [c.render(f, film_device_ptr=p.data_ptr()) for c, f, p in zip(ctxs, frames, plain_films)]
+        reduce(plain_flat)
+        return sts
+
+    def batch_step():
+        st = native.render_batch(ctxs, frames, films_device=[p.data_ptr() for p in films])
+        reduce(flat)
+        return [st]
+
+    arms = {"plain": plain_step}
+    if batched:
+        arms["batched"] = batch_step
+    res = {}
+    clk_summary = None
+    for name, step in arms.items():
+        for _ in range(args.warmup):
+            step()
+        if name == ("batched" if batched else "plain"):
+            with ClockSampler(local_rank) as clk:
+                res[name] = timed(step, args.steps, torch, dist)
+            clk_summary = clk.summary()
+        else:
+            res[name] = timed(step, args.steps, torch, dist)
+    head = "batched" if batched else "plain"
+    acc, step_ms, traced_all = res[head]
+    value = traced_all / args.steps / (step_ms / 1e3) / 1e6
+    films_identical = None
+    if batched:
+        films_identical = bool(torch.equal(flat, plain_flat))
+
+    # end to end through the C ABI from pinned host buffers: upload + build + render + readback
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        pinned = [pin_scene(j["scene"]) for j in jobs]
+        host_films = [torch.empty(s, dtype=torch.float32).pin_memory() for s in sizes]
+        e_frames = [native.make_frame(j["scene"], j["width"], j["height"], j["spp"], j["depth"], seed=0,
+                                      rr_start=j["rr_start"]) for j in jobs]
+        e_steps = max(1, min(args.steps, 3))
+
+        def e2e_step():
+            t0 = time.perf_counter()
+            for c, p in zip(ctxs, pinned):
+                c.upload(p)
+            t1 = time.perf_counter()
+            for c in ctxs:
+                c.build(width=args.bvh_width)
+            t2 = time.perf_counter()
+            hf = [h.numpy() for h in host_films]
+            if batched:
+                traced = native.render_batch(ctxs, e_frames, films_host=hf).traced
+            else:
+                traced = sum(c.render(f, film_host=h).traced for c, f, h in zip(ctxs, e_frames, hf))
+            t3 = time.perf_counter()
+            return traced, (t1 - t0, t2 - t1, t3 - t2)
+
+        e2e_step()  # untimed: first upload of pinned buffers
+        e_traced = 0
+        stages = np.zeros(3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            tr, st3 = e2e_step()
+            e_traced += tr
+            stages += st3
+        for c in ctxs:
+            c.synchronize()
+        e_s = time.perf_counter() - t0
+        e2e = {"value": e_traced / e_s / 1e6, "unit": "Mrays/s",
+               "h2d_bytes_per_step": int(sum(scene_bytes(j["scene"]) for j in jobs)),
+               "d2h_bytes_per_step": int(sum(sizes) * 4), "steps": e_steps, "warmup": 1,
+               "upload_ms": 1e3 * stages[0] / e_steps, "build_ms": 1e3 * stages[1] / e_steps,
+               "render_ms": 1e3 * stages[2] / e_steps,
+               "timing": "host wall clock around scene upload (pinned H2D) + BVH build + %s + film D2H" % (
+                   "one nova_b200_render_batch" if batched else "nova_b200_render")}
+
+    if rank != 0:
+        for c in ctxs:
+            c.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    cpu = None
+    if not args.no_cpu:
+        host = [f.cpu().numpy() for f in films] if batched else [f.cpu().numpy() for f in plain_films]
+        cpu = cpu_sample(jobs, cpu_stride(args.workload, "baseline"), films=host if world == 1 else None)
+    pk = peaks()
+    hbm = pk.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    # Algorithmic bytes per traced ray (reference binary BVH node/triangle counts measured by the
+    # oracle on this workload's rays): 32 B ray + 16 B hit + 64 B per inner-node visit + 36 B per
+    # triangle test.
+    b_ray = 32 + 16 + 64 * cpu["node_visits_per_ray"] + 36 * cpu["tri_tests_per_ray"] if cpu else None
+    trace_rate = acc.traced / (acc.trace_ms / 1e3) if acc.trace_ms > 0 else None
+    roof = None
+    if b_ray and trace_rate:
+        achieved = trace_rate * b_ray / 1e9
+        roof = {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_src, "traffic": None,
+                "bytes_per_ray": b_ray, "trace_ms_per_step": acc.trace_ms / args.steps}
+    extra = {"waves_per_step": acc.waves / args.steps, "traced_per_step": acc.traced / args.steps,
+             "paths_per_step": acc.paths / args.steps, "trace_ms_per_step": acc.trace_ms / args.steps,
+             "shade_ms_per_step": acc.shade_ms / args.steps, "bvh_build_s": build_s, "upload_s": upload_s,
+             "bvh_nodes": sum(i["nodes"] for i in infos), "triangles": sum(i["triangles"] for i in infos),
+             "device_bytes": sum(i["device_bytes"] for i in infos)}
+    if batched:
+        pacc, pms, ptraced = res["plain"]
+        pval = ptraced / args.steps / (pms / 1e3) / 1e6
+        extra["plain"] = {"value": pval, "unit": "Mrays/s", "ms_per_step": pms, "gpu_launches": pacc.kernels,
+                          "waves_per_step": pacc.waves / args.steps, "trace_ms_per_step": pacc.trace_ms / args.steps,
+                          "shade_ms_per_step": pacc.shade_ms / args.steps}
+        extra["batched_over_plain"] = value / pval
+        extra["films_identical"] = films_identical
+        extra["equal_rmse"] = ("batched and plain films compared bit for bit after the timed steps; "
+                               "rel_rmse_vs_cpu is the per-pixel relative RMSE of the film against the oracle "
+                               "on the CPU sample's pixels")
+    if cpu:
+        extra["rel_rmse_vs_cpu"] = cpu["rel_rmse"]
+    metric = BATCH_METRIC if batched else HF_METRIC
+    workload = BATCH_WORKLOAD if batched else HF_WORKLOAD
+    if args.frame or args.spp:
+        workload += " (overridden: frame %s, spp %s)" % (args.frame, args.spp)
+    line = {"metric": metric, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and env maps)",
+            "config": {"workload": workload, "jobs": nj, "bvh_width": args.bvh_width or 2,
+                       "parallelism": "sample-range partition + NCCL film all-reduce" if world > 1 else "single GPU",
+                       "l2": "working set larger than L2 (%d BVH nodes + %d tris over %d scenes, films %d MB)" % (
+                           extra["bvh_nodes"], extra["triangles"], nj, int(sum(sizes) * 4 / 1e6))},
+            "e2e": e2e, "roofline": roof,
+            "cpu_baseline": None if not cpu else {
+                "value": cpu["mrays"], "unit": "Mrays/s", "cores": cpu["cores"], "kind": "port",
+                "sample": "oracle on every %dth pixel of every frame, all samples (%d pixels, %.1f s)" % (
+                    cpu_stride(args.workload, "baseline"), cpu["pixels"], cpu["seconds"])},
+            "clocks": clk_summary, "gpu_launches": acc.kernels, "extra": extra}
+    print(json.dumps(line), flush=True)
+    for c in ctxs:
+        c.close()
+    if dist:
+        dist.destroy_process_group()
 
 
 def main():
@@ -332,21 +477,19 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "heightfield"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="override the frame size (profiling)")
-    ap.add_argument("--spp", type=int, help="override samples per pixel (profiling)")
+    ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="heightfield: override the frame size")
+    ap.add_argument("--spp", type=int, help="heightfield: override samples per pixel")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8], help="BVH layout (0 = library default)")
     args = ap.parse_args()
     if args.frame:
-        CFG["width"], CFG["height"] = args.frame
+        HF["width"], HF["height"] = args.frame
     if args.spp:
-        CFG["spp"] = args.spp
-    if args.frame or args.spp:
-        global WORKLOAD
-        WORKLOAD = WORKLOAD.replace("1920x1080, 64 spp", "%dx%d, %d spp" % (CFG["width"], CFG["height"], CFG["spp"]))
+        HF["spp"] = args.spp
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus else 1)))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if "RANK" not in os.environ:
         world = 1

@@ -186,6 +186,21 @@ nova_b200_status nova_b200_render_noalloc(nova_b200_ctx *ctx, const nova_b200_fr
 nova_b200_status nova_b200_trace(nova_b200_ctx *ctx, uint64_t n, const float *orig_dev, const float *dir_dev,
                                  int32_t *prim_dev, float *t_dev, float *u_dev, float *v_dev);
 
+/* One shading event for each of n given hits, all buffers in DEVICE memory: the hit record
+ * (Embree fillHitStructure semantics, aggregate/api/embree/embree.cpp:360-412), the principled
+ * scatter (material/NovaMaterials.h:89-137) with Sobol dimensions 2 + 4 * bounce .. 5 + 4 * bounce of
+ * sample `index`, and the spawned ray (ray/Ray.h:22-27) -- the per-hit step of the path integrator.
+ * Inputs: ray origin / direction (3 floats each), the hit (global primitive, t, u, v, as returned by
+ * nova_b200_trace), the Sobol sample index and bounce per hit, the seed.  Outputs: the next ray's
+ * origin and direction (3 floats each), the path weight f * |cos| / pdf and the emission (3 floats
+ * each), valid = 1 (scattered), 0 (scatter failed: the path ends black) or -1 (prim or bounce out of
+ * range; nothing else written). */
+nova_b200_status nova_b200_scatter(nova_b200_ctx *ctx, uint64_t n, const float *orig_dev, const float *dir_dev,
+                                   const int32_t *prim_dev, const float *t_dev, const float *u_dev, const float *v_dev,
+                                   const uint32_t *index_dev, const int32_t *bounce_dev, uint32_t seed,
+                                   float *next_orig_dev, float *next_dir_dev, float *weight_dev, float *emissive_dev,
+                                   int32_t *valid_dev);
+
 /* Sobol + Owen samples (math_random.h:73-98 SobolGenerator::generate) for n (index, dimension)
  * pairs in device memory. */
 nova_b200_status nova_b200_sobol(nova_b200_ctx *ctx, uint64_t n, const uint32_t *index_dev, const uint32_t *dim_dev,

@@ -125,8 +125,8 @@ V3 texel_irradiance(const Src &src, float x, float y, float z, unsigned W, unsig
     float r[3];
     pgc3d(px, py, s, r);
     float phi = (float)(2 * PI_D * r[0]);
-    float theta = std::asin(std::sqrt(r[1]));
-    V3 c{std::sin(theta) * std::cos(phi), std::sin(theta) * std::sin(phi), std::cos(theta)};
+    float theta = asin_rn(std::sqrt(r[1]));
+    V3 c{sin_rn(theta) * cos_rn(phi), sin_rn(theta) * sin_rn(phi), cos_rn(theta)};
     c = c.x * tangent + c.y * bitangent + c.z * normal;
     float su, sv;
     to_uv(c.x, c.y, c.z, su, sv);
@@ -157,7 +157,7 @@ extern "C" int32_t orc_bake_irradiance(const float *src, int32_t src_w, int32_t 
         for (unsigned y = 0; y < H; y++) {
           float u = (float)((double)x / (double)W), v = (float)((double)y / (double)H);
           float phi = (float)(2 * PI_D * u), theta = (float)(PI_D * v);
-          float cz = std::cos(theta), cx = std::sin(theta) * std::cos(phi), cy = std::sin(theta) * std::sin(phi);
+          float cz = cos_rn(theta), cx = sin_rn(theta) * cos_rn(phi), cy = sin_rn(theta) * sin_rn(phi);
           V3 irr = texel_irradiance(s, cx, cy, cz, W, H, (unsigned)samples);
           size_t idx = ((size_t)y * W + x) * channels;
           out[idx] = irr.x;

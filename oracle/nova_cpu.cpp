@@ -294,8 +294,8 @@ static inline V3 hemisphere_cosine_sample(const float u[2]) {
       r = sy;
       theta = (float)M_PI_2 - (float)M_PI_4 * (sx / sy);
     }
-    px = r * std::cos(theta);
-    py = r * std::sin(theta);
+    px = r * cos_rn(theta);
+    py = r * sin_rn(theta);
   }
   float z = std::sqrt(std::max(0.f, 1 - px * px - py * py));
   return {px, py, z};
@@ -303,7 +303,7 @@ static inline V3 hemisphere_cosine_sample(const float u[2]) {
 }  // namespace bx
 
 /* Fresnel (BxDF_math.h:170-224) */
-static inline float pow5(float x) { return std::pow(x, 5.f); }
+static inline float pow5(float x) { return pow5_rn(x); } /* std::pow(x, 5.f), correctly rounded */
 static inline float schlick(float c, float F0) { return F0 + (1.f - F0) * pow5(1.f - c); }
 static inline Spec schlick(float c, Spec F0) { return F0 + (1.f - F0) * pow5(1.f - c); }
 static inline float fresnel_real(float etar, float ci, float &new_eta) {
@@ -370,7 +370,7 @@ struct VNDF {
     /* sample_uniform_disk_polar, BxDF_math.h:160-164 */
     float r = msqrt(uc[0]);
     float th = 2.f * M_PI * uc[1];
-    float px = r * std::cos(th), py = r * std::sin(th);
+    float px = r * cos_rn(th), py = r * sin_rn(th);
     float s = 0.5f * (1.f + wh.z);
     py = msqrt(1.f - sqr(px)) * (1.f - s) + s * py; /* math::lerp(x, y, a) = x*(1-a) + a*y */
     V3 nh = px * t + py * b + msqrt(std::fmax(0.f, 1.f - sqr(px) - sqr(py))) * wh;
@@ -733,11 +733,21 @@ constexpr unsigned kRRDimBase = 200;
 
 /* PathIntegrator::Li, integrator/Integrator.cpp:60-99 (recursive; DENAN per level; miss or
  * depth < 0 returns the environment without an occlusion test; failed scatter returns black). */
+/* Optional per-thread segment log (orc_sample_path): origin, direction, hit prim, t, u, v. */
+thread_local std::vector<float> *g_segment_log = nullptr;
+
 static V4 Li(PathCtx &c, const Ray &ray, int depth, int bounce, Spec beta) {
   const Scene &s = *c.s;
   c.segments++;
   c.traced++;
   Hit hit = trace(s, ray, &c.tc);
+  if (g_segment_log) {
+    int32_t p = hit.is_hit ? hit.prim : -1;
+    float pf;
+    std::memcpy(&pf, &p, 4);
+    const float rec[10] = {ray.o.x, ray.o.y, ray.o.z, ray.d.x, ray.d.y, ray.d.z, pf, hit.t, hit.u, hit.v};
+    g_segment_log->insert(g_segment_log->end(), rec, rec + 10);
+  }
   if (hit.is_hit && depth >= 0) {
     HitRecord hr = make_record(s, ray, hit);
     const Material &mat = s.materials[s.inst_mat[s.prims[hit.prim].inst]];
@@ -905,6 +915,62 @@ extern "C" void orc_camera_rays(void *h, const orc_options *opt, uint64_t n, con
     Ray r = camera_ray(s, px[i], opt->height - py[i], opt->width, opt->height, r0 * 0.0005f, r1 * 0.0005f);
     orig[3 * i] = r.o.x, orig[3 * i + 1] = r.o.y, orig[3 * i + 2] = r.o.z;
     dir[3 * i] = r.d.x, dir[3 * i + 1] = r.d.y, dir[3 * i + 2] = r.d.z;
+  }
+}
+
+/* The segments of one path (sample s of pixel (x, y)): 10 floats each (origin, direction, hit
+ * primitive as int32 bits or -1, t, u, v); returns the number of segments written (<= max_segments). */
+extern "C" int32_t orc_sample_path(void *h, const orc_options *opt, int32_t x, int32_t y, int32_t s, float *out,
+                                   int32_t max_segments, float *radiance) {
+  const Scene &sc = *static_cast<Scene *>(h);
+  PathCtx c{&sc, 0, 0, opt->seed, opt->rr_start, 0, 0, {}};
+  std::vector<float> log;
+  g_segment_log = &log;
+  V4 L = render_sample(c, *opt, x, y, s);
+  g_segment_log = nullptr;
+  if (radiance) radiance[0] = L.x, radiance[1] = L.y, radiance[2] = L.z;
+  const int32_t n = std::min<int32_t>(max_segments, (int32_t)(log.size() / 10));
+  std::copy(log.begin(), log.begin() + 10 * (size_t)n, out);
+  return n;
+}
+
+/* One shading event per given hit (the body of Li for one level): make_record + scatter with
+ * dimensions 2 + 4 * bounce .. + spawn.  valid: 1 scattered, 0 scatter failed, -1 bad input. */
+extern "C" void orc_scatter(void *h, uint64_t n, const float *o, const float *d, const int32_t *prim, const float *t,
+                            const float *u, const float *v, const uint32_t *index, const int32_t *bounce,
+                            uint32_t seed, float *out_o, float *out_d, float *weight, float *emissive,
+                            int32_t *valid) {
+  const Scene &s = *static_cast<Scene *>(h);
+  for (uint64_t i = 0; i < n; i++) {
+    if (prim[i] < 0 || (size_t)prim[i] >= s.prims.size() || bounce[i] < 0) {
+      valid[i] = -1;
+      continue;
+    }
+    Ray ray;
+    ray.o = {o[3 * i], o[3 * i + 1], o[3 * i + 2]};
+    ray.d = {d[3 * i], d[3 * i + 1], d[3 * i + 2]};
+    Hit hit;
+    hit.is_hit = true;
+    hit.prim = prim[i];
+    hit.t = t[i];
+    hit.u = u[i];
+    hit.v = v[i];
+    HitRecord hr = make_record(s, ray, hit);
+    const Material &mat = s.materials[s.inst_mat[s.prims[hit.prim].inst]];
+    unsigned dim = 2u + 4u * (unsigned)bounce[i];
+    Scatter sc;
+    const bool ok = scatter(s, ray, hr, mat, index[i], dim, seed, sc);
+    Ray nx = spawn(sc.lobe.wi, hr.ng, hr.position);
+    Spec w = sc.attenuation * sc.lobe.costheta / sc.lobe.pdf;
+    const float oo[3] = {nx.o.x, nx.o.y, nx.o.z}, dd[3] = {nx.d.x, nx.d.y, nx.d.z}, ww[3] = {w.x, w.y, w.z},
+                ee[3] = {sc.emissive.x, sc.emissive.y, sc.emissive.z};
+    for (int k = 0; k < 3; k++) {
+      out_o[3 * i + k] = oo[k];
+      out_d[3 * i + k] = dd[k];
+      weight[3 * i + k] = ww[k];
+      emissive[3 * i + k] = ee[k];
+    }
+    valid[i] = ok ? 1 : 0;
   }
 }
 

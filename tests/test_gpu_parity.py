@@ -239,3 +239,79 @@ def test_batch_equals_individual_renders(torch_cuda):
     finally:
         for c in ctxs:
             c.close()
+
+
+def test_scatter_bit_exact(ctx, oracle, torch_cuda):
+    """nova_b200_scatter (hit record + principled scatter + spawn) equals the oracle bit for bit on
+    the hits of oracle paths through a mixed Lambert / GGX conductor / GGX dielectric scene."""
+    from axomae_b200 import scenes
+    torch = torch_cuda
+    s = scenes.mixed_scene(30000, 48, 48, seed=11)
+    ctx.upload(s)
+    ctx.build()
+    osc = oracle.OracleScene(s)
+    W = H = 48
+    spp, depth = 8, 8
+    opt = oracle.options(W, H, spp, depth)
+    rng = np.random.default_rng(5)
+    rows, idx, bnc = [], [], []
+    for _ in range(1500):
+        x, y, smp = int(rng.integers(W)), int(rng.integers(H)), int(rng.integers(spp))
+        segs, _ = osc.sample_path(opt, x, y, smp)
+        for b, r in enumerate(segs):
+            if np.float32(r[6]).view(np.int32) >= 0 and b <= depth:
+                rows.append(r)
+                idx.append((x * H + y) * spp + smp)
+                bnc.append(b)
+    R = np.asarray(rows, np.float32)
+    n = R.shape[0]
+    prim = R[:, 6].copy().view(np.int32)
+    index = np.asarray(idx, np.uint32)
+    bounce = np.asarray(bnc, np.int32)
+    ref = osc.scatter(R[:, :3], R[:, 3:6], prim, R[:, 7], R[:, 8], R[:, 9], index, bounce)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ins = [T(R[:, :3]), T(R[:, 3:6]), T(prim), T(R[:, 7]), T(R[:, 8]), T(R[:, 9]), T(index.view(np.int32)), T(bounce)]
+    outs = [torch.zeros((n, 3), dtype=torch.float32, device="cuda") for _ in range(4)]
+    valid = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ctx.scatter(n, *[a.data_ptr() for a in ins], 0, *[a.data_ptr() for a in outs], valid.data_ptr())
+    dev = [a.cpu().numpy() for a in outs]
+    v_dev = valid.cpu().numpy()
+    assert np.array_equal(v_dev, ref[4])
+    ok = v_dev == 1
+    assert ok.sum() > 0.8 * n
+    for a, b in zip(dev, ref[:4]):
+        assert np.array_equal(a[ok].view(np.uint32), b[ok].view(np.uint32))
+
+
+def test_converged_4096spp(ctx, oracle):
+    """Converged image of the 64-sphere scene at 4096 spp: per-pixel relative RMSE <= 1e-3."""
+    from axomae_b200 import scenes
+    W = H = 24
+    s = scenes.spheres_scene(W, H)
+    ctx.upload(s)
+    ctx.build()
+    film, st = _render(ctx, s, W, H, 4096, 5)
+    ref, _ = oracle.OracleScene(s).render(oracle.options(W, H, 4096, 5))
+    err = rel_rmse(film, ref)
+    assert err <= REL_RMSE_TOL, err
+    assert st.paths == W * H * 4096
+
+
+@pytest.fixture(scope="module")
+def batch_jobs():
+    from axomae_b200 import scenes
+    return scenes.batch_jobs(32, seed=0)
+
+
+@pytest.mark.parametrize("job", [0, 7, 12, 30])
+def test_batch_workload_scene_matches_oracle(job, ctx, oracle, batch_jobs):
+    """Scenes of the 32-job batched workload (dielectric-heavy, depth up to 12) at 48 x 48 with the
+    job's spp and depth, against the oracle."""
+    j = batch_jobs[job]
+    W = H = 48
+    ctx.upload(j["scene"])
+    ctx.build()
+    film, _ = _render(ctx, j["scene"], W, H, j["spp"], j["depth"])
+    ref, _ = oracle.OracleScene(j["scene"]).render(oracle.options(W, H, j["spp"], j["depth"]))
+    err = rel_rmse(film, ref)
+    assert err <= REL_RMSE_TOL, err
