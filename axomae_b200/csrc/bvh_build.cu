@@ -5,13 +5,13 @@
  * build to the driver (aggregate/api/optix/host.cpp:440-480).  Here the build runs on the GPU,
  * top-down and breadth-first, with centroid binning:
  *
- *   large nodes (> kSmallTask primitives), one level per host iteration:
+ *   large nodes (> small_task primitives), one level per host iteration:
  *     k_init_level   reset per-node centroid bounds and bins
  *     k_cbounds      centroid bounds, one CTA per chunk of 4096 primitives, merged with atomics
  *     k_bin          centroid bins per axis in shared memory, merged into the node's global bins
  *     k_split        one CTA per node: SAH over bins*3 candidate planes, node allocation, children
  *     k_partition    primitive ids scattered to the children's ranges of the other id buffer
- *   small nodes (<= kSmallTask): k_build_small, one CTA per node builds its whole subtree with a
+ *   small nodes (<= small_task): k_build_small, one CTA per node builds its whole subtree with a
  *     CTA-local task stack, shared-memory bins and a stable block-scan partition.
  *
  * Leaves list their primitives in a contiguous range of `order`; each leaf's range is finally
@@ -33,7 +33,7 @@ namespace nb {
 namespace {
 
 constexpr int kMaxBins = 32;
-constexpr uint32_t kSmallTask = 4096;
+constexpr uint32_t kSmallTaskDefault = 256;
 constexpr uint32_t kChunk = 4096;
 constexpr int kMedianDepth = 40;
 constexpr int kBlock = 256;
@@ -77,6 +77,7 @@ struct Shared {
   unsigned *leaf_count;
   int *max_depth;
   int bins, max_leaf, hard_leaf;
+  uint32_t small_task;
   float cost_trav;
 };
 
@@ -157,7 +158,7 @@ __device__ void finish_leaf(const Shared &s, const Task &t) {
 }
 
 __device__ __forceinline__ void push_task(const Shared &s, const Task &t) {
-  if (t.end - t.begin > kSmallTask) {
+  if (t.end - t.begin > s.small_task) {
     unsigned i = atomicAdd(s.large_next_count, 1u);
     s.large_next[i] = t;
   } else {
@@ -653,7 +654,8 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
   const int nb = std::max(4, std::min(kMaxBins, p.bins > 0 ? p.bins : 16));
   const int hard_leaf = std::max(1, std::min(kHardLeaf, p.hard_leaf > 0 ? p.hard_leaf : kHardLeaf));
   const int max_leaf = std::max(1, std::min(hard_leaf, p.max_leaf > 0 ? p.max_leaf : 8));
-  const size_t max_large = n / kSmallTask + 2;
+  const uint32_t small_task = p.small_task >= 64 ? p.small_task : kSmallTaskDefault;
+  const size_t max_large = n / small_task + 2;
   const size_t max_small = n + 1;
   /* scratch */
   uint32_t *ids0 = nullptr, *ids1 = nullptr;
@@ -717,10 +719,11 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     sh.max_leaf = max_leaf;
     sh.hard_leaf = hard_leaf;
     sh.cost_trav = p.cost_trav > 0.f ? p.cost_trav : 1.0f;
+    sh.small_task = small_task;
 
     Task root{0u, n, -1, 0, 0, 0, {hscene[0], hscene[1], hscene[2]}, {hscene[3], hscene[4], hscene[5]}};
     std::vector<Task> level;
-    if (n > kSmallTask) {
+    if (n > small_task) {
       level.push_back(root);
     } else {
       NB_TRY(cudaMemcpyAsync(small, &root, sizeof(Task), cudaMemcpyHostToDevice, stream));

@@ -10,6 +10,7 @@ struct BvhBuildParams {
   int hard_leaf;    /* nodes with more primitives are always split (median when SAH finds no plane) */
   int bins;         /* SAH bins per axis (<= 32) */
   float cost_trav;  /* SAH cost of one inner-node visit relative to one triangle test */
+  uint32_t small_task; /* nodes of at most this many primitives are built whole by one CTA (0: default) */
 };
 
 struct BvhBuildResult {

@@ -66,25 +66,85 @@ bool is_identity(const float *m) {
   return true;
 }
 
-template <class T>
-nova_b200_status upload(nova_b200_ctx *c, const T *src, size_t n, T **dst) {
-  *dst = nullptr;
-  if (n == 0) return NOVA_B200_SUCCESS;
-  void *p = nullptr;
-  NB_CUDA(c, cudaMalloc(&p, sizeof(T) * n), "cudaMalloc(scene)");
-  c->scene_allocs.push_back(p);
-  c->scene_bytes += sizeof(T) * n;
-  NB_CUDA(c, cudaMemcpyAsync(p, src, sizeof(T) * n, cudaMemcpyHostToDevice, c->stream), "cudaMemcpy(scene)");
-  *dst = static_cast<T *>(p);
+/* Scene uploads go to one device arena per scene (one pool allocation instead of one cudaMalloc per
+ * texture / mesh / table; cudaMalloc and cudaFree synchronise the device).  Pieces up to kSmallPiece
+ * bytes are gathered in a pinned host buffer and copied with one transfer; larger ones are copied
+ * directly from the caller's memory. */
+constexpr size_t kSmallPiece = 1 << 16;
+
+struct Piece {
+  const void *src;
+  size_t bytes;
+  size_t off;   /* offset in its region */
+  bool temp;    /* region: temporary SoA staging (true) or the persistent arena */
+};
+
+struct UploadPlan {
+  std::vector<Piece> pieces;
+  size_t arena = 0, temp = 0;
+  static size_t align(size_t b) { return (b + 255) & ~(size_t)255; }
+  size_t add(const void *src, size_t bytes, bool temp_region = false) {
+    size_t &top = temp_region ? temp : arena;
+    const size_t off = top;
+    top += align(bytes);
+    pieces.push_back(Piece{src, bytes, off, temp_region});
+    return off;
+  }
+};
+
+nova_b200_status ensure_pinned_stage(nova_b200_ctx *c, size_t bytes) {
+  if (c->h_stage_bytes >= bytes) return NOVA_B200_SUCCESS;
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  c->h_stage = nullptr;
+  c->h_stage_bytes = 0;
+  const size_t want = std::max<size_t>(bytes, 1 << 20);
+  NB_CUDA(c, cudaMallocHost(&c->h_stage, want), "cudaMallocHost(upload staging)");
+  c->h_stage_bytes = want;
+  return NOVA_B200_SUCCESS;
+}
+
+/* Copies the plan's pieces: small ones through the pinned buffer (one transfer per region), large
+ * ones directly. */
+nova_b200_status copy_pieces(nova_b200_ctx *c, const UploadPlan &plan, char *arena, char *temp) {
+  size_t small = 0;
+  for (const Piece &p : plan.pieces)
+    if (p.bytes <= kSmallPiece) small += UploadPlan::align(p.bytes);
+  nova_b200_status st = ensure_pinned_stage(c, small);
+  if (st != NOVA_B200_SUCCESS) return st;
+  /* small pieces are packed per region in plan order; each region's packed pieces are contiguous
+   * neither on the host nor on the device in general, so runs of adjacent pieces are merged */
+  char *h = static_cast<char *>(c->h_stage);
+  size_t hoff = 0;
+  struct Run {
+    char *dst;
+    size_t hbegin, bytes;
+  };
+  std::vector<Run> runs;
+  for (const Piece &p : plan.pieces) {
+    char *dst = (p.temp ? temp : arena) + p.off;
+    if (p.bytes > kSmallPiece) {
+      NB_CUDA(c, cudaMemcpyAsync(dst, p.src, p.bytes, cudaMemcpyHostToDevice, c->stream), "upload(scene)");
+      continue;
+    }
+    std::memcpy(h + hoff, p.src, p.bytes);
+    const size_t step = UploadPlan::align(p.bytes);
+    if (!runs.empty() && runs.back().dst + runs.back().bytes == dst && runs.back().hbegin + runs.back().bytes == hoff)
+      runs.back().bytes += step;
+    else
+      runs.push_back(Run{dst, hoff, step});
+    hoff += step;
+  }
+  for (const Run &r : runs)
+    NB_CUDA(c, cudaMemcpyAsync(r.dst, h + r.hbegin, r.bytes, cudaMemcpyHostToDevice, c->stream), "upload(scene)");
   return NOVA_B200_SUCCESS;
 }
 
 void free_scene(nova_b200_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (void *p : c->scene_allocs) cudaFree(p);
-  c->scene_allocs.clear();
-  cudaFree(c->d_nodes);
-  cudaFree(c->d_tris);
+  if (c->d_arena) cudaFreeAsync(c->d_arena, c->stream);
+  if (c->d_nodes) cudaFreeAsync(c->d_nodes, c->stream);
+  if (c->d_tris) cudaFreeAsync(c->d_tris, c->stream);
+  c->d_arena = nullptr;
   c->d_nodes = nullptr;
   c->d_tris = nullptr;
   c->scene = nb::DevScene{};
@@ -203,6 +263,8 @@ nova_b200_status nova_b200_destroy(nova_b200_ctx *c) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;
   cudaSetDevice(c->device);
   free_scene(c);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
   cudaFree(c->d_sobol);
   cudaFree(c->d_acos);
   cudaFree(c->d_counters);
@@ -238,8 +300,10 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
   if (d->envmap < 0 || (uint32_t)d->envmap >= d->n_textures || !d->textures[d->envmap].f32_pixels ||
       d->textures[d->envmap].channels != 4)
     return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "environment map must be a 4-channel float texture%s");
-  /* textures */
+  UploadPlan plan;
+  /* textures: the device pointers are patched in once the arena exists */
   std::vector<nb::DevTexture> tex(d->n_textures);
+  std::vector<size_t> tex_off(d->n_textures);
   for (uint32_t i = 0; i < d->n_textures; i++) {
     const nova_b200_texture &t = d->textures[i];
     if ((!t.u8_pixels) == (!t.f32_pixels) || t.width < 2 || t.height < 2 || t.channels < 1 || t.channels > 4)
@@ -248,18 +312,8 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     o.w = t.width, o.h = t.height, o.ch = t.channels;
     o.is_rgba = t.is_rgba, o.invert_u = t.invert_u, o.invert_v = t.invert_v;
     const size_t px = (size_t)t.width * t.height;
-    nova_b200_status st;
-    if (t.u8_pixels) {
-      uint32_t *p;
-      if ((st = upload(c, t.u8_pixels, px, &p)) != NOVA_B200_SUCCESS) return st;
-      o.u8 = p;
-      o.f32 = nullptr;
-    } else {
-      float *p;
-      if ((st = upload(c, t.f32_pixels, px * t.channels, &p)) != NOVA_B200_SUCCESS) return st;
-      o.f32 = p;
-      o.u8 = nullptr;
-    }
+    tex_off[i] = t.u8_pixels ? plan.add(t.u8_pixels, px * sizeof(uint32_t))
+                             : plan.add(t.f32_pixels, px * t.channels * sizeof(float));
   }
   /* materials */
   std::vector<nb::DevMaterial> mats(d->n_materials);
@@ -276,39 +330,30 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     mats[i].anisotropy = m.anisotropy;
     emissive |= m.emissive >= 0;
   }
-  /* meshes */
+  /* meshes: indices to the arena, SoA attributes to the temporary staging region, interleaved
+   * into the arena's 64 B records by k_interleave */
   std::vector<nb::DevMesh> meshes(d->n_meshes);
+  struct MeshOffsets {
+    size_t idx, attr, v, n, t, b, uv;
+  };
+  std::vector<MeshOffsets> moff(d->n_meshes);
   for (uint32_t i = 0; i < d->n_meshes; i++) {
     const nova_b200_mesh &m = d->meshes[i];
     if (!m.vertices || !m.normals || !m.tangents || !m.bitangents || !m.uv || !m.indices || m.n_tris == 0)
       return fail(c, NOVA_B200_INVALID_ARGUMENT, "mesh needs vertices, normals, tangents, bitangents, uv, indices%s");
     for (uint64_t k = 0; k < 3ull * m.n_tris; k++)
       if (m.indices[k] >= m.n_verts) return fail(c, NOVA_B200_INVALID_ARGUMENT, "mesh index out of range%s");
-    nb::DevMesh &o = meshes[i];
-    o.n_verts = m.n_verts, o.n_tris = m.n_tris;
-    nova_b200_status st;
+    meshes[i].n_verts = m.n_verts, meshes[i].n_tris = m.n_tris;
     const size_t nv = m.n_verts;
-    uint32_t *q;
-    if ((st = upload(c, m.indices, 3ull * m.n_tris, &q))) return st;
-    o.idx = q;
-    /* attributes: SoA staging on the stream, interleaved into the persistent 64 B records */
-    void *attr = nullptr;
-    NB_CUDA(c, cudaMalloc(&attr, nv * 64), "cudaMalloc(attributes)");
-    c->scene_allocs.push_back(attr);
-    c->scene_bytes += nv * 64;
-    float *stage = nullptr;
-    NB_CUDA(c, cudaMallocAsync(&stage, nv * 14 * sizeof(float), c->stream), "cudaMalloc(staging)");
-    float *sv = stage, *sn = stage + 3 * nv, *st_ = stage + 6 * nv, *sb = stage + 9 * nv, *suv = stage + 12 * nv;
-    NB_CUDA(c, cudaMemcpyAsync(sv, m.vertices, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(vertices)");
-    NB_CUDA(c, cudaMemcpyAsync(sn, m.normals, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(normals)");
-    NB_CUDA(c, cudaMemcpyAsync(st_, m.tangents, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(tangents)");
-    NB_CUDA(c, cudaMemcpyAsync(sb, m.bitangents, 12 * nv, cudaMemcpyHostToDevice, c->stream), "upload(bitangents)");
-    NB_CUDA(c, cudaMemcpyAsync(suv, m.uv, 8 * nv, cudaMemcpyHostToDevice, c->stream), "upload(uv)");
-    k_interleave<<<(unsigned)((nv + 255) / 256), 256, 0, c->stream>>>(sv, sn, st_, sb, suv, (uint32_t)nv,
-                                                                      static_cast<float4 *>(attr));
-    NB_CUDA(c, cudaGetLastError(), "k_interleave");
-    NB_CUDA(c, cudaFreeAsync(stage, c->stream), "cudaFree(staging)");
-    o.attr = static_cast<const float4 *>(attr);
+    MeshOffsets &o = moff[i];
+    o.idx = plan.add(m.indices, 3ull * m.n_tris * sizeof(uint32_t));
+    o.attr = plan.arena;
+    plan.arena += UploadPlan::align(nv * 64);
+    o.v = plan.add(m.vertices, 12 * nv, true);
+    o.n = plan.add(m.normals, 12 * nv, true);
+    o.t = plan.add(m.tangents, 12 * nv, true);
+    o.b = plan.add(m.bitangents, 12 * nv, true);
+    o.uv = plan.add(m.uv, 8 * nv, true);
   }
   /* instances + primitive tables */
   c->h_instances.resize(d->n_instances);
@@ -343,22 +388,54 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     }
   }
   if (c->h_valid.empty()) return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "scene has no non-degenerate triangle%s");
-  nova_b200_status st;
-  nb::DevTexture *dt;
-  nb::DevMaterial *dm;
-  nb::DevMesh *dme;
-  nb::DevInstance *di;
-  uint32_t *dpi;
-  if ((st = upload(c, tex.data(), tex.size(), &dt))) return st;
-  if ((st = upload(c, mats.data(), mats.size(), &dm))) return st;
-  if ((st = upload(c, meshes.data(), meshes.size(), &dme))) return st;
-  if ((st = upload(c, c->h_instances.data(), c->h_instances.size(), &di))) return st;
-  if ((st = upload(c, prim_inst.data(), prim_inst.size(), &dpi))) return st;
-  c->scene.textures = dt;
-  c->scene.materials = dm;
-  c->scene.meshes = dme;
-  c->scene.instances = di;
-  c->scene.prim_inst = dpi;
+  const size_t off_mats = plan.add(mats.data(), mats.size() * sizeof(nb::DevMaterial));
+  const size_t off_inst = plan.add(c->h_instances.data(), c->h_instances.size() * sizeof(nb::DevInstance));
+  const size_t off_pi = plan.add(prim_inst.data(), prim_inst.size() * sizeof(uint32_t));
+  /* texture and mesh tables hold device pointers: reserve their space now, fill after allocation */
+  const size_t off_tex = plan.arena;
+  plan.arena += UploadPlan::align(tex.size() * sizeof(nb::DevTexture));
+  const size_t off_mesh = plan.arena;
+  plan.arena += UploadPlan::align(meshes.size() * sizeof(nb::DevMesh));
+
+  char *arena = nullptr, *temp = nullptr;
+  NB_CUDA(c, cudaMallocAsync(reinterpret_cast<void **>(&arena), plan.arena, c->stream), "cudaMalloc(scene)");
+  c->d_arena = arena;
+  c->scene_bytes = plan.arena;
+  NB_CUDA(c, cudaMallocAsync(reinterpret_cast<void **>(&temp), std::max<size_t>(plan.temp, 256), c->stream),
+          "cudaMalloc(staging)");
+  for (uint32_t i = 0; i < d->n_textures; i++) {
+    if (d->textures[i].u8_pixels)
+      tex[i].u8 = reinterpret_cast<const uint32_t *>(arena + tex_off[i]), tex[i].f32 = nullptr;
+    else
+      tex[i].f32 = reinterpret_cast<const float *>(arena + tex_off[i]), tex[i].u8 = nullptr;
+  }
+  for (uint32_t i = 0; i < d->n_meshes; i++) {
+    meshes[i].idx = reinterpret_cast<const uint32_t *>(arena + moff[i].idx);
+    meshes[i].attr = reinterpret_cast<const float4 *>(arena + moff[i].attr);
+  }
+  plan.pieces.push_back(Piece{tex.data(), tex.size() * sizeof(nb::DevTexture), off_tex, false});
+  plan.pieces.push_back(Piece{meshes.data(), meshes.size() * sizeof(nb::DevMesh), off_mesh, false});
+  nova_b200_status st = copy_pieces(c, plan, arena, temp);
+  if (st != NOVA_B200_SUCCESS) {
+    cudaFreeAsync(temp, c->stream);
+    return st;
+  }
+  for (uint32_t i = 0; i < d->n_meshes; i++) {
+    const uint32_t nv = d->meshes[i].n_verts;
+    const MeshOffsets &o = moff[i];
+    k_interleave<<<(nv + 255) / 256, 256, 0, c->stream>>>(
+        reinterpret_cast<const float *>(temp + o.v), reinterpret_cast<const float *>(temp + o.n),
+        reinterpret_cast<const float *>(temp + o.t), reinterpret_cast<const float *>(temp + o.b),
+        reinterpret_cast<const float *>(temp + o.uv), nv, reinterpret_cast<float4 *>(arena + o.attr));
+  }
+  const cudaError_t e_launch = cudaGetLastError();
+  cudaFreeAsync(temp, c->stream);
+  if (e_launch != cudaSuccess) return cuda_fail(c, e_launch, "k_interleave");
+  c->scene.textures = reinterpret_cast<const nb::DevTexture *>(arena + off_tex);
+  c->scene.materials = reinterpret_cast<const nb::DevMaterial *>(arena + off_mats);
+  c->scene.meshes = reinterpret_cast<const nb::DevMesh *>(arena + off_mesh);
+  c->scene.instances = reinterpret_cast<const nb::DevInstance *>(arena + off_inst);
+  c->scene.prim_inst = reinterpret_cast<const uint32_t *>(arena + off_pi);
   c->scene.sobol_dv = c->d_sobol;
   c->scene.acos_lut = c->d_acos;
   c->scene.envmap = d->envmap;
@@ -382,18 +459,21 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   p.hard_leaf = width == 8 ? nb::kWideLeafMax : 16;
   p.bins = opts && opts->bins > 0 ? opts->bins : 16;
   p.cost_trav = 1.0f;
+  p.small_task = opts && opts->small_subtree > 0 ? (uint32_t)opts->small_subtree : 0u;
+  if (opts && (opts->small_subtree < 0 || (opts->small_subtree > 0 && (opts->small_subtree < 64 || opts->small_subtree > 65536))))
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "small_subtree must be 0 or 64..65536%s");
   if (p.max_leaf > p.hard_leaf || p.bins < 4 || p.bins > 32)
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "max_leaf_size must be 1..16 (1..4 for width 8) and bins 4..32%s");
-  cudaFree(c->d_nodes);
-  cudaFree(c->d_tris);
+  if (c->d_nodes) cudaFreeAsync(c->d_nodes, c->stream);
+  if (c->d_tris) cudaFreeAsync(c->d_tris, c->stream);
   c->d_nodes = nullptr;
   c->d_tris = nullptr;
   c->bvh_ready = false;
   uint32_t *d_valid = nullptr, *d_order = nullptr;
   float4 *d_lo = nullptr, *d_hi = nullptr;
   const size_t max_nodes = std::max<size_t>(2 * (size_t)n, 2);
-  NB_CUDA(c, cudaMalloc(&c->d_nodes, sizeof(float4) * 4 * max_nodes), "cudaMalloc(nodes)");
-  NB_CUDA(c, cudaMalloc(&c->d_tris, sizeof(float4) * 3 * (size_t)n), "cudaMalloc(tris)");
+  NB_CUDA(c, cudaMallocAsync(&c->d_nodes, sizeof(float4) * 4 * max_nodes, c->stream), "cudaMalloc(nodes)");
+  NB_CUDA(c, cudaMallocAsync(&c->d_tris, sizeof(float4) * 3 * (size_t)n, c->stream), "cudaMalloc(tris)");
   NB_CUDA(c, cudaMemsetAsync(c->d_nodes, 0, sizeof(float4) * 4 * max_nodes, c->stream), "memset(nodes)");
   NB_CUDA(c, cudaMallocAsync(&d_valid, sizeof(uint32_t) * n, c->stream), "cudaMalloc(valid)");
   NB_CUDA(c, cudaMallocAsync(&d_order, sizeof(uint32_t) * n, c->stream), "cudaMalloc(order)");
@@ -419,22 +499,23 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
     return fail(c, NOVA_B200_RENDERER_EXCEPTION, "BVH validation failed%s");
   if (width == 8) {
     float4 *wnodes = nullptr, *wtris = nullptr;
-    NB_CUDA(c, cudaMalloc(&wnodes, sizeof(float4) * 5 * ((size_t)r.n_nodes + 1)), "cudaMalloc(wide nodes)");
-    cudaError_t we = cudaMalloc(&wtris, sizeof(float4) * 3 * (size_t)n);
+    NB_CUDA(c, cudaMallocAsync(&wnodes, sizeof(float4) * 5 * ((size_t)r.n_nodes + 1), c->stream),
+            "cudaMalloc(wide nodes)");
+    cudaError_t we = cudaMallocAsync(&wtris, sizeof(float4) * 3 * (size_t)n, c->stream);
     if (we != cudaSuccess) {
-      cudaFree(wnodes);
+      cudaFreeAsync(wnodes, c->stream);
       return cuda_fail(c, we, "cudaMalloc(wide triangles)");
     }
     nb::WideBuildResult wr{};
     we = nb::build_wide_bvh(c->d_nodes, r.n_nodes, c->d_tris, n, wnodes, wtris, c->stream, &wr);
     if (we != cudaSuccess || wr.depth >= nb::kWideStack) {
-      cudaFree(wnodes);
-      cudaFree(wtris);
+      cudaFreeAsync(wnodes, c->stream);
+      cudaFreeAsync(wtris, c->stream);
       if (we != cudaSuccess) return cuda_fail(c, we, "build_wide_bvh");
       return fail(c, NOVA_B200_RENDERER_EXCEPTION, "wide BVH deeper than the traversal stack%s");
     }
-    cudaFree(c->d_nodes);
-    cudaFree(c->d_tris);
+    cudaFreeAsync(c->d_nodes, c->stream);
+    cudaFreeAsync(c->d_tris, c->stream);
     c->d_nodes = wnodes;
     c->d_tris = wtris;
     r.n_nodes = wr.n_nodes;

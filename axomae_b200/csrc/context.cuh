@@ -18,7 +18,9 @@ struct nova_b200_ctx {
   float *d_acos = nullptr;
 
   /* scene */
-  std::vector<void *> scene_allocs;
+  void *d_arena = nullptr;      /* every scene buffer (textures, meshes, tables) in one pool allocation */
+  void *h_stage = nullptr;      /* pinned upload staging for small pieces */
+  size_t h_stage_bytes = 0;
   nb::DevScene scene{};
   std::vector<nb::DevInstance> h_instances;
   std::vector<uint32_t> h_valid; /* global primitive ids that can be hit */

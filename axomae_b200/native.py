@@ -58,7 +58,8 @@ class SceneDesc(C.Structure):
 
 
 class BvhOptions(C.Structure):
-    _fields_ = [("max_leaf_size", C.c_int32), ("bins", C.c_int32), ("width", C.c_int32)]
+    _fields_ = [("max_leaf_size", C.c_int32), ("bins", C.c_int32), ("width", C.c_int32),
+                ("small_subtree", C.c_int32)]
 
 
 class Frame(C.Structure):
@@ -121,40 +122,79 @@ def _p(a, t):
     return a.ctypes.data_as(t)
 
 
-def make_scene_desc(scene: dict):
-    """Builds the C scene descriptor for a scene dictionary (axomae_b200.scenes layout).
-    Returns (desc, keepalive) — keep `keepalive` referenced until the upload call returns."""
-    keep = []
-    meshes = (Mesh * len(scene["meshes"]))()
-    for i, m in enumerate(scene["meshes"]):
-        arrs = [np.ascontiguousarray(m[k], np.float32) for k in ("vertices", "normals", "tangents", "bitangents", "uv")]
-        idx = np.ascontiguousarray(m["indices"], np.uint32)
-        keep += arrs + [idx]
-        meshes[i] = Mesh(*[_p(a, f32p) for a in arrs], _p(idx, u32p), arrs[0].size // 3, idx.size // 3)
-    insts = (Instance * len(scene["instances"]))()
-    for i, x in enumerate(scene["instances"]):
-        insts[i] = Instance(x["mesh"], x["material"], (C.c_float * 16)(*np.asarray(x["m"], np.float32).reshape(16)),
-                            (C.c_float * 16)(*np.asarray(x["inv"], np.float32).reshape(16)),
-                            (C.c_float * 9)(*np.asarray(x["n"], np.float32).reshape(9)))
-    mats = (Material * len(scene["materials"]))()
-    for i, m in enumerate(scene["materials"]):
-        mats[i] = Material(m.get("albedo", -1), m.get("metallic", -1), m.get("normalmap", -1), m.get("emissive", -1),
-                           (C.c_float * 3)(*m.get("eta", (0, 0, 0))), (C.c_float * 3)(*m.get("k", (0, 0, 0))),
-                           m.get("anisotropy", 0.0))
-    texs = (Texture * len(scene["textures"]))()
-    for i, t in enumerate(scene["textures"]):
-        if t["format"] == "u8":
-            px = np.ascontiguousarray(t["pixels"], np.uint32)
-            texs[i] = Texture(_p(px, u32p), None, t["width"], t["height"], t.get("channels", 4), int(t.get("is_rgba", 1)),
-                              int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+def _np_dtype(struct):
+    """numpy dtype with the layout of a ctypes Structure (pointer fields as uint64 addresses)."""
+    names, formats, offsets = [], [], []
+    for name, ctype in struct._fields_:
+        names.append(name)
+        offsets.append(getattr(struct, name).offset)
+        if issubclass(ctype, C._Pointer):
+            formats.append(np.uint64)
+        elif issubclass(ctype, C.Array):
+            formats.append((np.dtype(ctype._type_), ctype._length_))
         else:
-            px = np.ascontiguousarray(t["pixels"], np.float32)
-            texs[i] = Texture(None, _p(px, f32p), t["width"], t["height"], t.get("channels", 4), int(t.get("is_rgba", 1)),
-                              int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+            formats.append(np.dtype(ctype))
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": C.sizeof(struct)})
+
+
+def _addr(a) -> int:
+    return a.ctypes.data
+
+
+def make_scene_desc(scene: dict):
+    """Builds the C scene descriptor for a scene dictionary (axomae_b200.scenes layout), filling the
+    descriptor tables as numpy records with the C layout.  Returns (desc, keepalive) — keep
+    `keepalive` referenced until the upload call returns."""
+    keep = []
+    ms = scene["meshes"]
+    mt = np.zeros(len(ms), _np_dtype(Mesh))
+    for i, m in enumerate(ms):
+        for k in ("vertices", "normals", "tangents", "bitangents", "uv"):
+            a = m[k]
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
+                a = np.ascontiguousarray(a, np.float32)
+            keep.append(a)
+            mt[k][i] = _addr(a)
+        idx = m["indices"]
+        if not (isinstance(idx, np.ndarray) and idx.dtype == np.uint32 and idx.flags.c_contiguous):
+            idx = np.ascontiguousarray(idx, np.uint32)
+        keep.append(idx)
+        mt["indices"][i] = _addr(idx)
+        mt["n_verts"][i] = np.asarray(m["vertices"]).size // 3
+        mt["n_tris"][i] = idx.size // 3
+    xs = scene["instances"]
+    it = np.zeros(len(xs), _np_dtype(Instance))
+    it["mesh"] = [x["mesh"] for x in xs]
+    it["material"] = [x["material"] for x in xs]
+    it["m"] = np.asarray([x["m"] for x in xs], np.float32).reshape(-1, 16)
+    it["inv"] = np.asarray([x["inv"] for x in xs], np.float32).reshape(-1, 16)
+    it["n"] = np.asarray([x["n"] for x in xs], np.float32).reshape(-1, 9)
+    mats = scene["materials"]
+    mat = np.zeros(len(mats), _np_dtype(Material))
+    for k in ("albedo", "metallic", "normalmap", "emissive"):
+        mat[k] = [m.get(k, -1) for m in mats]
+    mat["eta"] = np.asarray([m.get("eta", (0, 0, 0)) for m in mats], np.float32).reshape(-1, 3)
+    mat["k"] = np.asarray([m.get("k", (0, 0, 0)) for m in mats], np.float32).reshape(-1, 3)
+    mat["anisotropy"] = [m.get("anisotropy", 0.0) for m in mats]
+    ts = scene["textures"]
+    tt = np.zeros(len(ts), _np_dtype(Texture))
+    for i, t in enumerate(ts):
+        want = np.uint32 if t["format"] == "u8" else np.float32
+        px = t["pixels"]
+        if not (isinstance(px, np.ndarray) and px.dtype == want and px.flags.c_contiguous):
+            px = np.ascontiguousarray(px, want)
         keep.append(px)
-    desc = SceneDesc(meshes, len(scene["meshes"]), insts, len(scene["instances"]), mats, len(scene["materials"]), texs,
-                     len(scene["textures"]), scene["envmap"])
-    keep += [meshes, insts, mats, texs]
+        tt["u8_pixels" if t["format"] == "u8" else "f32_pixels"][i] = _addr(px)
+    tt["width"] = [t["width"] for t in ts]
+    tt["height"] = [t["height"] for t in ts]
+    tt["channels"] = [t.get("channels", 4) for t in ts]
+    tt["is_rgba"] = [int(t.get("is_rgba", 1)) for t in ts]
+    tt["invert_u"] = [int(t.get("invert_u", 0)) for t in ts]
+    tt["invert_v"] = [int(t.get("invert_v", 0)) for t in ts]
+    keep += [mt, it, mat, tt]
+    desc = SceneDesc(C.cast(_addr(mt), C.POINTER(Mesh)), len(ms), C.cast(_addr(it), C.POINTER(Instance)), len(xs),
+                     C.cast(_addr(mat), C.POINTER(Material)), len(mats), C.cast(_addr(tt), C.POINTER(Texture)),
+                     len(ts), scene["envmap"])
     return desc, keep
 
 
@@ -215,8 +255,8 @@ class Context:
         self._check(lib().nova_b200_upload_scene(self.h, C.byref(desc)))
         del keep
 
-    def build(self, max_leaf=0, bins=0, width=0):
-        self._check(lib().nova_b200_build_bvh(self.h, C.byref(BvhOptions(max_leaf, bins, width))))
+    def build(self, max_leaf=0, bins=0, width=0, small_subtree=0):
+        self._check(lib().nova_b200_build_bvh(self.h, C.byref(BvhOptions(max_leaf, bins, width, small_subtree))))
 
     def info(self) -> dict:
         vals = [C.c_uint64() for _ in range(5)]

@@ -111,6 +111,9 @@ typedef struct {
   int32_t max_leaf_size; /* 1..16 (1..4 for width 8); 0 = default (8, or 4 for width 8) */
   int32_t bins;          /* SAH bins per axis, 4..32; 0 = default (16) */
   int32_t width;         /* 2: binary BVH (default, fastest measured); 8: compressed 8-wide BVH; 0 = 2 */
+  int32_t small_subtree; /* nodes of at most this many triangles are built whole by one thread block
+                            (64..65536; 0 = default 256); a build-speed knob, the tree is the same
+                            kind either way */
 } nova_b200_bvh_options;
 
 /* One render call.  Samples [sample_begin, sample_begin + sample_count) of every pixel are traced and
