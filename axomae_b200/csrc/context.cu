@@ -272,11 +272,12 @@ nova_b200_status nova_b200_destroy(nova_b200_ctx *c) {
   cudaFree(c->d_queue);
   cudaFree(c->d_radiance);
   cudaFree(c->d_film_out);
-  cudaFree(c->d_jobs);
   cudaFree(c->d_wave);
-  if (c->h_jobs) cudaFreeHost(c->h_jobs);
   if (c->h_wave) cudaFreeHost(c->h_wave);
-  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  for (cudaGraphExec_t g : c->graph_exec)
+    if (g) cudaGraphExecDestroy(g);
+  for (cudaEvent_t e : c->ev_done)
+    if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : c->ev_wave)
     if (e) cudaEventDestroy(e);
   if (c->h_counters) cudaFreeHost(c->h_counters);

@@ -52,11 +52,12 @@ struct nova_b200_ctx {
   size_t film_out_cap = 0;
 
   /* device-driven wave loop (integrator.cu) */
-  void *d_jobs = nullptr, *h_jobs = nullptr; /* job table, device copy and pinned staging */
-  void *d_wave = nullptr, *h_wave = nullptr; /* wave counters, device copy and pinned read-back */
-  cudaEvent_t ev_wave[24] = {};
-  cudaGraphExec_t graph_exec = nullptr;
-  int graph_width = 0;
+  void *d_wave = nullptr, *h_wave = nullptr; /* wave counters: device copy; pinned read-back slots 0, 1 + upload slot 2 */
+  cudaEvent_t ev_wave[24] = {};              /* per pipeline slot: start, trace end, shade end of each wave */
+  cudaEvent_t ev_done[2] = {};               /* per pipeline slot: the slot's counters are in host memory */
+  cudaGraphExec_t graph_exec[2] = {};        /* batch chunks: the wave group of each pipeline slot */
+  std::vector<char> graph_key;               /* job table, launch shape and width of the graphs */
+  nova_b200_tuning tuning{};                 /* launch parameters (zeros: defaults) */
 };
 
 namespace nbctx {

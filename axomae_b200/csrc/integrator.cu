@@ -16,25 +16,31 @@
  *              sample order and writes sum / samples (writeFramebuffer, api/engine.cpp:351-363)
  *
  * Jobs: every path carries its job index (a frame of one context: scene, BVH, camera, sample
- * range) and every kernel reads the job table, so a batch of frames of different scenes runs as
- * one wavefront.  A single render is a batch of one.  The per-path arithmetic does not depend on
- * the batch, and each pixel's samples are added in sample order, so a frame rendered in a batch
- * equals the same frame rendered alone, bit for bit.
+ * range) and every kernel reads the chunk's job table, so a batch of frames of different scenes
+ * runs as one wavefront.  A single render is a batch of one.  The table travels in the kernel
+ * parameter space (__grid_constant__, read through the constant cache): one Job for a single
+ * frame, up to kParamJobs for a batch chunk.  The per-path arithmetic does not depend on the batch,
+ * and each pixel's samples are added in sample order, so a frame rendered in a batch equals the
+ * same frame rendered alone, bit for bit.
  *
  * Wave loop: the counters (active paths, next path, hits, survivors) live on the device and the
- * kernels read device-resident counts, so the host never waits between waves; it enqueues four
- * waves at a time and checks the device's "done" flag after each group.  A chunk of one frame
- * passes its job by value as a kernel parameter and launches directly; a batch chunk reads the job
- * table from device memory and replays the four waves from a CUDA graph captured once (event
- * record nodes around each trace and shade kernel time them).
+ * kernels read device-resident counts, so the host never waits between waves.  Waves are enqueued
+ * in groups of four, two groups in flight: while the GPU runs one group the host reads the
+ * previous group's counters (pinned memory, event-synchronised) and enqueues the next, so the GPU
+ * does not wait for the host; a group issued after the last path finished finds empty queues and
+ * returns at once.  A single-frame chunk launches its kernels directly; a batch chunk replays each
+ * slot's group from a CUDA graph (captured once per job table, with event-record nodes timing
+ * every trace and shade kernel).
  *
  * The recursive estimator e_0 + c_0 (e_1 + c_1 (... env)) is evaluated forward as
  * sum_k beta_k e_k + beta_K env with beta_k = c_0 ... c_{k-1}; a path whose result is not finite
- * contributes 0 (DENAN, Integrator.cpp:92).  Path state: origin + path id, direction + bounce +
- * job, throughput (3 x 16 B); hits 16 B + 4 B slot; per-path radiance 16 B, written once.
+ * contributes 0 (DENAN, Integrator.cpp:92).  Path state: origin + radiance slot, direction + bounce +
+ * job, throughput + Sobol sample index (3 x 16 B); hits 16 B + 4 B slot; per-path radiance 16 B,
+ * written once.
  */
 #include <algorithm>
 #include <cfloat>
+#include <cstring>
 #include <vector>
 
 #include "context.cuh"
@@ -45,12 +51,11 @@ namespace {
 
 using namespace nb;
 
-constexpr uint32_t kQueueCap = 1u << 22;
+constexpr uint32_t kQueueCapDefault = 1u << 23; /* rays per wave unless tuned */
 constexpr size_t kRadianceCapBytes = 4ull << 30;
 constexpr unsigned kRRDimBase = 200; /* Russian roulette decisions use Sobol dimension 200 + bounce */
 constexpr int kMaxDepth = 48;        /* 2 + 4 (depth + 1) Sobol dimensions must stay below 200 */
 constexpr int kWavesPerGraph = 4;    /* even: the queues end each graph launch where they started */
-constexpr uint32_t kMaxJobs = 4096;
 
 struct RenderParams {
   int32_t W, H;
@@ -62,6 +67,7 @@ struct RenderParams {
   uint32_t seed;
   int32_t rr_start;
   float inv_P[16], inv_V[16];
+  uint32_t tile_w, tile_h; /* consecutive paths walk tile_w x tile_h pixel tiles (0: image rows) */
 };
 
 struct Job {
@@ -79,9 +85,36 @@ struct WaveCounters {
   uint32_t hit_count, out_count;
   uint32_t done;
   uint32_t waves; /* waves that did work */
-  uint32_t n_jobs;
   unsigned long long traced;
 };
+
+/* The chunk's job table as a kernel parameter. */
+struct OneJob {
+  Job j;
+  __device__ __forceinline__ const Job &at(uint32_t) const { return j; }
+  __device__ __forceinline__ uint32_t find(uint32_t) const { return 0u; }
+};
+
+constexpr uint32_t kParamJobs = 104;
+
+struct ManyJobs {
+  uint32_t n;
+  Job j[kParamJobs];
+  __device__ __forceinline__ const Job &at(uint32_t k) const { return j[k]; }
+  /* the last job whose first path id is <= g */
+  __device__ __forceinline__ uint32_t find(uint32_t g) const {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (j[mid].path_begin <= g)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    return lo;
+  }
+};
+static_assert(sizeof(ManyJobs) + 256 <= 32764, "a batch job table must fit the 32 KB kernel parameter space");
 
 struct Queue {
   float4 *o, *d, *beta;
@@ -91,54 +124,48 @@ __device__ __forceinline__ uint32_t wave_new(const WaveCounters &wc) {
   return min(wc.cap - wc.n_active, wc.total - wc.next);
 }
 
-__device__ __forceinline__ uint32_t job_of_path(const Job *jobs, uint32_t n_jobs, uint32_t g) {
-  uint32_t lo = 0, hi = n_jobs; /* last job with path_begin <= g */
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (jobs[mid].path_begin <= g)
-      lo = mid;
-    else
-      hi = mid;
+/* The q-th pixel a frame's paths visit: row-major, or tile_w x tile_h tiles in row-major tile
+ * order (partial tiles at the right and bottom edges), so a warp's primary rays cover a compact
+ * patch of the image. */
+__device__ __forceinline__ void tile_pixel(const RenderParams &rp, uint32_t q, uint32_t &x, uint32_t &y) {
+  const uint32_t W = (uint32_t)rp.W, H = (uint32_t)rp.H;
+  if (rp.tile_w == 0) {
+    y = q / W;
+    x = q - y * W;
+    return;
   }
-  return lo;
+  const uint32_t tw = rp.tile_w, th = rp.tile_h;
+  const uint32_t ty = q / (W * th), r = q - ty * W * th;
+  const uint32_t h_r = min(th, H - ty * th);
+  const uint32_t tx = r / (tw * h_r), r2 = r - tx * tw * h_r;
+  const uint32_t w_c = min(tw, W - tx * tw);
+  const uint32_t ly = r2 / w_c;
+  x = tx * tw + (r2 - ly * w_c);
+  y = ty * th + ly;
 }
 
-/* A chunk of one frame passes its job by value (kernel parameter space); a batch chunk reads the
- * job table in global memory. */
-template <bool SINGLE>
-__device__ __forceinline__ const Job &job_at(const Job &j0, const Job *jobs, uint32_t k) {
-  if constexpr (SINGLE)
-    return j0;
-  else
-    return jobs[k];
-}
-
-__device__ __forceinline__ uint32_t sample_index(const RenderParams &rp, uint32_t p) {
-  const uint32_t s_local = p / rp.NP, pix = p - s_local * rp.NP;
-  const uint32_t y = pix / (uint32_t)rp.W, x = pix - y * (uint32_t)rp.W;
-  return ((uint32_t)x * (uint32_t)rp.H + y) * rp.spp_total + (rp.begin + s_local);
-}
-
-template <bool SINGLE>
-__global__ void __launch_bounds__(256) k_refill(Queue q, const WaveCounters *wcp, const Job *jobs, const Job j0,
-                                                float4 *L) {
+template <class JS>
+__global__ void __launch_bounds__(256) k_refill(Queue q, const WaveCounters *wcp, float4 *L,
+                                                const __grid_constant__ JS js) {
   const WaveCounters wc = *wcp;
-  const uint32_t n_jobs = wc.n_jobs;
   const uint32_t n_new = wave_new(wc);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
     const uint32_t g = wc.next + i;
-    const uint32_t job = SINGLE ? 0u : job_of_path(jobs, n_jobs, g);
-    const Job &J = job_at<SINGLE>(j0, jobs, job);
+    const uint32_t job = js.find(g);
+    const Job &J = js.at(job);
     const RenderParams &rp = J.rp;
     const uint32_t p = g - J.path_begin;
-    const uint32_t s_local = p / rp.NP, pix = p - s_local * rp.NP;
-    const int y = (int)(pix / (uint32_t)rp.W), x = (int)(pix - (uint32_t)y * (uint32_t)rp.W);
+    const uint32_t s_local = p / rp.NP, q_pix = p - s_local * rp.NP;
+    uint32_t x, y;
+    tile_pixel(rp, q_pix, x, y);
+    /* the radiance slot stays keyed by the row-major pixel, whatever order paths start in */
+    const uint32_t rslot = J.path_begin + s_local * rp.NP + y * (uint32_t)rp.W + x;
     const uint32_t index = ((uint32_t)x * (uint32_t)rp.H + (uint32_t)y) * rp.spp_total + (rp.begin + s_local);
     const float r0 = sobol_sample(J.sc.sobol_dv, index, 0, rp.seed);
     const float r1 = sobol_sample(J.sc.sobol_dv, index, 1, rp.seed);
     const float dx = r0 * 0.0005f, dy = r1 * 0.0005f; /* RAND_DX / RAND_DY, Integrator.h:54-55 */
-    const int ys = rp.H - y;                          /* screen row, Integrator.h:84 */
-    const float ndc_x = (float)(2 * x - rp.W) / (float)rp.W;
+    const int ys = rp.H - (int)y;                     /* screen row, Integrator.h:84 */
+    const float ndc_x = (float)(2 * (int)x - rp.W) / (float)rp.W;
     const float ndc_y = (float)(rp.H - 2 * ys) / (float)rp.H;
     const float nx = ndc_x + dx, ny = ndc_y + dy;
     const M4 iP = m4_load(rp.inv_P), iV = m4_load(rp.inv_V);
@@ -148,10 +175,10 @@ __global__ void __launch_bounds__(256) k_refill(Queue q, const WaveCounters *wcp
     V4 d = mul(iP, V4{nx, ny, -1.f, 0.f});
     d = normalize(mul(iV, V4{d.x, d.y, -1.f, 0.f}));
     const uint32_t slot = wc.n_active + i;
-    q.o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(g));
+    q.o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(rslot));
     q.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(job << 8));
-    q.beta[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
-    if (J.sc.has_emissive) L[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    q.beta[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(index));
+    if (J.sc.has_emissive) L[rslot] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
@@ -187,9 +214,9 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
 /* Closest hit of every queued ray.  A miss finishes its path here (environment lookup,
  * Integrator.cpp:94-98); hits are appended to a compact hit list so the shading kernel only runs
  * on rays that hit. */
-template <int WIDTH, bool SINGLE>
+template <int WIDTH, class JS>
 __global__ void __launch_bounds__(128) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
-                                               const Job *jobs, const Job j0) {
+                                               const __grid_constant__ JS js) {
   const uint32_t n = wcp->n_active + wave_new(*wcp);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if ((i & ~31u) >= n) return; /* whole warps leave together (the append below is a warp ballot) */
@@ -198,7 +225,7 @@ __global__ void __launch_bounds__(128) k_trace(Queue q, WaveCounters *wcp, float
     TraceResult r{-1, 0.f, 0.f, 0.f};
     if (i < n) {
       const float4 o = q.o[i], d = q.d[i];
-      const DevScene &sc = job_at<SINGLE>(j0, jobs, __float_as_uint(d.w) >> 8).sc;
+      const DevScene &sc = js.at(__float_as_uint(d.w) >> 8).sc;
       r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
       if (r.prim < 0) {
         const float4 b4 = q.beta[i];
@@ -218,9 +245,9 @@ __global__ void __launch_bounds__(128) k_trace(Queue q, WaveCounters *wcp, float
   }
 }
 
-template <bool SINGLE>
-__global__ void __launch_bounds__(128) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
-                                               const uint32_t *hit_slot, float4 *L, const Job *jobs, const Job j0) {
+template <class JS>
+__global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
+                                               const uint32_t *hit_slot, float4 *L, const __grid_constant__ JS js) {
   const uint32_t n = wcp->hit_count;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if ((i & ~31u) >= n) return;
@@ -233,10 +260,10 @@ __global__ void __launch_bounds__(128) k_shade(Queue in, Queue out, WaveCounters
       const uint32_t g = __float_as_uint(o4.w);
       const uint32_t tag = __float_as_uint(d4.w);
       const int bounce = (int)(tag & 0xffu);
-      const Job &J = job_at<SINGLE>(j0, jobs, tag >> 8);
+      const Job &J = js.at(tag >> 8);
       const DevScene &sc = J.sc;
       const RenderParams &rp = J.rp;
-      const uint32_t index = sample_index(rp, g - J.path_begin);
+      const uint32_t index = __float_as_uint(b4.w); /* the path's Sobol index, set by k_refill */
       const V3 ro{o4.x, o4.y, o4.z}, rd{d4.x, d4.y, d4.z};
       V3 beta{b4.x, b4.y, b4.z};
       const int prim = __float_as_int(h.w);
@@ -282,7 +309,7 @@ __global__ void __launch_bounds__(128) k_shade(Queue in, Queue out, WaveCounters
             enq = true;
             no = make_float4(no3.x, no3.y, no3.z, o4.w);
             nd = make_float4(nd3.x, nd3.y, nd3.z, __uint_as_float(tag + 1u));
-            nbeta = make_float4(beta.x, beta.y, beta.z, 0.f);
+            nbeta = make_float4(beta.x, beta.y, beta.z, b4.w);
           }
         }
       }
@@ -419,27 +446,33 @@ nova_b200_status ensure_wave_buffers(nova_b200_ctx *c, uint32_t cap, size_t radi
     c->radiance_cap = radiance;
     changed = true;
   }
-  if (!c->d_jobs) {
-    NB_CUDA(c, cudaMalloc(&c->d_jobs, sizeof(Job) * kMaxJobs), "cudaMalloc(jobs)");
+  if (!c->d_wave) {
     NB_CUDA(c, cudaMalloc(&c->d_wave, sizeof(WaveCounters)), "cudaMalloc(wave counters)");
-    NB_CUDA(c, cudaMallocHost(&c->h_wave, sizeof(WaveCounters)), "cudaMallocHost(wave counters)");
-    NB_CUDA(c, cudaMallocHost(&c->h_jobs, sizeof(Job) * kMaxJobs), "cudaMallocHost(jobs)");
-    for (int k = 0; k < 3 * kWavesPerGraph; k++) NB_CUDA(c, cudaEventCreate(&c->ev_wave[k]), "cudaEventCreate");
+    NB_CUDA(c, cudaMallocHost(&c->h_wave, 3 * sizeof(WaveCounters)), "cudaMallocHost(wave counters)");
+    for (int k = 0; k < 2 * 3 * kWavesPerGraph; k++) NB_CUDA(c, cudaEventCreate(&c->ev_wave[k]), "cudaEventCreate");
+    for (int k = 0; k < 2; k++)
+      NB_CUDA(c, cudaEventCreateWithFlags(&c->ev_done[k], cudaEventDisableTiming), "cudaEventCreate");
     changed = true;
   }
-  if (changed && c->graph_exec) {
-    cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
+  if (changed) {
+    for (cudaGraphExec_t &g : c->graph_exec)
+      if (g) cudaGraphExecDestroy(g), g = nullptr;
+    c->graph_key.clear();
   }
   return NOVA_B200_SUCCESS;
 }
+
+/* Launch shape of one render: rays per wave and the trace / shade block sizes. */
+struct LaunchShape {
+  uint32_t cap;
+  uint32_t trace_block, shade_block;
+};
 
 struct WaveBuffers {
   Queue qa, qb;
   float4 *hits;
   uint32_t *hit_slot;
   WaveCounters *wc;
-  const Job *jobs;
 };
 
 WaveBuffers wave_buffers(nova_b200_ctx *c) {
@@ -451,67 +484,80 @@ WaveBuffers wave_buffers(nova_b200_ctx *c) {
   b.hits = base + 6 * (size_t)cap;
   b.hit_slot = reinterpret_cast<uint32_t *>(base + 7 * (size_t)cap);
   b.wc = static_cast<WaveCounters *>(c->d_wave);
-  b.jobs = static_cast<const Job *>(c->d_jobs);
   return b;
 }
 
-/* Enqueues kWavesPerGraph waves (queues alternating A -> B -> A ...), an event record around each
- * trace and shade kernel (`external` while capturing, so they become graph event-record nodes) and
- * the read-back of the counters into pinned memory. */
-template <bool SINGLE, int WIDTH>
-void enqueue_waves(nova_b200_ctx *c, const Job &j0, bool external) {
+/* Enqueues one group of kWavesPerGraph waves for pipeline slot `slot` (queues alternating
+ * A -> B -> A ...): an event record around each trace and shade kernel (`external` while capturing,
+ * so they become graph event-record nodes), the read-back of the counters into the slot's pinned
+ * copy and the slot's completion event. */
+template <class JS, int WIDTH>
+void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int slot, bool external) {
   const WaveBuffers b = wave_buffers(c);
   int dev_sms = 148, occ_r = 1;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, k_refill<SINGLE>, 256, 0);
-  /* trace and shade: one ray per thread over the whole queue capacity, so the hardware block
-   * scheduler balances rays of very different cost; blocks past the live count exit at once */
-  const unsigned g_trace = (c->queue_cap + 127) / 128, g_shade = (c->queue_cap + 127) / 128;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_r, k_refill<JS>, 256, 0);
+  /* trace and shade: one ray per thread over the wave capacity, so the hardware block scheduler
+   * balances rays of very different cost; blocks past the live count exit at once */
+  const unsigned g_trace = (ls.cap + ls.trace_block - 1) / ls.trace_block;
+  const unsigned g_shade = (ls.cap + ls.shade_block - 1) / ls.shade_block;
   const unsigned g_refill = (unsigned)(dev_sms * std::max(1, occ_r) * 2);
   const unsigned flags = external ? cudaEventRecordExternal : cudaEventRecordDefault;
+  cudaEvent_t *ev = c->ev_wave + 3 * kWavesPerGraph * slot;
   for (int w = 0; w < kWavesPerGraph; w++) {
     const Queue &in = (w & 1) ? b.qb : b.qa;
     const Queue &out = (w & 1) ? b.qa : b.qb;
-    k_refill<SINGLE><<<g_refill, 256, 0, c->stream>>>(in, b.wc, b.jobs, j0, c->d_radiance);
-    cudaEventRecordWithFlags(c->ev_wave[3 * w + 0], c->stream, flags);
-    k_trace<WIDTH, SINGLE><<<g_trace, 128, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, b.jobs, j0);
-    cudaEventRecordWithFlags(c->ev_wave[3 * w + 1], c->stream, flags);
-    k_shade<SINGLE><<<g_shade, 128, 0, c->stream>>>(in, out, b.wc, b.hits, b.hit_slot, c->d_radiance, b.jobs, j0);
-    cudaEventRecordWithFlags(c->ev_wave[3 * w + 2], c->stream, flags);
+    k_refill<JS><<<g_refill, 256, 0, c->stream>>>(in, b.wc, c->d_radiance, js);
+    cudaEventRecordWithFlags(ev[3 * w + 0], c->stream, flags);
+    k_trace<WIDTH, JS><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+    cudaEventRecordWithFlags(ev[3 * w + 1], c->stream, flags);
+    k_shade<JS><<<g_shade, ls.shade_block, 0, c->stream>>>(in, out, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+    cudaEventRecordWithFlags(ev[3 * w + 2], c->stream, flags);
     k_wave_end<<<1, 1, 0, c->stream>>>(b.wc);
   }
-  cudaMemcpyAsync(c->h_wave, b.wc, sizeof(WaveCounters), cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(static_cast<WaveCounters *>(c->h_wave) + slot, b.wc, sizeof(WaveCounters), cudaMemcpyDeviceToHost,
+                  c->stream);
+  cudaEventRecordWithFlags(c->ev_done[slot], c->stream, flags);
 }
 
-/* Batch chunks: the waves are captured once into a CUDA graph (their arguments are buffer
- * pointers only; the job table and counters are read from device memory). */
-nova_b200_status capture_graph(nova_b200_ctx *c, int width) {
-  if (c->graph_exec && c->graph_width == width) return NOVA_B200_SUCCESS;
-  if (c->graph_exec) {
-    cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
-  }
-  cudaGraph_t graph = nullptr;
-  NB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "capture");
-  const Job unused{};
+template <class JS>
+void enqueue_group(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int width, int slot, bool external) {
   if (width == 8)
-    enqueue_waves<false, 8>(c, unused, true);
+    enqueue_waves<JS, 8>(c, js, ls, slot, external);
   else
-    enqueue_waves<false, 2>(c, unused, true);
-  const cudaError_t e_launch = cudaGetLastError();
-  const cudaError_t e_end = cudaStreamEndCapture(c->stream, &graph);
-  if (e_launch != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    return nbctx::cuda_fail(c, e_launch, "capture kernels");
+    enqueue_waves<JS, 2>(c, js, ls, slot, external);
+}
+
+/* Batch chunks: each slot's group is captured into a CUDA graph for the chunk's job table (the
+ * table is a kernel parameter); the graphs are kept while the same table and width come back. */
+nova_b200_status capture_graphs(nova_b200_ctx *c, const ManyJobs &js, const LaunchShape &ls, int width) {
+  const size_t key_bytes = sizeof(ManyJobs) + sizeof(LaunchShape) + sizeof(int);
+  std::vector<char> key(key_bytes);
+  std::memcpy(key.data(), &js, sizeof(ManyJobs));
+  std::memcpy(key.data() + sizeof(ManyJobs), &ls, sizeof(LaunchShape));
+  std::memcpy(key.data() + sizeof(ManyJobs) + sizeof(LaunchShape), &width, sizeof(int));
+  if (c->graph_exec[0] && c->graph_exec[1] && c->graph_key == key) return NOVA_B200_SUCCESS;
+  c->graph_key.clear();
+  for (int slot = 0; slot < 2; slot++) {
+    if (c->graph_exec[slot]) cudaGraphExecDestroy(c->graph_exec[slot]), c->graph_exec[slot] = nullptr;
+    cudaGraph_t graph = nullptr;
+    NB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "capture");
+    enqueue_group(c, js, ls, width, slot, true);
+    const cudaError_t e_launch = cudaGetLastError();
+    const cudaError_t e_end = cudaStreamEndCapture(c->stream, &graph);
+    if (e_launch != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return nbctx::cuda_fail(c, e_launch, "capture kernels");
+    }
+    if (e_end != cudaSuccess) return nbctx::cuda_fail(c, e_end, "cudaStreamEndCapture");
+    const cudaError_t e_inst = cudaGraphInstantiate(&c->graph_exec[slot], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e_inst != cudaSuccess) {
+      c->graph_exec[slot] = nullptr;
+      return nbctx::cuda_fail(c, e_inst, "cudaGraphInstantiate");
+    }
   }
-  if (e_end != cudaSuccess) return nbctx::cuda_fail(c, e_end, "cudaStreamEndCapture");
-  const cudaError_t e_inst = cudaGraphInstantiate(&c->graph_exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e_inst != cudaSuccess) {
-    c->graph_exec = nullptr;
-    return nbctx::cuda_fail(c, e_inst, "cudaGraphInstantiate");
-  }
-  c->graph_width = width;
+  c->graph_key = std::move(key);
   return NOVA_B200_SUCCESS;
 }
 
@@ -555,7 +601,10 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   }
   const uint64_t cap_entries = kRadianceCapBytes / sizeof(float4);
   const uint64_t radiance = std::max<uint64_t>(max_np, std::min<uint64_t>(total, cap_entries));
-  const uint32_t cap = (uint32_t)std::min<uint64_t>(kQueueCap, std::max<uint64_t>(radiance, 1024));
+  const nova_b200_tuning &tu = x->tuning;
+  const uint32_t qc = tu.queue_capacity ? tu.queue_capacity : kQueueCapDefault;
+  const uint32_t cap = (uint32_t)std::min<uint64_t>(qc, std::max<uint64_t>(radiance, 1024));
+  const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u};
   nova_b200_status st = ensure_wave_buffers(x, cap, radiance);
   if (st != NOVA_B200_SUCCESS) return st;
   for (size_t j = 0; j < nj; j++) {
@@ -571,7 +620,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   /* scene uploads and film clears of other contexts ran on their own streams */
   for (size_t j = 0; j < nj; j++)
     if (ctxs[j] != x) NB_CUDA(x, cudaStreamSynchronize(ctxs[j]->stream), "sync batch context");
-  /* cut the work into chunks of at most `radiance` paths */
+  /* cut the work into chunks of at most `radiance` paths and kParamJobs frame pieces */
   std::vector<std::vector<Piece>> chunks(1);
   uint64_t in_chunk = 0;
   for (size_t j = 0; j < nj; j++) {
@@ -580,7 +629,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
     uint32_t s = 0;
     while (s < (uint32_t)f->sample_count) {
       uint64_t room = (radiance - in_chunk) / np;
-      if (room == 0) {
+      if (room == 0 || chunks.back().size() == kParamJobs) {
         chunks.emplace_back();
         in_chunk = 0;
         room = radiance / np;
@@ -594,16 +643,16 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   nova_b200_render_stats sum{};
   float t_trace = 0.f, t_shade = 0.f;
   NB_CUDA(x, cudaEventRecord(x->ev_begin, x->stream), "event");
-  Job *hj = static_cast<Job *>(x->h_jobs);
+  std::vector<Job> hj(kParamJobs);
+  ManyJobs many{};
+  WaveCounters *hw = static_cast<WaveCounters *>(x->h_wave); /* [0], [1]: read-back slots, [2]: upload */
   for (const auto &chunk : chunks) {
     if (chunk.empty()) continue;
-    if (chunk.size() > kMaxJobs) return fail(x, NOVA_B200_INVALID_ARGUMENT, "more than 4096 frame pieces in a chunk%s");
-    /* the previous chunk's resolve kernels read the pinned job table: wait before rewriting it */
-    NB_CUDA(x, cudaStreamSynchronize(x->stream), "chunk");
     uint32_t pb = 0;
     for (size_t k = 0; k < chunk.size(); k++) {
       const Piece &P = chunk[k];
       Job &J = hj[k];
+      J = Job{};
       J.sc = P.ctx->scene;
       RenderParams &rp = J.rp;
       rp.W = P.f->width, rp.H = P.f->height, rp.NP = (uint32_t)((uint64_t)P.f->width * P.f->height);
@@ -615,47 +664,62 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
       rp.rr_start = P.f->rr_start;
       std::copy(P.f->inv_P, P.f->inv_P + 16, rp.inv_P);
       std::copy(P.f->inv_V, P.f->inv_V + 16, rp.inv_V);
+      rp.tile_w = tu.tile_w;
+      rp.tile_h = tu.tile_w ? tu.tile_h : 0u;
       J.path_begin = pb;
       J.n_paths = rp.NP * P.count;
       pb += J.n_paths;
     }
     const bool single = chunk.size() == 1;
-    if (!single) {
-      if ((st = capture_graph(x, width)) != NOVA_B200_SUCCESS) return st;
-      NB_CUDA(x, cudaMemcpyAsync(x->d_jobs, hj, sizeof(Job) * chunk.size(), cudaMemcpyHostToDevice, x->stream),
-              "upload(jobs)");
+    OneJob one{};
+    if (single) {
+      one.j = hj[0];
+    } else {
+      many = ManyJobs{};
+      many.n = (uint32_t)chunk.size();
+      std::copy(hj.begin(), hj.begin() + chunk.size(), many.j);
+      if ((st = capture_graphs(x, many, ls, width)) != NOVA_B200_SUCCESS) return st;
     }
-    WaveCounters *hw = static_cast<WaveCounters *>(x->h_wave);
-    *hw = WaveCounters{};
-    hw->total = pb;
-    hw->cap = x->queue_cap;
-    hw->n_jobs = (uint32_t)chunk.size();
-    NB_CUDA(x, cudaMemcpyAsync(x->d_wave, hw, sizeof(WaveCounters), cudaMemcpyHostToDevice, x->stream),
+    /* the previous chunk's last (empty) group may still be running: it is stream-ordered before
+     * this upload, and the upload slot is only rewritten once the previous upload has completed */
+    hw[2] = WaveCounters{};
+    hw[2].total = pb;
+    hw[2].cap = cap;
+    NB_CUDA(x, cudaMemcpyAsync(x->d_wave, hw + 2, sizeof(WaveCounters), cudaMemcpyHostToDevice, x->stream),
             "upload(wave counters)");
-    NB_CUDA(x, cudaStreamSynchronize(x->stream), "upload(wave counters)");
+    auto launch = [&](int slot) {
+      if (!single) return cudaGraphLaunch(x->graph_exec[slot], x->stream);
+      enqueue_group(x, one, ls, width, slot, false);
+      return cudaGetLastError();
+    };
+    NB_CUDA(x, launch(0), "wave group");
+    NB_CUDA(x, launch(1), "wave group");
+    int slot = 0;
+    uint32_t waves = 0;
+    unsigned long long traced = 0;
     for (;;) {
-      if (!single) {
-        NB_CUDA(x, cudaGraphLaunch(x->graph_exec, x->stream), "cudaGraphLaunch");
-      } else if (width == 8) {
-        enqueue_waves<true, 8>(x, hj[0], false);
-      } else {
-        enqueue_waves<true, 2>(x, hj[0], false);
-      }
-      NB_CUDA(x, cudaGetLastError(), "wave kernels");
-      NB_CUDA(x, cudaStreamSynchronize(x->stream), "waves");
+      NB_CUDA(x, cudaEventSynchronize(x->ev_done[slot]), "waves");
+      const cudaEvent_t *ev = x->ev_wave + 3 * kWavesPerGraph * slot;
       for (int w = 0; w < kWavesPerGraph; w++) {
         float a = 0.f, b = 0.f;
-        cudaEventElapsedTime(&a, x->ev_wave[3 * w], x->ev_wave[3 * w + 1]);
-        cudaEventElapsedTime(&b, x->ev_wave[3 * w + 1], x->ev_wave[3 * w + 2]);
+        cudaEventElapsedTime(&a, ev[3 * w], ev[3 * w + 1]);
+        cudaEventElapsedTime(&b, ev[3 * w + 1], ev[3 * w + 2]);
         t_trace += a;
         t_shade += b;
       }
       sum.kernels += 4 * kWavesPerGraph;
-      if (hw->done) break;
+      const WaveCounters r = hw[slot];
+      waves = r.waves;
+      traced = r.traced;
+      if (r.done) break;
+      NB_CUDA(x, launch(slot), "wave group");
+      slot ^= 1;
     }
-    sum.traced += hw->traced;
-    sum.segments += hw->traced;
-    sum.waves += hw->waves;
+    /* the group in flight in the other slot finds nothing to do */
+    sum.kernels += 4 * kWavesPerGraph;
+    sum.traced += traced;
+    sum.segments += traced;
+    sum.waves += waves;
     sum.paths += pb;
     for (size_t k = 0; k < chunk.size(); k++) {
       const Piece &P = chunk[k];

@@ -57,6 +57,17 @@ class SceneDesc(C.Structure):
                 ("textures", C.POINTER(Texture)), ("n_textures", C.c_uint32), ("envmap", C.c_int32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("queue_capacity", C.c_uint32), ("trace_block", C.c_uint32), ("shade_block", C.c_uint32),
+                ("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("bvh_width", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+TUNE_BVH_WIDTH = 1
+
+
 class BvhOptions(C.Structure):
     _fields_ = [("max_leaf_size", C.c_int32), ("bins", C.c_int32), ("width", C.c_int32),
                 ("small_subtree", C.c_int32)]
@@ -83,7 +94,7 @@ _lib = None
 EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "nova_b200_build_bvh",
            "nova_b200_render", "nova_b200_trace", "nova_b200_sobol", "nova_b200_bake_irradiance",
            "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
-           "nova_b200_scatter"]
+           "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune"]
 
 
 def lib():
@@ -101,6 +112,10 @@ def lib():
         L.nova_b200_render.argtypes = [vp, C.POINTER(Frame), vp, vp, C.POINTER(RenderStats)]
         L.nova_b200_trace.argtypes = [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]
         L.nova_b200_sobol.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, vp]
+        L.nova_b200_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.nova_b200_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.nova_b200_autotune.argtypes = [C.POINTER(vp), C.POINTER(Frame), C.c_uint32, C.c_char_p, C.c_uint32,
+                                         C.POINTER(Tuning)]
         L.nova_b200_scatter.argtypes = [vp, C.c_uint64] + [vp] * 8 + [C.c_uint32] + [vp] * 5
         L.nova_b200_bake_irradiance.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                 C.c_int32, vp]
@@ -220,6 +235,19 @@ def render_batch(contexts, frames, films_host=None, films_device=None) -> "Rende
     return st
 
 
+def autotune(contexts, frames, cache_path=None, flags=0) -> Tuning:
+    """nova_b200_autotune: picks and applies the fastest launch tuning for these frames."""
+    n = len(contexts)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    fs = (Frame * n)(*frames)
+    out = Tuning()
+    path = None if cache_path is None else os.fsencode(cache_path)
+    rc = lib().nova_b200_autotune(hs, fs, n, path, flags, C.byref(out))
+    if rc != 0:
+        raise NovaError(rc, contexts[0].error())
+    return out
+
+
 class Context:
     """One device context: scene upload, BVH build, render, queries."""
 
@@ -286,6 +314,16 @@ class Context:
         outs = [out_o_ptr, out_d_ptr, weight_ptr, emissive_ptr, valid_ptr]
         self._check(lib().nova_b200_scatter(self.h, n, *[C.c_void_p(p) for p in ptrs], seed,
                                             *[C.c_void_p(p) for p in outs]))
+
+    def set_tuning(self, tuning=None, **kw):
+        """Sets the launch tuning (a Tuning, or keyword fields; nothing = defaults)."""
+        t = tuning if tuning is not None else Tuning(**kw)
+        self._check(lib().nova_b200_set_tuning(self.h, C.byref(t) if (tuning is not None or kw) else None))
+
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        self._check(lib().nova_b200_get_tuning(self.h, C.byref(t)))
+        return t
 
     def sobol(self, idx_ptr, dim_ptr, n, seed, out_ptr):
         self._check(lib().nova_b200_sobol(self.h, n, C.c_void_p(idx_ptr), C.c_void_p(dim_ptr), seed,

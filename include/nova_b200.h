@@ -204,6 +204,35 @@ nova_b200_status nova_b200_scatter(nova_b200_ctx *ctx, uint64_t n, const float *
                                    float *next_orig_dev, float *next_dir_dev, float *weight_dev, float *emissive_dev,
                                    int32_t *valid_dev);
 
+/* Launch parameters of the wavefront (no counterpart in the reference, whose CPU path has tiles and
+ * threads only).  They change speed, never results: every tuning renders the same image, bit for
+ * bit.  A batch render uses the tuning of its first context. */
+typedef struct {
+  uint32_t queue_capacity; /* rays per wave, 65536 .. 67108864; 0 = default (8388608) */
+  uint32_t trace_block;    /* threads per block of the trace kernel: 32, 64, 96 or 128; 0 = 128 */
+  uint32_t shade_block;    /* threads per block of the shade kernel: 32, 64, 96 or 128; 0 = 128 */
+  uint32_t tile_w, tile_h; /* consecutive paths walk tile_w x tile_h pixel tiles (tile_w * tile_h a
+                              multiple of 32, both <= 64); 0 x 0 = image rows (default) */
+  int32_t bvh_width;       /* reported by nova_b200_autotune: the BVH width it left the contexts
+                              built with (0: not tuned); ignored by nova_b200_set_tuning */
+} nova_b200_tuning;
+
+/* tuning = NULL restores the defaults. */
+nova_b200_status nova_b200_set_tuning(nova_b200_ctx *ctx, const nova_b200_tuning *tuning);
+nova_b200_status nova_b200_get_tuning(nova_b200_ctx *ctx, nova_b200_tuning *tuning);
+
+#define NOVA_B200_TUNE_BVH_WIDTH 1u /* also try the 8-wide BVH (rebuilds every context's BVH) */
+
+/* Autotuner for a batch (or a single frame, n = 1): times probe renders of the given frames with
+ * a reduced sample count under candidate tunings (queue capacity, block sizes, pixel tiles and,
+ * with NOVA_B200_TUNE_BVH_WIDTH, the BVH width), applies the fastest to every context and writes
+ * it to *best.  The tuning fields never change a result bit; the BVH width can change which of two
+ * triangles hit at exactly the same distance is reported.  Results are cached in the text file cache_path (NULL: no cache) under a key of
+ * device, frame count, path count, depth and BVH width; a cached entry is applied without probing.
+ * The probe renders reset the contexts' accumulation films. */
+nova_b200_status nova_b200_autotune(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
+                                    const char *cache_path, uint32_t flags, nova_b200_tuning *best);
+
 /* Sobol + Owen samples (math_random.h:73-98 SobolGenerator::generate) for n (index, dimension)
  * pairs in device memory. */
 nova_b200_status nova_b200_sobol(nova_b200_ctx *ctx, uint64_t n, const uint32_t *index_dev, const uint32_t *dim_dev,
