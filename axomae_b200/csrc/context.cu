@@ -265,6 +265,7 @@ nova_b200_status nova_b200_destroy(nova_b200_ctx *c) {
   free_scene(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->h_stage) cudaFreeHost(c->h_stage);
+  cudaFree(c->d_adj);
   cudaFree(c->d_sobol);
   cudaFree(c->d_acos);
   cudaFree(c->d_counters);
@@ -376,6 +377,7 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
   if (offset >= (1ull << 27))
     return fail(c, NOVA_B200_OUT_OF_MEMORY, "more than 2^27 triangles are not supported by the leaf encoding%s");
   c->n_prims = offset;
+  c->n_materials = d->n_materials;
   std::vector<uint32_t> prim_inst(offset);
   c->h_valid.clear();
   c->h_valid.reserve(offset);
@@ -580,6 +582,21 @@ void nova_b200_get_error(nova_b200_ctx *c, char buf[1024], size_t *size) {
   std::memcpy(buf, e.data(), n);
   buf[n] = 0;
   if (size) *size = n;
+}
+
+nova_b200_status nova_b200_set_diff_params(nova_b200_ctx *c, const float *albedo, const float *roughness) {
+  using namespace nbctx;
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  if (!c->scene_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "upload a scene first%s");
+  c->scene.diff_albedo = albedo;
+  c->scene.diff_rough = roughness;
+  return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nova_b200_backward(nova_b200_ctx *c, const nova_b200_frame *f, const float *d_image,
+                                    float *grad_albedo, float *grad_roughness, nova_b200_render_stats *stats) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  return nb_backward(c, f, d_image, grad_albedo, grad_roughness, stats);
 }
 
 nova_b200_status nova_b200_scene_info(nova_b200_ctx *c, uint64_t *tris, uint64_t *insts, uint64_t *nodes,

@@ -25,6 +25,7 @@ struct nova_b200_ctx {
   std::vector<nb::DevInstance> h_instances;
   std::vector<uint32_t> h_valid; /* global primitive ids that can be hit */
   uint64_t n_prims = 0;
+  uint32_t n_materials = 0;
   bool scene_ready = false;
   bool bvh_ready = false;
   uint32_t n_nodes = 0, n_leaves = 0;
@@ -58,6 +59,10 @@ struct nova_b200_ctx {
   cudaGraphExec_t graph_exec[2] = {};        /* batch chunks: the wave group of each pipeline slot */
   std::vector<char> graph_key;               /* job table, launch shape and width of the graphs */
   nova_b200_tuning tuning{};                 /* launch parameters (zeros: defaults) */
+
+  /* adjoint: the replay queues' extra path state (remaining radiance, image adjoint) */
+  float4 *d_adj = nullptr;
+  uint32_t adj_cap = 0;
 };
 
 namespace nbctx {
@@ -91,6 +96,8 @@ nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *fi
                            nova_b200_render_stats *stats);
 nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
                                  float *const *films_host, float *const *films_device, nova_b200_render_stats *stats);
+nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const float *d_image, float *grad_albedo,
+                             float *grad_roughness, nova_b200_render_stats *stats);
 nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,
                           float *u, float *v);
 nova_b200_status nb_scatter(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, const int32_t *prim,

@@ -70,6 +70,8 @@ struct DevScene {
   int32_t envmap;
   uint32_t n_prims;
   uint32_t has_emissive;
+  const float *diff_albedo;  /* differentiable parameters (NULL: textures): 3 x n_prims RGB albedo */
+  const float *diff_rough;   /* and n_materials roughness values */
 };
 
 constexpr int kAcosPrecision = 500000;

@@ -68,6 +68,7 @@ struct RenderParams {
   int32_t rr_start;
   float inv_P[16], inv_V[16];
   uint32_t tile_w, tile_h; /* consecutive paths walk tile_w x tile_h pixel tiles (0: image rows) */
+  int32_t vinv;            /* film rows stored top-down (vertical_invert) */
 };
 
 struct Job {
@@ -144,41 +145,58 @@ __device__ __forceinline__ void tile_pixel(const RenderParams &rp, uint32_t q, u
   y = ty * th + ly;
 }
 
+/* The camera ray of path g of the chunk: pixel (x, y), radiance slot and Sobol index. */
+struct CameraPath {
+  uint32_t job, x, y, rslot, index;
+  V4 o, d;
+};
+
+template <class JS>
+__device__ __forceinline__ CameraPath camera_path(const JS &js, uint32_t g) {
+  CameraPath c;
+  c.job = js.find(g);
+  const Job &J = js.at(c.job);
+  const RenderParams &rp = J.rp;
+  const uint32_t p = g - J.path_begin;
+  const uint32_t s_local = p / rp.NP, q_pix = p - s_local * rp.NP;
+  uint32_t x, y;
+  tile_pixel(rp, q_pix, x, y);
+  c.x = x;
+  c.y = y;
+  /* the radiance slot stays keyed by the row-major pixel, whatever order paths start in */
+  c.rslot = J.path_begin + s_local * rp.NP + y * (uint32_t)rp.W + x;
+  const uint32_t index = ((uint32_t)x * (uint32_t)rp.H + (uint32_t)y) * rp.spp_total + (rp.begin + s_local);
+  c.index = index;
+  const float r0 = sobol_sample(J.sc.sobol_dv, index, 0, rp.seed);
+  const float r1 = sobol_sample(J.sc.sobol_dv, index, 1, rp.seed);
+  const float dx = r0 * 0.0005f, dy = r1 * 0.0005f; /* RAND_DX / RAND_DY, Integrator.h:54-55 */
+  const int ys = rp.H - (int)y;                     /* screen row, Integrator.h:84 */
+  const float ndc_x = (float)(2 * (int)x - rp.W) / (float)rp.W;
+  const float ndc_y = (float)(rp.H - 2 * ys) / (float)rp.H;
+  const float nx = ndc_x + dx, ny = ndc_y + dy;
+  const M4 iP = m4_load(rp.inv_P), iV = m4_load(rp.inv_V);
+  V4 o = mul(iP, V4{nx, ny, -1.f, 1.f});
+  o = o / o.w;
+  o = mul(iV, V4{o.x, o.y, o.z, 1.f});
+  V4 d = mul(iP, V4{nx, ny, -1.f, 0.f});
+  d = normalize(mul(iV, V4{d.x, d.y, -1.f, 0.f}));
+  c.o = o;
+  c.d = d;
+  return c;
+}
+
 template <class JS>
 __global__ void __launch_bounds__(256) k_refill(Queue q, const WaveCounters *wcp, float4 *L,
                                                 const __grid_constant__ JS js) {
   const WaveCounters wc = *wcp;
   const uint32_t n_new = wave_new(wc);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
-    const uint32_t g = wc.next + i;
-    const uint32_t job = js.find(g);
-    const Job &J = js.at(job);
-    const RenderParams &rp = J.rp;
-    const uint32_t p = g - J.path_begin;
-    const uint32_t s_local = p / rp.NP, q_pix = p - s_local * rp.NP;
-    uint32_t x, y;
-    tile_pixel(rp, q_pix, x, y);
-    /* the radiance slot stays keyed by the row-major pixel, whatever order paths start in */
-    const uint32_t rslot = J.path_begin + s_local * rp.NP + y * (uint32_t)rp.W + x;
-    const uint32_t index = ((uint32_t)x * (uint32_t)rp.H + (uint32_t)y) * rp.spp_total + (rp.begin + s_local);
-    const float r0 = sobol_sample(J.sc.sobol_dv, index, 0, rp.seed);
-    const float r1 = sobol_sample(J.sc.sobol_dv, index, 1, rp.seed);
-    const float dx = r0 * 0.0005f, dy = r1 * 0.0005f; /* RAND_DX / RAND_DY, Integrator.h:54-55 */
-    const int ys = rp.H - (int)y;                     /* screen row, Integrator.h:84 */
-    const float ndc_x = (float)(2 * (int)x - rp.W) / (float)rp.W;
-    const float ndc_y = (float)(rp.H - 2 * ys) / (float)rp.H;
-    const float nx = ndc_x + dx, ny = ndc_y + dy;
-    const M4 iP = m4_load(rp.inv_P), iV = m4_load(rp.inv_V);
-    V4 o = mul(iP, V4{nx, ny, -1.f, 1.f});
-    o = o / o.w;
-    o = mul(iV, V4{o.x, o.y, o.z, 1.f});
-    V4 d = mul(iP, V4{nx, ny, -1.f, 0.f});
-    d = normalize(mul(iV, V4{d.x, d.y, -1.f, 0.f}));
+    const CameraPath c = camera_path(js, wc.next + i);
     const uint32_t slot = wc.n_active + i;
-    q.o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(rslot));
-    q.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(job << 8));
-    q.beta[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(index));
-    if (J.sc.has_emissive) L[rslot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    q.o[slot] = make_float4(c.o.x, c.o.y, c.o.z, __uint_as_float(c.rslot));
+    q.d[slot] = make_float4(c.d.x, c.d.y, c.d.z, __uint_as_float(c.job << 8));
+    q.beta[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(c.index));
+    if (js.at(c.job).sc.has_emissive) L[c.rslot] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
@@ -214,7 +232,7 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
 /* Closest hit of every queued ray.  A miss finishes its path here (environment lookup,
  * Integrator.cpp:94-98); hits are appended to a compact hit list so the shading kernel only runs
  * on rays that hit. */
-template <int WIDTH, class JS>
+template <int WIDTH, class JS, bool ADJ = false>
 __global__ void __launch_bounds__(128) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
                                                const __grid_constant__ JS js) {
   const uint32_t n = wcp->n_active + wave_new(*wcp);
@@ -227,14 +245,14 @@ __global__ void __launch_bounds__(128) k_trace(Queue q, WaveCounters *wcp, float
       const float4 o = q.o[i], d = q.d[i];
       const DevScene &sc = js.at(__float_as_uint(d.w) >> 8).sc;
       r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
-      if (r.prim < 0) {
+      if (r.prim >= 0) {
+        is_hit = true;
+      } else if (!ADJ) { /* a replayed path's radiance is already known */
         const float4 b4 = q.beta[i];
         const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
         finish_path(sc, L, __float_as_uint(o.w),
                     finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z},
                                    (float)(__float_as_uint(d.w) & 0xffu) + e.w));
-      } else {
-        is_hit = true;
       }
     }
     const unsigned slot = warp_append(is_hit, &wcp->hit_count);
@@ -272,7 +290,8 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
       const uint32_t inst = __ldg(sc.prim_inst + prim);
       const DevInstance &I = sc.instances[inst];
       const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)prim - I.prim_offset, h.x, h.y, h.z);
-      const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed);
+      const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed,
+                                       (uint32_t)prim, I.material);
       if (sc.has_emissive && any_nonzero(sr.emissive)) {
         const V3 em = beta * sr.emissive;
         const float4 acc = L[g];
@@ -321,6 +340,120 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
       out.d[slot] = nd;
       out.beta[slot] = nbeta;
     }
+  }
+}
+
+/* ---------------------------------------------------------------- replay adjoint
+ *
+ * Path-replay backpropagation (detached sampling).  A path's estimate is
+ *   I = sum_k beta_k e_k + beta_K env,  beta_k = w_0 ... w_{k-1},  w_k = f_k |cos| / pdf_k.
+ * With the sampling densities held fixed, d w_k / d theta = w_k d ln f_k / d theta, and theta_k
+ * (the albedo of the triangle hit at vertex k, the roughness of its material) scales everything
+ * the path gathers after vertex k's own emission: R_k = I - sum_{m <= k} beta_m e_m.  So
+ *   dLoss/dtheta_k += sum_c dLoss/dI_c R_k,c d ln f_k,c / d theta_k.
+ * The replay starts with R = I (the path's radiance from the primal pass, read from the radiance
+ * buffer) and subtracts emission as it walks the path again from the same Sobol index; vertices
+ * add their terms to the gradients with atomics.  Extra path state: R and dLoss/dI (2 x 16 B). */
+
+struct AdjQueue {
+  float4 *rem, *dl;
+};
+
+template <class JS>
+__global__ void __launch_bounds__(256) k_refill_adj(Queue q, AdjQueue a, const WaveCounters *wcp, const float4 *L,
+                                                    const float4 *d_image, const __grid_constant__ JS js) {
+  const WaveCounters wc = *wcp;
+  const uint32_t n_new = wave_new(wc);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
+    const CameraPath c = camera_path(js, wc.next + i);
+    const RenderParams &rp = js.at(c.job).rp;
+    const uint32_t slot = wc.n_active + i;
+    q.o[slot] = make_float4(c.o.x, c.o.y, c.o.z, __uint_as_float(c.rslot));
+    q.d[slot] = make_float4(c.d.x, c.d.y, c.d.z, __uint_as_float(c.job << 8));
+    q.beta[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(c.index));
+    const float4 I = L[c.rslot];
+    a.rem[slot] = make_float4(I.x, I.y, I.z, 0.f);
+    /* the film pixel of (x, y): rows flipped when the frame asks for it (k_resolve) */
+    const uint32_t row = rp.vinv ? (uint32_t)rp.H - 1u - c.y : c.y;
+    const float4 g = d_image[(size_t)row * rp.W + c.x];
+    const float inv = 1.f / (float)rp.count; /* the image is the mean of the frame's samples */
+    a.dl[slot] = make_float4(g.x * inv, g.y * inv, g.z * inv, 0.f);
+  }
+}
+
+template <class JS>
+__global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQueue ain, AdjQueue aout,
+                                                      WaveCounters *wcp, const float4 *hits, const uint32_t *hit_slot,
+                                                      float *g_alb, float *g_rough, const __grid_constant__ JS js) {
+  const uint32_t n = wcp->hit_count;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i & ~31u) >= n) return;
+  bool enq = false;
+  float4 no{}, nd{}, nbeta{}, nrem{}, ndl{};
+  if (i < n) {
+    const uint32_t slot_in = hit_slot[i];
+    const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
+    const float4 r4 = ain.rem[slot_in], l4 = ain.dl[slot_in];
+    const uint32_t tag = __float_as_uint(d4.w);
+    const int bounce = (int)(tag & 0xffu);
+    const Job &J = js.at(tag >> 8);
+    const DevScene &sc = J.sc;
+    const RenderParams &rp = J.rp;
+    const uint32_t index = __float_as_uint(b4.w);
+    const V3 ro{o4.x, o4.y, o4.z}, rd{d4.x, d4.y, d4.z};
+    V3 beta{b4.x, b4.y, b4.z};
+    V3 rem{r4.x, r4.y, r4.z};
+    const V3 dl{l4.x, l4.y, l4.z};
+    const int prim = __float_as_int(h.w);
+    const uint32_t inst = __ldg(sc.prim_inst + prim);
+    const DevInstance &I = sc.instances[inst];
+    const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)prim - I.prim_offset, h.x, h.y, h.z);
+    Scores scs;
+    const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed,
+                                     (uint32_t)prim, I.material, &scs);
+    if (sc.has_emissive) rem = rem - beta * sr.emissive;
+    if (sr.valid) {
+      const V3 cw = dl * rem;
+      if (g_alb) {
+        float *ga = g_alb + 3 * (size_t)prim;
+        if (cw.x * scs.albedo.x != 0.f) atomicAdd(ga, cw.x * scs.albedo.x);
+        if (cw.y * scs.albedo.y != 0.f) atomicAdd(ga + 1, cw.y * scs.albedo.y);
+        if (cw.z * scs.albedo.z != 0.f) atomicAdd(ga + 2, cw.z * scs.albedo.z);
+      }
+      const float gr = ((cw.x + cw.y) + cw.z) * scs.roughness;
+      if (g_rough && gr != 0.f && isfinite(gr)) atomicAdd(g_rough + I.material, gr);
+      V3 c = sr.weight;
+      bool alive = true;
+      if (rp.rr_start >= 0 && bounce >= rp.rr_start) {
+        const V3 nbt = beta * c;
+        const float q = fmin_std(1.f, fmax_std(0.05f, fmax_std(nbt.x, fmax_std(nbt.y, nbt.z))));
+        const float urr = sobol_sample(sc.sobol_dv, index, kRRDimBase + (unsigned)bounce, rp.seed);
+        if (!(urr < q))
+          alive = false;
+        else
+          c = c / q;
+      }
+      if (alive && bounce + 1 <= rp.max_depth) {
+        beta = beta * c;
+        const float eps = 1e-3f;
+        const V3 nd3 = normalize(sr.wi);
+        const V3 no3 = hr.position + hr.ng * (eps + eps * fsign(dot(hr.ng, sr.wi)));
+        enq = true;
+        no = make_float4(no3.x, no3.y, no3.z, o4.w);
+        nd = make_float4(nd3.x, nd3.y, nd3.z, __uint_as_float(tag + 1u));
+        nbeta = make_float4(beta.x, beta.y, beta.z, b4.w);
+        nrem = make_float4(rem.x, rem.y, rem.z, 0.f);
+        ndl = l4;
+      }
+    }
+  }
+  const unsigned slot = warp_append(enq, &wcp->out_count);
+  if (enq) {
+    out.o[slot] = no;
+    out.d[slot] = nd;
+    out.beta[slot] = nbeta;
+    aout.rem[slot] = nrem;
+    aout.dl[slot] = ndl;
   }
 }
 
@@ -382,7 +515,8 @@ __global__ void k_scatter_api(DevScene sc, uint64_t n, const float *o, const flo
   const DevInstance &I = sc.instances[__ldg(sc.prim_inst + p)];
   const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)p - I.prim_offset, t[i], u[i], v[i]);
   const ScatterResult sr =
-      scatter(sc, rd, hr, sc.materials[I.material], index[i], 2u + 4u * (unsigned)bounce[i], seed);
+      scatter(sc, rd, hr, sc.materials[I.material], index[i], 2u + 4u * (unsigned)bounce[i], seed, (uint32_t)p,
+              I.material);
   const float eps = 1e-3f;
   const V3 nd3 = normalize(sr.wi);
   const V3 no3 = hr.position + hr.ng * (eps + eps * fsign(dot(hr.ng, sr.wi)));
@@ -491,8 +625,16 @@ WaveBuffers wave_buffers(nova_b200_ctx *c) {
  * A -> B -> A ...): an event record around each trace and shade kernel (`external` while capturing,
  * so they become graph event-record nodes), the read-back of the counters into the slot's pinned
  * copy and the slot's completion event. */
-template <class JS, int WIDTH>
-void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int slot, bool external) {
+/* Replay-loop arguments: the adjoint queues (A, B), the image adjoint and the gradients. */
+struct AdjArgs {
+  AdjQueue qa, qb;
+  const float4 *d_image;
+  float *g_alb, *g_rough;
+};
+
+template <class JS, int WIDTH, bool ADJ = false>
+void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int slot, bool external,
+                   const AdjArgs *adj = nullptr) {
   const WaveBuffers b = wave_buffers(c);
   int dev_sms = 148, occ_r = 1;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -507,12 +649,24 @@ void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int sl
   for (int w = 0; w < kWavesPerGraph; w++) {
     const Queue &in = (w & 1) ? b.qb : b.qa;
     const Queue &out = (w & 1) ? b.qa : b.qb;
-    k_refill<JS><<<g_refill, 256, 0, c->stream>>>(in, b.wc, c->d_radiance, js);
-    cudaEventRecordWithFlags(ev[3 * w + 0], c->stream, flags);
-    k_trace<WIDTH, JS><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
-    cudaEventRecordWithFlags(ev[3 * w + 1], c->stream, flags);
-    k_shade<JS><<<g_shade, ls.shade_block, 0, c->stream>>>(in, out, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
-    cudaEventRecordWithFlags(ev[3 * w + 2], c->stream, flags);
+    if constexpr (ADJ) {
+      const AdjQueue &ain = (w & 1) ? adj->qb : adj->qa;
+      const AdjQueue &aout = (w & 1) ? adj->qa : adj->qb;
+      k_refill_adj<JS><<<g_refill, 256, 0, c->stream>>>(in, ain, b.wc, c->d_radiance, adj->d_image, js);
+      cudaEventRecordWithFlags(ev[3 * w + 0], c->stream, flags);
+      k_trace<WIDTH, JS, true><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, nullptr, js);
+      cudaEventRecordWithFlags(ev[3 * w + 1], c->stream, flags);
+      k_shade_adj<JS><<<g_shade, ls.shade_block, 0, c->stream>>>(in, out, ain, aout, b.wc, b.hits, b.hit_slot,
+                                                                 adj->g_alb, adj->g_rough, js);
+      cudaEventRecordWithFlags(ev[3 * w + 2], c->stream, flags);
+    } else {
+      k_refill<JS><<<g_refill, 256, 0, c->stream>>>(in, b.wc, c->d_radiance, js);
+      cudaEventRecordWithFlags(ev[3 * w + 0], c->stream, flags);
+      k_trace<WIDTH, JS><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+      cudaEventRecordWithFlags(ev[3 * w + 1], c->stream, flags);
+      k_shade<JS><<<g_shade, ls.shade_block, 0, c->stream>>>(in, out, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+      cudaEventRecordWithFlags(ev[3 * w + 2], c->stream, flags);
+    }
     k_wave_end<<<1, 1, 0, c->stream>>>(b.wc);
   }
   cudaMemcpyAsync(static_cast<WaveCounters *>(c->h_wave) + slot, b.wc, sizeof(WaveCounters), cudaMemcpyDeviceToHost,
@@ -558,6 +712,62 @@ nova_b200_status capture_graphs(nova_b200_ctx *c, const ManyJobs &js, const Laun
     }
   }
   c->graph_key = std::move(key);
+  return NOVA_B200_SUCCESS;
+}
+
+/* Counters of wave loops. */
+struct LoopStats {
+  float t_trace = 0.f, t_shade = 0.f;
+  uint64_t kernels = 0, traced = 0;
+  uint32_t waves = 0;
+  void add_to(nova_b200_render_stats &s) const {
+    s.traced += traced;
+    s.segments += traced;
+    s.waves += waves;
+    s.kernels += kernels;
+    s.trace_ms += t_trace;
+    s.shade_ms += t_shade;
+  }
+};
+
+/* Runs the device-driven wave loop over `total` paths: uploads the counters, keeps two groups of
+ * waves in flight (launch(slot) enqueues one), reads each finished group's counters and event
+ * times, and stops once the device reports every path finished.  The group still in flight then
+ * finds empty queues. */
+template <class Launch>
+nova_b200_status run_waves(nova_b200_ctx *x, uint32_t total, uint32_t cap, Launch &&launch, LoopStats &ls) {
+  WaveCounters *hw = static_cast<WaveCounters *>(x->h_wave); /* [0], [1]: read-back slots, [2]: upload */
+  /* a previous loop's last (empty) group may still be running: it is stream-ordered before this
+   * upload, and the upload slot is only rewritten once the previous upload has completed */
+  hw[2] = WaveCounters{};
+  hw[2].total = total;
+  hw[2].cap = cap;
+  NB_CUDA(x, cudaMemcpyAsync(x->d_wave, hw + 2, sizeof(WaveCounters), cudaMemcpyHostToDevice, x->stream),
+          "upload(wave counters)");
+  NB_CUDA(x, launch(0), "wave group");
+  NB_CUDA(x, launch(1), "wave group");
+  int slot = 0;
+  for (;;) {
+    NB_CUDA(x, cudaEventSynchronize(x->ev_done[slot]), "waves");
+    const cudaEvent_t *ev = x->ev_wave + 3 * kWavesPerGraph * slot;
+    for (int w = 0; w < kWavesPerGraph; w++) {
+      float a = 0.f, b = 0.f;
+      cudaEventElapsedTime(&a, ev[3 * w], ev[3 * w + 1]);
+      cudaEventElapsedTime(&b, ev[3 * w + 1], ev[3 * w + 2]);
+      ls.t_trace += a;
+      ls.t_shade += b;
+    }
+    ls.kernels += 4 * kWavesPerGraph;
+    const WaveCounters r = hw[slot];
+    if (r.done) {
+      ls.waves += r.waves;
+      ls.traced += r.traced;
+      break;
+    }
+    NB_CUDA(x, launch(slot), "wave group");
+    slot ^= 1;
+  }
+  ls.kernels += 4 * kWavesPerGraph; /* the empty group */
   return NOVA_B200_SUCCESS;
 }
 
@@ -641,11 +851,10 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
     }
   }
   nova_b200_render_stats sum{};
-  float t_trace = 0.f, t_shade = 0.f;
+  LoopStats loop;
   NB_CUDA(x, cudaEventRecord(x->ev_begin, x->stream), "event");
   std::vector<Job> hj(kParamJobs);
   ManyJobs many{};
-  WaveCounters *hw = static_cast<WaveCounters *>(x->h_wave); /* [0], [1]: read-back slots, [2]: upload */
   for (const auto &chunk : chunks) {
     if (chunk.empty()) continue;
     uint32_t pb = 0;
@@ -664,6 +873,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
       rp.rr_start = P.f->rr_start;
       std::copy(P.f->inv_P, P.f->inv_P + 16, rp.inv_P);
       std::copy(P.f->inv_V, P.f->inv_V + 16, rp.inv_V);
+      rp.vinv = P.f->vertical_invert;
       rp.tile_w = tu.tile_w;
       rp.tile_h = tu.tile_w ? tu.tile_h : 0u;
       J.path_begin = pb;
@@ -680,46 +890,12 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
       std::copy(hj.begin(), hj.begin() + chunk.size(), many.j);
       if ((st = capture_graphs(x, many, ls, width)) != NOVA_B200_SUCCESS) return st;
     }
-    /* the previous chunk's last (empty) group may still be running: it is stream-ordered before
-     * this upload, and the upload slot is only rewritten once the previous upload has completed */
-    hw[2] = WaveCounters{};
-    hw[2].total = pb;
-    hw[2].cap = cap;
-    NB_CUDA(x, cudaMemcpyAsync(x->d_wave, hw + 2, sizeof(WaveCounters), cudaMemcpyHostToDevice, x->stream),
-            "upload(wave counters)");
     auto launch = [&](int slot) {
       if (!single) return cudaGraphLaunch(x->graph_exec[slot], x->stream);
       enqueue_group(x, one, ls, width, slot, false);
       return cudaGetLastError();
     };
-    NB_CUDA(x, launch(0), "wave group");
-    NB_CUDA(x, launch(1), "wave group");
-    int slot = 0;
-    uint32_t waves = 0;
-    unsigned long long traced = 0;
-    for (;;) {
-      NB_CUDA(x, cudaEventSynchronize(x->ev_done[slot]), "waves");
-      const cudaEvent_t *ev = x->ev_wave + 3 * kWavesPerGraph * slot;
-      for (int w = 0; w < kWavesPerGraph; w++) {
-        float a = 0.f, b = 0.f;
-        cudaEventElapsedTime(&a, ev[3 * w], ev[3 * w + 1]);
-        cudaEventElapsedTime(&b, ev[3 * w + 1], ev[3 * w + 2]);
-        t_trace += a;
-        t_shade += b;
-      }
-      sum.kernels += 4 * kWavesPerGraph;
-      const WaveCounters r = hw[slot];
-      waves = r.waves;
-      traced = r.traced;
-      if (r.done) break;
-      NB_CUDA(x, launch(slot), "wave group");
-      slot ^= 1;
-    }
-    /* the group in flight in the other slot finds nothing to do */
-    sum.kernels += 4 * kWavesPerGraph;
-    sum.traced += traced;
-    sum.segments += traced;
-    sum.waves += waves;
+    if ((st = run_waves(x, pb, cap, launch, loop)) != NOVA_B200_SUCCESS) return st;
     sum.paths += pb;
     for (size_t k = 0; k < chunk.size(); k++) {
       const Piece &P = chunk[k];
@@ -746,9 +922,8 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   NB_CUDA(x, cudaStreamSynchronize(x->stream), "render");
   float total_ms = 0.f;
   cudaEventElapsedTime(&total_ms, x->ev_begin, x->ev_end);
+  loop.add_to(sum);
   sum.device_ms = total_ms;
-  sum.trace_ms = t_trace;
-  sum.shade_ms = t_shade;
   if (stats) *stats = sum;
   return NOVA_B200_SUCCESS;
 }
@@ -785,6 +960,88 @@ nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_fra
   }
   cudaSetDevice(x->device);
   return render_jobs(x, cs, fs, films_host, films_device, stats);
+}
+
+nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const float *d_image, float *grad_albedo,
+                             float *grad_roughness, nova_b200_render_stats *stats) {
+  using namespace nbctx;
+  nova_b200_status st = validate_frame(c, f);
+  if (st != NOVA_B200_SUCCESS) return st;
+  if (!d_image) return fail(c, NOVA_B200_INVALID_ARGUMENT, "d_image is null%s");
+  cudaSetDevice(c->device);
+  const uint32_t NP = (uint32_t)((uint64_t)f->width * f->height);
+  const uint64_t total = (uint64_t)NP * (uint64_t)f->sample_count;
+  const uint64_t radiance = std::max<uint64_t>(NP, std::min<uint64_t>(total, kRadianceCapBytes / sizeof(float4)));
+  const nova_b200_tuning &tu = c->tuning;
+  const uint32_t qc = tu.queue_capacity ? tu.queue_capacity : kQueueCapDefault;
+  const uint32_t cap = (uint32_t)std::min<uint64_t>(qc, std::max<uint64_t>(radiance, 1024));
+  const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u};
+  if ((st = ensure_wave_buffers(c, cap, radiance)) != NOVA_B200_SUCCESS) return st;
+  if (c->adj_cap < c->queue_cap) {
+    cudaFree(c->d_adj);
+    c->d_adj = nullptr;
+    c->adj_cap = 0;
+    NB_CUDA(c, cudaMalloc(&c->d_adj, sizeof(float4) * 4 * (size_t)c->queue_cap), "cudaMalloc(adjoint queues)");
+    c->adj_cap = c->queue_cap;
+  }
+  AdjArgs adj;
+  const size_t qcap = c->adj_cap;
+  adj.qa = AdjQueue{c->d_adj, c->d_adj + qcap};
+  adj.qb = AdjQueue{c->d_adj + 2 * qcap, c->d_adj + 3 * qcap};
+  adj.d_image = reinterpret_cast<const float4 *>(d_image);
+  adj.g_alb = grad_albedo;
+  adj.g_rough = grad_roughness;
+  const int width = c->bvh_width;
+  nova_b200_render_stats sum{};
+  LoopStats primal, replay;
+  NB_CUDA(c, cudaEventRecord(c->ev_begin, c->stream), "event");
+  const uint32_t per_chunk = (uint32_t)std::max<uint64_t>(1, radiance / NP);
+  for (uint32_t s0 = 0; s0 < (uint32_t)f->sample_count; s0 += per_chunk) {
+    const uint32_t take = std::min<uint32_t>(per_chunk, (uint32_t)f->sample_count - s0);
+    OneJob one{};
+    Job &J = one.j;
+    J.sc = c->scene;
+    RenderParams &rp = J.rp;
+    rp.W = f->width, rp.H = f->height, rp.NP = NP;
+    rp.count = (uint32_t)f->sample_count; /* the image averages all of the frame's samples */
+    rp.begin = (uint32_t)f->sample_begin + s0;
+    rp.spp_total = (uint32_t)f->spp_total;
+    rp.max_depth = f->max_depth;
+    rp.seed = f->seed;
+    rp.rr_start = f->rr_start;
+    std::copy(f->inv_P, f->inv_P + 16, rp.inv_P);
+    std::copy(f->inv_V, f->inv_V + 16, rp.inv_V);
+    rp.vinv = f->vertical_invert;
+    rp.tile_w = tu.tile_w;
+    rp.tile_h = tu.tile_w ? tu.tile_h : 0u;
+    J.path_begin = 0;
+    J.n_paths = NP * take;
+    /* primal: each path's radiance into the radiance buffer */
+    auto fwd = [&](int slot) {
+      enqueue_group(c, one, ls, width, slot, false);
+      return cudaGetLastError();
+    };
+    if ((st = run_waves(c, J.n_paths, cap, fwd, primal)) != NOVA_B200_SUCCESS) return st;
+    /* replay with the adjoint */
+    auto bwd = [&](int slot) {
+      if (width == 8)
+        enqueue_waves<OneJob, 8, true>(c, one, ls, slot, false, &adj);
+      else
+        enqueue_waves<OneJob, 2, true>(c, one, ls, slot, false, &adj);
+      return cudaGetLastError();
+    };
+    if ((st = run_waves(c, J.n_paths, cap, bwd, replay)) != NOVA_B200_SUCCESS) return st;
+    sum.paths += J.n_paths;
+  }
+  NB_CUDA(c, cudaEventRecord(c->ev_end, c->stream), "event");
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "backward");
+  float total_ms = 0.f;
+  cudaEventElapsedTime(&total_ms, c->ev_begin, c->ev_end);
+  primal.add_to(sum);
+  replay.add_to(sum);
+  sum.device_ms = total_ms;
+  if (stats) *stats = sum;
+  return NOVA_B200_SUCCESS;
 }
 
 nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,

@@ -332,7 +332,36 @@ struct VNDF { /* BxDF_math.h:226-343 */
     return normalize(V3{ax * nh.x, ay * nh.y, fmax_std(1e-6f, nh.z)});
   }
   NB_D bool full_specular() const { return fmax_std(ax, ay) < 1e-5f; }
+
+  /* Derivatives with respect to the base width a (ax = a / aspect, ay = a * aspect, both
+   * proportional to a).  D = 1 / (pi ax ay cos^4 (1 + E)^2) with E proportional to a^-2. */
+  NB_D float dlnD_da(V3 wm, float a) const {
+    if (wm.z < 1e-6f) return 0.f;
+    const float E = tan2theta(wm) * (sqr(cosphi(wm)) * sqr(ax_inv) + sqr(sinphi(wm)) * sqr(ay_inv));
+    return -2.f / a + 4.f * E / (a * (1.f + E));
+  }
+  /* lambda = (sqrt(1 + a2 t) - 1) / 2 with a2 proportional to a^2 */
+  NB_D float dlambda_da(V3 v, float a) const {
+    const float t2 = tan2theta(v);
+    if (isinf(t2) || isnan(t2)) return 0.f;
+    const float a2 = sqr(ax) * sqr(cosphi(v)) + sqr(ay) * sqr(sinphi(v));
+    return a2 * t2 / (2.f * a * msqrt(1 + a2 * t2));
+  }
+  NB_D float dlnG_da(V3 wo, V3 wi, float a) const {
+    return -(dlambda_da(wo, a) + dlambda_da(wi, a)) / (1.f + lambda(wo) + lambda(wi));
+  }
 };
+
+/* d ln f / d theta of the sampled lobe at the sampled directions (the sampling density held fixed):
+ * albedo per colour channel and the material's roughness.  Zero where f does not depend on it. */
+struct Scores {
+  V3 albedo;
+  float roughness;
+};
+
+NB_D V3 inv_or_zero(V3 a) {
+  return {a.x != 0.f ? 1.f / a.x : 0.f, a.y != 0.f ? 1.f / a.y : 0.f, a.z != 0.f ? 1.f / a.z : 0.f};
+}
 
 enum : unsigned { F_REFL = 1, F_TRANS = 2, F_DIFFUSE = 4, F_GLOSSY = 8, F_SPECULAR = 16, F_ALL = 31 };
 enum Lobe : int { L_NONE = 0, L_DIFFUSE = 1, L_SPECULAR = 2, L_DIELECTRIC = 3 };
@@ -402,7 +431,7 @@ struct PrincipledBSDF {
     return 0u;
   }
 
-  NB_D bool diffuse_sample(V3 wo, float u0, float u1, BsdfSample &s) const { /* BxDF.h:285-324 */
+  NB_D bool diffuse_sample(V3 wo, float u0, float u1, BsdfSample &s, Scores *sc) const { /* BxDF.h:285-324 */
     V3 wi = normalize(hemisphere_cosine_sample(u0, u1));
     V3 h = normalize(wi + wo);
     float ci = wi.z, co = wo.z;
@@ -419,10 +448,26 @@ struct PrincipledBSDF {
     s.costheta = ci;
     s.pdf = lobe_p * (ci * kInvPiF);
     s.wi = wi;
+    if (sc) {
+      /* f = K albedo (0.5 + fwi fwo A), fss90 = r^2 cos^2(theta_d) */
+      const float A = -0.5f + 1 / (co + ci);
+      const float Pi = pow5f(1.f - fabsf(wi.z)), Po = pow5f(1.f - fabsf(wo.z));
+      const float dfss90 = 2.f * p.roughness * sqr(absdot(h, wi));
+      sc->albedo = inv_or_zero(p.albedo);
+      const float den = 0.5f + fwi * fwo * A;
+      sc->roughness = den != 0.f ? A * (Pi * fwo + fwi * Po) * dfss90 / den : 0.f;
+    }
     return true;
   }
 
-  NB_D bool specular_sample(V3 wo, float u0, float u1, BsdfSample &s) const { /* BxDF.h:367-397 */
+  /* d ln(D G) / d roughness at fixed directions (alpha = r^2; the 1e-6 floor at r = 0 is constant) */
+  NB_D float dlnDG_dr(V3 wo, V3 wi, V3 wm) const {
+    if (p.roughness == 0.f) return 0.f;
+    const float a = p.roughness * p.roughness;
+    return (ggx.dlnD_da(wm, a) + ggx.dlnG_da(wo, wi, a)) * 2.f * p.roughness;
+  }
+
+  NB_D bool specular_sample(V3 wo, float u0, float u1, BsdfSample &s, Scores *sc) const { /* BxDF.h:367-397 */
     V3 wm = ggx.sample(wo, u0, u1);
     V3 wi = reflect(-wo, wm);
     float co = wo.z, ci = wi.z;
@@ -437,10 +482,22 @@ struct PrincipledBSDF {
     s.pdf = lobe_p * pdf;
     s.wi = wi;
     s.costheta = ci;
+    if (sc) {
+      /* Fr = F0 + (1 - F0) P with F0 = 0.04 (1 - metal) + metal albedo */
+      const float P = pow5f(1.f - wmwo);
+      const float dF = p.metal * (1.f - P);
+      sc->albedo = V3{Fr.x != 0.f ? dF / Fr.x : 0.f, Fr.y != 0.f ? dF / Fr.y : 0.f, Fr.z != 0.f ? dF / Fr.z : 0.f};
+      sc->roughness = dlnDG_dr(wo, wi, wm);
+    }
     return true;
   }
 
-  NB_D bool dielectric_sample(V3 wo, float uc, float u0, float u1, BsdfSample &s) const { /* BxDF.h:547-594 */
+  NB_D bool dielectric_sample(V3 wo, float uc, float u0, float u1, BsdfSample &s, Scores *sc) const {
+    /* BxDF.h:547-594; f is proportional to the albedo in every branch */
+    if (sc) {
+      sc->albedo = inv_or_zero(p.albedo);
+      sc->roughness = 0.f;
+    }
     const float ior = p.eta.x;
     if (ggx.full_specular() || p.eta.x == 1.f) {
       float R = fresnel_real(ior, wo.z), T = 1 - R;
@@ -481,6 +538,7 @@ struct PrincipledBSDF {
       s.pdf = lobe_p * pdf;
       s.wi = wi;
       s.costheta = fabsf(wi.z);
+      if (sc) sc->roughness = dlnDG_dr(wo, wi, wm);
       return true;
     }
     V3 wi{0.f, 0.f, 0.f};
@@ -498,20 +556,21 @@ struct PrincipledBSDF {
     s.costheta = fabsf(wi.z);
     s.pdf = lobe_p * pdf;
     s.wi = wi;
+    if (sc) sc->roughness = dlnDG_dr(wo, wi, wm);
     return true;
   }
 
-  NB_D bool sample_f(V3 wo, float uc, float u0, float u1, BsdfSample &s) const { /* BSDF.h:107-130 */
+  NB_D bool sample_f(V3 wo, float uc, float u0, float u1, BsdfSample &s, Scores *sc) const { /* BSDF.h:107-130 */
     if (lobe == L_NONE) return false;
     V3 lwo = normalize(mul_t(frame, wo));
     if (!(flags() & F_ALL) || lwo.z == 0.f) return false;
     bool ok;
     if (lobe == L_DIFFUSE)
-      ok = diffuse_sample(lwo, u0, u1, s);
+      ok = diffuse_sample(lwo, u0, u1, s, sc);
     else if (lobe == L_SPECULAR)
-      ok = specular_sample(lwo, u0, u1, s);
+      ok = specular_sample(lwo, u0, u1, s, sc);
     else
-      ok = dielectric_sample(lwo, uc, u0, u1, s);
+      ok = dielectric_sample(lwo, uc, u0, u1, s, sc);
     if (!ok) return false;
     if (!any_nonzero(s.f) || s.pdf == 0.f || s.wi.z == 0.f) return false;
     s.wi = normalize(mul(frame, s.wi));
@@ -548,9 +607,12 @@ struct ScatterResult {
 };
 
 /* PrincipledMaterial::scatter + sampleBSDF (NovaMaterials.h:56-137).  Consumes four Sobol
- * dimensions starting at `dim`: uc (lobe choice), u0[2] (direction), uc (sample_f). */
+ * dimensions starting at `dim`: uc (lobe choice), u0[2] (direction), uc (sample_f).  `prim` and
+ * `mat_id` select the differentiable parameters when the scene has them (per-triangle albedo and
+ * per-material roughness replace the albedo texture and the metallic texture's roughness channel);
+ * `scores`, when given, receives d ln f / d(albedo, roughness) of the sampled lobe. */
 NB_D ScatterResult scatter(const DevScene &sc, V3 rd, const HitRecord &hr, const DevMaterial &mat, uint32_t index,
-                           unsigned dim, uint32_t seed) {
+                           unsigned dim, uint32_t seed, uint32_t prim, uint32_t mat_id, Scores *scores = nullptr) {
   const float u = hr.u, v = hr.v;
   V3 nmap{0.f, 0.f, 1.f};
   if (mat.normalmap >= 0) {
@@ -570,6 +632,7 @@ NB_D ScatterResult scatter(const DevScene &sc, V3 rd, const HitRecord &hr, const
     V4 t = sample_u8(sc.textures[mat.albedo], u, v);
     albedo = {u8f(t.x), u8f(t.y), u8f(t.z)};
   }
+  if (sc.diff_albedo) albedo = {sc.diff_albedo[3 * prim], sc.diff_albedo[3 * prim + 1], sc.diff_albedo[3 * prim + 2]};
   bp.albedo = albedo;
   float rough = 0.f, metal = 0.f;
   if (mat.metallic >= 0) {
@@ -577,6 +640,7 @@ NB_D ScatterResult scatter(const DevScene &sc, V3 rd, const HitRecord &hr, const
     rough = u8f(t.y);
     metal = u8f(t.z);
   }
+  if (sc.diff_rough) rough = sc.diff_rough[mat_id];
   bp.roughness = rough;
   bp.metal = metal;
   const V3 eta{mat.eta[0], mat.eta[1], mat.eta[2]}, k{mat.k[0], mat.k[1], mat.k[2]};
@@ -601,7 +665,8 @@ NB_D ScatterResult scatter(const DevScene &sc, V3 rd, const HitRecord &hr, const
   s.pdf = 0.f;
   s.costheta = 0.f;
   ScatterResult out;
-  out.valid = bsdf.sample_f(wo, uc, u0, u1, s);
+  if (scores) *scores = Scores{v3(0.f), 0.f};
+  out.valid = bsdf.sample_f(wo, uc, u0, u1, s, scores);
   out.weight = s.f * s.costheta / s.pdf;
   out.wi = s.wi;
   out.emissive = v3(0.f);

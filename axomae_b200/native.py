@@ -94,7 +94,8 @@ _lib = None
 EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "nova_b200_build_bvh",
            "nova_b200_render", "nova_b200_trace", "nova_b200_sobol", "nova_b200_bake_irradiance",
            "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
-           "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune"]
+           "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune",
+           "nova_b200_set_diff_params", "nova_b200_backward"]
 
 
 def lib():
@@ -112,6 +113,8 @@ def lib():
         L.nova_b200_render.argtypes = [vp, C.POINTER(Frame), vp, vp, C.POINTER(RenderStats)]
         L.nova_b200_trace.argtypes = [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]
         L.nova_b200_sobol.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, vp]
+        L.nova_b200_set_diff_params.argtypes = [vp, vp, vp]
+        L.nova_b200_backward.argtypes = [vp, C.POINTER(Frame), vp, vp, vp, C.POINTER(RenderStats)]
         L.nova_b200_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.nova_b200_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.nova_b200_autotune.argtypes = [C.POINTER(vp), C.POINTER(Frame), C.c_uint32, C.c_char_p, C.c_uint32,
@@ -314,6 +317,20 @@ class Context:
         outs = [out_o_ptr, out_d_ptr, weight_ptr, emissive_ptr, valid_ptr]
         self._check(lib().nova_b200_scatter(self.h, n, *[C.c_void_p(p) for p in ptrs], seed,
                                             *[C.c_void_p(p) for p in outs]))
+
+    def set_diff_params(self, albedo_ptr=None, roughness_ptr=None):
+        """Per-triangle RGB albedo / per-material roughness in device memory (None: textures)."""
+        self._check(lib().nova_b200_set_diff_params(self.h, C.c_void_p(albedo_ptr) if albedo_ptr else None,
+                                                    C.c_void_p(roughness_ptr) if roughness_ptr else None))
+
+    def backward(self, frame, d_image_ptr, grad_albedo_ptr=None, grad_roughness_ptr=None) -> "RenderStats":
+        """Replay adjoint: adds dLoss/dparams to the gradient buffers (device pointers)."""
+        st = RenderStats()
+        self._check(lib().nova_b200_backward(self.h, C.byref(frame), C.c_void_p(d_image_ptr),
+                                             C.c_void_p(grad_albedo_ptr) if grad_albedo_ptr else None,
+                                             C.c_void_p(grad_roughness_ptr) if grad_roughness_ptr else None,
+                                             C.byref(st)))
+        return st
 
     def set_tuning(self, tuning=None, **kw):
         """Sets the launch tuning (a Tuning, or keyword fields; nothing = defaults)."""

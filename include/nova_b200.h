@@ -204,6 +204,24 @@ nova_b200_status nova_b200_scatter(nova_b200_ctx *ctx, uint64_t n, const float *
                                    float *next_orig_dev, float *next_dir_dev, float *weight_dev, float *emissive_dev,
                                    int32_t *valid_dev);
 
+/* Differentiable rendering (extension; no counterpart in the reference).  Parameters: per-triangle
+ * RGB albedo (3 floats per global triangle, replacing the albedo texture) and per-material
+ * roughness (1 float per material, replacing the metallic texture's roughness channel), both in
+ * caller-owned DEVICE memory that must stay valid while the context renders; NULL keeps the
+ * texture.  Every render of the context uses them (nova_b200_render is the forward pass).  A new
+ * upload_scene clears them. */
+nova_b200_status nova_b200_set_diff_params(nova_b200_ctx *ctx, const float *albedo_dev, const float *roughness_dev);
+
+/* Replay adjoint (path-replay backpropagation): given d_image = dLoss/dImage (width*height*4
+ * floats in DEVICE memory, laid out like the film nova_b200_render returns for this frame; alpha
+ * ignored) for the image of `frame` rendered alone (reset = 1), adds dLoss/dAlbedo (3 floats per
+ * triangle) to grad_albedo_dev and dLoss/dRoughness (1 float per material) to grad_roughness_dev
+ * (either may be NULL).  No tape is stored: each path is recomputed from its Sobol index, once
+ * for its radiance and once to push the adjoint through its vertices, where the derivative of the
+ * sampled lobe's f (its sampling density held fixed) is applied.  The film is not touched. */
+nova_b200_status nova_b200_backward(nova_b200_ctx *ctx, const nova_b200_frame *frame, const float *d_image_dev,
+                                    float *grad_albedo_dev, float *grad_roughness_dev, nova_b200_render_stats *stats);
+
 /* Launch parameters of the wavefront (no counterpart in the reference, whose CPU path has tiles and
  * threads only).  They change speed, never results: every tuning renders the same image, bit for
  * bit.  A batch render uses the tuning of its first context. */

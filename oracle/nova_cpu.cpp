@@ -417,6 +417,8 @@ struct PrincipledBSDF {
   Lobe lobe = L_NONE;
   float lobe_w = 1.f, lobe_p = 1.f;
   VNDF ggx;
+  const V3 *force_wm = nullptr; /* evaluate at this microfacet normal instead of sampling one */
+  mutable V3 wm_used{0, 0, 1};
 
   void weights() {
     float ac = std::fabs(params.wo_dot_ng);
@@ -498,7 +500,8 @@ struct PrincipledBSDF {
 
   /* SpecularBxDF::sample_f, BxDF.h:367-397 */
   bool specular_sample(V3 wo, const float u[2], Sample &s) const {
-    V3 wm = ggx.sample(wo, u);
+    V3 wm = force_wm ? *force_wm : ggx.sample(wo, u);
+    wm_used = wm;
     V3 wi = reflect(-wo, wm);
     float co = bx::costheta(wo), ci = bx::costheta(wi);
     if (co <= 0 || ci <= 0) return false;
@@ -552,7 +555,8 @@ struct PrincipledBSDF {
       s.wi = wi;
       return true;
     }
-    V3 wm = ggx.sample(wo, u);
+    V3 wm = force_wm ? *force_wm : ggx.sample(wo, u);
+    wm_used = wm;
     float wo_dot_wm = dot(wo, wm);
     float R = fresnel_real(ior, wo_dot_wm, eta_computed), T = 1 - R;
     float pr = R, pt = T;
@@ -640,8 +644,19 @@ static inline float u8f(float v) { return v * (1.f / 255.f); } /* rgb_uint2float
 
 /* PrincipledMaterial::scatter + sampleBSDF (NovaMaterials.h:56-137).  Consumes four sampler
  * dimensions: uc, u0[2] (lobe choice and direction), then uc again for sample_f. */
+/* Optional inputs of scatter beyond the reference's: parameter values that replace the base
+ * albedo / roughness, a microfacet normal to evaluate at instead of sampling, and where to report
+ * the microfacet normal used. */
+struct ScatterOpts {
+  const Spec *albedo = nullptr;
+  const float *roughness = nullptr;
+  const V3 *force_wm = nullptr;
+  V3 *wm_out = nullptr;
+};
+
 static bool scatter(const Scene &s, const Ray &in, const HitRecord &hr, const Material &mat, uint32_t index,
-                    unsigned &dim, uint32_t seed, Scatter &out) {
+                    unsigned &dim, uint32_t seed, Scatter &out, int32_t prim, uint32_t mat_id,
+                    const ScatterOpts &so = ScatterOpts{}) {
   float u = hr.u, v = hr.v;
   V3 nmap{0.f, 0.f, 1.f};
   if (mat.normalmap >= 0) {
@@ -665,12 +680,17 @@ static bool scatter(const Scene &s, const Ray &in, const HitRecord &hr, const Ma
     alb = {u8f(t.x), u8f(t.y), u8f(t.z), u8f(t.w)};
   }
   bp.albedo = {alb.x, alb.y, alb.z};
+  if (!s.diff_albedo.empty())
+    bp.albedo = {s.diff_albedo[3 * prim], s.diff_albedo[3 * prim + 1], s.diff_albedo[3 * prim + 2]};
+  if (so.albedo) bp.albedo = *so.albedo;
   V3 met{0.f, 0.f, 0.f};
   if (mat.metallic >= 0) {
     V4 t = sample_u8(s.textures[mat.metallic], u, v);
     met = {u8f(t.x), u8f(t.y), u8f(t.z)};
   }
   bp.roughness = met.y;
+  if (!s.diff_rough.empty()) bp.roughness = s.diff_rough[mat_id];
+  if (so.roughness) bp.roughness = *so.roughness;
   bp.metal = met.z;
   bp.transmission = (spec_nonzero(mat.eta) && !spec_nonzero(mat.k)) ? 1.f : 0.f;
   bp.anisotropy = mat.anisotropy;
@@ -683,6 +703,7 @@ static bool scatter(const Scene &s, const Ray &in, const HitRecord &hr, const Ma
   u0[0] = sobol_sample(index, dim++, seed);
   u0[1] = sobol_sample(index, dim++, seed);
   PrincipledBSDF bsdf(bp, uc);
+  bsdf.force_wm = so.force_wm;
   if (bsdf.flags() & (F_GLOSSY | F_REFL)) {
     if (bp.wo_dot_ng >= 0) {
       V3 cns = normalize(correct_specular_shading_normal(bp.ng, wo, bp.ns));
@@ -694,6 +715,7 @@ static bool scatter(const Scene &s, const Ray &in, const HitRecord &hr, const Ma
   uc = sobol_sample(index, dim++, seed);
   Sample lobe;
   bool valid = bsdf.sample_f(wo, uc, u0, lobe);
+  if (so.wm_out) *so.wm_out = bsdf.wm_used;
   out = Scatter{};
   out.attenuation = lobe.f;
   if (mat.emissive >= 0) {
@@ -733,6 +755,34 @@ constexpr unsigned kRRDimBase = 200;
 
 /* PathIntegrator::Li, integrator/Integrator.cpp:60-99 (recursive; DENAN per level; miss or
  * depth < 0 returns the environment without an occlusion test; failed scatter returns black). */
+/* The albedo / roughness a vertex shades with (differentiable parameters or textures). */
+static Spec vertex_albedo(const Scene &s, const Material &mat, const HitRecord &hr, int32_t prim) {
+  if (!s.diff_albedo.empty()) return {s.diff_albedo[3 * prim], s.diff_albedo[3 * prim + 1], s.diff_albedo[3 * prim + 2]};
+  if (mat.albedo < 0) return {1.f, 1.f, 1.f};
+  V4 t = sample_u8(s.textures[mat.albedo], hr.u, hr.v);
+  return {u8f(t.x), u8f(t.y), u8f(t.z)};
+}
+static float vertex_roughness(const Scene &s, const Material &mat, const HitRecord &hr, uint32_t mat_id) {
+  if (!s.diff_rough.empty()) return s.diff_rough[mat_id];
+  if (mat.metallic < 0) return 0.f;
+  return u8f(sample_u8(s.textures[mat.metallic], hr.u, hr.v).y);
+}
+
+/* f of the lobe that `dim0` selects, at the directions of the unperturbed sample (microfacet
+ * normal wm), with the given albedo / roughness. */
+static Spec perturbed_f(const Scene &s, const Ray &ray, const HitRecord &hr, const Material &mat, uint32_t index,
+                        unsigned dim0, uint32_t seed, int32_t prim, uint32_t mat_id, V3 wm, const Spec *albedo,
+                        const float *roughness) {
+  ScatterOpts so;
+  so.albedo = albedo;
+  so.roughness = roughness;
+  so.force_wm = &wm;
+  Scatter sc;
+  unsigned dim = dim0;
+  if (!scatter(s, ray, hr, mat, index, dim, seed, sc, prim, mat_id, so)) return {0.f, 0.f, 0.f};
+  return sc.attenuation;
+}
+
 /* Optional per-thread segment log (orc_sample_path): origin, direction, hit prim, t, u, v. */
 thread_local std::vector<float> *g_segment_log = nullptr;
 
@@ -750,9 +800,23 @@ static V4 Li(PathCtx &c, const Ray &ray, int depth, int bounce, Spec beta) {
   }
   if (hit.is_hit && depth >= 0) {
     HitRecord hr = make_record(s, ray, hit);
-    const Material &mat = s.materials[s.inst_mat[s.prims[hit.prim].inst]];
+    const uint32_t mat_id = s.inst_mat[s.prims[hit.prim].inst];
+    const Material &mat = s.materials[mat_id];
     Scatter sc;
-    if (!scatter(s, ray, hr, mat, c.index, c.dim, c.seed, sc)) return {0, 0, 0, 0};
+    const unsigned dim0 = c.dim;
+    V3 wm{0, 0, 1};
+    ScatterOpts so;
+    so.wm_out = &wm;
+    if (!scatter(s, ray, hr, mat, c.index, c.dim, c.seed, sc, hit.prim, mat_id, so)) return {0, 0, 0, 0};
+    if ((s.pert_kind == 1 && s.pert_index == (uint32_t)hit.prim) || (s.pert_kind == 2 && s.pert_index == mat_id)) {
+      Spec a = vertex_albedo(s, mat, hr, hit.prim);
+      float r = vertex_roughness(s, mat, hr, mat_id);
+      if (s.pert_kind == 1)
+        (s.pert_channel == 0 ? a.x : s.pert_channel == 1 ? a.y : a.z) += s.pert_delta;
+      else
+        r += s.pert_delta;
+      sc.attenuation = perturbed_f(s, ray, hr, mat, c.index, dim0, c.seed, hit.prim, mat_id, wm, &a, &r);
+    }
     Ray out = spawn(sc.lobe.wi, hr.ng, hr.position);
     Spec color = sc.attenuation * sc.lobe.costheta / sc.lobe.pdf;
     if (c.rr_start >= 0 && bounce >= c.rr_start) {
@@ -956,10 +1020,11 @@ extern "C" void orc_scatter(void *h, uint64_t n, const float *o, const float *d,
     hit.u = u[i];
     hit.v = v[i];
     HitRecord hr = make_record(s, ray, hit);
-    const Material &mat = s.materials[s.inst_mat[s.prims[hit.prim].inst]];
+    const uint32_t mat_id = s.inst_mat[s.prims[hit.prim].inst];
+    const Material &mat = s.materials[mat_id];
     unsigned dim = 2u + 4u * (unsigned)bounce[i];
     Scatter sc;
-    const bool ok = scatter(s, ray, hr, mat, index[i], dim, seed, sc);
+    const bool ok = scatter(s, ray, hr, mat, index[i], dim, seed, sc, hit.prim, mat_id);
     Ray nx = spawn(sc.lobe.wi, hr.ng, hr.position);
     Spec w = sc.attenuation * sc.lobe.costheta / sc.lobe.pdf;
     const float oo[3] = {nx.o.x, nx.o.y, nx.o.z}, dd[3] = {nx.d.x, nx.d.y, nx.d.z}, ww[3] = {w.x, w.y, w.z},
@@ -972,6 +1037,131 @@ extern "C" void orc_scatter(void *h, uint64_t n, const float *o, const float *d,
     }
     valid[i] = ok ? 1 : 0;
   }
+}
+
+extern "C" int32_t orc_set_diff_params(void *h, const float *albedo, const float *roughness) {
+  Scene &s = *static_cast<Scene *>(h);
+  if (albedo)
+    s.diff_albedo.assign(albedo, albedo + 3 * s.prims.size());
+  else
+    s.diff_albedo.clear();
+  if (roughness)
+    s.diff_rough.assign(roughness, roughness + s.materials.size());
+  else
+    s.diff_rough.clear();
+  return 0;
+}
+
+extern "C" int32_t orc_set_perturbation(void *h, int32_t kind, uint32_t index, int32_t channel, float delta) {
+  Scene &s = *static_cast<Scene *>(h);
+  if (kind < 0 || kind > 2 || channel < 0 || channel > 2) return 1;
+  s.pert_kind = kind;
+  s.pert_index = index;
+  s.pert_channel = channel;
+  s.pert_delta = delta;
+  return 0;
+}
+
+/* Replay adjoint on the CPU, the checker of nova_b200_backward: for every sample, the path's
+ * radiance I (primal), then the same path again from its Sobol index; at each vertex the score
+ * d ln f / d theta of the sampled lobe comes from central differences of f at the sampled
+ * directions (h = 1e-3, the sampling density held fixed), and
+ *   grad[theta] += sum_c dI_c R_c score_c,  R = I - emission gathered up to the vertex,
+ * dI = d_image / spp.  Gradients are summed in double per thread and added to the outputs. */
+extern "C" int32_t orc_backward(void *h, const orc_options *opt, const float *d_image, float *grad_albedo,
+                                float *grad_roughness, int32_t threads) {
+  const Scene &s = *static_cast<Scene *>(h);
+  if (opt->width <= 0 || opt->height <= 0 || opt->spp <= 0 || opt->max_depth < 0 || !d_image) return 1;
+  const int W = opt->width, H = opt->height;
+  const unsigned nt = threads > 0 ? (unsigned)threads : std::max(1u, std::thread::hardware_concurrency());
+  const size_t na = 3 * s.prims.size(), nm = s.materials.size();
+  std::vector<std::vector<double>> ga(nt, std::vector<double>(grad_albedo ? na : 0, 0.0));
+  std::vector<std::vector<double>> gr(nt, std::vector<double>(grad_roughness ? nm : 0, 0.0));
+  std::atomic<int> next_row{0};
+  auto work = [&](unsigned wid) {
+    PathCtx c{&s, 0, 0, opt->seed, opt->rr_start, 0, 0, {}};
+    const float hd = 1e-3f;
+    for (int y; (y = next_row.fetch_add(1)) < H;) {
+      for (int x = 0; x < W; x++) {
+        const size_t row = opt->vertical_invert ? (size_t)(H - 1 - y) : (size_t)y;
+        const float *dp = d_image + (row * W + x) * 4;
+        const Spec dl{dp[0] / (float)opt->spp, dp[1] / (float)opt->spp, dp[2] / (float)opt->spp};
+        for (int smp = 0; smp < opt->spp; smp++) {
+          const V4 I = render_sample(c, *opt, x, y, smp);
+          /* replay */
+          constexpr float RAND_DX = 0.0005f, RAND_DY = 0.0005f;
+          c.index = sample_index(*opt, x, y, smp);
+          c.dim = 0;
+          const float r0 = sobol_sample(c.index, c.dim++, c.seed);
+          const float r1 = sobol_sample(c.index, c.dim++, c.seed);
+          Ray ray = camera_ray(s, x, opt->height - y, W, H, r0 * RAND_DX, r1 * RAND_DY);
+          Spec beta = v3(1.f), rem{I.x, I.y, I.z};
+          for (int depth = opt->max_depth, bounce = 0;; depth--, bounce++) {
+            const Hit hit = trace(s, ray, nullptr);
+            if (!hit.is_hit || depth < 0) break;
+            const HitRecord hr = make_record(s, ray, hit);
+            const uint32_t mat_id = s.inst_mat[s.prims[hit.prim].inst];
+            const Material &mat = s.materials[mat_id];
+            const unsigned dim0 = c.dim;
+            V3 wm{0, 0, 1};
+            ScatterOpts so;
+            so.wm_out = &wm;
+            Scatter sc;
+            const bool valid = scatter(s, ray, hr, mat, c.index, c.dim, c.seed, sc, hit.prim, mat_id, so);
+            rem = rem - beta * sc.emissive;
+            if (!valid) break;
+            const Spec f = sc.attenuation;
+            const float fv[3] = {f.x, f.y, f.z}, dv[3] = {dl.x * rem.x, dl.y * rem.y, dl.z * rem.z};
+            const Spec a0 = vertex_albedo(s, mat, hr, hit.prim);
+            const float r0v = vertex_roughness(s, mat, hr, mat_id);
+            if (grad_albedo) {
+              for (int ch = 0; ch < 3; ch++) {
+                if (fv[ch] == 0.f || dv[ch] == 0.f) continue;
+                Spec ap = a0, am = a0;
+                (ch == 0 ? ap.x : ch == 1 ? ap.y : ap.z) += hd;
+                (ch == 0 ? am.x : ch == 1 ? am.y : am.z) -= hd;
+                const Spec fp = perturbed_f(s, ray, hr, mat, c.index, dim0, c.seed, hit.prim, mat_id, wm, &ap, &r0v);
+                const Spec fm = perturbed_f(s, ray, hr, mat, c.index, dim0, c.seed, hit.prim, mat_id, wm, &am, &r0v);
+                const float fpc = ch == 0 ? fp.x : ch == 1 ? fp.y : fp.z, fmc = ch == 0 ? fm.x : ch == 1 ? fm.y : fm.z;
+                ga[wid][3 * (size_t)hit.prim + ch] += (double)dv[ch] * ((double)fpc - fmc) / (2.0 * hd * fv[ch]);
+              }
+            }
+            if (grad_roughness && r0v > hd) {
+              const float rp = r0v + hd, rm = r0v - hd;
+              const Spec fp = perturbed_f(s, ray, hr, mat, c.index, dim0, c.seed, hit.prim, mat_id, wm, &a0, &rp);
+              const Spec fm = perturbed_f(s, ray, hr, mat, c.index, dim0, c.seed, hit.prim, mat_id, wm, &a0, &rm);
+              const float pv[3] = {fp.x, fp.y, fp.z}, mv[3] = {fm.x, fm.y, fm.z};
+              double g = 0.0;
+              for (int ch = 0; ch < 3; ch++)
+                if (fv[ch] != 0.f) g += (double)dv[ch] * ((double)pv[ch] - mv[ch]) / (2.0 * hd * fv[ch]);
+              gr[wid][mat_id] += g;
+            }
+            Ray out = spawn(sc.lobe.wi, hr.ng, hr.position);
+            Spec color = sc.attenuation * sc.lobe.costheta / sc.lobe.pdf;
+            if (c.rr_start >= 0 && bounce >= c.rr_start) {
+              Spec nb = beta * color;
+              float q = std::min(1.f, std::max(0.05f, std::max(nb.x, std::max(nb.y, nb.z))));
+              float urr = sobol_sample(c.index, kRRDimBase + (unsigned)bounce, c.seed);
+              if (!(urr < q)) break;
+              color = color / q;
+            }
+            beta = beta * color;
+            ray = out;
+          }
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned i = 0; i < nt; i++) pool.emplace_back(work, i);
+  for (auto &t : pool) t.join();
+  for (unsigned w = 0; w < nt; w++) {
+    if (grad_albedo)
+      for (size_t k = 0; k < na; k++) grad_albedo[k] += (float)ga[w][k];
+    if (grad_roughness)
+      for (size_t k = 0; k < nm; k++) grad_roughness[k] += (float)gr[w][k];
+  }
+  return 0;
 }
 
 extern "C" void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int32_t *px, const int32_t *py,

@@ -116,12 +116,22 @@ void orc_camera_rays(void *h, const orc_options *opt, uint64_t n, const int32_t 
 int32_t orc_render(void *h, const orc_options *opt, float *out_rgba, const int32_t *pixel_ids, int64_t n_pixels,
                    orc_stats *stats);
 
-/* Radiance of single samples (pixel x, y, sample s), RGB into out (3 per sample). */
+/* The segments of one path: 10 floats each (origin, direction, hit primitive bits, t, u, v). */
 int32_t orc_sample_path(void *h, const orc_options *opt, int32_t x, int32_t y, int32_t s, float *out,
                         int32_t max_segments, float *radiance);
+/* One shading event per hit: next origin / direction, weight, emission, valid. */
 void orc_scatter(void *h, uint64_t n, const float *o, const float *d, const int32_t *prim, const float *t,
                  const float *u, const float *v, const uint32_t *index, const int32_t *bounce, uint32_t seed,
                  float *out_o, float *out_d, float *weight, float *emissive, int32_t *valid);
+/* Differentiable parameters (3 x triangles albedo, materials roughness; NULL = textures). */
+int32_t orc_set_diff_params(void *h, const float *albedo, const float *roughness);
+/* Detached perturbation (kind 0 none, 1 albedo of triangle `index` channel `channel`, 2 roughness
+ * of material `index`): f evaluated with the parameter moved by delta, sampling unperturbed. */
+int32_t orc_set_perturbation(void *h, int32_t kind, uint32_t index, int32_t channel, float delta);
+/* Replay adjoint: adds dLoss/dalbedo, dLoss/droughness for d_image = dLoss/dImage (W*H*4). */
+int32_t orc_backward(void *h, const orc_options *opt, const float *d_image, float *grad_albedo,
+                     float *grad_roughness, int32_t threads);
+/* Radiance of single samples (pixel x, y, sample s), RGB into out (3 per sample). */
 void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int32_t *px, const int32_t *py,
                          const int32_t *s, float *out);
 

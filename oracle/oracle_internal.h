@@ -74,6 +74,17 @@ struct Scene {
   int envmap = -1;
   M4 inv_P, inv_V;
   std::vector<Prim> prims;
+  /* differentiable parameters (extension): per-triangle RGB albedo, per-material roughness;
+   * empty = textures */
+  std::vector<float> diff_albedo, diff_rough;
+  /* detached perturbation of one parameter (finite differences of the detached-sampling
+   * estimator): f is evaluated with the parameter moved by pert_delta at the directions and
+   * densities of the unperturbed parameters.  kind 0: none, 1: albedo of triangle pert_index,
+   * channel pert_channel, 2: roughness of material pert_index. */
+  int pert_kind = 0;
+  uint32_t pert_index = 0;
+  int pert_channel = 0;
+  float pert_delta = 0.f;
   /* native BVH */
   std::vector<Node> nodes;
   std::vector<int32_t> prim_idx;

@@ -80,6 +80,12 @@ def lib():
         L.orc_sample_path.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int32, C.c_int32, C.c_int32, f32p,
                                       C.c_int32, f32p]
         L.orc_sample_path.restype = C.c_int32
+        L.orc_set_diff_params.argtypes = [C.c_void_p, f32p, f32p]
+        L.orc_set_diff_params.restype = C.c_int32
+        L.orc_set_perturbation.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_int32, C.c_float]
+        L.orc_set_perturbation.restype = C.c_int32
+        L.orc_backward.argtypes = [C.c_void_p, C.POINTER(OrcOptions), f32p, f32p, f32p, C.c_int32]
+        L.orc_backward.restype = C.c_int32
         L.orc_scatter.argtypes = [C.c_void_p, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, u32p, i32p, C.c_uint32,
                                   f32p, f32p, f32p, f32p, i32p]
         L.orc_trace.argtypes = [C.c_void_p, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, C.POINTER(OrcStats)]
@@ -233,6 +239,29 @@ class OracleScene:
         lib().orc_scatter(self.h, n, _p(o, f32p), _p(d, f32p), _p(prim, i32p), _p(t, f32p), _p(u, f32p), _p(v, f32p),
                           _p(index, u32p), _p(bounce, i32p), seed, *[_p(a, f32p) for a in outs], _p(valid, i32p))
         return (*outs, valid)
+
+    def set_diff_params(self, albedo=None, roughness=None):
+        """Per-triangle RGB albedo ((n_tris, 3)) / per-material roughness; None = textures."""
+        self._alb = None if albedo is None else np.ascontiguousarray(albedo, np.float32).reshape(-1)
+        self._rough = None if roughness is None else np.ascontiguousarray(roughness, np.float32)
+        lib().orc_set_diff_params(self.h, None if self._alb is None else _p(self._alb, f32p),
+                                  None if self._rough is None else _p(self._rough, f32p))
+
+    def set_perturbation(self, kind=0, index=0, channel=0, delta=0.0):
+        """Detached perturbation: 1 = albedo of triangle `index` (channel), 2 = roughness of
+        material `index`; f is evaluated with the moved parameter, sampling is unperturbed."""
+        if lib().orc_set_perturbation(self.h, kind, index, channel, delta) != 0:
+            raise ValueError("bad perturbation")
+
+    def backward(self, opt, d_image, n_tris, n_materials, threads=0):
+        """Replay adjoint on the CPU: (grad_albedo (n_tris, 3), grad_roughness (n_materials,))."""
+        d_image = np.ascontiguousarray(d_image, np.float32)
+        ga = np.zeros(3 * n_tris, np.float32)
+        gr = np.zeros(n_materials, np.float32)
+        rc = lib().orc_backward(self.h, C.byref(opt), _p(d_image, f32p), _p(ga, f32p), _p(gr, f32p), threads)
+        if rc != 0:
+            raise ValueError("oracle backward failed")
+        return ga.reshape(n_tris, 3), gr
 
     def sample_radiance(self, opt, px, py, ps):
         px, py, ps = (np.ascontiguousarray(a, np.int32) for a in (px, py, ps))
