@@ -151,6 +151,7 @@ void free_scene(nova_b200_ctx *c) {
   c->h_instances.clear();
   c->h_valid.clear();
   c->scene_ready = c->bvh_ready = false;
+  c->primal_valid = false;
   c->scene_bytes = 0;
   c->n_nodes = c->n_leaves = 0;
 }
@@ -472,6 +473,7 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   c->d_nodes = nullptr;
   c->d_tris = nullptr;
   c->bvh_ready = false;
+  c->primal_valid = false;
   uint32_t *d_valid = nullptr, *d_order = nullptr;
   float4 *d_lo = nullptr, *d_hi = nullptr;
   const size_t max_nodes = std::max<size_t>(2 * (size_t)n, 2);
@@ -590,13 +592,15 @@ nova_b200_status nova_b200_set_diff_params(nova_b200_ctx *c, const float *albedo
   if (!c->scene_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "upload a scene first%s");
   c->scene.diff_albedo = albedo;
   c->scene.diff_rough = roughness;
+  c->primal_valid = false;
   return NOVA_B200_SUCCESS;
 }
 
 nova_b200_status nova_b200_backward(nova_b200_ctx *c, const nova_b200_frame *f, const float *d_image,
-                                    float *grad_albedo, float *grad_roughness, nova_b200_render_stats *stats) {
+                                    float *grad_albedo, float *grad_roughness, uint32_t flags,
+                                    nova_b200_render_stats *stats) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;
-  return nb_backward(c, f, d_image, grad_albedo, grad_roughness, stats);
+  return nb_backward(c, f, d_image, grad_albedo, grad_roughness, flags, stats);
 }
 
 nova_b200_status nova_b200_scene_info(nova_b200_ctx *c, uint64_t *tris, uint64_t *insts, uint64_t *nodes,

@@ -63,6 +63,10 @@ struct nova_b200_ctx {
   /* adjoint: the replay queues' extra path state (remaining radiance, image adjoint) */
   float4 *d_adj = nullptr;
   uint32_t adj_cap = 0;
+  /* the radiance buffer holds every path of this frame (last single render, one pass) */
+  bool primal_valid = false;
+  nova_b200_frame primal_frame{};
+  const float *primal_albedo = nullptr, *primal_rough = nullptr;
 };
 
 namespace nbctx {
@@ -97,7 +101,7 @@ nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *fi
 nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
                                  float *const *films_host, float *const *films_device, nova_b200_render_stats *stats);
 nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const float *d_image, float *grad_albedo,
-                             float *grad_roughness, nova_b200_render_stats *stats);
+                             float *grad_roughness, uint32_t flags, nova_b200_render_stats *stats);
 nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,
                           float *u, float *v);
 nova_b200_status nb_scatter(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, const int32_t *prim,

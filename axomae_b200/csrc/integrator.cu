@@ -359,6 +359,42 @@ struct AdjQueue {
   float4 *rem, *dl;
 };
 
+/* Adds v[0..N) to base[key * N + 0..N) for every active lane.  Lanes of the warp with the same key
+ * are summed first (pointer jumping along the lanes that share the key: after five rounds the
+ * first lane of each key holds its sum), so a key costs one atomic per value per warp.  Camera
+ * paths of neighbouring pixels share triangles and materials, and a large triangle can be hit by a
+ * sizeable part of the image: without the warp sum, its atomics serialise.  All 32 lanes must call
+ * this together. */
+template <int N>
+__device__ __forceinline__ void warp_add_by_key(bool active, uint32_t key, const float (&v)[N], float *base) {
+  const unsigned full = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned peers = __match_any_sync(full, active ? key : 0xffffffffu);
+  const unsigned above = lane == 31u ? 0u : (peers & (0xffffffffu << (lane + 1u)));
+  int nxt = above ? __ffs(above) - 1 : 32;
+  float sum[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) sum[k] = active ? v[k] : 0.f;
+#pragma unroll
+  for (int it = 0; it < 5; it++) {
+    const int src = nxt < 32 ? nxt : (int)lane;
+    float t[N];
+#pragma unroll
+    for (int k = 0; k < N; k++) t[k] = __shfl_sync(full, sum[k], src);
+    const int nn = __shfl_sync(full, nxt, src);
+    if (nxt < 32) {
+#pragma unroll
+      for (int k = 0; k < N; k++) sum[k] += t[k];
+      nxt = nn;
+    }
+  }
+  if (active && lane == (unsigned)(__ffs(peers) - 1)) {
+#pragma unroll
+    for (int k = 0; k < N; k++)
+      if (sum[k] != 0.f) atomicAdd(base + (size_t)key * N + k, sum[k]);
+  }
+}
+
 template <class JS>
 __global__ void __launch_bounds__(256) k_refill_adj(Queue q, AdjQueue a, const WaveCounters *wcp, const float4 *L,
                                                     const float4 *d_image, const __grid_constant__ JS js) {
@@ -388,8 +424,10 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
   const uint32_t n = wcp->hit_count;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if ((i & ~31u) >= n) return;
-  bool enq = false;
+  bool enq = false, g_act = false;
   float4 no{}, nd{}, nbeta{}, nrem{}, ndl{};
+  uint32_t g_prim = 0, g_mat = 0;
+  float va[3] = {0.f, 0.f, 0.f}, vr[1] = {0.f};
   if (i < n) {
     const uint32_t slot_in = hit_slot[i];
     const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
@@ -414,14 +452,14 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
     if (sc.has_emissive) rem = rem - beta * sr.emissive;
     if (sr.valid) {
       const V3 cw = dl * rem;
-      if (g_alb) {
-        float *ga = g_alb + 3 * (size_t)prim;
-        if (cw.x * scs.albedo.x != 0.f) atomicAdd(ga, cw.x * scs.albedo.x);
-        if (cw.y * scs.albedo.y != 0.f) atomicAdd(ga + 1, cw.y * scs.albedo.y);
-        if (cw.z * scs.albedo.z != 0.f) atomicAdd(ga + 2, cw.z * scs.albedo.z);
-      }
+      g_act = true;
+      g_prim = (uint32_t)prim;
+      g_mat = I.material;
+      va[0] = cw.x * scs.albedo.x;
+      va[1] = cw.y * scs.albedo.y;
+      va[2] = cw.z * scs.albedo.z;
       const float gr = ((cw.x + cw.y) + cw.z) * scs.roughness;
-      if (g_rough && gr != 0.f && isfinite(gr)) atomicAdd(g_rough + I.material, gr);
+      vr[0] = isfinite(gr) ? gr : 0.f;
       V3 c = sr.weight;
       bool alive = true;
       if (rp.rr_start >= 0 && bounce >= rp.rr_start) {
@@ -447,6 +485,8 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
       }
     }
   }
+  if (g_alb) warp_add_by_key<3>(g_act, g_prim, va, g_alb);
+  if (g_rough) warp_add_by_key<1>(g_act, g_mat, vr, g_rough);
   const unsigned slot = warp_append(enq, &wcp->out_count);
   if (enq) {
     out.o[slot] = no;
@@ -817,6 +857,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u};
   nova_b200_status st = ensure_wave_buffers(x, cap, radiance);
   if (st != NOVA_B200_SUCCESS) return st;
+  x->primal_valid = false; /* this render overwrites the radiance buffer */
   for (size_t j = 0; j < nj; j++) {
     nova_b200_ctx *c = ctxs[j];
     if ((st = ensure_film(c, frames[j]->width, frames[j]->height)) != NOVA_B200_SUCCESS) return st;
@@ -920,6 +961,12 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
               "copy film");
   }
   NB_CUDA(x, cudaStreamSynchronize(x->stream), "render");
+  if (nj == 1 && chunks.size() == 1 && chunks[0].size() == 1) {
+    x->primal_valid = true;
+    x->primal_frame = *frames[0];
+    x->primal_albedo = x->scene.diff_albedo;
+    x->primal_rough = x->scene.diff_rough;
+  }
   float total_ms = 0.f;
   cudaEventElapsedTime(&total_ms, x->ev_begin, x->ev_end);
   loop.add_to(sum);
@@ -962,8 +1009,16 @@ nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_fra
   return render_jobs(x, cs, fs, films_host, films_device, stats);
 }
 
+/* The frame fields that decide every path of a render (reset and vertical_invert do not). */
+bool same_paths(const nova_b200_frame &a, const nova_b200_frame &b) {
+  return a.width == b.width && a.height == b.height && a.spp_total == b.spp_total &&
+         a.sample_begin == b.sample_begin && a.sample_count == b.sample_count && a.max_depth == b.max_depth &&
+         a.seed == b.seed && a.rr_start == b.rr_start && std::memcmp(a.inv_P, b.inv_P, sizeof(a.inv_P)) == 0 &&
+         std::memcmp(a.inv_V, b.inv_V, sizeof(a.inv_V)) == 0;
+}
+
 nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const float *d_image, float *grad_albedo,
-                             float *grad_roughness, nova_b200_render_stats *stats) {
+                             float *grad_roughness, uint32_t flags, nova_b200_render_stats *stats) {
   using namespace nbctx;
   nova_b200_status st = validate_frame(c, f);
   if (st != NOVA_B200_SUCCESS) return st;
@@ -996,6 +1051,9 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
   LoopStats primal, replay;
   NB_CUDA(c, cudaEventRecord(c->ev_begin, c->stream), "event");
   const uint32_t per_chunk = (uint32_t)std::max<uint64_t>(1, radiance / NP);
+  const bool reuse = (flags & NOVA_B200_BACKWARD_REUSE_PRIMAL) && c->primal_valid &&
+                     per_chunk >= (uint32_t)f->sample_count && same_paths(c->primal_frame, *f) &&
+                     c->primal_albedo == c->scene.diff_albedo && c->primal_rough == c->scene.diff_rough;
   for (uint32_t s0 = 0; s0 < (uint32_t)f->sample_count; s0 += per_chunk) {
     const uint32_t take = std::min<uint32_t>(per_chunk, (uint32_t)f->sample_count - s0);
     OneJob one{};
@@ -1021,7 +1079,7 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
       enqueue_group(c, one, ls, width, slot, false);
       return cudaGetLastError();
     };
-    if ((st = run_waves(c, J.n_paths, cap, fwd, primal)) != NOVA_B200_SUCCESS) return st;
+    if (!reuse && (st = run_waves(c, J.n_paths, cap, fwd, primal)) != NOVA_B200_SUCCESS) return st;
     /* replay with the adjoint */
     auto bwd = [&](int slot) {
       if (width == 8)
@@ -1041,6 +1099,11 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
   replay.add_to(sum);
   sum.device_ms = total_ms;
   if (stats) *stats = sum;
+  /* a one-pass backward leaves this frame's radiance in the buffer */
+  c->primal_valid = per_chunk >= (uint32_t)f->sample_count;
+  c->primal_frame = *f;
+  c->primal_albedo = c->scene.diff_albedo;
+  c->primal_rough = c->scene.diff_rough;
   return NOVA_B200_SUCCESS;
 }
 

@@ -66,6 +66,7 @@ class Tuning(C.Structure):
 
 
 TUNE_BVH_WIDTH = 1
+BACKWARD_REUSE_PRIMAL = 1
 
 
 class BvhOptions(C.Structure):
@@ -114,7 +115,7 @@ def lib():
         L.nova_b200_trace.argtypes = [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]
         L.nova_b200_sobol.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, vp]
         L.nova_b200_set_diff_params.argtypes = [vp, vp, vp]
-        L.nova_b200_backward.argtypes = [vp, C.POINTER(Frame), vp, vp, vp, C.POINTER(RenderStats)]
+        L.nova_b200_backward.argtypes = [vp, C.POINTER(Frame), vp, vp, vp, C.c_uint32, C.POINTER(RenderStats)]
         L.nova_b200_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.nova_b200_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.nova_b200_autotune.argtypes = [C.POINTER(vp), C.POINTER(Frame), C.c_uint32, C.c_char_p, C.c_uint32,
@@ -323,13 +324,14 @@ class Context:
         self._check(lib().nova_b200_set_diff_params(self.h, C.c_void_p(albedo_ptr) if albedo_ptr else None,
                                                     C.c_void_p(roughness_ptr) if roughness_ptr else None))
 
-    def backward(self, frame, d_image_ptr, grad_albedo_ptr=None, grad_roughness_ptr=None) -> "RenderStats":
+    def backward(self, frame, d_image_ptr, grad_albedo_ptr=None, grad_roughness_ptr=None,
+                 reuse_primal=False) -> "RenderStats":
         """Replay adjoint: adds dLoss/dparams to the gradient buffers (device pointers)."""
         st = RenderStats()
         self._check(lib().nova_b200_backward(self.h, C.byref(frame), C.c_void_p(d_image_ptr),
                                              C.c_void_p(grad_albedo_ptr) if grad_albedo_ptr else None,
                                              C.c_void_p(grad_roughness_ptr) if grad_roughness_ptr else None,
-                                             C.byref(st)))
+                                             BACKWARD_REUSE_PRIMAL if reuse_primal else 0, C.byref(st)))
         return st
 
     def set_tuning(self, tuning=None, **kw):

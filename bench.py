@@ -44,7 +44,8 @@ HF_METRIC = "Mrays/s (plain wavefront path tracing, heightfield workload)"
 BATCH_WORKLOAD = ("32 jobs: mixed spheres+boxes scenes of 50k-500k tris (Lambert / GGX conductor / GGX "
                   "dielectric IOR 1.5), square frames log-uniform 256^2-2048^2, spp in {1,4,16,64}, "
                   "depth in {3,6,12}, seed 0")
-BATCH_METRIC = "Mrays/s batched wavefront (32-job batch; plain wavefront on the same jobs in extra.plain)"
+BATCH_METRIC = ("Mrays/s batched wavefront (32-job batch; plain wavefront on the same jobs in extra.plain; "
+                "adjoint/forward time ratio in extra.adjoint)")
 
 
 def peaks():
@@ -290,6 +291,55 @@ def timed(step, steps, torch, dist, clock=None):
     return acc, step_ms, traced
 
 
+ADJ_CFG = dict(width=256, height=256, spp=64, depth=4)
+
+
+def adjoint_timing(local_rank, reps=3):
+    """The differentiable configuration: the 64-sphere scene at 256 x 256, 64 spp, depth 4, with
+    per-triangle albedo (init 0.5) and per-material roughness (init 0.3) as parameters and an L2
+    loss against a target rendered with seeded albedo U[0.2, 0.8] and roughness U[0.1, 0.6].
+    Returns the device times of one forward render and one replay-adjoint backward."""
+    import torch
+    from axomae_b200 import native, scenes
+    W, H, spp, depth = ADJ_CFG["width"], ADJ_CFG["height"], ADJ_CFG["spp"], ADJ_CFG["depth"]
+    s = scenes.spheres_scene(W, H)
+    c = native.Context(local_rank)
+    c.upload(s)
+    c.build()
+    ntri, nmat = c.info()["triangles"], len(s["materials"])
+    rng = np.random.default_rng(0)
+    alb_t = torch.tensor(rng.uniform(0.2, 0.8, (ntri, 3)), dtype=torch.float32, device="cuda")
+    rough_t = torch.tensor(rng.uniform(0.1, 0.6, nmat), dtype=torch.float32, device="cuda")
+    alb = torch.full((ntri, 3), 0.5, device="cuda")
+    rough = torch.full((nmat,), 0.3, device="cuda")
+    fr = native.make_frame(s, W, H, spp, depth)
+    T = torch.zeros((H, W, 4), device="cuda")
+    c.set_diff_params(alb_t.data_ptr(), rough_t.data_ptr())
+    c.render(fr, film_device_ptr=T.data_ptr())
+    c.set_diff_params(alb.data_ptr(), rough.data_ptr())
+    img = torch.zeros((H, W, 4), device="cuda")
+    ga = torch.zeros_like(alb)
+    gr = torch.zeros_like(rough)
+    fwd, bwd, bwd_reuse = [], [], []
+    for _ in range(reps + 1):
+        st = c.render(fr, film_device_ptr=img.data_ptr())
+        dI = torch.zeros_like(img)
+        dI[..., :3] = 2.0 * (img[..., :3] - T[..., :3])
+        rst = c.backward(fr, dI.data_ptr(), ga.data_ptr(), gr.data_ptr(), reuse_primal=True)
+        bst = c.backward(fr, dI.data_ptr(), ga.data_ptr(), gr.data_ptr())
+        fwd.append(st.device_ms)
+        bwd.append(bst.device_ms)
+        bwd_reuse.append(rst.device_ms)
+    c.close()
+    f, b, br = float(np.median(fwd[1:])), float(np.median(bwd[1:])), float(np.median(bwd_reuse[1:]))
+    return {"workload": "64 spheres (65,538 tris) 256x256, 64 spp, depth 4; params: %d x 3 albedo + %d roughness"
+                        % (ntri, nmat), "forward_ms": f, "backward_ms": b, "backward_over_forward": b / f,
+            "backward_reusing_forward_ms": br, "backward_reusing_forward_over_forward": br / f,
+            "forward_mrays": st.traced / f / 1e3,
+            "note": "device time (CUDA events); backward = radiance replay + adjoint replay (no stored tape); the "
+                    "reusing variant takes the per-path radiance the forward render left in the radiance buffer"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from axomae_b200 import native
@@ -457,6 +507,8 @@ def run_ours(args, rank, world, local_rank):
                                "on the CPU sample's pixels")
     if cpu:
         extra["rel_rmse_vs_cpu"] = cpu["rel_rmse"]
+    if batched and not args.no_adjoint:
+        extra["adjoint"] = adjoint_timing(local_rank)
     metric = BATCH_METRIC if batched else HF_METRIC
     workload = BATCH_WORKLOAD if batched else HF_WORKLOAD
     if args.frame or args.spp:
@@ -491,6 +543,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="batched arm: keep the default launch tuning")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
     ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="heightfield: override the frame size")
     ap.add_argument("--spp", type=int, help="heightfield: override samples per pixel")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8], help="BVH layout (0 = library default)")

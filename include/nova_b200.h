@@ -219,8 +219,16 @@ nova_b200_status nova_b200_set_diff_params(nova_b200_ctx *ctx, const float *albe
  * (either may be NULL).  No tape is stored: each path is recomputed from its Sobol index, once
  * for its radiance and once to push the adjoint through its vertices, where the derivative of the
  * sampled lobe's f (its sampling density held fixed) is applied.  The film is not touched. */
+#define NOVA_B200_BACKWARD_REUSE_PRIMAL 1u /* see nova_b200_backward */
+
+/* flags: NOVA_B200_BACKWARD_REUSE_PRIMAL skips the radiance pass when the context's last render was
+ * nova_b200_render of this same frame with the same parameter buffers (one pass over the radiance
+ * buffer, nothing rendered on the context since): the paths' radiance is still in the context's
+ * radiance buffer.  The caller guarantees the parameters' contents did not change in between;
+ * when the context cannot reuse the buffer it recomputes it. */
 nova_b200_status nova_b200_backward(nova_b200_ctx *ctx, const nova_b200_frame *frame, const float *d_image_dev,
-                                    float *grad_albedo_dev, float *grad_roughness_dev, nova_b200_render_stats *stats);
+                                    float *grad_albedo_dev, float *grad_roughness_dev, uint32_t flags,
+                                    nova_b200_render_stats *stats);
 
 /* Launch parameters of the wavefront (no counterpart in the reference, whose CPU path has tiles and
  * threads only).  They change speed, never results: every tuning renders the same image, bit for

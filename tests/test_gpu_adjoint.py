@@ -136,3 +136,58 @@ def test_adjoint_cost_and_accumulation(problem, grads):
     # timing on a small frame is launch-dominated; the ratio is checked loosely here and measured
     # at full size by the benchmark
     assert bst.device_ms <= 4.0 * fst.device_ms + 2.0
+
+
+def test_backward_reusing_forward_radiance(problem, grads):
+    """NOVA_B200_BACKWARD_REUSE_PRIMAL right after the forward render gives the same gradients as a
+    standalone backward and skips the radiance pass; after another render it recomputes."""
+    P = problem
+    torch = P["torch"]
+    a = torch.from_numpy(np.ascontiguousarray(P["alb"])).cuda()
+    r = torch.from_numpy(np.ascontiguousarray(P["rough"])).cuda()
+    dI = torch.from_numpy(np.ascontiguousarray(grads["dI"], np.float32)).cuda()
+    img = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    P["c"].set_diff_params(a.data_ptr(), r.data_ptr())
+    try:
+        fst = P["c"].render(P["fr"], film_device_ptr=img.data_ptr())
+        ga = torch.zeros((P["ntri"], 3), dtype=torch.float32, device="cuda")
+        gr = torch.zeros(P["nmat"], dtype=torch.float32, device="cuda")
+        bst = P["c"].backward(P["fr"], dI.data_ptr(), ga.data_ptr(), gr.data_ptr(), reuse_primal=True)
+        assert bst.traced < 0.6 * 2 * fst.traced  # only the replay traced rays
+        ref_a, ref_r = grads["ga"], grads["gr"]
+        assert np.allclose(ga.cpu().numpy(), ref_a, rtol=1e-4, atol=1e-6 * np.abs(ref_a).max())
+        assert np.allclose(gr.cpu().numpy(), ref_r, rtol=1e-4, atol=1e-6 * np.abs(ref_r).max())
+        # a different frame in between: the flag must not reuse the stale radiance
+        other = P["native"].make_frame(P["s"], W, H, SPP, DEPTH, seed=7)
+        P["c"].render(other, film_device_ptr=img.data_ptr())
+        ga.zero_()
+        gr.zero_()
+        bst2 = P["c"].backward(P["fr"], dI.data_ptr(), ga.data_ptr(), gr.data_ptr(), reuse_primal=True)
+        assert bst2.traced > 1.5 * fst.traced
+        assert np.allclose(ga.cpu().numpy(), ref_a, rtol=1e-4, atol=1e-6 * np.abs(ref_a).max())
+    finally:
+        P["c"].set_diff_params(None, None)
+
+
+def test_autograd_optimisation_reduces_loss(problem):
+    """The forward/backward pair wrapped in torch.autograd.Function drives Adam on the L2 image loss
+    toward the target's albedo and roughness."""
+    import nova_autograd
+    P = problem
+    torch = P["torch"]
+    target = torch.from_numpy(_render(P, P["alb_t"], P["rough_t"])[0]).cuda()
+    alb = torch.full((P["ntri"], 3), 0.5, device="cuda", requires_grad=True)
+    rough = torch.full((P["nmat"],), 0.3, device="cuda", requires_grad=True)
+    opt = torch.optim.Adam([alb, rough], lr=0.02)
+    losses = []
+    for _ in range(12):
+        opt.zero_grad()
+        img = nova_autograd.render(alb, rough, P["c"], P["fr"], H, W)
+        loss = ((img[..., :3] - target[..., :3]) ** 2).sum()
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            alb.clamp_(0.0, 1.0)
+            rough.clamp_(0.01, 1.0)
+        losses.append(float(loss.detach()))
+    assert losses[-1] < 0.7 * losses[0], losses
