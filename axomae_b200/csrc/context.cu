@@ -194,11 +194,34 @@ __global__ void k_write_tris(nb::DevScene sc, const uint32_t *valid, const uint3
   tris[3 * k + 2] = make_float4(e2.x, e2.y, e2.z, 0.f);
 }
 
-/* Interleaves the SoA vertex attributes of one mesh into 64 B records (layout in device_scene.cuh). */
-__global__ void k_interleave(const float *v, const float *n, const float *t, const float *b, const float *uv,
-                             uint32_t nv, float4 *attr) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
+/* Where one mesh's SoA attributes sit in the staging region and its 64 B records in the arena
+ * (byte offsets), and its first vertex in the scene-wide vertex numbering. */
+struct InterleaveMesh {
+  uint64_t v, n, t, b, uv, attr;
+  uint32_t first_vertex, n_verts;
+};
+
+/* Interleaves the SoA vertex attributes of every mesh into 64 B records (layout in
+ * device_scene.cuh): one thread per vertex of the scene, the mesh found by binary search. */
+__global__ void k_interleave(const InterleaveMesh *meshes, uint32_t n_meshes, uint32_t total, const char *stage,
+                             char *arena) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  uint32_t lo = 0, hi = n_meshes;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (meshes[mid].first_vertex <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const InterleaveMesh &m = meshes[lo];
+  const uint32_t i = g - m.first_vertex;
+  if (i >= m.n_verts) return;
+  const float *v = reinterpret_cast<const float *>(stage + m.v), *n = reinterpret_cast<const float *>(stage + m.n);
+  const float *t = reinterpret_cast<const float *>(stage + m.t), *b = reinterpret_cast<const float *>(stage + m.b);
+  const float *uv = reinterpret_cast<const float *>(stage + m.uv);
+  float4 *attr = reinterpret_cast<float4 *>(arena + m.attr);
   attr[4 * (size_t)i + 0] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], n[3 * i]);
   attr[4 * (size_t)i + 1] = make_float4(n[3 * i + 1], n[3 * i + 2], t[3 * i], t[3 * i + 1]);
   attr[4 * (size_t)i + 2] = make_float4(t[3 * i + 2], b[3 * i], b[3 * i + 1], b[3 * i + 2]);
@@ -340,6 +363,8 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     size_t idx, attr, v, n, t, b, uv;
   };
   std::vector<MeshOffsets> moff(d->n_meshes);
+  std::vector<InterleaveMesh> ilv(d->n_meshes);
+  uint64_t total_verts = 0;
   for (uint32_t i = 0; i < d->n_meshes; i++) {
     const nova_b200_mesh &m = d->meshes[i];
     if (!m.vertices || !m.normals || !m.tangents || !m.bitangents || !m.uv || !m.indices || m.n_tris == 0)
@@ -357,7 +382,11 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     o.t = plan.add(m.tangents, 12 * nv, true);
     o.b = plan.add(m.bitangents, 12 * nv, true);
     o.uv = plan.add(m.uv, 8 * nv, true);
+    ilv[i] = InterleaveMesh{o.v, o.n, o.t, o.b, o.uv, o.attr, (uint32_t)total_verts, m.n_verts};
+    total_verts += nv;
   }
+  if (total_verts >= (1ull << 32)) return fail(c, NOVA_B200_OUT_OF_MEMORY, "more than 2^32 vertices%s");
+  const size_t off_ilv = plan.add(ilv.data(), ilv.size() * sizeof(InterleaveMesh), true);
   /* instances + primitive tables */
   c->h_instances.resize(d->n_instances);
   uint64_t offset = 0;
@@ -424,14 +453,9 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     cudaFreeAsync(temp, c->stream);
     return st;
   }
-  for (uint32_t i = 0; i < d->n_meshes; i++) {
-    const uint32_t nv = d->meshes[i].n_verts;
-    const MeshOffsets &o = moff[i];
-    k_interleave<<<(nv + 255) / 256, 256, 0, c->stream>>>(
-        reinterpret_cast<const float *>(temp + o.v), reinterpret_cast<const float *>(temp + o.n),
-        reinterpret_cast<const float *>(temp + o.t), reinterpret_cast<const float *>(temp + o.b),
-        reinterpret_cast<const float *>(temp + o.uv), nv, reinterpret_cast<float4 *>(arena + o.attr));
-  }
+  if (total_verts)
+    k_interleave<<<(unsigned)((total_verts + 255) / 256), 256, 0, c->stream>>>(
+        reinterpret_cast<const InterleaveMesh *>(temp + off_ilv), d->n_meshes, (uint32_t)total_verts, temp, arena);
   const cudaError_t e_launch = cudaGetLastError();
   cudaFreeAsync(temp, c->stream);
   if (e_launch != cudaSuccess) return cuda_fail(c, e_launch, "k_interleave");
