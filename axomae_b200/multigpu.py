@@ -1,0 +1,44 @@
+"""Multi-GPU partition of a render by sample range (one process per GPU, torch.distributed).
+
+Every rank renders the same frame over its own range of sample indices (the index mapping
+(x * H + y) * spp_total + s keeps the samples disjoint and identical to a single-GPU render of
+spp_total samples), then one all-reduce combines the films.  A rank's film is the mean of its
+samples, so the combination weights each film by its sample count:
+
+    mean = sum_r count_r * film_r / sum_r count_r
+
+The path has no other exchange: scenes and BVHs are built on every rank, and nothing crosses
+between ranks while a frame renders.
+"""
+
+
+def weak_range(spp_per_rank: int, rank: int, world: int):
+    """Weak scaling: every rank adds spp_per_rank samples; returns (spp_total, sample_begin, count)."""
+    if spp_per_rank <= 0 or not 0 <= rank < world:
+        raise ValueError("bad sample partition")
+    return spp_per_rank * world, rank * spp_per_rank, spp_per_rank
+
+
+def strong_range(spp_total: int, rank: int, world: int):
+    """Strong scaling: spp_total samples split as evenly as possible; returns (spp_total, begin, count).
+    Ranks beyond spp_total get an empty range (count 0) and must skip the render but still take part
+    in the reduction."""
+    if spp_total <= 0 or not 0 <= rank < world:
+        raise ValueError("bad sample partition")
+    begin = rank * spp_total // world
+    end = (rank + 1) * spp_total // world
+    return spp_total, begin, end - begin
+
+
+def reduce_films(film, count: int, group=None):
+    """In place: film (a float tensor, this rank's mean over `count` samples) becomes the mean over
+    every rank's samples.  Collective: all ranks call it in the same order."""
+    import torch
+    import torch.distributed as dist
+    total = torch.tensor([float(count)], dtype=torch.float64, device=film.device)
+    film.mul_(float(count))
+    dist.all_reduce(film, group=group)
+    dist.all_reduce(total, group=group)
+    if total.item() > 0:
+        film.div_(total.item())
+    return film

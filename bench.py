@@ -48,6 +48,12 @@ BATCH_METRIC = ("Mrays/s batched wavefront (32-job batch; plain wavefront on the
                 "adjoint/forward time ratio in extra.adjoint)")
 
 
+# DRAM bytes per traced ray that ncu measured for k_trace (dram__bytes_read.sum +
+# dram__bytes_write.sum over full waves of 8,388,608 rays): batched workload waves 1-2, and the
+# heightfield's first wave (camera rays only).
+K_TRACE_DRAM_BYTES_PER_RAY = {"batched": 72.0, "heightfield": 238.4}
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -362,9 +368,12 @@ def run_ours(args, rank, world, local_rank):
         c.build(width=args.bvh_width)
     build_s = time.perf_counter() - t0
     infos = [c.info() for c in ctxs]
-    frames = [native.make_frame(j["scene"], j["width"], j["height"], j["spp"] * world, j["depth"], seed=0,
-                                sample_begin=rank * j["spp"], sample_count=j["spp"], rr_start=j["rr_start"], reset=1)
-              for j in jobs]
+    from axomae_b200 import multigpu
+    frames = []
+    for j in jobs:
+        spp_total, begin, count = multigpu.weak_range(j["spp"], rank, world)
+        frames.append(native.make_frame(j["scene"], j["width"], j["height"], spp_total, j["depth"], seed=0,
+                                        sample_begin=begin, sample_count=count, rr_start=j["rr_start"], reset=1))
     sizes = [j["width"] * j["height"] * 4 for j in jobs]
     offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
     flat = torch.zeros(int(offs[-1]), dtype=torch.float32, device="cuda")
@@ -373,9 +382,8 @@ def run_ours(args, rank, world, local_rank):
     plain_films = [plain_flat[int(offs[k]):int(offs[k + 1])] for k in range(nj)]
 
     def reduce(buf):
-        if dist:
-            dist.all_reduce(buf)
-            buf.div_(world)
+        if dist:  # every rank rendered the same number of samples of every frame
+            multigpu.reduce_films(buf, 1)
 
     def plain_step():
         sts = [c.render(f, film_device_ptr=p.data_ptr()) for c, f, p in zip(ctxs, frames, plain_films)]
@@ -484,8 +492,16 @@ def run_ours(args, rank, world, local_rank):
     roof = None
     if b_ray and trace_rate:
         achieved = trace_rate * b_ray / 1e9
+        rays_per_wave = acc.traced / max(1, acc.waves)
+        dram_ray = K_TRACE_DRAM_BYTES_PER_RAY[args.workload]
         roof = {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": peak_src, "traffic": None,
+                "frac": achieved / hbm, "peak_source": peak_src,
+                "traffic": dram_ray * rays_per_wave,
+                "traffic_note": "DRAM bytes of one full wave (%.0f rays) at %.0f B/ray measured by ncu "
+                                "(dram__bytes_read.sum + dram__bytes_write.sum) on this workload's k_trace waves; "
+                                "achieved uses the algorithmic bytes (reference-BVH node/triangle visits)"
+                                % (rays_per_wave, dram_ray),
+                "dram_gbs_from_traffic": trace_rate * dram_ray / 1e9,
                 "bytes_per_ray": b_ray, "trace_ms_per_step": acc.trace_ms / args.steps}
     extra = {"waves_per_step": acc.waves / args.steps, "traced_per_step": acc.traced / args.steps,
              "paths_per_step": acc.paths / args.steps, "trace_ms_per_step": acc.trace_ms / args.steps,

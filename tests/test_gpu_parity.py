@@ -315,3 +315,24 @@ def test_batch_workload_scene_matches_oracle(job, ctx, oracle, batch_jobs):
     ref, _ = oracle.OracleScene(j["scene"]).render(oracle.options(W, H, j["spp"], j["depth"]))
     err = rel_rmse(film, ref)
     assert err <= REL_RMSE_TOL, err
+
+
+@pytest.mark.parametrize("width", [2, 8], ids=["bvh2", "bvh8"])
+def test_instanced_scene_matches_oracle(ctx, oracle, torch_cuda, width):
+    """Seeded meshes placed many times with random rigid transforms: rays are brought into each
+    instance's object space (Triangle.h:150-153) exactly as the reference does."""
+    from axomae_b200 import scenes
+    s = scenes.instanced_scene(n_meshes=3, n_instances=40, tris_per_mesh=1500, width=64, height=48, seed=8,
+                               box_size=20.0, env_w=64, env_h=32)
+    ctx.upload(s)
+    ctx.build(width=width)
+    film, _ = _render(ctx, s, 64, 48, 8, 8)
+    osc = oracle.OracleScene(s)
+    ref, _ = osc.render(oracle.options(64, 48, 8, 8))
+    assert rel_rmse(film, ref) <= REL_RMSE_TOL
+    rng = np.random.default_rng(3)
+    n = 40000
+    o = rng.uniform(-12, 12, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    _check_hits(ctx, torch_cuda, osc, o, d.astype(np.float32), 1e-4)

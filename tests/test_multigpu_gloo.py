@@ -1,0 +1,83 @@
+"""Sample-range partition and film reduction across ranks (axomae_b200.multigpu), run as gloo
+process groups on the CPU.  Each rank's "render" is the oracle's per-sample radiance averaged over
+the rank's sample range, the same quantity a GPU rank's film holds; the reduced film must equal the
+mean over all samples computed in one process."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+W, H, DEPTH = 12, 9, 3
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_film(osc, ob, spp_total, begin, count):
+    opt = ob.options(W, H, spp_total, DEPTH)
+    ys, xs = np.mgrid[0:H, 0:W]
+    px, py = xs.reshape(-1), ys.reshape(-1)
+    acc = np.zeros((px.size, 3), np.float64)
+    for s in range(begin, begin + count):
+        acc += osc.sample_radiance(opt, px, py, np.full(px.size, s))
+    return (acc / max(count, 1)).astype(np.float32)
+
+
+def _worker(rank, world, port, mode, per, out_dir):
+    import torch
+    import torch.distributed as dist
+    import oracle_binding as ob
+    from axomae_b200 import multigpu, scenes
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        s = scenes.spheres_scene(W, H, n_spheres=6, seed=2)
+        osc = ob.OracleScene(s)
+        if mode == "weak":
+            spp_total, begin, count = multigpu.weak_range(per, rank, world)
+        else:
+            spp_total, begin, count = multigpu.strong_range(per, rank, world)
+        film = torch.from_numpy(_rank_film(osc, ob, spp_total, begin, count) if count else
+                                np.zeros((W * H, 3), np.float32))
+        multigpu.reduce_films(film, count)
+        if rank == 0:
+            np.save(os.path.join(out_dir, "reduced.npy"), film.numpy())
+            full = _rank_film(osc, ob, spp_total, 0, spp_total)
+            np.save(os.path.join(out_dir, "full.npy"), full)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode,world,per", [("weak", 2, 3), ("strong", 2, 7), ("strong", 3, 2)],
+                         ids=["weak-2x3", "strong-7-over-2", "strong-2-over-3"])
+def test_partitioned_render_equals_single_render(oracle, tmp_path, mode, world, per):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_worker, args=(world, port, mode, per, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    reduced = np.load(tmp_path / "reduced.npy")
+    full = np.load(tmp_path / "full.npy")
+    np.testing.assert_allclose(reduced, full, rtol=1e-5, atol=1e-6)
+
+
+def test_ranges_cover_the_frame_once():
+    from axomae_b200 import multigpu
+    for world in (1, 2, 3, 8):
+        for spp in (1, 5, 64):
+            seen = []
+            for r in range(world):
+                tot, b, c = multigpu.strong_range(spp, r, world)
+                assert tot == spp
+                seen += list(range(b, b + c))
+            assert seen == list(range(spp))
+            tot, b, c = multigpu.weak_range(spp, world - 1, world)
+            assert tot == spp * world and b + c == tot
+    with pytest.raises(ValueError):
+        multigpu.weak_range(0, 0, 1)
+    with pytest.raises(ValueError):
+        multigpu.strong_range(4, 2, 2)
