@@ -41,6 +41,11 @@ sys.path.insert(0, ROOT)
 HF = dict(n=1024, width=1920, height=1080, spp=64, depth=8, rr_start=3, env_w=2048, env_h=1024, seed=0)
 HF_WORKLOAD = "heightfield 1024^2 quads (2,097,152 tris), env 2048x1024, 1920x1080, 64 spp, depth 8, RR from 3"
 HF_METRIC = "Mrays/s (plain wavefront path tracing, heightfield workload)"
+IN = dict(width=3840, height=2160, spp=16, depth=12)
+IN_WORKLOAD = ("instanced: 1000 rigid instances of 10 seeded 10k-tri meshes (10,000,000 instanced tris, "
+               "Lambert / GGX conductor / GGX dielectric / Burley) in a 100^3 box, env 4096x2048, 3840x2160, "
+               "16 spp, depth 12")
+IN_METRIC = "Mrays/s (plain wavefront path tracing, instanced workload)"
 BATCH_WORKLOAD = ("32 jobs: mixed spheres+boxes scenes of 50k-500k tris (Lambert / GGX conductor / GGX "
                   "dielectric IOR 1.5), square frames log-uniform 256^2-2048^2, spp in {1,4,16,64}, "
                   "depth in {3,6,12}, seed 0")
@@ -51,7 +56,7 @@ BATCH_METRIC = ("Mrays/s batched wavefront (32-job batch; plain wavefront on the
 # DRAM bytes per traced ray that ncu measured for k_trace (dram__bytes_read.sum +
 # dram__bytes_write.sum over full waves of 8,388,608 rays): batched workload waves 1-2, and the
 # heightfield's first wave (camera rays only).
-K_TRACE_DRAM_BYTES_PER_RAY = {"batched": 72.0, "heightfield": 238.4}
+K_TRACE_DRAM_BYTES_PER_RAY = {"batched": 72.0, "heightfield": 238.4, "instanced": None}
 
 
 def peaks():
@@ -125,6 +130,11 @@ def make_jobs(workload):
                                      env_h=HF["env_h"], seed=HF["seed"])
         return [{"scene": s, "width": HF["width"], "height": HF["height"], "spp": HF["spp"], "depth": HF["depth"],
                  "rr_start": HF["rr_start"]}]
+    if workload == "instanced":
+        s = scenes.instanced_scene(n_meshes=10, n_instances=1000, tris_per_mesh=10000, width=IN["width"],
+                                   height=IN["height"], seed=0, env_w=4096, env_h=2048)
+        return [{"scene": s, "width": IN["width"], "height": IN["height"], "spp": IN["spp"], "depth": IN["depth"],
+                 "rr_start": -1}]
     jobs = scenes.batch_jobs(32, seed=0)
     for j in jobs:
         j["rr_start"] = -1
@@ -199,6 +209,8 @@ def cpu_stride(workload, kind):
     # reference arm: a few seconds per step
     if workload == "heightfield":
         return 2 if kind == "baseline" else 8
+    if workload == "instanced":
+        return 64 if kind == "baseline" else 256
     return 16 if kind == "baseline" else 64
 
 
@@ -217,8 +229,8 @@ def run_reference(args, rank, world):
         vals.append(last["mrays"])
         secs.append(last["seconds"])
     v = float(np.median(vals))
-    metric = HF_METRIC if args.workload == "heightfield" else BATCH_METRIC
-    workload = HF_WORKLOAD if args.workload == "heightfield" else BATCH_WORKLOAD
+    metric = {"heightfield": HF_METRIC, "instanced": IN_METRIC}.get(args.workload, BATCH_METRIC)
+    workload = {"heightfield": HF_WORKLOAD, "instanced": IN_WORKLOAD}.get(args.workload, BATCH_WORKLOAD)
     sample = ("oracle (CPU restatement of the reference Nova path, thread pool of %d workers, 20x20 tiles) on every "
               "%dth pixel of every frame, all samples: %d pixels" % (last["cores"], stride, last["pixels"]))
     line = {"impl": "reference", "metric": metric, "value": v, "unit": "Mrays/s", "n_gpus": world,
@@ -493,10 +505,10 @@ def run_ours(args, rank, world, local_rank):
     if b_ray and trace_rate:
         achieved = trace_rate * b_ray / 1e9
         rays_per_wave = acc.traced / max(1, acc.waves)
-        dram_ray = K_TRACE_DRAM_BYTES_PER_RAY[args.workload]
+        dram_ray = K_TRACE_DRAM_BYTES_PER_RAY[args.workload] or 0.0
         roof = {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_src,
-                "traffic": dram_ray * rays_per_wave,
+                "traffic": dram_ray * rays_per_wave if dram_ray else None,
                 "traffic_note": "DRAM bytes of one full wave (%.0f rays) at %.0f B/ray measured by ncu "
                                 "(dram__bytes_read.sum + dram__bytes_write.sum) on this workload's k_trace waves; "
                                 "achieved uses the algorithmic bytes (reference-BVH node/triangle visits)"
@@ -525,8 +537,8 @@ def run_ours(args, rank, world, local_rank):
         extra["rel_rmse_vs_cpu"] = cpu["rel_rmse"]
     if batched and not args.no_adjoint:
         extra["adjoint"] = adjoint_timing(local_rank)
-    metric = BATCH_METRIC if batched else HF_METRIC
-    workload = BATCH_WORKLOAD if batched else HF_WORKLOAD
+    metric = {"heightfield": HF_METRIC, "instanced": IN_METRIC}.get(args.workload, BATCH_METRIC)
+    workload = {"heightfield": HF_WORKLOAD, "instanced": IN_WORKLOAD}.get(args.workload, BATCH_WORKLOAD)
     if args.frame or args.spp:
         workload += " (overridden: frame %s, spp %s)" % (args.frame, args.spp)
     line = {"metric": metric, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
@@ -555,7 +567,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "heightfield"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "heightfield", "instanced"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="batched arm: keep the default launch tuning")
