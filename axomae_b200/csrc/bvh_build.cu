@@ -645,7 +645,122 @@ __global__ void k_sort_leaves(const uint2 *leaves, unsigned n, uint32_t *order) 
   }
 }
 
+/* ------------------------------------------------------------------ depth-first node order
+ *
+ * Nodes are numbered as they are created: level by level for large nodes, then by many CTAs at
+ * once for the small subtrees, so a subtree's nodes end up interleaved with other subtrees'.  The
+ * final pass renumbers them in depth-first preorder (left child first), so a node's descendants
+ * follow it in memory.  Subtree sizes come bottom-up (the last child to finish continues to its
+ * parent); a node's preorder number is its depth plus the sizes of the left siblings along its
+ * path to the root. */
+
+constexpr uint32_t kNoParent = 0xffffffffu;
+
+__global__ void k_dfs_init(const float4 *nodes, uint32_t n, uint32_t *parent, uint8_t *side, uint32_t *need,
+                           uint32_t *arrived) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 n3 = nodes[4 * i + 3];
+  const int32_t r[2] = {__float_as_int(n3.x), __float_as_int(n3.y)};
+  uint32_t k = 0;
+  for (int c = 0; c < 2; c++)
+    if (r[c] >= 0 && (uint32_t)r[c] < n) {
+      parent[r[c]] = i;
+      side[r[c]] = (uint8_t)c;
+      k++;
+    }
+  need[i] = k;
+  arrived[i] = 0;
+  if (i == 0) parent[0] = kNoParent;
+}
+
+__global__ void k_dfs_sizes(const float4 *nodes, uint32_t n, const uint32_t *parent, const uint32_t *need,
+                            uint32_t *arrived, uint32_t *size) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || need[i] != 0) return;
+  uint32_t v = i;
+  size[v] = 1;
+  for (int guard = 0; guard < 4 * kSmallStack; guard++) {
+    __threadfence();
+    const uint32_t p = parent[v];
+    if (p == kNoParent || p >= n) return;
+    if (atomicAdd(&arrived[p], 1u) + 1u < need[p]) return; /* a sibling subtree is still open */
+    __threadfence();
+    const float4 n3 = nodes[4 * p + 3];
+    const int32_t r[2] = {__float_as_int(n3.x), __float_as_int(n3.y)};
+    uint32_t sz = 1;
+    for (int c = 0; c < 2; c++)
+      if (r[c] >= 0 && (uint32_t)r[c] < n) sz += __ldcg(size + r[c]);
+    size[p] = sz;
+    v = p;
+  }
+}
+
+__global__ void k_dfs_number(const float4 *nodes, uint32_t n, const uint32_t *parent, const uint8_t *side,
+                             const uint32_t *size, uint32_t *number) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t idx = 0, v = i;
+  for (int guard = 0; guard < 4 * kSmallStack && v != 0; guard++) {
+    const uint32_t p = parent[v];
+    if (p >= n) break;
+    idx += 1;
+    if (side[v] == 1) {
+      const int32_t left = __float_as_int(nodes[4 * p + 3].x);
+      if (left >= 0 && (uint32_t)left < n) idx += size[left];
+    }
+    v = p;
+  }
+  number[i] = idx;
+}
+
+__global__ void k_dfs_permute(const float4 *nodes, uint32_t n, const uint32_t *number, float4 *out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t j = number[i];
+  if (j >= n) return;
+  float4 n3 = nodes[4 * i + 3];
+  const int32_t r0 = __float_as_int(n3.x), r1 = __float_as_int(n3.y);
+  if (r0 >= 0 && (uint32_t)r0 < n) n3.x = __int_as_float((int32_t)number[r0]);
+  if (r1 >= 0 && (uint32_t)r1 < n) n3.y = __int_as_float((int32_t)number[r1]);
+  out[4 * j + 0] = nodes[4 * i + 0];
+  out[4 * j + 1] = nodes[4 * i + 1];
+  out[4 * j + 2] = nodes[4 * i + 2];
+  out[4 * j + 3] = n3;
+}
+
 }  // namespace
+
+cudaError_t reorder_depth_first(float4 *nodes, uint32_t n, cudaStream_t stream) {
+  if (n <= 1) return cudaSuccess;
+  uint32_t *parent = nullptr, *need = nullptr, *arrived = nullptr, *size = nullptr, *number = nullptr;
+  uint8_t *side = nullptr;
+  float4 *tmp = nullptr;
+  cudaError_t err = cudaSuccess;
+  const unsigned grid = (n + 255) / 256;
+  if ((err = cudaMallocAsync(&parent, sizeof(uint32_t) * n, stream)) != cudaSuccess) goto done;
+  if ((err = cudaMallocAsync(&need, sizeof(uint32_t) * n, stream)) != cudaSuccess) goto done;
+  if ((err = cudaMallocAsync(&arrived, sizeof(uint32_t) * n, stream)) != cudaSuccess) goto done;
+  if ((err = cudaMallocAsync(&size, sizeof(uint32_t) * n, stream)) != cudaSuccess) goto done;
+  if ((err = cudaMallocAsync(&number, sizeof(uint32_t) * n, stream)) != cudaSuccess) goto done;
+  if ((err = cudaMallocAsync(&side, n, stream)) != cudaSuccess) goto done;
+  if ((err = cudaMallocAsync(&tmp, sizeof(float4) * 4 * (size_t)n, stream)) != cudaSuccess) goto done;
+  k_dfs_init<<<grid, 256, 0, stream>>>(nodes, n, parent, side, need, arrived);
+  k_dfs_sizes<<<grid, 256, 0, stream>>>(nodes, n, parent, need, arrived, size);
+  k_dfs_number<<<grid, 256, 0, stream>>>(nodes, n, parent, side, size, number);
+  k_dfs_permute<<<grid, 256, 0, stream>>>(nodes, n, number, tmp);
+  if ((err = cudaGetLastError()) != cudaSuccess) goto done;
+  err = cudaMemcpyAsync(nodes, tmp, sizeof(float4) * 4 * (size_t)n, cudaMemcpyDeviceToDevice, stream);
+done:
+  cudaFreeAsync(parent, stream);
+  cudaFreeAsync(need, stream);
+  cudaFreeAsync(arrived, stream);
+  cudaFreeAsync(size, stream);
+  cudaFreeAsync(number, stream);
+  cudaFreeAsync(side, stream);
+  cudaFreeAsync(tmp, stream);
+  return err;
+}
 
 cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhBuildParams &p, float4 *nodes,
                       uint32_t *order, cudaStream_t stream, BvhBuildResult *res) {
@@ -772,6 +887,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
       err = cudaErrorUnknown; /* partition inconsistency: never expected, reported as a build failure */
       goto cleanup;
     }
+    NB_TRY(reorder_depth_first(nodes, hc[0], stream));
     if (res) {
       res->n_nodes = hc[0];
       res->n_leaves = hc[3];

@@ -27,4 +27,8 @@ struct BvhBuildResult {
 cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhBuildParams &p, float4 *nodes,
                       uint32_t *order, cudaStream_t stream, BvhBuildResult *res);
 
+/* Renumbers the n nodes of a built binary BVH in depth-first preorder (root stays 0, every child
+ * after its parent, a subtree contiguous).  Scratch comes from the stream's memory pool. */
+cudaError_t reorder_depth_first(float4 *nodes, uint32_t n, cudaStream_t stream);
+
 }  // namespace nb
