@@ -11,8 +11,11 @@
  * (bvh_build.cu) -> structural validation (every inner reference points to a later node, every
  * leaf range is in bounds, so traversal always terminates) -> triangle records in leaf order.
  */
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "bvh_build.cuh"
 #include "bvh_wide.cuh"
@@ -241,6 +244,34 @@ __global__ void k_validate(const float4 *nodes, uint32_t n_nodes, uint32_t n_tri
       if (f + cnt > n_tris) atomicAdd(bad, 1u);
     }
   }
+}
+
+/* Runs op(k) for k < n on up to 16 host threads; returns the first failing status (its message is
+ * copied to ctxs[0]). */
+template <class Op>
+nova_b200_status for_each_context(nova_b200_ctx *const *ctxs, uint32_t n, Op op) {
+  if (!ctxs || n == 0 || !ctxs[0]) return NOVA_B200_INVALID_ARGUMENT;
+  for (uint32_t k = 0; k < n; k++)
+    if (!ctxs[k]) return nbctx::fail(ctxs[0], NOVA_B200_INVALID_ARGUMENT, "null context in batch%s");
+  for (uint32_t k = 0; k < n; k++)
+    for (uint32_t m = 0; m < k; m++)
+      if (ctxs[k] == ctxs[m]) return nbctx::fail(ctxs[0], NOVA_B200_INVALID_ARGUMENT, "a context appears twice%s");
+  std::vector<nova_b200_status> st(n, NOVA_B200_SUCCESS);
+  std::atomic<uint32_t> next{0};
+  const unsigned nt = std::max(1u, std::min(std::min(n, 16u), std::max(1u, std::thread::hardware_concurrency())));
+  auto work = [&] {
+    for (uint32_t k; (k = next.fetch_add(1)) < n;) st[k] = op(k);
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
+  work();
+  for (auto &t : pool) t.join();
+  for (uint32_t k = 0; k < n; k++)
+    if (st[k] != NOVA_B200_SUCCESS) {
+      if (k != 0) ctxs[0]->error = ctxs[k]->error;
+      return st[k];
+    }
+  return NOVA_B200_SUCCESS;
 }
 
 }  // namespace
@@ -561,6 +592,17 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   c->bvh_ms = r.ms;
   c->bvh_ready = true;
   return NOVA_B200_SUCCESS;
+}
+
+nova_b200_status nova_b200_upload_scene_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                              uint32_t n) {
+  if (!descs) return ctxs && ctxs[0] ? nbctx::fail(ctxs[0], NOVA_B200_INVALID_ARGUMENT, "descs is null%s")
+                                     : NOVA_B200_INVALID_ARGUMENT;
+  return for_each_context(ctxs, n, [&](uint32_t k) { return nova_b200_upload_scene(ctxs[k], &descs[k]); });
+}
+
+nova_b200_status nova_b200_build_bvh_batch(nova_b200_ctx *const *ctxs, uint32_t n, const nova_b200_bvh_options *opts) {
+  return for_each_context(ctxs, n, [&](uint32_t k) { return nova_b200_build_bvh(ctxs[k], opts); });
 }
 
 nova_b200_status nova_b200_render(nova_b200_ctx *c, const nova_b200_frame *f, float *film_host, float *film_device,

@@ -96,7 +96,8 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_render", "nova_b200_trace", "nova_b200_sobol", "nova_b200_bake_irradiance",
            "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
            "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune",
-           "nova_b200_set_diff_params", "nova_b200_backward"]
+           "nova_b200_set_diff_params", "nova_b200_backward", "nova_b200_upload_scene_batch",
+           "nova_b200_build_bvh_batch"]
 
 
 def lib():
@@ -114,6 +115,8 @@ def lib():
         L.nova_b200_render.argtypes = [vp, C.POINTER(Frame), vp, vp, C.POINTER(RenderStats)]
         L.nova_b200_trace.argtypes = [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]
         L.nova_b200_sobol.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, vp]
+        L.nova_b200_upload_scene_batch.argtypes = [C.POINTER(vp), C.POINTER(SceneDesc), C.c_uint32]
+        L.nova_b200_build_bvh_batch.argtypes = [C.POINTER(vp), C.c_uint32, C.POINTER(BvhOptions)]
         L.nova_b200_set_diff_params.argtypes = [vp, vp, vp]
         L.nova_b200_backward.argtypes = [vp, C.POINTER(Frame), vp, vp, vp, C.c_uint32, C.POINTER(RenderStats)]
         L.nova_b200_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
@@ -237,6 +240,30 @@ def render_batch(contexts, frames, films_host=None, films_device=None) -> "Rende
     if rc != 0:
         raise NovaError(rc, contexts[0].error())
     return st
+
+
+def upload_batch(contexts, scenes):
+    """nova_b200_upload_scene_batch: uploads scenes[k] to contexts[k], the contexts concurrently."""
+    n = len(contexts)
+    keep, descs = [], (SceneDesc * n)()
+    for k, sc in enumerate(scenes):
+        d, kp = make_scene_desc(sc)
+        descs[k] = d
+        keep.append(kp)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    rc = lib().nova_b200_upload_scene_batch(hs, descs, n)
+    del keep
+    if rc != 0:
+        raise NovaError(rc, contexts[0].error())
+
+
+def build_batch(contexts, max_leaf=0, bins=0, width=0, small_subtree=0):
+    """nova_b200_build_bvh_batch: builds every context's BVH, the contexts concurrently."""
+    n = len(contexts)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    rc = lib().nova_b200_build_bvh_batch(hs, n, C.byref(BvhOptions(max_leaf, bins, width, small_subtree)))
+    if rc != 0:
+        raise NovaError(rc, contexts[0].error())
 
 
 def autotune(contexts, frames, cache_path=None, flags=0) -> Tuning:

@@ -157,6 +157,14 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *ctx, const nova_b200_scen
  * and DeviceAcceleratorInterface::build (aggregate/device_acceleration_interface.h:25). */
 nova_b200_status nova_b200_build_bvh(nova_b200_ctx *ctx, const nova_b200_bvh_options *opts);
 
+/* Uploads / builds many contexts at once (no counterpart in the reference): the per-context calls
+ * run on up to 16 host threads, each on its context's stream, so the host work and the GPU builds
+ * of different scenes overlap.  Every context must be distinct; the first failing status is
+ * returned and its message is available from ctxs[0]. */
+nova_b200_status nova_b200_upload_scene_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                              uint32_t n);
+nova_b200_status nova_b200_build_bvh_batch(nova_b200_ctx *const *ctxs, uint32_t n, const nova_b200_bvh_options *opts);
+
 /* Renders one frame batch (renderGpu, api/engine.cpp:457-496).  film_host (width*height*4 floats,
  * pageable or pinned) and/or film_device (a device pointer) receive the running-mean RGBA image;
  * either may be NULL.  stats may be NULL. */
