@@ -292,7 +292,8 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
       const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)prim - I.prim_offset, h.x, h.y, h.z);
       const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed,
                                        (uint32_t)prim, I.material);
-      if (sc.has_emissive && any_nonzero(sr.emissive)) {
+      /* a failed scatter returns black, emission included (Integrator.cpp:73-79) */
+      if (sr.valid && sc.has_emissive && any_nonzero(sr.emissive)) {
         const V3 em = beta * sr.emissive;
         const float4 acc = L[g];
         L[g] = make_float4(acc.x + em.x, acc.y + em.y, acc.z + em.z, acc.w);
@@ -449,7 +450,7 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
     Scores scs;
     const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed,
                                      (uint32_t)prim, I.material, &scs);
-    if (sc.has_emissive) rem = rem - beta * sr.emissive;
+    if (sr.valid && sc.has_emissive) rem = rem - beta * sr.emissive;
     if (sr.valid) {
       const V3 cw = dl * rem;
       g_act = true;

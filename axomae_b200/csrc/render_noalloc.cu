@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(128) k_path_noalloc(DevScene sc, Params rp, fl
     const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)h.prim - I.prim_offset, h.t, h.u, h.v);
     const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed,
                                      (uint32_t)h.prim, I.material);
-    if (sc.has_emissive && any_nonzero(sr.emissive)) {
+    if (sr.valid && sc.has_emissive && any_nonzero(sr.emissive)) { /* failed scatter: black */
       const V3 em = beta * sr.emissive;
       lacc = make_float4(lacc.x + em.x, lacc.y + em.y, lacc.z + em.z, lacc.w);
     }

@@ -611,15 +611,21 @@ struct ScatterResult {
  * `mat_id` select the differentiable parameters when the scene has them (per-triangle albedo and
  * per-material roughness replace the albedo texture and the metallic texture's roughness channel);
  * `scores`, when given, receives d ln f / d(albedo, roughness) of the sampled lobe. */
+/* The normal-mapped shading normal (NovaMaterials.h:103-104 with compute_local_normal): a missing
+ * normal map reads as (0, 0, 1), i.e. the local normal (-1, -1, 1). */
+NB_D V3 shading_normal(const DevScene &sc, const HitRecord &hr, const DevMaterial &mat) {
+  V3 nmap{0.f, 0.f, 1.f};
+  if (mat.normalmap >= 0) {
+    V4 t = sample_u8(sc.textures[mat.normalmap], hr.u, hr.v);
+    nmap = {u8f(t.x), u8f(t.y), u8f(t.z)};
+  }
+  return normalize(mul(hr.frame, nmap * 2.f - 1.f));
+}
+
 NB_D ScatterResult scatter(const DevScene &sc, V3 rd, const HitRecord &hr, const DevMaterial &mat, uint32_t index,
                            unsigned dim, uint32_t seed, uint32_t prim, uint32_t mat_id, Scores *scores = nullptr) {
   const float u = hr.u, v = hr.v;
-  V3 nmap{0.f, 0.f, 1.f};
-  if (mat.normalmap >= 0) {
-    V4 t = sample_u8(sc.textures[mat.normalmap], u, v);
-    nmap = {u8f(t.x), u8f(t.y), u8f(t.z)};
-  }
-  const V3 ns = normalize(mul(hr.frame, nmap * 2.f - 1.f));
+  const V3 ns = shading_normal(sc, hr, mat);
   BsdfParams bp;
   bp.dpdu = hr.dpdu;
   bp.dpdv = hr.dpdv;

@@ -66,6 +66,7 @@ class Tuning(C.Structure):
 
 
 TUNE_BVH_WIDTH = 1
+AOV_NORMAL, AOV_DEPTH, AOV_EMISSIVE = 1, 2, 4
 BACKWARD_REUSE_PRIMAL = 1
 
 
@@ -97,7 +98,7 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
            "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune",
            "nova_b200_set_diff_params", "nova_b200_backward", "nova_b200_upload_scene_batch",
-           "nova_b200_build_bvh_batch"]
+           "nova_b200_build_bvh_batch", "nova_b200_render_aov"]
 
 
 def lib():
@@ -115,6 +116,7 @@ def lib():
         L.nova_b200_render.argtypes = [vp, C.POINTER(Frame), vp, vp, C.POINTER(RenderStats)]
         L.nova_b200_trace.argtypes = [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]
         L.nova_b200_sobol.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, vp]
+        L.nova_b200_render_aov.argtypes = [vp, C.POINTER(Frame), C.c_int32, C.c_float, C.c_float, vp, vp]
         L.nova_b200_upload_scene_batch.argtypes = [C.POINTER(vp), C.POINTER(SceneDesc), C.c_uint32]
         L.nova_b200_build_bvh_batch.argtypes = [C.POINTER(vp), C.c_uint32, C.POINTER(BvhOptions)]
         L.nova_b200_set_diff_params.argtypes = [vp, vp, vp]
@@ -345,6 +347,12 @@ class Context:
         outs = [out_o_ptr, out_d_ptr, weight_ptr, emissive_ptr, valid_ptr]
         self._check(lib().nova_b200_scatter(self.h, n, *[C.c_void_p(p) for p in ptrs], seed,
                                             *[C.c_void_p(p) for p in outs]))
+
+    def render_aov(self, frame, kind, near_plane=0.1, far_plane=1000.0, film_host=None, film_device_ptr=None):
+        """AOV integrator image (AOV_NORMAL, AOV_DEPTH, AOV_EMISSIVE) into a host and/or device film."""
+        fh = film_host.ctypes.data_as(C.c_void_p) if film_host is not None else None
+        fd = C.c_void_p(film_device_ptr) if film_device_ptr else None
+        self._check(lib().nova_b200_render_aov(self.h, C.byref(frame), kind, near_plane, far_plane, fh, fd))
 
     def set_diff_params(self, albedo_ptr=None, roughness_ptr=None):
         """Per-triangle RGB albedo / per-material roughness in device memory (None: textures)."""

@@ -157,6 +157,20 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *ctx, const nova_b200_scen
  * and DeviceAcceleratorInterface::build (aggregate/device_acceleration_interface.h:25). */
 nova_b200_status nova_b200_build_bvh(nova_b200_ctx *ctx, const nova_b200_bvh_options *opts);
 
+/* AOV integrators (integrator/NormalIntegrator.cpp, DepthIntegrator.cpp, EmissiveIntegrator.cpp;
+ * the integrator_flag bits of api_common.h:30-47): one unjittered camera ray per pixel, one value per
+ * pixel.  NORMAL: the closest hit's normal-mapped shading normal, (n, 1), 0 on a miss.  DEPTH: from
+ * the closest-hit distance and the camera's near / far planes, the reference's normalised depth / far
+ * in every channel, far on a miss.  EMISSIVE: the hit material's emission, (e, 1), when its BSDF
+ * sample succeeds (Sobol dimensions 0-3 of index pixel_offset * 4), else 0.  The frame supplies the
+ * size, camera, seed and vertical_invert; its sample fields are not used.  film_host / film_device
+ * (width * height * 4 floats) receive the image; either may be NULL. */
+#define NOVA_B200_AOV_NORMAL 1
+#define NOVA_B200_AOV_DEPTH 2
+#define NOVA_B200_AOV_EMISSIVE 4
+nova_b200_status nova_b200_render_aov(nova_b200_ctx *ctx, const nova_b200_frame *frame, int32_t kind,
+                                      float near_plane, float far_plane, float *film_host, float *film_device);
+
 /* Uploads / builds many contexts at once (no counterpart in the reference): the per-context calls
  * run on up to 16 host threads, each on its context's stream, so the host work and the GPU builds
  * of different scenes overlap.  Every context must be distinct; the first failing status is

@@ -1164,6 +1164,55 @@ extern "C" int32_t orc_backward(void *h, const orc_options *opt, const float *d_
   return 0;
 }
 
+/* AOV integrators (NormalIntegrator.cpp, DepthIntegrator.cpp, EmissiveIntegrator.cpp): one
+ * unjittered camera ray per pixel; out = W*H*4 floats in film layout. */
+extern "C" int32_t orc_render_aov(void *h, const orc_options *opt, int32_t kind, float near_plane, float far_plane,
+                                  float *out) {
+  const Scene &s = *static_cast<Scene *>(h);
+  if (opt->width <= 0 || opt->height <= 0 || (kind != 1 && kind != 2 && kind != 4)) return 1;
+  const int W = opt->width, H = opt->height;
+  for (int y = 0; y < H; y++)
+    for (int x = 0; x < W; x++) {
+      const Ray ray = camera_ray(s, x, H - y, W, H, 0.f, 0.f); /* screen2ndc(x, H - y), no jitter */
+      const Hit hit = trace(s, ray, nullptr);
+      const size_t row = opt->vertical_invert ? (size_t)(H - 1 - y) : (size_t)y;
+      float *o = out + (row * W + x) * 4;
+      V4 res{0.f, 0.f, 0.f, 0.f};
+      if (kind == 2) {
+        if (!hit.is_hit) {
+          res = {far_plane, far_plane, far_plane, far_plane};
+        } else {
+          float depth = 1 - (hit.t - near_plane) / (far_plane - near_plane);
+          depth = (2.0f * near_plane * far_plane) / (far_plane + near_plane - depth * (far_plane - near_plane)) * 2.f -
+                  1.f; /* normalize_depth, DepthIntegrator.cpp:6 */
+          const float v = depth / far_plane;
+          res = {v, v, v, v};
+        }
+      } else if (hit.is_hit) {
+        const HitRecord hr = make_record(s, ray, hit);
+        const uint32_t mat_id = s.inst_mat[s.prims[hit.prim].inst];
+        const Material &mat = s.materials[mat_id];
+        if (kind == 1) { /* mat_rec.normal = ns, NovaMaterials.h:103-104,135 */
+          V3 nmap{0.f, 0.f, 1.f};
+          if (mat.normalmap >= 0) {
+            V4 t = sample_u8(s.textures[mat.normalmap], hr.u, hr.v);
+            nmap = {u8f(t.x), u8f(t.y), u8f(t.z)};
+          }
+          const V3 ns = normalize(mul(hr.frame, nmap * 2.f - 1.f));
+          res = {ns.x, ns.y, ns.z, 1.f};
+        } else { /* sampler.reset(generateImageOffset(...)), dimensions from 0 */
+          const uint32_t index = (uint32_t)((row * W + x) * 4);
+          unsigned dim = 0;
+          Scatter sc;
+          if (scatter(s, ray, hr, mat, index, dim, opt->seed, sc, hit.prim, mat_id))
+            res = {sc.emissive.x, sc.emissive.y, sc.emissive.z, 1.f};
+        }
+      }
+      o[0] = res.x, o[1] = res.y, o[2] = res.z, o[3] = res.w;
+    }
+  return 0;
+}
+
 extern "C" void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int32_t *px, const int32_t *py,
                                     const int32_t *ps, float *out) {
   PathCtx c{static_cast<Scene *>(h), 0, 0, opt->seed, opt->rr_start, 0, 0, {}};

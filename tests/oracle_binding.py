@@ -80,6 +80,8 @@ def lib():
         L.orc_sample_path.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int32, C.c_int32, C.c_int32, f32p,
                                       C.c_int32, f32p]
         L.orc_sample_path.restype = C.c_int32
+        L.orc_render_aov.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int32, C.c_float, C.c_float, f32p]
+        L.orc_render_aov.restype = C.c_int32
         L.orc_set_diff_params.argtypes = [C.c_void_p, f32p, f32p]
         L.orc_set_diff_params.restype = C.c_int32
         L.orc_set_perturbation.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_int32, C.c_float]
@@ -239,6 +241,13 @@ class OracleScene:
         lib().orc_scatter(self.h, n, _p(o, f32p), _p(d, f32p), _p(prim, i32p), _p(t, f32p), _p(u, f32p), _p(v, f32p),
                           _p(index, u32p), _p(bounce, i32p), seed, *[_p(a, f32p) for a in outs], _p(valid, i32p))
         return (*outs, valid)
+
+    def render_aov(self, opt, kind, near_plane=0.1, far_plane=1000.0):
+        """AOV integrator image (kind 1 normal, 2 depth, 4 emissive), (H, W, 4)."""
+        out = np.zeros((opt.height, opt.width, 4), np.float32)
+        if lib().orc_render_aov(self.h, C.byref(opt), kind, near_plane, far_plane, _p(out, f32p)) != 0:
+            raise ValueError("bad AOV request")
+        return out
 
     def set_diff_params(self, albedo=None, roughness=None):
         """Per-triangle RGB albedo ((n_tris, 3)) / per-material roughness; None = textures."""
