@@ -37,6 +37,7 @@ constexpr uint32_t kSmallTaskDefault = 256;
 constexpr uint32_t kChunk = 4096;
 constexpr int kMedianDepth = 40;
 constexpr int kBlock = 256;
+constexpr int kSmallBlock = 64; /* a subtree of <= small_task primitives needs few threads per node */
 constexpr int kHardLeaf = 16;
 constexpr int kSmallStack = 64;
 
@@ -481,7 +482,7 @@ __device__ unsigned block_exclusive_scan(unsigned v, unsigned *sh /* 32 */, unsi
   return r;
 }
 
-__global__ void __launch_bounds__(kBlock) k_build_small(Shared s, const Task *small_tasks) {
+__global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Task *small_tasks) {
   __shared__ Task stack[kSmallStack];
   __shared__ int sp, have;
   __shared__ unsigned scnt[3][kMaxBins];
@@ -873,7 +874,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     unsigned n_small = 0;
     NB_TRY(cudaMemcpyAsync(&n_small, counters + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     NB_TRY(cudaStreamSynchronize(stream));
-    if (n_small) k_build_small<<<n_small, kBlock, 0, stream>>>(sh, small);
+    if (n_small) k_build_small<<<n_small, kSmallBlock, 0, stream>>>(sh, small);
     NB_TRY(cudaGetLastError());
     unsigned hc[5];
     int hdepth = 0;
