@@ -34,6 +34,7 @@ nova_b200_status check_tuning(nova_b200_ctx *c, const nova_b200_tuning &t) {
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "block sizes must be 0, 32, 64, 96 or 128%s");
   if ((t.tile_w == 0) != (t.tile_h == 0))
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "tile_w and tile_h must both be 0 or both be set%s");
+  if (t.trace_mode > 1) return fail(c, NOVA_B200_INVALID_ARGUMENT, "trace_mode must be 0 or 1%s");
   if (t.tile_w && (t.tile_w > 64 || t.tile_h > 64 || (t.tile_w * t.tile_h) % 32 != 0))
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "tiles must be at most 64 x 64 with a multiple of 32 pixels%s");
   return NOVA_B200_SUCCESS;
@@ -87,7 +88,8 @@ bool read_cache(const char *path, const std::string &key, nova_b200_tuning &t) {
     std::istringstream ls(line);
     std::string k;
     nova_b200_tuning v{};
-    if (ls >> k >> v.queue_capacity >> v.trace_block >> v.shade_block >> v.tile_w >> v.tile_h >> v.bvh_width &&
+    if (ls >> k >> v.queue_capacity >> v.trace_block >> v.shade_block >> v.tile_w >> v.tile_h >> v.bvh_width >>
+            v.trace_mode &&
         k == key) {
       t = v;
       return true;
@@ -108,7 +110,7 @@ void write_cache(const char *path, const std::string &key, const nova_b200_tunin
   std::ofstream out(path, std::ios::trunc);
   for (const std::string &l : keep) out << l << "\n";
   out << key << " " << t.queue_capacity << " " << t.trace_block << " " << t.shade_block << " " << t.tile_w << " "
-      << t.tile_h << " " << t.bvh_width << "\n";
+      << t.tile_h << " " << t.bvh_width << " " << t.trace_mode << "\n";
 }
 
 nova_b200_status rebuild_all(const std::vector<nova_b200_ctx *> &ctxs, int width) {
@@ -217,6 +219,11 @@ nova_b200_status nova_b200_autotune(nova_b200_ctx *const *ctxs, const nova_b200_
   for (uint32_t b : {64u, 96u}) {
     nova_b200_tuning cand = cur;
     cand.shade_block = b;
+    if ((s = consider(cand)) != NOVA_B200_SUCCESS) return s;
+  }
+  if (x->bvh_width != 8) {
+    nova_b200_tuning cand = cur;
+    cand.trace_mode = 1;
     if ((s = consider(cand)) != NOVA_B200_SUCCESS) return s;
   }
   const uint32_t tiles[3][2] = {{8, 4}, {16, 2}, {8, 8}};

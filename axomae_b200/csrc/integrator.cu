@@ -86,6 +86,7 @@ struct WaveCounters {
   uint32_t hit_count, out_count;
   uint32_t done;
   uint32_t waves; /* waves that did work */
+  uint32_t trace_next; /* next queued ray handed out by the persistent trace kernel */
   unsigned long long traced;
 };
 
@@ -260,6 +261,64 @@ __global__ void __launch_bounds__(128) k_trace(Queue q, WaveCounters *wcp, float
       hits[slot] = make_float4(r.t, r.u, r.v, __int_as_float(r.prim));
       hit_slot[slot] = i;
     }
+  }
+}
+
+/* Persistent variant of k_trace (binary BVH): a fixed grid of warps hands out the queued rays with
+ * a warp-wide counter, and a lane whose walk ends takes the next ray while the warp's other lanes
+ * keep walking, so lanes do not idle behind the warp's longest walk.  A warp refills once at least
+ * kRefillLanes lanes are idle (or none is busy).  Every walk is Walk2, i.e. trace_closest2's
+ * iteration, so the hits are the same. */
+constexpr int kRefillLanes = 8;
+
+template <class JS>
+__global__ void __launch_bounds__(128) k_trace_dyn(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot,
+                                                   float4 *L, const __grid_constant__ JS js) {
+  const uint32_t n = wcp->n_active + wave_new(*wcp);
+  const unsigned full = 0xffffffffu, lane = threadIdx.x & 31u;
+  Walk2 w;
+  int32_t stack[kTraversalStack];
+  int32_t ray = -1;
+  uint32_t job = 0;
+  bool exhausted = false;
+  /* every iteration advances a walk or hands out rays; the bound only guards against a bug */
+  for (uint32_t it = 0; it < (1u << 30); it++) {
+    const bool idle = ray < 0 && !exhausted;
+    const unsigned need = __ballot_sync(full, idle), busy = __ballot_sync(full, ray >= 0);
+    if (need && (__popc(need) >= kRefillLanes || busy == 0)) {
+      const int leader = __ffs(need) - 1;
+      uint32_t base = 0;
+      if ((int)lane == leader) base = atomicAdd(&wcp->trace_next, (unsigned)__popc(need));
+      base = __shfl_sync(full, base, leader);
+      if (idle) {
+        const uint32_t i = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+        if (i < n) {
+          const float4 o = q.o[i], d = q.d[i];
+          ray = (int32_t)i;
+          job = __float_as_uint(d.w) >> 8;
+          w.init(V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (__ballot_sync(full, ray >= 0 || !exhausted) == 0) break;
+    bool fin = false;
+    if (ray >= 0) fin = !w.step(js.at(job).sc, stack);
+    const bool is_hit = fin && w.r.prim >= 0;
+    if (fin && !is_hit) {
+      const DevScene &sc = js.at(job).sc;
+      const float4 o = q.o[ray], b4 = q.beta[ray], d = q.d[ray];
+      const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
+      finish_path(sc, L, __float_as_uint(o.w),
+                  finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z}, (float)(__float_as_uint(d.w) & 0xffu) + e.w));
+    }
+    const unsigned slot = warp_append(is_hit, &wcp->hit_count);
+    if (is_hit) {
+      hits[slot] = make_float4(w.r.t, w.r.u, w.r.v, __int_as_float(w.r.prim));
+      hit_slot[slot] = (uint32_t)ray;
+    }
+    if (fin) ray = -1;
   }
 }
 
@@ -509,6 +568,7 @@ __global__ void k_wave_end(WaveCounters *wc) {
   wc->n_active = wc->out_count;
   wc->out_count = 0;
   wc->hit_count = 0;
+  wc->trace_next = 0;
   wc->done = (wc->n_active == 0 && wc->next == wc->total) ? 1u : 0u;
 }
 
@@ -641,6 +701,7 @@ nova_b200_status ensure_wave_buffers(nova_b200_ctx *c, uint32_t cap, size_t radi
 struct LaunchShape {
   uint32_t cap;
   uint32_t trace_block, shade_block;
+  uint32_t trace_mode; /* 0: one ray per thread, 1: persistent warps with ray hand-out (binary BVH) */
 };
 
 struct WaveBuffers {
@@ -685,6 +746,10 @@ void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int sl
   const unsigned g_trace = (ls.cap + ls.trace_block - 1) / ls.trace_block;
   const unsigned g_shade = (ls.cap + ls.shade_block - 1) / ls.shade_block;
   const unsigned g_refill = (unsigned)(dev_sms * std::max(1, occ_r) * 2);
+  int occ_t = 1;
+  if (WIDTH == 2 && ls.trace_mode == 1)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace_dyn<JS>, 128, 0);
+  const unsigned g_dyn = (unsigned)std::min<uint64_t>((uint64_t)dev_sms * std::max(1, occ_t), (ls.cap + 127) / 128);
   const unsigned flags = external ? cudaEventRecordExternal : cudaEventRecordDefault;
   cudaEvent_t *ev = c->ev_wave + 3 * kWavesPerGraph * slot;
   for (int w = 0; w < kWavesPerGraph; w++) {
@@ -703,7 +768,10 @@ void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int sl
     } else {
       k_refill<JS><<<g_refill, 256, 0, c->stream>>>(in, b.wc, c->d_radiance, js);
       cudaEventRecordWithFlags(ev[3 * w + 0], c->stream, flags);
-      k_trace<WIDTH, JS><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+      if (WIDTH == 2 && ls.trace_mode == 1)
+        k_trace_dyn<JS><<<g_dyn, 128, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+      else
+        k_trace<WIDTH, JS><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
       cudaEventRecordWithFlags(ev[3 * w + 1], c->stream, flags);
       k_shade<JS><<<g_shade, ls.shade_block, 0, c->stream>>>(in, out, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
       cudaEventRecordWithFlags(ev[3 * w + 2], c->stream, flags);
@@ -855,7 +923,8 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   const nova_b200_tuning &tu = x->tuning;
   const uint32_t qc = tu.queue_capacity ? tu.queue_capacity : kQueueCapDefault;
   const uint32_t cap = (uint32_t)std::min<uint64_t>(qc, std::max<uint64_t>(radiance, 1024));
-  const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u};
+  const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u,
+                       tu.trace_mode};
   nova_b200_status st = ensure_wave_buffers(x, cap, radiance);
   if (st != NOVA_B200_SUCCESS) return st;
   x->primal_valid = false; /* this render overwrites the radiance buffer */
@@ -1031,7 +1100,8 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
   const nova_b200_tuning &tu = c->tuning;
   const uint32_t qc = tu.queue_capacity ? tu.queue_capacity : kQueueCapDefault;
   const uint32_t cap = (uint32_t)std::min<uint64_t>(qc, std::max<uint64_t>(radiance, 1024));
-  const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u};
+  const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u,
+                       tu.trace_mode};
   if ((st = ensure_wave_buffers(c, cap, radiance)) != NOVA_B200_SUCCESS) return st;
   if (c->adj_cap < c->queue_cap) {
     cudaFree(c->d_adj);

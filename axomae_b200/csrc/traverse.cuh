@@ -177,6 +177,76 @@ NB_D void test_triangles(const DevScene &sc, uint32_t first, uint32_t count, V3 
   }
 }
 
+/* The binary-BVH walk of trace_closest2 as a resumable state: step() does one loop iteration (an
+ * inner node, or a leaf and the pop after it) with the same arithmetic and order, so a walk driven
+ * to the end reports exactly trace_closest2's hit.  Used where a thread interleaves several rays.
+ * The traversal stack (kTraversalStack entries) is the caller's, so the scalar state can stay in
+ * registers. */
+struct Walk2 {
+  V3 o, d;
+  float ix, iy, iz, tmax;
+  TraceResult r;
+  int32_t cur, cached_inst;
+  int sp;
+  V3 lo_o, lo_d;
+
+  NB_D void init(V3 ro, V3 rd) {
+    o = ro;
+    d = rd;
+    ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
+    tmax = FLT_MAX;
+    r = TraceResult{-1, 0.f, 0.f, 0.f};
+    cur = 0;
+    cached_inst = -1;
+    sp = 0;
+    lo_o = o;
+    lo_d = d;
+  }
+
+  /* false once the walk is over (r holds the closest hit) */
+  NB_D bool step(const DevScene &sc, int32_t *stack) {
+    if (cur >= 0) {
+      const float4 n0 = __ldg(&sc.nodes[4 * cur + 0]);
+      const float4 n1 = __ldg(&sc.nodes[4 * cur + 1]);
+      const float4 n2 = __ldg(&sc.nodes[4 * cur + 2]);
+      const float4 n3 = __ldg(&sc.nodes[4 * cur + 3]);
+      const float a0 = (n0.x - o.x) * ix, b0 = (n0.y - o.x) * ix;
+      const float a1 = (n0.z - o.y) * iy, b1 = (n0.w - o.y) * iy;
+      const float a2 = (n2.x - o.z) * iz, b2 = (n2.y - o.z) * iz;
+      const float c0n = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), 0.f));
+      const float c0f = fminf(fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fmaxf(a2, b2)) * kFarScale, tmax);
+      const float d0 = (n1.x - o.x) * ix, e0 = (n1.y - o.x) * ix;
+      const float d1 = (n1.z - o.y) * iy, e1 = (n1.w - o.y) * iy;
+      const float d2 = (n2.z - o.z) * iz, e2 = (n2.w - o.z) * iz;
+      const float c1n = fmaxf(fmaxf(fminf(d0, e0), fminf(d1, e1)), fmaxf(fminf(d2, e2), 0.f));
+      const float c1f = fminf(fminf(fminf(fmaxf(d0, e0), fmaxf(d1, e1)), fmaxf(d2, e2)) * kFarScale, tmax);
+      const bool h0 = c0n <= c0f, h1 = c1n <= c1f;
+      const int32_t r0 = __float_as_int(n3.x), r1 = __float_as_int(n3.y);
+      if (h0 && h1) {
+        int32_t first = r0, second = r1;
+        if (c1n < c0n) {
+          first = r1;
+          second = r0;
+        }
+        if (sp < kTraversalStack) stack[sp++] = second;
+        cur = first;
+        return true;
+      } else if (h0) {
+        cur = r0;
+        return true;
+      } else if (h1) {
+        cur = r1;
+        return true;
+      }
+    } else {
+      test_triangles(sc, leaf_first(cur), leaf_count(cur), o, d, cached_inst, lo_o, lo_d, tmax, r);
+    }
+    if (sp == 0) return false;
+    cur = stack[--sp];
+    return true;
+  }
+};
+
 /* Closest hit on the compressed 8-wide BVH (layout in bvh_wide.cuh).  Every visited node tests its
  * eight quantised child boxes, tests the triangles of hit leaf children in slot order, then
  * descends into the first hit inner child; the other hit inner children stay on a stack as one

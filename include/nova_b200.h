@@ -263,6 +263,8 @@ typedef struct {
                               multiple of 32, both <= 64); 0 x 0 = image rows (default) */
   int32_t bvh_width;       /* reported by nova_b200_autotune: the BVH width it left the contexts
                               built with (0: not tuned); ignored by nova_b200_set_tuning */
+  uint32_t trace_mode;     /* 0: one ray per thread (default); 1: persistent warps that hand out rays
+                              as their lanes finish (binary BVH only; the 8-wide BVH ignores it) */
 } nova_b200_tuning;
 
 /* tuning = NULL restores the defaults. */

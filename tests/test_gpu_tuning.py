@@ -31,7 +31,9 @@ def _film(c, s, W=61, H=47, spp=32, depth=6):
     dict(tile_w=8, tile_h=4),
     dict(tile_w=16, tile_h=2, queue_capacity=1 << 20, trace_block=64, shade_block=64),
     dict(tile_w=64, tile_h=64),                                # tiles larger than the frame's last row / column
-], ids=["small-waves", "blocks", "tile8x4", "mixed", "tile64"])
+    dict(trace_mode=1),                                        # persistent trace warps
+    dict(trace_mode=1, queue_capacity=65536, tile_w=8, tile_h=4),
+], ids=["small-waves", "blocks", "tile8x4", "mixed", "tile64", "persistent", "persistent-small-waves"])
 def test_tuning_does_not_change_results(scene_ctx, tuning):
     s, c = scene_ctx
     c.set_tuning()
@@ -50,7 +52,8 @@ def test_tuning_does_not_change_results(scene_ctx, tuning):
 def test_invalid_tuning_rejected(scene_ctx):
     from axomae_b200 import native
     _, c = scene_ctx
-    for bad in (dict(queue_capacity=100), dict(trace_block=256), dict(tile_w=8), dict(tile_w=5, tile_h=5)):
+    for bad in (dict(queue_capacity=100), dict(trace_block=256), dict(tile_w=8), dict(tile_w=5, tile_h=5),
+                dict(trace_mode=2)):
         with pytest.raises(native.NovaError) as e:
             c.set_tuning(**bad)
         assert e.value.status == 15
@@ -78,7 +81,7 @@ def test_autotune_applies_and_caches(tmp_path):
         t = native.autotune(ctxs, frames, str(cache), flags=native.TUNE_BVH_WIDTH)
         assert t.bvh_width in (2, 8)
         lines = cache.read_text().strip().splitlines()
-        assert len(lines) == 1 and len(lines[0].split()) == 7
+        assert len(lines) == 1 and len(lines[0].split()) == 8
         for c in ctxs:
             got = c.get_tuning()
             assert (got.queue_capacity, got.trace_block, got.shade_block, got.tile_w, got.tile_h) == (
