@@ -18,6 +18,7 @@
 #include <thread>
 
 #include "bvh_build.cuh"
+#include "sampler.cuh"
 #include "bvh_wide.cuh"
 #include "context.cuh"
 #include "traverse.cuh"
@@ -52,6 +53,21 @@ void sobol_table(std::vector<uint32_t> &t) {
     }
     for (int i = 0; i < 32; i++) t[d * 32 + i] = (uint32_t)(m[i] << (31 - i));
   }
+}
+
+/* The device form of the direction vectors: for every dimension four 256-entry tables, entry b of
+ * table k the XOR of the vectors of the set bits of byte value b at bit position 8k..8k+7, so the
+ * XOR over the set bits of a 32-bit gray code is four lookups (sampler.cuh). */
+void sobol_byte_tables(const std::vector<uint32_t> &dv, std::vector<uint32_t> &t) {
+  t.assign((size_t)nb::kSobolDims * nb::kSobolByteTable, 0u);
+  for (int d = 0; d < nb::kSobolDims; d++)
+    for (int k = 0; k < 4; k++)
+      for (int b = 0; b < 256; b++) {
+        uint32_t x = 0;
+        for (int j = 0; j < 8; j++)
+          if ((b >> j) & 1) x ^= dv[d * 32 + 8 * k + j];
+        t[(size_t)d * nb::kSobolByteTable + 256 * k + b] = x;
+      }
 }
 
 /* acos table f(i) = acos(2 i / P - 1), P = 500000, rounded to float
@@ -299,9 +315,10 @@ nova_b200_status nova_b200_create(nova_b200_ctx **out, int32_t device) {
     uint64_t keep = ~0ull;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
-  std::vector<uint32_t> sob;
+  std::vector<uint32_t> dv, sob;
   std::vector<float> ac;
-  sobol_table(sob);
+  sobol_table(dv);
+  sobol_byte_tables(dv, sob);
   acos_table(ac);
   if (cudaMalloc(&c->d_sobol, sob.size() * 4) != cudaSuccess || cudaMalloc(&c->d_acos, ac.size() * 4) != cudaSuccess ||
       cudaMalloc(&c->d_counters, 64) != cudaSuccess || cudaMallocHost(&c->h_counters, 64) != cudaSuccess) {

@@ -65,7 +65,7 @@ struct DevScene {
   const DevInstance *instances;
   const DevMaterial *materials;
   const DevTexture *textures;
-  const uint32_t *sobol_dv;  /* 256 x 32 direction vectors */
+  const uint32_t *sobol_dv;  /* byte-sliced direction vectors: 256 dims x 4 x 256 (sampler.cuh) */
   const float *acos_lut;     /* 500000 entries */
   int32_t envmap;
   uint32_t n_prims;
