@@ -117,5 +117,12 @@ NB_D float pow5f(float x) {
 }
 NB_D float cos_rn(float x) { return (float)cos((double)x); }
 NB_D float sin_rn(float x) { return (float)sin((double)x); }
+/* sin and cos of one argument, one shared double-precision evaluation, each rounded once */
+NB_D void sincos_rn(float x, float &s, float &c) {
+  double sd, cd;
+  sincos((double)x, &sd, &cd);
+  s = (float)sd;
+  c = (float)cd;
+}
 
 }  // namespace nb

@@ -262,8 +262,10 @@ NB_D V3 hemisphere_cosine_sample(float u0, float u1) { /* shirley_chiu, BxDF_mat
       r = sy;
       theta = kPi2F - kPi4F * (sx / sy);
     }
-    px = r * cos_rn(theta);
-    py = r * sin_rn(theta);
+    float st, ct;
+    sincos_rn(theta, st, ct);
+    px = r * ct;
+    py = r * st;
   }
   float z = sqrtf(fmax_std(0.f, 1 - px * px - py * py));
   return {px, py, z};
@@ -325,7 +327,9 @@ struct VNDF { /* BxDF_math.h:226-343 */
     V3 b = cross(wh, t);
     float r = msqrt(u0);
     float th = (float)(2.0 * kPiD * (double)u1);
-    float px = r * cos_rn(th), py = r * sin_rn(th);
+    float sth, cth;
+    sincos_rn(th, sth, cth);
+    float px = r * cth, py = r * sth;
     float s = 0.5f * (1.f + wh.z);
     py = msqrt(1.f - sqr(px)) * (1.f - s) + s * py;
     V3 nh = px * t + py * b + msqrt(fmaxf(0.f, 1.f - sqr(px) - sqr(py))) * wh;
