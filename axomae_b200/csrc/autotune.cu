@@ -35,8 +35,9 @@ nova_b200_status check_tuning(nova_b200_ctx *c, const nova_b200_tuning &t) {
   if ((t.tile_w == 0) != (t.tile_h == 0))
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "tile_w and tile_h must both be 0 or both be set%s");
   if (t.trace_mode > 1) return fail(c, NOVA_B200_INVALID_ARGUMENT, "trace_mode must be 0 or 1%s");
-  if (t.tile_w && (t.tile_w > 64 || t.tile_h > 64 || (t.tile_w * t.tile_h) % 32 != 0))
-    return fail(c, NOVA_B200_INVALID_ARGUMENT, "tiles must be at most 64 x 64 with a multiple of 32 pixels%s");
+  if (t.tile_w && !(t.tile_w == 1 && t.tile_h == 1) &&
+      (t.tile_w > 64 || t.tile_h > 64 || (t.tile_w * t.tile_h) % 32 != 0))
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "tiles must be 1 x 1 or at most 64 x 64 with a multiple of 32 pixels%s");
   return NOVA_B200_SUCCESS;
 }
 
@@ -226,7 +227,7 @@ nova_b200_status nova_b200_autotune(nova_b200_ctx *const *ctxs, const nova_b200_
     cand.trace_mode = 1;
     if ((s = consider(cand)) != NOVA_B200_SUCCESS) return s;
   }
-  const uint32_t tiles[3][2] = {{8, 4}, {16, 2}, {8, 8}};
+  const uint32_t tiles[3][2] = {{1, 1}, {16, 2}, {8, 8}}; /* rows and two other tiles; 0 x 0 is 8 x 4 */
   for (const auto &tl : tiles) {
     nova_b200_tuning cand = cur;
     cand.tile_w = tl[0];

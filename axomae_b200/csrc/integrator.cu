@@ -126,6 +126,21 @@ __device__ __forceinline__ uint32_t wave_new(const WaveCounters &wc) {
   return min(wc.cap - wc.n_active, wc.total - wc.next);
 }
 
+constexpr uint32_t kTileW = 8, kTileH = 4; /* default pixel tile: one warp of camera rays per tile */
+
+/* Tiles of a tuning: 0 x 0 = the default tile, 1 x 1 = image rows (tile_w = 0 below). */
+void set_tiles(RenderParams &rp, const nova_b200_tuning &tu) {
+  if (tu.tile_w == 0) {
+    rp.tile_w = kTileW;
+    rp.tile_h = kTileH;
+  } else if (tu.tile_w == 1 && tu.tile_h == 1) {
+    rp.tile_w = rp.tile_h = 0u;
+  } else {
+    rp.tile_w = tu.tile_w;
+    rp.tile_h = tu.tile_h;
+  }
+}
+
 /* The q-th pixel a frame's paths visit: row-major, or tile_w x tile_h tiles in row-major tile
  * order (partial tiles at the right and bottom edges), so a warp's primary rays cover a compact
  * patch of the image. */
@@ -985,8 +1000,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
       std::copy(P.f->inv_P, P.f->inv_P + 16, rp.inv_P);
       std::copy(P.f->inv_V, P.f->inv_V + 16, rp.inv_V);
       rp.vinv = P.f->vertical_invert;
-      rp.tile_w = tu.tile_w;
-      rp.tile_h = tu.tile_w ? tu.tile_h : 0u;
+      set_tiles(rp, tu);
       J.path_begin = pb;
       J.n_paths = rp.NP * P.count;
       pb += J.n_paths;
@@ -1141,8 +1155,7 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
     std::copy(f->inv_P, f->inv_P + 16, rp.inv_P);
     std::copy(f->inv_V, f->inv_V + 16, rp.inv_V);
     rp.vinv = f->vertical_invert;
-    rp.tile_w = tu.tile_w;
-    rp.tile_h = tu.tile_w ? tu.tile_h : 0u;
+    set_tiles(rp, tu);
     J.path_begin = 0;
     J.n_paths = NP * take;
     /* primal: each path's radiance into the radiance buffer */

@@ -260,7 +260,7 @@ typedef struct {
   uint32_t trace_block;    /* threads per block of the trace kernel: 32, 64, 96 or 128; 0 = 128 */
   uint32_t shade_block;    /* threads per block of the shade kernel: 32, 64, 96 or 128; 0 = 128 */
   uint32_t tile_w, tile_h; /* consecutive paths walk tile_w x tile_h pixel tiles (tile_w * tile_h a
-                              multiple of 32, both <= 64); 0 x 0 = image rows (default) */
+                              multiple of 32, both <= 64); 0 x 0 = default 8 x 4; 1 x 1 = image rows */
   int32_t bvh_width;       /* reported by nova_b200_autotune: the BVH width it left the contexts
                               built with (0: not tuned); ignored by nova_b200_set_tuning */
   uint32_t trace_mode;     /* 0: one ray per thread (default); 1: persistent warps that hand out rays

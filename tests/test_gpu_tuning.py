@@ -31,9 +31,10 @@ def _film(c, s, W=61, H=47, spp=32, depth=6):
     dict(tile_w=8, tile_h=4),
     dict(tile_w=16, tile_h=2, queue_capacity=1 << 20, trace_block=64, shade_block=64),
     dict(tile_w=64, tile_h=64),                                # tiles larger than the frame's last row / column
+    dict(tile_w=1, tile_h=1),                                  # image rows
     dict(trace_mode=1),                                        # persistent trace warps
     dict(trace_mode=1, queue_capacity=65536, tile_w=8, tile_h=4),
-], ids=["small-waves", "blocks", "tile8x4", "mixed", "tile64", "persistent", "persistent-small-waves"])
+], ids=["small-waves", "blocks", "tile8x4", "mixed", "tile64", "rows", "persistent", "persistent-small-waves"])
 def test_tuning_does_not_change_results(scene_ctx, tuning):
     s, c = scene_ctx
     c.set_tuning()
