@@ -7,6 +7,13 @@ samples, so the combination weights each film by its sample count:
 
     mean = sum_r count_r * film_r / sum_r count_r
 
+The differentiable render partitions the same way: a rank's backward gives the gradient of its own
+film (the mean over its samples), so the gradient of the combined film is the count-weighted sum
+
+    grad = sum_r count_r * grad_r / sum_r count_r
+
+(one all-reduce of the 3 * triangles + materials parameter gradients).
+
 The path has no other exchange: scenes and BVHs are built on every rank, and nothing crosses
 between ranks while a frame renders.
 """
@@ -42,3 +49,28 @@ def reduce_films(film, count: int, group=None):
     if total.item() > 0:
         film.div_(total.item())
     return film
+
+
+def reduce_gradients(grads, count: int, group=None):
+    """In place: each tensor in `grads` (this rank's gradient of the mean over its `count` samples,
+    e.g. per-triangle albedo and per-material roughness gradients) becomes the gradient of the mean
+    over every rank's samples.  One all-reduce of the concatenated gradients, one of the counts.
+    Collective: all ranks call it in the same order, with the same tensor shapes."""
+    import torch
+    import torch.distributed as dist
+    grads = list(grads)
+    if not grads:
+        return grads
+    flat = torch.cat([g.reshape(-1) for g in grads]).to(torch.float32)
+    total = torch.tensor([float(count)], dtype=torch.float64, device=flat.device)
+    flat.mul_(float(count))
+    dist.all_reduce(flat, group=group)
+    dist.all_reduce(total, group=group)
+    if total.item() > 0:
+        flat.div_(total.item())
+    off = 0
+    for g in grads:
+        n = g.numel()
+        g.copy_(flat[off:off + n].reshape(g.shape))
+        off += n
+    return grads

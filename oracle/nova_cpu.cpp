@@ -1070,8 +1070,18 @@ extern "C" int32_t orc_set_perturbation(void *h, int32_t kind, uint32_t index, i
  * dI = d_image / spp.  Gradients are summed in double per thread and added to the outputs. */
 extern "C" int32_t orc_backward(void *h, const orc_options *opt, const float *d_image, float *grad_albedo,
                                 float *grad_roughness, int32_t threads) {
+  return orc_backward_range(h, opt, 0, opt->spp, d_image, grad_albedo, grad_roughness, threads);
+}
+
+/* The same over samples [sample_begin, sample_begin + sample_count) of an opt->spp-sample frame:
+ * the gradient of the mean over that range (dI = d_image / sample_count), as one rank of a
+ * sample-range partition computes it. */
+extern "C" int32_t orc_backward_range(void *h, const orc_options *opt, int32_t sample_begin, int32_t sample_count,
+                                      const float *d_image, float *grad_albedo, float *grad_roughness,
+                                      int32_t threads) {
   const Scene &s = *static_cast<Scene *>(h);
   if (opt->width <= 0 || opt->height <= 0 || opt->spp <= 0 || opt->max_depth < 0 || !d_image) return 1;
+  if (sample_begin < 0 || sample_count <= 0 || sample_begin + sample_count > opt->spp) return 1;
   const int W = opt->width, H = opt->height;
   const unsigned nt = threads > 0 ? (unsigned)threads : std::max(1u, std::thread::hardware_concurrency());
   const size_t na = 3 * s.prims.size(), nm = s.materials.size();
@@ -1085,8 +1095,8 @@ extern "C" int32_t orc_backward(void *h, const orc_options *opt, const float *d_
       for (int x = 0; x < W; x++) {
         const size_t row = opt->vertical_invert ? (size_t)(H - 1 - y) : (size_t)y;
         const float *dp = d_image + (row * W + x) * 4;
-        const Spec dl{dp[0] / (float)opt->spp, dp[1] / (float)opt->spp, dp[2] / (float)opt->spp};
-        for (int smp = 0; smp < opt->spp; smp++) {
+        const Spec dl{dp[0] / (float)sample_count, dp[1] / (float)sample_count, dp[2] / (float)sample_count};
+        for (int smp = sample_begin; smp < sample_begin + sample_count; smp++) {
           const V4 I = render_sample(c, *opt, x, y, smp);
           /* replay */
           constexpr float RAND_DX = 0.0005f, RAND_DY = 0.0005f;

@@ -131,6 +131,8 @@ int32_t orc_set_perturbation(void *h, int32_t kind, uint32_t index, int32_t chan
 /* Replay adjoint: adds dLoss/dalbedo, dLoss/droughness for d_image = dLoss/dImage (W*H*4). */
 int32_t orc_backward(void *h, const orc_options *opt, const float *d_image, float *grad_albedo,
                      float *grad_roughness, int32_t threads);
+int32_t orc_backward_range(void *h, const orc_options *opt, int32_t sample_begin, int32_t sample_count,
+                           const float *d_image, float *grad_albedo, float *grad_roughness, int32_t threads);
 /* AOV integrators: kind 1 normal, 2 depth (camera near / far planes), 4 emissive; out = W*H*4. */
 int32_t orc_render_aov(void *h, const orc_options *opt, int32_t kind, float near_plane, float far_plane, float *out);
 /* Radiance of single samples (pixel x, y, sample s), RGB into out (3 per sample). */

@@ -88,6 +88,9 @@ def lib():
         L.orc_set_perturbation.restype = C.c_int32
         L.orc_backward.argtypes = [C.c_void_p, C.POINTER(OrcOptions), f32p, f32p, f32p, C.c_int32]
         L.orc_backward.restype = C.c_int32
+        L.orc_backward_range.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int32, C.c_int32, f32p, f32p, f32p,
+                                         C.c_int32]
+        L.orc_backward_range.restype = C.c_int32
         L.orc_scatter.argtypes = [C.c_void_p, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, u32p, i32p, C.c_uint32,
                                   f32p, f32p, f32p, f32p, i32p]
         L.orc_trace.argtypes = [C.c_void_p, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, C.POINTER(OrcStats)]
@@ -268,6 +271,17 @@ class OracleScene:
         ga = np.zeros(3 * n_tris, np.float32)
         gr = np.zeros(n_materials, np.float32)
         rc = lib().orc_backward(self.h, C.byref(opt), _p(d_image, f32p), _p(ga, f32p), _p(gr, f32p), threads)
+        if rc != 0:
+            raise ValueError("oracle backward failed")
+        return ga.reshape(n_tris, 3), gr
+
+    def backward_range(self, opt, sample_begin, sample_count, d_image, n_tris, n_materials, threads=0):
+        """Replay adjoint of the mean over samples [sample_begin, sample_begin + sample_count)."""
+        d_image = np.ascontiguousarray(d_image, np.float32)
+        ga = np.zeros(3 * n_tris, np.float32)
+        gr = np.zeros(n_materials, np.float32)
+        rc = lib().orc_backward_range(self.h, C.byref(opt), sample_begin, sample_count, _p(d_image, f32p),
+                                      _p(ga, f32p), _p(gr, f32p), threads)
         if rc != 0:
             raise ValueError("oracle backward failed")
         return ga.reshape(n_tris, 3), gr

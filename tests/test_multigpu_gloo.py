@@ -65,6 +65,50 @@ def test_partitioned_render_equals_single_render(oracle, tmp_path, mode, world, 
     np.testing.assert_allclose(reduced, full, rtol=1e-5, atol=1e-6)
 
 
+def _grad_worker(rank, world, port, per, out_dir):
+    import torch
+    import torch.distributed as dist
+    import oracle_binding as ob
+    from axomae_b200 import multigpu, scenes
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        s = scenes.spheres_scene(W, H, n_spheres=6, seed=2)
+        n_tris = sum(len(m["indices"]) // 3 for m in s["meshes"])
+        n_mat = len(s["materials"])
+        osc = ob.OracleScene(s)
+        spp_total, begin, count = multigpu.strong_range(per, rank, world)
+        opt = ob.options(W, H, spp_total, DEPTH, threads=2)
+        d_image = np.random.default_rng(5).standard_normal((H, W, 4)).astype(np.float32)
+        if count:
+            ga, gr = osc.backward_range(opt, begin, count, d_image, n_tris, n_mat, threads=2)
+        else:
+            ga, gr = np.zeros((n_tris, 3), np.float32), np.zeros(n_mat, np.float32)
+        ga_t, gr_t = torch.from_numpy(ga.copy()), torch.from_numpy(gr.copy())
+        multigpu.reduce_gradients([ga_t, gr_t], count)
+        if rank == 0:
+            fa, fr = osc.backward(opt, d_image, n_tris, n_mat, threads=2)
+            np.savez(os.path.join(out_dir, "grads.npz"), ga=ga_t.numpy(), gr=gr_t.numpy(), fa=fa, fr=fr)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,per", [(2, 4), (3, 2)], ids=["4-over-2", "2-over-3"])
+def test_partitioned_gradients_equal_single_backward(oracle, tmp_path, world, per):
+    """The replay adjoint split by sample range over gloo ranks, each rank's gradient reduced with
+    reduce_gradients, equals the oracle's backward over all samples in one process (in "2-over-3"
+    rank 0 has an empty range and contributes zeros)."""
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_grad_worker, args=(world, port, per, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    g = np.load(tmp_path / "grads.npz")
+    assert np.abs(g["fa"]).max() > 0 and np.abs(g["fr"]).max() > 0
+    np.testing.assert_allclose(g["ga"], g["fa"], rtol=1e-4, atol=1e-6 * np.abs(g["fa"]).max())
+    np.testing.assert_allclose(g["gr"], g["fr"], rtol=1e-4, atol=1e-6 * np.abs(g["fr"]).max())
+
+
 def test_ranges_cover_the_frame_once():
     from axomae_b200 import multigpu
     for world in (1, 2, 3, 8):
