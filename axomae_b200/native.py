@@ -99,7 +99,9 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
            "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune",
            "nova_b200_set_diff_params", "nova_b200_backward", "nova_b200_upload_scene_batch",
-           "nova_b200_build_bvh_batch", "nova_b200_render_aov"]
+           "nova_b200_build_bvh_batch", "nova_b200_render_aov", "nova_b200_film_accumulate",
+           "nova_b200_display_blend", "nova_b200_snapshot", "nova_b200_hdr_info", "nova_b200_hdr_read",
+           "nova_b200_hdr_write", "nova_b200_last_call_ms", "nova_b200_bake_texture"]
 
 
 def lib():
@@ -134,6 +136,15 @@ def lib():
         L.nova_b200_scene_info.argtypes = [vp] + [C.POINTER(C.c_uint64)] * 5
         L.nova_b200_synchronize.argtypes = [vp]
         L.nova_b200_render_noalloc.argtypes = [vp, C.POINTER(Frame), vp]
+        L.nova_b200_film_accumulate.argtypes = [vp, vp, vp, vp, C.c_uint64, C.c_uint32]
+        L.nova_b200_display_blend.argtypes = [vp, vp, vp, vp, C.c_uint64, C.c_uint32]
+        L.nova_b200_snapshot.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_int32, C.c_int32]
+        L.nova_b200_hdr_info.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.nova_b200_hdr_read.argtypes = [vp, C.c_char_p, vp, vp, C.c_uint64]
+        L.nova_b200_hdr_write.argtypes = [vp, C.c_char_p, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+        L.nova_b200_last_call_ms.argtypes = [vp, C.POINTER(C.c_float)]
+        L.nova_b200_bake_texture.argtypes = [vp, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p,
+                                             C.c_char_p]
         L.nova_b200_render_batch.argtypes = [C.POINTER(vp), C.POINTER(Frame), C.c_uint32, C.POINTER(vp),
                                              C.POINTER(vp), C.POINTER(RenderStats)]
         for name in EXPORTS:
@@ -388,5 +399,62 @@ class Context:
         self._check(lib().nova_b200_bake_irradiance(self.h, C.c_void_p(src_ptr), sw, sh, ch, ow, oh, samples,
                                                     C.c_void_p(out_ptr)))
 
+    def film_accumulate(self, partial_ptr, accum_ptr, final_ptr, n, frame_index):
+        """accum += partial; final = accum / (frame_index + 1) over n device floats."""
+        self._check(lib().nova_b200_film_accumulate(self.h, C.c_void_p(partial_ptr), C.c_void_p(accum_ptr),
+                                                    C.c_void_p(final_ptr) if final_ptr else None, n, frame_index))
+
+    def display_blend(self, partial_ptr, accum_ptr, out_ptr, n, current_frame):
+        """The editor's display value over n device floats."""
+        self._check(lib().nova_b200_display_blend(self.h, C.c_void_p(partial_ptr), C.c_void_p(accum_ptr),
+                                                  C.c_void_p(out_ptr), n, current_frame))
+
+    def snapshot(self, film_ptr, width, height, channels, dst_ptr, dst_width, dst_height):
+        """The film resampled to dst_width x dst_height (device buffers)."""
+        self._check(lib().nova_b200_snapshot(self.h, C.c_void_p(film_ptr), width, height, channels,
+                                             C.c_void_p(dst_ptr), dst_width, dst_height))
+
+    def hdr_read(self, path, rgba_host=None, rgba_device_ptr=None, capacity=None):
+        """Reads a .hdr file as (height, width, 4) floats into a host array and / or device buffer."""
+        w, h = hdr_info(path)
+        cap = capacity if capacity is not None else w * h * 4
+        if rgba_host is not None and rgba_host.size < cap:
+            raise ValueError("host array too small")
+        fh = rgba_host.ctypes.data_as(C.c_void_p) if rgba_host is not None else None
+        fd = C.c_void_p(rgba_device_ptr) if rgba_device_ptr else None
+        self._check(lib().nova_b200_hdr_read(self.h, os.fsencode(path), fh, fd, cap))
+        return w, h
+
+    def hdr_write(self, path, width, height, channels, pixels_host=None, pixels_device_ptr=None, flip=False):
+        """Writes path + ".hdr" from host or device pixels (width * height * channels floats)."""
+        if pixels_host is not None:
+            pixels_host = np.ascontiguousarray(pixels_host, np.float32)
+            if pixels_host.size < width * height * channels:
+                raise ValueError("pixel array too small")
+        fh = pixels_host.ctypes.data_as(C.c_void_p) if pixels_host is not None else None
+        fd = C.c_void_p(pixels_device_ptr) if pixels_device_ptr else None
+        self._check(lib().nova_b200_hdr_write(self.h, os.fsencode(path), fh, fd, width, height, channels,
+                                              1 if flip else 0))
+
+    def bake_texture(self, kind, width, height, samples, path_in, path_out):
+        """The bake command: path_in (.hdr) -> irradiance map path_out + ".hdr"."""
+        self._check(lib().nova_b200_bake_texture(self.h, kind.encode(), width, height, samples,
+                                                 os.fsencode(path_in), os.fsencode(path_out)))
+
+    def last_call_ms(self) -> float:
+        """Device time of the kernel of the last film / .hdr call."""
+        ms = C.c_float(0.0)
+        self._check(lib().nova_b200_last_call_ms(self.h, C.byref(ms)))
+        return ms.value
+
     def synchronize(self):
         self._check(lib().nova_b200_synchronize(self.h))
+
+
+def hdr_info(path):
+    """(width, height) of a Radiance .hdr file (header only; no device needed)."""
+    w, h = C.c_int32(0), C.c_int32(0)
+    st = lib().nova_b200_hdr_info(None, os.fsencode(path), C.byref(w), C.byref(h))
+    if st != 0:
+        raise NovaError(st, "not a readable Radiance .hdr file: %s" % path)
+    return w.value, h.value

@@ -315,6 +315,72 @@ def timed(step, steps, torch, dist, clock=None):
 ADJ_CFG = dict(width=256, height=256, spp=64, depth=4)
 
 
+def film_io_timing(local_rank, cpu_baseline=True, reps=10):
+    """The film outputs and the .hdr path at 3840 x 2160 RGBA float (133 MB per film): device time
+    of each kernel (CUDA events, median of `reps` calls) against its algorithmic bytes and the HBM
+    copy peak; the whole nova_b200_hdr_write (H2D of host pixels, encode, D2H of 4 B/pixel, run-
+    length packing, file write) by wall clock; and the oracle's RGBE encode on one host core."""
+    import tempfile
+    import torch
+    from axomae_b200 import native
+    W, H = 3840, 2160
+    n = W * H * 4
+    px_bytes = W * H * 16
+    hbm = peaks().get("hbm_gbs") or 6650.0
+    rng = np.random.default_rng(1)
+    host = rng.lognormal(0, 1, (H, W, 4)).astype(np.float32)
+    c = native.Context(local_rank)
+    part = torch.from_numpy(host).cuda()
+    acc = torch.rand((H, W, 4), device="cuda")
+    fin = torch.empty_like(acc)
+    disp = torch.empty_like(acc)
+    snap = torch.zeros((1080, 1920, 4), device="cuda")
+    back = torch.empty_like(acc)
+    out = {}
+
+    def timed(name, fn, algo_bytes):
+        ms = []
+        for _ in range(reps + 1):
+            fn()
+            ms.append(c.last_call_ms())
+        t = float(np.median(ms[1:]))
+        gbs = algo_bytes / (t / 1e3) / 1e9
+        out[name] = {"device_ms": t, "algorithmic_bytes": algo_bytes, "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm}
+
+    timed("k_accumulate", lambda: c.film_accumulate(part.data_ptr(), acc.data_ptr(), fin.data_ptr(), n, 3),
+          4 * px_bytes)
+    timed("k_display_blend", lambda: c.display_blend(part.data_ptr(), acc.data_ptr(), disp.data_ptr(), n, 3),
+          3 * px_bytes)
+    timed("k_snapshot", lambda: c.snapshot(fin.data_ptr(), W, H, 4, snap.data_ptr(), 1920, 1080),
+          1920 * 1080 * (12 + 12))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "film")
+        timed("k_rgbe_encode", lambda: c.hdr_write(path, W, H, 4, pixels_device_ptr=fin.data_ptr()), W * H * (16 + 4))
+        timed("k_rgbe_decode", lambda: c.hdr_read(path + ".hdr", rgba_device_ptr=back.data_ptr()), W * H * (4 + 16))
+        walls = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            c.hdr_write(path, W, H, 4, pixels_host=host)
+            walls.append(time.perf_counter() - t0)
+        file_mb = os.path.getsize(path + ".hdr") / 1e6
+    wall = float(np.median(walls))
+    out["hdr_write_e2e"] = {"seconds": wall, "mpix_per_s": W * H / wall / 1e6, "file_mb": file_mb,
+                            "h2d_bytes": px_bytes, "d2h_bytes": W * H * 4,
+                            "note": "nova_b200_hdr_write from host pixels, wall clock: H2D, device encode, D2H, "
+                                    "run-length packing and file write on one host thread"}
+    if cpu_baseline:
+        oracle_binding = oracle_module()
+        rows = host[:540]  # a quarter of the frame
+        t0 = time.perf_counter()
+        oracle_binding.rgbe_encode(rows, 4)
+        cs = time.perf_counter() - t0
+        out["cpu_rgbe_encode"] = {"mpix_per_s": rows.shape[0] * W / cs / 1e6, "cores": 1, "kind": "port",
+                                  "sample": "oracle RGBE encode of 540 of the 2160 rows"}
+    c.close()
+    out["workload"] = "3840x2160 RGBA float film; snapshot to 1920x1080; .hdr file in a temporary directory"
+    return out
+
+
 def adjoint_timing(local_rank, reps=3):
     """The differentiable configuration: the 64-sphere scene at 256 x 256, 64 spp, depth 4, with
     per-triangle albedo (init 0.5) and per-material roughness (init 0.3) as parameters and an L2
@@ -549,6 +615,8 @@ def run_ours(args, rank, world, local_rank):
         extra["rel_rmse_vs_cpu"] = cpu["rel_rmse"]
     if batched and not args.no_adjoint:
         extra["adjoint"] = adjoint_timing(local_rank)
+    if batched and not args.no_film_io:
+        extra["film_io"] = film_io_timing(local_rank, cpu_baseline=not args.no_cpu and local_rank == 0)
     metric = {"heightfield": HF_METRIC, "instanced": IN_METRIC}.get(args.workload, BATCH_METRIC)
     workload = {"heightfield": HF_WORKLOAD, "instanced": IN_WORKLOAD}.get(args.workload, BATCH_WORKLOAD)
     if args.frame or args.spp:
@@ -584,6 +652,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="batched arm: keep the default launch tuning")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
+    ap.add_argument("--no-film-io", action="store_true", help="skip the film output / .hdr timing")
     ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="heightfield: override the frame size")
     ap.add_argument("--spp", type=int, help="heightfield: override samples per pixel")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8], help="BVH layout (0 = library default)")

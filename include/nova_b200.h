@@ -294,6 +294,53 @@ nova_b200_status nova_b200_bake_irradiance(nova_b200_ctx *ctx, const float *src_
                                            int32_t channels, int32_t out_w, int32_t out_h, int32_t samples,
                                            float *out_dev);
 
+/* ---- Film outputs (device buffers, the context's device and stream) ---------------------------
+ *
+ * Progressive accumulation: Engine::writeFramebuffer (corelib/nova/api/engine.cpp:351-363).
+ * accumulator += partial; final = accumulator / (frame_index + 1) (final may be NULL).  n floats,
+ * buffers 16-byte aligned. */
+nova_b200_status nova_b200_film_accumulate(nova_b200_ctx *ctx, const float *partial_dev, float *accumulator_dev,
+                                           float *final_dev, uint64_t n, uint32_t frame_index);
+/* The editor's display value: NovaRenderer::copyBufferToPbo (sources/renderer/nova/NovaRenderer_draw.cpp:35-45).
+ * old = accumulated / (current_frame + 1); display = old + 0.8 (partial - old).  n floats. */
+nova_b200_status nova_b200_display_blend(nova_b200_ctx *ctx, const float *partial_dev, const float *accumulated_dev,
+                                         float *display_dev, uint64_t n, uint32_t current_frame);
+/* A film resampled to another size: NovaRenderer::getSnapshotFloat (sources/renderer/nova/NovaRenderer.cpp:139-153)
+ * with TextureOperations::processTexture (sources/processing/TextureProcessing.h:157-250).  dst holds
+ * dst_width * dst_height * channels floats; channels 0-2 of each pixel are written, channel 3 is left
+ * as it is.  dst_height <= 65535. */
+nova_b200_status nova_b200_snapshot(nova_b200_ctx *ctx, const float *film_dev, int32_t width, int32_t height,
+                                    int32_t channels, float *dst_dev, int32_t dst_width, int32_t dst_height);
+
+/* ---- Radiance .hdr files (the bake CLI's input and output, the render saved to disk) -----------
+ *
+ * Size of a .hdr file: the header checks of IO::Loader::loadHdrEnvmap / loadRadianceFile
+ * (sources/IO/Loader_image.cpp:64-90, 146-160).  ctx may be NULL (no error text then). */
+nova_b200_status nova_b200_hdr_info(nova_b200_ctx *ctx, const char *path, int32_t *width, int32_t *height);
+/* Reads a .hdr file as width * height * 4 floats, RGB and alpha 1: IO::Loader::loadRadianceFile
+ * (Loader_image.cpp:146-192).  The RGBE pixels are decoded on the device.  rgba_host and / or
+ * rgba_device (16-byte aligned) receive the image; capacity is their size in floats.  OpenEXR files
+ * are rejected (INVALID_ARGUMENT). */
+nova_b200_status nova_b200_hdr_read(nova_b200_ctx *ctx, const char *path, float *rgba_host, float *rgba_device,
+                                    uint64_t capacity);
+/* Writes path + ".hdr": IO::Loader::writeHdr (Loader_image.cpp:50-62).  pixels: width * height *
+ * channels floats (1-4 channels; 1 or 2 write the first channel as grey) on the host or on the
+ * device; encoded to RGBE on the device, rows run-length packed for widths in [8, 32768).  flip
+ * writes the rows bottom-up.  height <= 65535. */
+nova_b200_status nova_b200_hdr_write(nova_b200_ctx *ctx, const char *path, const float *pixels_host,
+                                     const float *pixels_device, int32_t width, int32_t height, int32_t channels,
+                                     int32_t flip);
+/* The bake command's work: API::bakeTexture (sources/controller/cmd/API.cpp:44-62, options of
+ * ProgramOptionsManager.cpp:76-79, 116-137) without the viewer it opens.  Reads the Radiance map
+ * path_in (RGBA, alpha 1), bakes the diffuse irradiance map of out_width x out_height texels (powers
+ * of two) with `samples` samples per texel on the device, writes path_out + ".hdr" (alpha 0, as the
+ * reference leaves it).  type must be "irradiance" (the only type the reference bakes). */
+nova_b200_status nova_b200_bake_texture(nova_b200_ctx *ctx, const char *type, int32_t out_width, int32_t out_height,
+                                        int32_t samples, const char *path_in, const char *path_out);
+/* Device time in ms of the kernel of the last film_accumulate / display_blend / snapshot /
+ * hdr_read / hdr_write call (CUDA events).  No counterpart in the reference. */
+nova_b200_status nova_b200_last_call_ms(nova_b200_ctx *ctx, float *device_ms);
+
 /* Last error message: Engine::getRenderEngineError (api_engine.h:185).  buf holds 1024 chars. */
 void nova_b200_get_error(nova_b200_ctx *ctx, char buf[1024], size_t *size);
 

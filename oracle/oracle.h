@@ -143,6 +143,15 @@ void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int3
 int32_t orc_bake_irradiance(const float *src, int32_t src_w, int32_t src_h, int32_t channels, int32_t out_w,
                             int32_t out_h, int32_t samples, int32_t threads, float *out);
 
+/* Film outputs and the Radiance .hdr format (film_io.cpp). */
+void orc_film_accumulate(const float *partial, float *accum, float *final_buf, uint64_t n, uint32_t frame_index);
+void orc_display_blend(const float *partial, const float *accum, float *out, uint64_t n, uint32_t current_frame);
+void orc_snapshot(const float *film, int32_t width, int32_t height, int32_t channels, float *dst, int32_t dst_width,
+                  int32_t dst_height);
+void orc_rgbe_encode(const float *px, uint64_t n, int32_t channels, uint8_t *out);
+void orc_rgbe_decode(const uint8_t *in, uint64_t n, float *out_rgba);
+int32_t orc_hdr_parse(const uint8_t *bytes, uint64_t size, int32_t *width, int32_t *height, uint8_t *rgbe);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,14 @@ def lib():
         L.orc_bake_irradiance.argtypes = [f32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                           C.c_int32, f32p]
         L.orc_bake_irradiance.restype = C.c_int32
+        u8p = C.POINTER(C.c_uint8)
+        L.orc_film_accumulate.argtypes = [f32p, f32p, f32p, C.c_uint64, C.c_uint32]
+        L.orc_display_blend.argtypes = [f32p, f32p, f32p, C.c_uint64, C.c_uint32]
+        L.orc_snapshot.argtypes = [f32p, C.c_int32, C.c_int32, C.c_int32, f32p, C.c_int32, C.c_int32]
+        L.orc_rgbe_encode.argtypes = [f32p, C.c_uint64, C.c_int32, u8p]
+        L.orc_rgbe_decode.argtypes = [u8p, C.c_uint64, f32p]
+        L.orc_hdr_parse.argtypes = [u8p, C.c_uint64, i32p, i32p, u8p]
+        L.orc_hdr_parse.restype = C.c_int32
         _lib = L
     return _lib
 
@@ -302,3 +310,59 @@ def bake_irradiance(src: np.ndarray, out_w: int, out_h: int, samples: int, threa
     if rc != 0:
         raise ValueError("bake rejected")
     return out
+
+
+# ---- film outputs and the Radiance .hdr format (oracle/film_io.cpp) ----
+
+def film_accumulate(partial, accum, frame_index):
+    """Returns (accum + partial, its mean over frame_index + 1 frames); inputs unchanged."""
+    partial = np.ascontiguousarray(partial, np.float32).reshape(-1)
+    acc = np.array(accum, np.float32).reshape(-1)
+    final = np.zeros_like(acc)
+    lib().orc_film_accumulate(_p(partial, f32p), _p(acc, f32p), _p(final, f32p), acc.size, frame_index)
+    return acc, final
+
+
+def display_blend(partial, accum, current_frame):
+    partial = np.ascontiguousarray(partial, np.float32).reshape(-1)
+    accum = np.ascontiguousarray(accum, np.float32).reshape(-1)
+    out = np.zeros_like(accum)
+    lib().orc_display_blend(_p(partial, f32p), _p(accum, f32p), _p(out, f32p), out.size, current_frame)
+    return out
+
+
+def snapshot(film, dst_w, dst_h, dst_init=None):
+    """film: (H, W, C) floats; returns (dst_h, dst_w, C) with channel 3 left as dst_init's (zeros)."""
+    film = np.ascontiguousarray(film, np.float32)
+    h, w, ch = film.shape
+    out = np.zeros((dst_h, dst_w, ch), np.float32) if dst_init is None else np.array(dst_init, np.float32)
+    lib().orc_snapshot(_p(film, f32p), w, h, ch, _p(out, f32p), dst_w, dst_h)
+    return out
+
+
+def rgbe_encode(pixels, channels):
+    px = np.ascontiguousarray(pixels, np.float32).reshape(-1)
+    n = px.size // channels
+    out = np.zeros((n, 4), np.uint8)
+    lib().orc_rgbe_encode(_p(px, f32p), n, channels, _p(out, C.POINTER(C.c_uint8)))
+    return out
+
+
+def rgbe_decode(rgbe):
+    q = np.ascontiguousarray(rgbe, np.uint8).reshape(-1, 4)
+    out = np.zeros((q.shape[0], 4), np.float32)
+    lib().orc_rgbe_decode(_p(q, C.POINTER(C.c_uint8)), q.shape[0], _p(out, f32p))
+    return out
+
+
+def hdr_parse(data: bytes):
+    """(code, width, height, rgbe (H, W, 4) uint8 or None): code 0 on success."""
+    buf = np.frombuffer(data, np.uint8).copy() if len(data) else np.zeros(1, np.uint8)
+    w, h = C.c_int32(0), C.c_int32(0)
+    u8p = C.POINTER(C.c_uint8)
+    code = lib().orc_hdr_parse(_p(buf, u8p), len(data), C.byref(w), C.byref(h), None)
+    if code:
+        return code, 0, 0, None
+    rgbe = np.zeros((h.value, w.value, 4), np.uint8)
+    code = lib().orc_hdr_parse(_p(buf, u8p), len(data), C.byref(w), C.byref(h), _p(rgbe, u8p))
+    return code, w.value, h.value, (rgbe if code == 0 else None)
