@@ -21,7 +21,6 @@
  */
 #include <cstring>
 #include <fstream>
-#include <iterator>
 #include <string>
 #include <vector>
 
@@ -143,17 +142,23 @@ __device__ __forceinline__ uchar4 rgbe_encode(float r, float g, float b) {
 }
 
 /* Encodes rows in file order (flip: bottom row first).  planar = 1 writes each row as four planes
- * of width bytes (R, G, B, E: the order of run-length scanlines), 0 as interleaved pixels. */
-__global__ void k_rgbe_encode(const float *src, int w, int h, int ch, int flip, int planar, unsigned char *dst) {
+ * of width bytes (R, G, B, E: the order of run-length scanlines), 0 as interleaved pixels.  vec4:
+ * 4-channel pixels at a 16-byte aligned address, read as one float4. */
+__global__ void k_rgbe_encode(const float *src, int w, int h, int ch, int flip, int planar, int vec4,
+                              unsigned char *dst) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, row = blockIdx.y;
   if (x >= w || row >= h) return;
   const int srow = flip ? h - 1 - row : row;
-  const float *p = src + ((size_t)srow * w + x) * ch;
+  const size_t px = (size_t)srow * w + x;
   float r, g, b;
-  if (ch >= 3) {
+  if (vec4) {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(src) + px);
+    r = v.x, g = v.y, b = v.z;
+  } else if (ch >= 3) {
+    const float *p = src + px * ch;
     r = p[0], g = p[1], b = p[2];
   } else {
-    r = g = b = p[0];
+    r = g = b = src[px * ch];
   }
   const uchar4 q = rgbe_encode(r, g, b);
   if (planar) {
@@ -166,16 +171,164 @@ __global__ void k_rgbe_encode(const float *src, int w, int h, int ch, int flip, 
 
 /* RGBE -> float: exponent byte 0 -> (0, 0, 0); else c = byte 2^(e - 136), exact; alpha 1 (the
  * loader widens 3-channel files to RGBA with alpha 1, Loader_image.cpp:161-170). */
-__global__ void k_rgbe_decode(const uchar4 *src, uint64_t n, float4 *dst) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uchar4 q = src[i];
-  if (q.w == 0) {
-    dst[i] = make_float4(0.f, 0.f, 0.f, 1.f);
-    return;
+__device__ __forceinline__ float4 rgbe_decode(uint32_t word) {
+  const uint32_t e = word >> 24;
+  if (e == 0) return make_float4(0.f, 0.f, 0.f, 1.f);
+  const double s = __longlong_as_double((long long)((int)e - 136 + 1023) << 52);
+  return make_float4((float)((word & 0xffu) * s), (float)(((word >> 8) & 0xffu) * s),
+                     (float)(((word >> 16) & 0xffu) * s), 1.f);
+}
+
+/* Four pixels per thread: one 16-byte load of RGBE words, four float4 stores (both buffers 16-byte
+ * aligned); the last thread takes the ragged end pixel by pixel. */
+__global__ void k_rgbe_decode(const uint32_t *src, uint64_t n, float4 *dst) {
+  const uint64_t i4 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i4 + 4 <= n) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(src + i4));
+    dst[i4] = rgbe_decode(q.x);
+    dst[i4 + 1] = rgbe_decode(q.y);
+    dst[i4 + 2] = rgbe_decode(q.z);
+    dst[i4 + 3] = rgbe_decode(q.w);
+  } else {
+    for (uint64_t i = i4; i < n; i++) dst[i] = rgbe_decode(src[i]);
   }
-  const double s = __longlong_as_double((long long)((int)q.w - 136 + 1023) << 52);
-  dst[i] = make_float4((float)(q.x * s), (float)(q.y * s), (float)(q.z * s), 1.f);
+}
+
+/* Run-length packing, one warp per (row, plane) of the planar RGBE rows: runs of 3 or more equal
+ * bytes become run packets (count + 128, value; count <= 127), the rest dump packets (count,
+ * bytes; count <= 128).  The greedy scan is the serial one (next run start = first position whose
+ * byte equals the next two; a run ends at the first different byte), with 32 positions tested per
+ * step by a ballot; dump bytes are copied by all lanes.  Each warp writes its packets into its own
+ * region of `cap` bytes (cap bounds the packets of any row: width + width / 128 + 2) and their size
+ * into sizes; a region that would overflow sets *err and is cut. */
+__global__ void k_rle_pack(const unsigned char *planar, int w, int n_planes, int cap, unsigned char *regions,
+                           uint32_t *sizes, unsigned *err) {
+  const int e = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (e >= n_planes) return; /* whole warps leave together */
+  const unsigned char *p = planar + (size_t)e * w; /* planes are consecutive: row-major (row, plane) */
+  unsigned char *o = regions + (size_t)e * cap;
+  int n = 0, x = 0;
+  bool over = false;
+  while (x < w) {
+    int lit = w;
+    for (int base = x; base < w; base += 32) {
+      const int i = base + lane;
+      const bool t = i + 2 < w && p[i] == p[i + 1] && p[i] == p[i + 2];
+      const unsigned m = __ballot_sync(0xffffffffu, t);
+      if (m) {
+        lit = base + __ffs(m) - 1;
+        break;
+      }
+    }
+    while (x < lit) {
+      const int cnt = min(lit - x, 128);
+      if (n + 1 + cnt > cap) {
+        over = true;
+        break;
+      }
+      if (lane == 0) o[n] = (unsigned char)cnt;
+      for (int k = lane; k < cnt; k += 32) o[n + 1 + k] = p[x + k];
+      n += 1 + cnt;
+      x += cnt;
+    }
+    if (over) break;
+    if (lit < w) {
+      const unsigned char v = p[lit];
+      int end = w;
+      for (int base = lit; base < w; base += 32) {
+        const int i = base + lane;
+        const unsigned m = __ballot_sync(0xffffffffu, i >= w || p[i] != v);
+        if (m) {
+          end = min(base + __ffs(m) - 1, w);
+          break;
+        }
+      }
+      while (x < end) {
+        const int cnt = min(end - x, 127);
+        if (n + 2 > cap) {
+          over = true;
+          break;
+        }
+        if (lane == 0) o[n] = (unsigned char)(128 + cnt), o[n + 1] = v;
+        n += 2;
+        x += cnt;
+      }
+      if (over) break;
+    }
+  }
+  if (lane == 0) {
+    if (over) atomicAdd(err, 1u);
+    sizes[e] = (uint32_t)n;
+  }
+}
+
+/* Exclusive scan of the packed sizes into file offsets, one block of 1024 threads: element
+ * (row, plane 0) also carries the row's 4-byte header.  offsets[n] = total bytes. */
+__global__ void __launch_bounds__(1024) k_rle_scan(const uint32_t *sizes, int n, uint64_t *offsets) {
+  __shared__ uint64_t part[1024];
+  const int t = threadIdx.x;
+  const int chunk = (n + 1023) / 1024;
+  const int b = min(t * chunk, n), e = min(b + chunk, n);
+  uint64_t sum = 0;
+  for (int i = b; i < e; i++) sum += sizes[i] + ((i & 3) == 0 ? 4u : 0u);
+  part[t] = sum;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) { /* inclusive Hillis-Steele scan */
+    const uint64_t v = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  uint64_t run = part[t] - sum;
+  for (int i = b; i < e; i++) {
+    offsets[i] = run;
+    run += sizes[i] + ((i & 3) == 0 ? 4u : 0u);
+  }
+  if (t == 1023) offsets[n] = part[1023];
+}
+
+/* One warp per (row, plane): its packets to their file offset; plane 0 writes the row header
+ * (2, 2, width >> 8, width & 255) first. */
+__global__ void k_rle_gather(const unsigned char *regions, const uint32_t *sizes, const uint64_t *offsets, int w,
+                             int cap, int n_planes, unsigned char *out) {
+  const int e = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (e >= n_planes) return;
+  uint64_t dst = offsets[e];
+  if ((e & 3) == 0) {
+    if (lane < 4) out[dst + lane] = lane < 2 ? 2 : (lane == 2 ? (unsigned char)(w >> 8) : (unsigned char)(w & 255));
+    dst += 4;
+  }
+  const unsigned char *src = regions + (size_t)e * cap;
+  const uint32_t n = sizes[e];
+  for (uint32_t j = lane; j < n; j += 32) out[dst + j] = src[j];
+}
+
+/* Run-length expansion, one warp per (row, plane): the packets starting at file offset starts[e]
+ * (found and checked on the host) into byte `plane` of each RGBE pixel of the row; lane 0 reads
+ * each packet's count, all lanes copy or fill.  The body buffer is zero-padded past the file's end,
+ * which the loader reads as zeros. */
+__global__ void k_rle_unpack(const unsigned char *body, const uint64_t *starts, int w, int n_planes,
+                             unsigned char *rgbe) {
+  const int e = (int)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (e >= n_planes) return;
+  const unsigned char *p = body + starts[e];
+  unsigned char *o = rgbe + (size_t)(e >> 2) * w * 4 + (e & 3);
+  int x = 0;
+  while (x < w) {
+    int cnt = __shfl_sync(0xffffffffu, lane == 0 ? (int)p[0] : 0, 0);
+    if (cnt == 0) break; /* excluded by the host's check; never loops without progress */
+    if (cnt > 128) {
+      cnt = min(cnt - 128, w - x);
+      const unsigned char v = p[1];
+      for (int k = lane; k < cnt; k += 32) o[4 * (size_t)(x + k)] = v;
+      p += 2;
+    } else {
+      cnt = min(cnt, w - x);
+      for (int k = lane; k < cnt; k += 32) o[4 * (size_t)(x + k)] = p[1 + k];
+      p += 1 + cnt;
+    }
+    x += cnt;
+  }
 }
 
 /* ---- host: the file format ----------------------------------------------------------------- */
@@ -241,90 +394,81 @@ nova_b200_status parse_header(nova_b200_ctx *c, const std::vector<unsigned char>
   return NOVA_B200_SUCCESS;
 }
 
-/* Scanlines -> interleaved RGBE bytes.  Rows of a width in [8, 32768) are run-length packets:
- * a row header (2, 2, width >> 8, width & 255), then for each of R, G, B, E packets that are
- * either a run (count + 128, value) or a dump (count, count bytes), count in 1..remaining.  A row
- * whose first bytes are not a run-length header means the file is flat from there: those 4 bytes
- * are pixel 0 of row 0 and the rest follow in order (the stb loader's rule, kept as is). */
-nova_b200_status unpack(nova_b200_ctx *c, const std::vector<unsigned char> &bytes, const Header &hd,
-                        std::vector<unsigned char> &rgbe) {
+/* Where the scanlines are.  Rows of a width in [8, 32768) are run-length packets: a row header
+ * (2, 2, width >> 8, width & 255), then for each of R, G, B, E packets that are either a run
+ * (count + 128, value) or a dump (count, count bytes), count in 1..remaining.  The host walks the
+ * packet headers only (one byte per packet; dump data is skipped) to check them and to find where
+ * each (row, plane) starts; the device expands them.  A row whose first bytes are not a run-length
+ * header means the file is flat from there: those 4 bytes are pixel 0 of row 0 and the rest follow
+ * in order (the stb loader's rule, kept as is).  Reading past the end yields zeros. */
+struct Layout {
+  bool flat = false;
+  std::vector<unsigned char> flat_rgbe; /* flat files: the interleaved RGBE pixels */
+  std::vector<uint64_t> starts;         /* run-length files: file offset of each (row, plane) */
+};
+
+nova_b200_status scan_rows(nova_b200_ctx *c, const std::vector<unsigned char> &bytes, const Header &hd,
+                           Layout &L) {
   using namespace nbctx;
   const size_t w = (size_t)hd.w, h = (size_t)hd.h;
-  rgbe.assign(w * h * 4, 0);
   Reader r{bytes, hd.data};
-  auto flat_from = [&](size_t first_pixel) {
-    for (size_t i = first_pixel; i < w * h * 4; i++) rgbe[i] = r.get();
+  auto flat_from = [&](size_t first_byte) {
+    L.flat = true;
+    L.flat_rgbe.assign(w * h * 4, 0);
+    const size_t avail = r.pos < bytes.size() ? bytes.size() - r.pos : 0;
+    const size_t n = std::min(avail, w * h * 4 - first_byte);
+    if (n) std::memcpy(&L.flat_rgbe[first_byte], &bytes[r.pos], n);
   };
   if (!rle_width(hd.w)) {
     flat_from(0);
     return NOVA_B200_SUCCESS;
   }
-  std::vector<unsigned char> line(w * 4);
+  L.starts.resize(4 * h);
   for (size_t j = 0; j < h; j++) {
     const unsigned char c1 = r.get(), c2 = r.get(), c3 = r.get();
     if (c1 != 2 || c2 != 2 || (c3 & 0x80)) {
-      rgbe[0] = c1, rgbe[1] = c2, rgbe[2] = c3, rgbe[3] = r.get();
+      const unsigned char c4 = r.get();
       flat_from(4);
+      L.flat_rgbe[0] = c1, L.flat_rgbe[1] = c2, L.flat_rgbe[2] = c3, L.flat_rgbe[3] = c4;
       return NOVA_B200_SUCCESS;
     }
     const size_t len = ((size_t)c3 << 8) | r.get();
     if (len != w) return fail(c, NOVA_B200_INVALID_ARGUMENT, "invalid decoded scanline length%s");
     for (int k = 0; k < 4; k++) {
+      L.starts[4 * j + k] = r.pos;
       size_t i = 0;
       while (i < w) {
         unsigned count = r.get();
         const size_t left = w - i;
-        if (count > 128) {
-          const unsigned char value = r.get();
-          count -= 128;
-          if (count == 0 || count > left) return fail(c, NOVA_B200_INVALID_ARGUMENT, "bad RLE data in HDR%s");
-          for (unsigned z = 0; z < count; z++) line[(i++) * 4 + k] = value;
-        } else {
-          if (count == 0 || count > left) return fail(c, NOVA_B200_INVALID_ARGUMENT, "bad RLE data in HDR%s");
-          for (unsigned z = 0; z < count; z++) line[(i++) * 4 + k] = r.get();
-        }
+        const bool run = count > 128;
+        if (run) count -= 128;
+        if (count == 0 || count > left) return fail(c, NOVA_B200_INVALID_ARGUMENT, "bad RLE data in HDR%s");
+        if (run)
+          r.get();
+        else
+          r.pos = std::min(r.pos + count, bytes.size() + 256); /* dump data: skipped, zeros past the end */
+        i += count;
       }
     }
-    std::memcpy(&rgbe[j * w * 4], line.data(), w * 4);
   }
   return NOVA_B200_SUCCESS;
 }
 
-/* One plane of a run-length row: runs of 3 or more equal bytes become run packets (at most 127),
- * everything else dump packets (at most 128). */
-void pack_plane(const unsigned char *p, int w, std::string &out) {
-  int x = 0;
-  while (x < w) {
-    int lit = x; /* start of the next run of >= 3, or w */
-    while (lit < w) {
-      if (lit + 2 < w && p[lit] == p[lit + 1] && p[lit] == p[lit + 2]) break;
-      lit++;
-    }
-    while (x < lit) {
-      const int n = std::min(lit - x, 128);
-      out.push_back((char)n);
-      out.append(reinterpret_cast<const char *>(p + x), (size_t)n);
-      x += n;
-    }
-    if (lit < w) {
-      int end = lit;
-      while (end < w && p[end] == p[lit]) end++;
-      while (x < end) {
-        const int n = std::min(end - x, 127);
-        out.push_back((char)(128 + n));
-        out.push_back((char)p[lit]);
-        x += n;
-      }
-    }
-  }
-}
-
-nova_b200_status read_file(nova_b200_ctx *c, const char *path, std::vector<unsigned char> &bytes) {
+/* The file, or its first `limit` bytes (limit 0: all); *whole tells whether all of it was read. */
+nova_b200_status read_file(nova_b200_ctx *c, const char *path, std::vector<unsigned char> &bytes, size_t limit = 0,
+                           bool *whole = nullptr) {
   using namespace nbctx;
   if (!path) return fail(c, NOVA_B200_INVALID_ARGUMENT, "path is null%s");
-  std::ifstream f(path, std::ios::binary);
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
   if (!f) return fail(c, NOVA_B200_INVALID_ARGUMENT, "cannot open %s", path);
-  bytes.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+  const std::streamoff size = f.tellg();
+  if (size < 0) return fail(c, NOVA_B200_INVALID_ARGUMENT, "cannot read %s", path);
+  const size_t n = limit ? std::min((size_t)size, limit) : (size_t)size;
+  bytes.resize(n);
+  f.seekg(0);
+  if (n && !f.read(reinterpret_cast<char *>(bytes.data()), (std::streamsize)n))
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "cannot read %s", path);
+  if (whole) *whole = n == (size_t)size;
   return NOVA_B200_SUCCESS;
 }
 
@@ -391,11 +535,18 @@ extern "C" nova_b200_status nova_b200_snapshot(nova_b200_ctx *c, const float *fi
 }
 
 extern "C" nova_b200_status nova_b200_hdr_info(nova_b200_ctx *c, const char *path, int32_t *width, int32_t *height) {
+  /* the header from the first 64 KB; the whole file only when the header runs past them */
   std::vector<unsigned char> bytes;
-  nova_b200_status st = read_file(c, path, bytes);
+  bool whole = false;
+  nova_b200_status st = read_file(c, path, bytes, 65536, &whole);
   if (st) return st;
   Header hd;
-  if ((st = parse_header(c, bytes, hd))) return st;
+  st = parse_header(c, bytes, hd);
+  if (!whole && (st || hd.data >= bytes.size())) {
+    if ((st = read_file(c, path, bytes))) return st;
+    st = parse_header(c, bytes, hd);
+  }
+  if (st) return st;
   if (width) *width = hd.w;
   if (height) *height = hd.h;
   return NOVA_B200_SUCCESS;
@@ -405,7 +556,7 @@ extern "C" nova_b200_status nova_b200_hdr_read(nova_b200_ctx *c, const char *pat
                                                float *rgba_device, uint64_t capacity) {
   using namespace nbctx;
   if (check_ctx(c)) return NOVA_B200_INVALID_ARGUMENT;
-  std::vector<unsigned char> bytes, rgbe;
+  std::vector<unsigned char> bytes;
   nova_b200_status st = read_file(c, path, bytes);
   if (st) return st;
   Header hd;
@@ -415,20 +566,42 @@ extern "C" nova_b200_status nova_b200_hdr_read(nova_b200_ctx *c, const char *pat
   if (capacity < npx * 4) return fail(c, NOVA_B200_INVALID_ARGUMENT, "output holds fewer than width * height * 4 floats%s");
   if (rgba_device && (reinterpret_cast<uintptr_t>(rgba_device) & 15))
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "rgba_device must be 16-byte aligned%s");
-  if ((st = unpack(c, bytes, hd, rgbe))) return st;
+  Layout L;
+  if ((st = scan_rows(c, bytes, hd, L))) return st;
   cudaSetDevice(c->device);
-  unsigned char *d_rgbe = nullptr;
+  const int n_planes = 4 * hd.h;
+  /* run-length files: the body (padded with zeros) and the plane offsets go to the device */
+  const size_t body_n = L.flat ? 0 : bytes.size() - hd.data + 256;
+  unsigned char *d_rgbe = nullptr, *d_body = nullptr;
+  uint64_t *d_starts = nullptr;
   float4 *d_out = reinterpret_cast<float4 *>(rgba_device), *tmp = nullptr;
   NB_CUDA(c, cudaMallocAsync(&d_rgbe, npx * 4, c->stream), "cudaMalloc(hdr bytes)");
-  cudaError_t e = cudaMemcpyAsync(d_rgbe, rgbe.data(), npx * 4, cudaMemcpyHostToDevice, c->stream);
+  cudaError_t e = cudaSuccess;
+  if (L.flat) {
+    e = cudaMemcpyAsync(d_rgbe, L.flat_rgbe.data(), npx * 4, cudaMemcpyHostToDevice, c->stream);
+  } else {
+    const size_t file_n = bytes.size() - hd.data;
+    for (auto &o : L.starts) o -= hd.data;
+    e = cudaMallocAsync(&d_body, body_n, c->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_starts, n_planes * sizeof(uint64_t), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_body + file_n, 0, body_n - file_n, c->stream);
+    if (e == cudaSuccess && file_n)
+      e = cudaMemcpyAsync(d_body, bytes.data() + hd.data, file_n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_starts, L.starts.data(), n_planes * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream);
+  }
   if (e == cudaSuccess && !d_out) {
     e = cudaMallocAsync(&tmp, npx * sizeof(float4), c->stream);
     d_out = tmp;
   }
   if (e == cudaSuccess) {
     cudaEventRecord(c->ev_begin, c->stream);
-    k_rgbe_decode<<<(unsigned)((npx + 255) / 256), 256, 0, c->stream>>>(reinterpret_cast<const uchar4 *>(d_rgbe), npx,
-                                                                         d_out);
+    if (!L.flat)
+      k_rle_unpack<<<(unsigned)(((uint64_t)n_planes * 32 + 127) / 128), 128, 0, c->stream>>>(d_body, d_starts, hd.w,
+                                                                                               n_planes, d_rgbe);
+    const uint64_t threads = (npx + 3) / 4;
+    k_rgbe_decode<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(reinterpret_cast<const uint32_t *>(d_rgbe),
+                                                                              npx, d_out);
     e = cudaGetLastError();
     cudaEventRecord(c->ev_end, c->stream);
   }
@@ -436,6 +609,8 @@ extern "C" nova_b200_status nova_b200_hdr_read(nova_b200_ctx *c, const char *pat
     e = cudaMemcpyAsync(rgba_host, d_out, npx * sizeof(float4), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFreeAsync(d_rgbe, c->stream);
+  if (d_body) cudaFreeAsync(d_body, c->stream);
+  if (d_starts) cudaFreeAsync(d_starts, c->stream);
   if (tmp) cudaFreeAsync(tmp, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "hdr_read");
   NB_CUDA(c, cudaStreamSynchronize(c->stream), "hdr_read");
@@ -453,9 +628,15 @@ extern "C" nova_b200_status nova_b200_hdr_write(nova_b200_ctx *c, const char *pa
   if (channels < 1 || channels > 4) return fail(c, NOVA_B200_INVALID_ARGUMENT, "channels must be 1 to 4%s");
   const uint64_t npx = (uint64_t)w * h;
   const bool rle = rle_width(w);
+  const bool vec4 = channels == 4 && !(reinterpret_cast<uintptr_t>(pixels_device) & 15);
   cudaSetDevice(c->device);
-  std::vector<unsigned char> rgbe(npx * 4);
-  unsigned char *d_rgbe = nullptr;
+  const int n_planes = 4 * h;
+  const int cap = w + w / 64 + 8; /* > width + width / 128 + 2, the most packets a row plane takes */
+  const size_t regions_n = rle ? (size_t)n_planes * cap : 0, out_cap = rle ? regions_n + 4 * (size_t)h : npx * 4;
+  unsigned char *d_rgbe = nullptr, *d_regions = nullptr, *d_out = nullptr;
+  uint32_t *d_sizes = nullptr;
+  uint64_t *d_offsets = nullptr;
+  unsigned *d_err = nullptr;
   float *d_src = const_cast<float *>(pixels_device), *tmp = nullptr;
   NB_CUDA(c, cudaMallocAsync(&d_rgbe, npx * 4, c->stream), "cudaMalloc(hdr bytes)");
   cudaError_t e = cudaSuccess;
@@ -465,31 +646,49 @@ extern "C" nova_b200_status nova_b200_hdr_write(nova_b200_ctx *c, const char *pa
       e = cudaMemcpyAsync(tmp, pixels_host, npx * channels * sizeof(float), cudaMemcpyHostToDevice, c->stream);
     d_src = tmp;
   }
+  if (rle) {
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_regions, regions_n, c->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_out, out_cap, c->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_sizes, n_planes * sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_offsets, (n_planes + 1) * sizeof(uint64_t) + 16, c->stream);
+    if (e == cudaSuccess) {
+      d_err = reinterpret_cast<unsigned *>(d_offsets + n_planes + 1);
+      e = cudaMemsetAsync(d_err, 0, sizeof(unsigned), c->stream);
+    }
+  }
   if (e == cudaSuccess) {
     cudaEventRecord(c->ev_begin, c->stream);
-    k_rgbe_encode<<<dim3((unsigned)((w + 127) / 128), (unsigned)h), 128, 0, c->stream>>>(d_src, w, h, channels, flip,
-                                                                                         rle ? 1 : 0, d_rgbe);
+    k_rgbe_encode<<<dim3((unsigned)((w + 127) / 128), (unsigned)h), 128, 0, c->stream>>>(
+        d_src, w, h, channels, flip, rle ? 1 : 0, (vec4 || (tmp && channels == 4)) ? 1 : 0, d_rgbe);
+    if (rle) {
+      k_rle_pack<<<(unsigned)(((uint64_t)n_planes * 32 + 127) / 128), 128, 0, c->stream>>>(d_rgbe, w, n_planes, cap,
+                                                                                             d_regions, d_sizes, d_err);
+      k_rle_scan<<<1, 1024, 0, c->stream>>>(d_sizes, n_planes, d_offsets);
+      k_rle_gather<<<(unsigned)(((uint64_t)n_planes * 32 + 255) / 256), 256, 0, c->stream>>>(
+          d_regions, d_sizes, d_offsets, w, cap, n_planes, d_out);
+    }
     e = cudaGetLastError();
     cudaEventRecord(c->ev_end, c->stream);
   }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(rgbe.data(), d_rgbe, npx * 4, cudaMemcpyDeviceToHost, c->stream);
+  /* the packed size and the overflow flag, then exactly the packed bytes */
+  uint64_t tail[2] = {npx * 4, 0};
+  if (e == cudaSuccess && rle)
+    e = cudaMemcpyAsync(tail, d_offsets + n_planes, sizeof(uint64_t) + sizeof(unsigned), cudaMemcpyDeviceToHost,
+                        c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFreeAsync(d_rgbe, c->stream);
-  if (tmp) cudaFreeAsync(tmp, c->stream);
-  if (e != cudaSuccess) return cuda_fail(c, e, "hdr_write");
   std::string out = "#?RADIANCE\n# nova_b200\nFORMAT=32-bit_rle_rgbe\n\n-Y " + std::to_string(h) + " +X " +
                     std::to_string(w) + "\n";
-  if (!rle) {
-    out.append(reinterpret_cast<const char *>(rgbe.data()), rgbe.size());
-  } else {
-    out.reserve(out.size() + rgbe.size() + (size_t)h * 8);
-    for (int row = 0; row < h; row++) {
-      const char head[4] = {2, 2, (char)((w >> 8) & 0xff), (char)(w & 0xff)};
-      out.append(head, 4);
-      const unsigned char *p = rgbe.data() + (size_t)row * w * 4;
-      for (int k = 0; k < 4; k++) pack_plane(p + (size_t)k * w, w, out);
-    }
+  const size_t head_n = out.size(), body_n = (size_t)tail[0];
+  const bool overflow = rle && (uint32_t)tail[1] != 0;
+  if (e == cudaSuccess && !overflow && body_n <= out_cap) {
+    out.resize(head_n + body_n);
+    e = cudaMemcpyAsync(&out[head_n], rle ? d_out : d_rgbe, body_n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   }
+  for (void *ptr : {(void *)d_rgbe, (void *)d_regions, (void *)d_out, (void *)d_sizes, (void *)d_offsets, (void *)tmp})
+    if (ptr) cudaFreeAsync(ptr, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "hdr_write");
+  if (overflow || body_n > out_cap) return fail(c, NOVA_B200_RENDERER_EXCEPTION, "run-length packing overflow%s");
   /* IO::Loader::writeHdr appends the extension (Loader_image.cpp:51-52) */
   const std::string file = std::string(path) + ".hdr";
   std::ofstream f(file, std::ios::binary);

@@ -13,6 +13,7 @@
  *                         (Loader_image.cpp:146-192), widened to RGBA with alpha 1 (:161-170)
  *   orc_hdr_parse         the header and scanline rules of the same loader (with the magic check of
  *                         load_magic_header, Loader_image.cpp:64-78)
+ *   orc_hdr_write         the whole file as IO::Loader::writeHdr writes it (Loader_image.cpp:50-62)
  *
  * stb (github.com/nothings/stb, stb_image.h / stb_image_write.h) is an un-vendored submodule of the
  * reference (vendor/stb is empty; the snapshot records no pinned commit).  What is restated here is
@@ -21,8 +22,10 @@
  * bytes truncated; decode c = byte * 2^(e - 136); run-length scanlines as in Radiance's "new" RLE.
  * Written independently of the device code: scalar loops, libm frexp / ldexp, x86-64 conversions.
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -244,4 +247,56 @@ extern "C" int32_t orc_hdr_parse(const uint8_t *bytes, uint64_t size, int32_t *w
       for (int comp = 0; comp < 4; comp++) dst[4 * x + comp] = planes[(size_t)comp * w + x];
   }
   return 0;
+}
+
+/* A whole .hdr file as IO::Loader::writeHdr writes it (path + ".hdr"; stbi_write_hdr's layout):
+ * the Radiance header, then per row either flat RGBE pixels (width < 8 or >= 32768) or a run-length
+ * scanline: (2, 2, width >> 8, width & 255) and, per component, dumps of up to 128 bytes up to the
+ * next run of 3 or more equal bytes, then that run in packets of up to 127.  flip: rows bottom-up.
+ * Returns 0, or 1 if the file cannot be written. */
+extern "C" int32_t orc_hdr_write(const char *path, const float *px, int32_t width, int32_t height, int32_t channels,
+                                 int32_t flip) {
+  std::string file = std::string(path) + ".hdr";
+  FILE *f = std::fopen(file.c_str(), "wb");
+  if (!f) return 1;
+  std::fprintf(f, "#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y %d +X %d\n", height, width);
+  std::vector<uint8_t> pix((size_t)width * 4), comp((size_t)width), buf;
+  buf.reserve((size_t)width * 5 + 16);
+  for (int i = 0; i < height; i++) {
+    const int row = flip ? height - 1 - i : i;
+    orc_rgbe_encode(px + (size_t)row * width * channels, (uint64_t)width, channels, pix.data());
+    buf.clear();
+    if (width < 8 || width >= 32768) {
+      buf.insert(buf.end(), pix.begin(), pix.end());
+    } else {
+      buf.push_back(2), buf.push_back(2), buf.push_back((uint8_t)(width >> 8)), buf.push_back((uint8_t)(width & 255));
+      for (int k = 0; k < 4; k++) {
+        for (int x = 0; x < width; x++) comp[x] = pix[4 * (size_t)x + k];
+        int x = 0;
+        while (x < width) {
+          int r = x;
+          while (r + 2 < width && !(comp[r] == comp[r + 1] && comp[r] == comp[r + 2])) r++;
+          if (r + 2 >= width) r = width;
+          while (x < r) {
+            const int len = std::min(r - x, 128);
+            buf.push_back((uint8_t)len);
+            buf.insert(buf.end(), comp.begin() + x, comp.begin() + x + len);
+            x += len;
+          }
+          if (r + 2 < width) {
+            const uint8_t v = comp[r];
+            while (r < width && comp[r] == v) r++;
+            while (x < r) {
+              const int len = std::min(r - x, 127);
+              buf.push_back((uint8_t)(128 + len));
+              buf.push_back(v);
+              x += len;
+            }
+          }
+        }
+      }
+    }
+    std::fwrite(buf.data(), 1, buf.size(), f);
+  }
+  return std::fclose(f) == 0 ? 0 : 1;
 }

@@ -151,6 +151,7 @@ void orc_snapshot(const float *film, int32_t width, int32_t height, int32_t chan
 void orc_rgbe_encode(const float *px, uint64_t n, int32_t channels, uint8_t *out);
 void orc_rgbe_decode(const uint8_t *in, uint64_t n, float *out_rgba);
 int32_t orc_hdr_parse(const uint8_t *bytes, uint64_t size, int32_t *width, int32_t *height, uint8_t *rgbe);
+int32_t orc_hdr_write(const char *path, const float *px, int32_t width, int32_t height, int32_t channels, int32_t flip);
 
 #ifdef __cplusplus
 }

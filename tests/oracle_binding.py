@@ -109,6 +109,8 @@ def lib():
         L.orc_rgbe_decode.argtypes = [u8p, C.c_uint64, f32p]
         L.orc_hdr_parse.argtypes = [u8p, C.c_uint64, i32p, i32p, u8p]
         L.orc_hdr_parse.restype = C.c_int32
+        L.orc_hdr_write.argtypes = [C.c_char_p, f32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+        L.orc_hdr_write.restype = C.c_int32
         _lib = L
     return _lib
 
@@ -366,3 +368,16 @@ def hdr_parse(data: bytes):
     rgbe = np.zeros((h.value, w.value, 4), np.uint8)
     code = lib().orc_hdr_parse(_p(buf, u8p), len(data), C.byref(w), C.byref(h), _p(rgbe, u8p))
     return code, w.value, h.value, (rgbe if code == 0 else None)
+
+
+def hdr_write(path, pixels, width, height, channels, flip=0):
+    """Writes path + ".hdr" the way IO::Loader::writeHdr does."""
+    px = np.ascontiguousarray(pixels, np.float32).reshape(-1)
+    if lib().orc_hdr_write(os.fsencode(path), _p(px, f32p), width, height, channels, flip) != 0:
+        raise OSError("cannot write %s.hdr" % path)
+
+
+def hdr_body(data: bytes) -> bytes:
+    """The scanline bytes of a .hdr file (after the resolution line)."""
+    head_end = data.index(b"\n\n") + 2
+    return data[data.index(b"\n", head_end) + 1:]

@@ -152,7 +152,8 @@ def test_hdr_info_header_logic(tmp_path):
     rgbe = np.full((3, 17, 4), 130, np.uint8)
     cases = {"ok": make_file(rgbe), "flat": make_file(rgbe, rle=False), "rgbe_magic": make_file(rgbe, first="#?RGBE"),
              "no_format": make_file(rgbe, fmt=None), "exr": b"\x76\x2f\x31\x01" + bytes(40),
-             "bad_res": b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y 3 -X 17\n"}
+             "bad_res": b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y 3 -X 17\n",
+             "long_header": make_file(rgbe, extra=["# " + "x" * 2000] * 80)}  # 160 KB of comment lines
     for name, data in cases.items():
         p = tmp_path / (name + ".hdr")
         p.write_bytes(data)

@@ -113,6 +113,43 @@ def test_hdr_write_matches_oracle(ctx, oracle, torch_cuda, tmp_path, w, h, chann
         np.testing.assert_array_equal(got, want)
         if 8 <= w < 32768:
             assert data.count(b"\x02\x02" + bytes([w >> 8, w & 255])) >= h  # run-length rows
+        # the packets themselves: the same greedy packing as the oracle's writer, byte for byte
+        oracle.hdr_write(str(tmp_path / "oracle"), px, w, h, channels, flip)
+        assert oracle.hdr_body(data) == oracle.hdr_body(open(str(tmp_path / "oracle.hdr"), "rb").read())
+
+
+@pytest.mark.parametrize("w", [300, 32767, 32768], ids=["w300", "max-rle-width", "flat-width"])
+def test_hdr_runs_round_trip(ctx, oracle, torch_cuda, tmp_path, w):
+    """Rows of long and short runs (lengths 1-3, 127-129, 254-256, a whole row) between literal
+    stretches: the written packets equal the oracle writer's, and reading them back gives exactly
+    the decoded RGBE pixels, on the host and on the device."""
+    torch = torch_cuda
+    rng = np.random.default_rng(w)
+    h = 3
+    px = np.zeros((h, w, 4), np.float32)
+    px[0] = 1.0
+    pieces, x = [], 0
+    for n in (1, 2, 3, 127, 128, 129, 254, 255, 256, 5, 40):
+        pieces.append((x, n))
+        x += n + 7
+    for k, (x0, n) in enumerate(pieces):
+        if x0 + n <= w:
+            px[1, x0:x0 + n] = [0.5, 1.0, 0.0, 1.0][k % 4]
+    px[2] = rng.lognormal(0, 1, (w, 4))
+    px[2, w // 3: w // 3 + 200] = 0.0
+    base = str(tmp_path / "runs")
+    ctx.hdr_write(base, w, h, 4, pixels_host=px)
+    data = open(base + ".hdr", "rb").read()
+    oracle.hdr_write(str(tmp_path / "oracle"), px, w, h, 4)
+    assert oracle.hdr_body(data) == oracle.hdr_body(open(str(tmp_path / "oracle.hdr"), "rb").read())
+    code, fw, fh, q = oracle.hdr_parse(data)
+    assert (code, fw, fh) == (0, w, h)
+    want = oracle.rgbe_decode(q.reshape(-1, 4)).reshape(h, w, 4)
+    host = np.zeros((h, w, 4), np.float32)
+    dev = torch.zeros((h, w, 4), device="cuda")
+    ctx.hdr_read(base + ".hdr", rgba_host=host, rgba_device_ptr=dev.data_ptr())
+    same_bits(host, want)
+    same_bits(dev.cpu().numpy(), want)
 
 
 def test_hdr_read_matches_oracle(ctx, oracle, torch_cuda, tmp_path):
