@@ -12,7 +12,8 @@
  *     k_split        one CTA per node: SAH over bins*3 candidate planes, node allocation, children
  *     k_partition    primitive ids scattered to the children's ranges of the other id buffer
  *   small nodes (<= small_task): k_build_small, one CTA per node builds its whole subtree with a
- *     CTA-local task stack, shared-memory bins and a stable block-scan partition.
+ *     CTA-local task stack, shared-memory bins and a stable block-scan partition; nodes of at most
+ *     32 primitives are handed to single warps (exact sweep SAH over sorted centroids, no barriers).
  *
  * Leaves list their primitives in a contiguous range of `order`; each leaf's range is finally
  * sorted by primitive index so the layout is deterministic (atomics only reorder primitives
@@ -482,6 +483,158 @@ __device__ unsigned block_exclusive_scan(unsigned v, unsigned *sh /* 32 */, unsi
   return r;
 }
 
+/* ------------------------------------------------------------------ warp subtrees (<= 32 primitives)
+ *
+ * A node of at most 32 primitives is built by one warp, one primitive per lane, without block
+ * barriers: per axis the lanes sort their centroids (bitonic, ties by lane), scan the sorted boxes
+ * from both ends and evaluate the SAH of every split position (an exact sweep, where the larger
+ * nodes use bins); the best (cost, axis, position) wins, the ids go to the other buffer in that
+ * axis's sorted order and the left child continues on the warp while the right one waits on the
+ * warp's stack.  Leaf rules, cost model and the median split below kMedianDepth are those of the
+ * CTA path. */
+constexpr int kWarpPrims = 32;
+constexpr int kWarpList = 256;   /* subtrees of <= kWarpPrims handed from the CTA loop to its warps */
+constexpr int kWarpStack = 40;   /* right siblings along one path: depth <= 31 below a 32-prim node */
+
+/* Sorts (key, idx) ascending over the warp (ties by idx); returns the idx now at this lane. */
+__device__ __forceinline__ int warp_sort_idx(float key, int idx) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 2; k <= 32; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const float ok = __shfl_xor_sync(0xffffffffu, key, j);
+      const int oi = __shfl_xor_sync(0xffffffffu, idx, j);
+      const bool other_less = ok < key || (ok == key && oi < idx);
+      const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+      if (keep_min ? other_less : !other_less) key = ok, idx = oi;
+    }
+  return idx;
+}
+
+/* Inclusive prefix (from lane 0) and suffix (from lane 31) bounds of the boxes held by the lanes. */
+__device__ __forceinline__ void warp_scan_boxes(const float lo[3], const float hi[3], float pl[3], float ph[3],
+                                                float sl[3], float sh[3]) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 0; k < 3; k++) pl[k] = sl[k] = lo[k], ph[k] = sh[k] = hi[k];
+  for (int o = 1; o < 32; o <<= 1)
+    for (int k = 0; k < 3; k++) {
+      const float a = __shfl_up_sync(0xffffffffu, pl[k], o), b = __shfl_up_sync(0xffffffffu, ph[k], o);
+      const float c = __shfl_down_sync(0xffffffffu, sl[k], o), d = __shfl_down_sync(0xffffffffu, sh[k], o);
+      if (lane >= o) pl[k] = fminf(pl[k], a), ph[k] = fmaxf(ph[k], b);
+      if (lane + o < 32) sl[k] = fminf(sl[k], c), sh[k] = fmaxf(sh[k], d);
+    }
+}
+
+__device__ __forceinline__ Best warp_best(Best b) {
+  for (int o = 16; o > 0; o >>= 1) {
+    Best q{__shfl_xor_sync(0xffffffffu, b.cost, o), __shfl_xor_sync(0xffffffffu, b.key, o)};
+    if (better(q, b)) b = q;
+  }
+  return b;
+}
+
+/* Builds the subtree of `root` (<= 32 primitives) with the calling warp; all 32 lanes call it. */
+__device__ void warp_build(const Shared &s, Task root, Task *wstack) {
+  const int lane = threadIdx.x & 31;
+  int wsp = 0;
+  Task t = root;
+  for (int guard = 0; guard < 4 * kWarpPrims; guard++) {
+    const uint32_t n = t.end - t.begin;
+    const uint32_t *src = ids_of(s, t.buf);
+    uint32_t *dst = ids_of(s, 1 - t.buf);
+    const bool act = (uint32_t)lane < n;
+    const uint32_t id = act ? src[t.begin + lane] : 0u;
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX}, c[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    if (act) {
+      const float4 a = __ldg(s.lo + id), b = __ldg(s.hi + id);
+      lo[0] = a.x, lo[1] = a.y, lo[2] = a.z, hi[0] = b.x, hi[1] = b.y, hi[2] = b.z;
+      c[0] = (a.x + b.x) * 0.5f, c[1] = (a.y + b.y) * 0.5f, c[2] = (a.z + b.z) * 0.5f;
+    }
+    bool make_leaf = n <= 1;
+    const float area = half_area(t.lo, t.hi);
+    Best best{FLT_MAX, 0x7fffffff};
+    float pl[3], ph[3], sl[3], sh[3];
+    if (!make_leaf && area > 0.f && t.depth < kMedianDepth) {
+      for (int a = 0; a < 3; a++) {
+        const int from = warp_sort_idx(act ? c[a] : FLT_MAX, lane);
+        float bl[3], bh[3];
+        for (int k = 0; k < 3; k++)
+          bl[k] = __shfl_sync(0xffffffffu, lo[k], from), bh[k] = __shfl_sync(0xffffffffu, hi[k], from);
+        warp_scan_boxes(bl, bh, pl, ph, sl, sh);
+        float rl[3], rh[3];
+        for (int k = 0; k < 3; k++)
+          rl[k] = __shfl_down_sync(0xffffffffu, sl[k], 1), rh[k] = __shfl_down_sync(0xffffffffu, sh[k], 1);
+        Best mine{FLT_MAX, 0x7fffffff};
+        if ((uint32_t)lane + 1 < n) { /* split after sorted position lane: left = lane + 1 primitives */
+          const float cost =
+              s.cost_trav + (half_area(pl, ph) * (float)(lane + 1) + half_area(rl, rh) * (float)(n - 1 - lane)) / area;
+          mine = Best{cost, a * 64 + lane};
+        }
+        mine = warp_best(mine);
+        if (better(mine, best)) best = mine;
+      }
+    }
+    const bool has_split = best.key != 0x7fffffff;
+    if (!make_leaf) {
+      if ((int)n <= s.max_leaf && (!has_split || (float)n <= best.cost)) make_leaf = true;
+      if ((int)n <= s.hard_leaf && !has_split) make_leaf = true;
+    }
+    if (make_leaf) {
+      if (act) s.order[t.begin + lane] = id;
+      if (lane == 0) finish_leaf(s, t);
+      if (wsp == 0) return;
+      __syncwarp();
+      t = wstack[--wsp];
+      __syncwarp();
+      continue;
+    }
+    /* the split: best SAH position, or the median along the widest centroid extent */
+    int axis, left_n;
+    if (has_split) {
+      axis = best.key / 64;
+      left_n = best.key % 64 + 1;
+    } else {
+      float ext[3];
+      for (int k = 0; k < 3; k++) {
+        float mn = act ? c[k] : FLT_MAX, mx = act ? c[k] : -FLT_MAX;
+        for (int o = 16; o > 0; o >>= 1)
+          mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o)), mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        ext[k] = mx - mn;
+      }
+      axis = ext[1] > ext[0] ? (ext[2] > ext[1] ? 2 : 1) : (ext[2] > ext[0] ? 2 : 0);
+      left_n = (int)n / 2;
+    }
+    const int from = warp_sort_idx(act ? c[axis] : FLT_MAX, lane);
+    const uint32_t sid = __shfl_sync(0xffffffffu, id, from);
+    float bl[3], bh[3];
+    for (int k = 0; k < 3; k++)
+      bl[k] = __shfl_sync(0xffffffffu, lo[k], from), bh[k] = __shfl_sync(0xffffffffu, hi[k], from);
+    if (act) dst[t.begin + lane] = sid;
+    warp_scan_boxes(bl, bh, pl, ph, sl, sh);
+    float cl[3], ch[3], dl[3], dh[3];
+    for (int k = 0; k < 3; k++) {
+      cl[k] = __shfl_sync(0xffffffffu, pl[k], left_n - 1), ch[k] = __shfl_sync(0xffffffffu, ph[k], left_n - 1);
+      dl[k] = __shfl_sync(0xffffffffu, sl[k], left_n), dh[k] = __shfl_sync(0xffffffffu, sh[k], left_n);
+    }
+    const uint32_t mid = t.begin + (uint32_t)left_n;
+    int node = 0;
+    if (lane == 0) {
+      node = (int)atomicAdd(s.node_counter, 1u);
+      if (t.parent >= 0) write_ref(s.nodes, t.parent, t.slot, node);
+      write_child(s.nodes, node, 0, cl, ch);
+      write_child(s.nodes, node, 1, dl, dh);
+      if (wsp < kWarpStack)
+        wstack[wsp] = Task{mid, t.end, node, 1, t.depth + 1, 1 - t.buf, {dl[0], dl[1], dl[2]}, {dh[0], dh[1], dh[2]}};
+      else
+        atomicAdd(s.leaf_count + 1, 1u); /* cannot happen (depth <= 31): reported as a build failure */
+    }
+    node = __shfl_sync(0xffffffffu, node, 0);
+    if (wsp < kWarpStack) wsp++;
+    __syncwarp(); /* the children read ids written by other lanes */
+    t = Task{t.begin, mid, node, 0, t.depth + 1, 1 - t.buf, {cl[0], cl[1], cl[2]}, {ch[0], ch[1], ch[2]}};
+  }
+  if (lane == 0) atomicAdd(s.leaf_count + 1, 1u); /* a subtree that did not finish: a build failure */
+}
+
 __global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Task *small_tasks) {
   __shared__ Task stack[kSmallStack];
   __shared__ int sp, have;
@@ -492,10 +645,18 @@ __global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Tas
   __shared__ Best best_sh[kBlock / 32];
   __shared__ Task cur;
   __shared__ float cmin_s[3], scale_s[3];
+  __shared__ Task wlist[kWarpList];
+  __shared__ Task wstack[kSmallBlock / 32][kWarpStack];
+  __shared__ int wl_count, wl_next;
   const int nb = s.bins;
   if (threadIdx.x == 0) {
-    stack[0] = small_tasks[blockIdx.x];
-    sp = 1;
+    const Task t0 = small_tasks[blockIdx.x];
+    wl_count = wl_next = 0;
+    sp = 0;
+    if (t0.end - t0.begin <= (uint32_t)kWarpPrims)
+      wlist[wl_count++] = t0;
+    else
+      stack[sp++] = t0;
   }
   while (true) {
     __syncthreads();
@@ -622,11 +783,26 @@ __global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Tas
       write_child(s.nodes, node, 1, dl, dh);
       Task L{t.begin, mid, node, 0, t.depth + 1, 1 - t.buf, {cl[0], cl[1], cl[2]}, {ch[0], ch[1], ch[2]}};
       Task R{mid, t.end, node, 1, t.depth + 1, 1 - t.buf, {dl[0], dl[1], dl[2]}, {dh[0], dh[1], dh[2]}};
-      if (sp + 2 <= kSmallStack) { /* depth-first: at most one pending sibling per level */
-        stack[sp++] = R;
-        stack[sp++] = L;
+      /* subtrees of <= kWarpPrims primitives go to the warps; larger ones stay on the CTA stack
+       * (depth-first: at most one pending sibling per level) */
+      for (const Task &ch : {R, L}) {
+        if (ch.end - ch.begin <= (uint32_t)kWarpPrims && wl_count < kWarpList)
+          wlist[wl_count++] = ch;
+        else if (sp < kSmallStack)
+          stack[sp++] = ch;
+        else
+          atomicAdd(s.leaf_count + 1, 1u); /* a lost subtree: reported as a build failure */
       }
     }
+  }
+  /* the warps build the small subtrees, each taking the next one from the list */
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(&wl_next, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= wl_count) break;
+    warp_build(s, wlist[item], wstack[warp]);
   }
 }
 

@@ -184,20 +184,24 @@ def make_scene_desc(scene: dict):
     keep = []
     ms = scene["meshes"]
     mt = np.zeros(len(ms), _np_dtype(Mesh))
-    for i, m in enumerate(ms):
+
+    def as_c(a, dtype):
+        if not (type(a) is np.ndarray and a.dtype == dtype and a.flags.c_contiguous):
+            a = np.ascontiguousarray(a, dtype)
+        keep.append(a)
+        return a
+
+    f32, u32 = np.dtype(np.float32), np.dtype(np.uint32)
+    cols = {k: [] for k in ("vertices", "normals", "tangents", "bitangents", "uv", "indices", "n_verts", "n_tris")}
+    for m in ms:
         for k in ("vertices", "normals", "tangents", "bitangents", "uv"):
-            a = m[k]
-            if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
-                a = np.ascontiguousarray(a, np.float32)
-            keep.append(a)
-            mt[k][i] = _addr(a)
-        idx = m["indices"]
-        if not (isinstance(idx, np.ndarray) and idx.dtype == np.uint32 and idx.flags.c_contiguous):
-            idx = np.ascontiguousarray(idx, np.uint32)
-        keep.append(idx)
-        mt["indices"][i] = _addr(idx)
-        mt["n_verts"][i] = np.asarray(m["vertices"]).size // 3
-        mt["n_tris"][i] = idx.size // 3
+            cols[k].append(as_c(m[k], f32).__array_interface__["data"][0])
+        idx = as_c(m["indices"], u32)
+        cols["indices"].append(idx.__array_interface__["data"][0])
+        cols["n_verts"].append(np.size(m["vertices"]) // 3)
+        cols["n_tris"].append(idx.size // 3)
+    for k, v in cols.items():
+        mt[k] = v
     xs = scene["instances"]
     it = np.zeros(len(xs), _np_dtype(Instance))
     it["mesh"] = [x["mesh"] for x in xs]
@@ -256,12 +260,32 @@ def render_batch(contexts, frames, films_host=None, films_device=None) -> "Rende
     return st
 
 
+class PreparedScene:
+    """A scene's C descriptor built once (make_scene_desc) for repeated uploads: it points at the
+    scene's arrays, which it keeps alive, so the arrays must not be modified in place between an
+    upload and the next (their contents are copied to the device at every upload)."""
+
+    def __init__(self, scene: dict):
+        self.desc, self._keep = make_scene_desc(scene)
+
+
+def prepare_scene(scene: dict) -> PreparedScene:
+    return PreparedScene(scene)
+
+
+def _desc_of(scene):
+    if isinstance(scene, PreparedScene):
+        return scene.desc, scene
+    return make_scene_desc(scene)
+
+
 def upload_batch(contexts, scenes):
-    """nova_b200_upload_scene_batch: uploads scenes[k] to contexts[k], the contexts concurrently."""
+    """nova_b200_upload_scene_batch: uploads scenes[k] (a scene dictionary or a PreparedScene) to
+    contexts[k], the contexts concurrently."""
     n = len(contexts)
     keep, descs = [], (SceneDesc * n)()
     for k, sc in enumerate(scenes):
-        d, kp = make_scene_desc(sc)
+        d, kp = _desc_of(sc)
         descs[k] = d
         keep.append(kp)
     hs = (C.c_void_p * n)(*[c.h for c in contexts])
@@ -323,8 +347,9 @@ class Context:
         if st != 0:
             raise NovaError(st, self.error())
 
-    def upload(self, scene: dict):
-        desc, keep = make_scene_desc(scene)
+    def upload(self, scene):
+        """nova_b200_upload_scene of a scene dictionary or a PreparedScene."""
+        desc, keep = _desc_of(scene)
         self._check(lib().nova_b200_upload_scene(self.h, C.byref(desc)))
         del keep
 

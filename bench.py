@@ -527,7 +527,9 @@ def run_ours(args, rank, world, local_rank):
     # end to end through the C ABI from pinned host buffers: upload + build + render + readback
     e2e = None
     if rank == 0 and not args.no_e2e:
-        pinned = [pin_scene(j["scene"]) for j in jobs]
+        # pinned host copies of the scenes and their C descriptors, made once like a C++ caller's
+        # buffers and structs; every step still copies all of the scene data to the device
+        pinned = [native.prepare_scene(pin_scene(j["scene"])) for j in jobs]
         host_films = [torch.empty(s, dtype=torch.float32).pin_memory() for s in sizes]
         e_frames = [native.make_frame(j["scene"], j["width"], j["height"], j["spp"], j["depth"], seed=0,
                                       rr_start=j["rr_start"]) for j in jobs]
