@@ -486,7 +486,7 @@ __device__ unsigned block_exclusive_scan(unsigned v, unsigned *sh /* 32 */, unsi
 /* ------------------------------------------------------------------ warp subtrees (<= 32 primitives)
  *
  * A node of at most 32 primitives is built by one warp, one primitive per lane, without block
- * barriers: per axis the lanes sort their centroids (bitonic, ties by lane), scan the sorted boxes
+ * barriers: per axis the lanes sort their centroids (bitonic, ties by primitive id), scan the sorted boxes
  * from both ends and evaluate the SAH of every split position (an exact sweep, where the larger
  * nodes use bins); the best (cost, axis, position) wins, the ids go to the other buffer in that
  * axis's sorted order and the left child continues on the warp while the right one waits on the
@@ -496,16 +496,20 @@ constexpr int kWarpPrims = 32;
 constexpr int kWarpList = 256;   /* subtrees of <= kWarpPrims handed from the CTA loop to its warps */
 constexpr int kWarpStack = 40;   /* right siblings along one path: depth <= 31 below a 32-prim node */
 
-/* Sorts (key, idx) ascending over the warp (ties by idx); returns the idx now at this lane. */
-__device__ __forceinline__ int warp_sort_idx(float key, int idx) {
+/* Sorts the lanes' (key, tie) pairs ascending over the warp and returns, for this lane's rank, the
+ * lane that held it.  tie must be unique per lane (the primitive id, so equal centroids sort the
+ * same way whatever order the ids arrive in; empty lanes use 0xffffffff - lane). */
+__device__ __forceinline__ int warp_sort_idx(float key, uint32_t tie) {
   const int lane = threadIdx.x & 31;
+  int idx = lane;
   for (int k = 2; k <= 32; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
       const float ok = __shfl_xor_sync(0xffffffffu, key, j);
+      const uint32_t ot = __shfl_xor_sync(0xffffffffu, tie, j);
       const int oi = __shfl_xor_sync(0xffffffffu, idx, j);
-      const bool other_less = ok < key || (ok == key && oi < idx);
+      const bool other_less = ok < key || (ok == key && ot < tie);
       const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
-      if (keep_min ? other_less : !other_less) key = ok, idx = oi;
+      if (keep_min ? other_less : !other_less) key = ok, tie = ot, idx = oi;
     }
   return idx;
 }
@@ -555,7 +559,7 @@ __device__ void warp_build(const Shared &s, Task root, Task *wstack) {
     float pl[3], ph[3], sl[3], sh[3];
     if (!make_leaf && area > 0.f && t.depth < kMedianDepth) {
       for (int a = 0; a < 3; a++) {
-        const int from = warp_sort_idx(act ? c[a] : FLT_MAX, lane);
+        const int from = warp_sort_idx(act ? c[a] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane);
         float bl[3], bh[3];
         for (int k = 0; k < 3; k++)
           bl[k] = __shfl_sync(0xffffffffu, lo[k], from), bh[k] = __shfl_sync(0xffffffffu, hi[k], from);
@@ -603,7 +607,7 @@ __device__ void warp_build(const Shared &s, Task root, Task *wstack) {
       axis = ext[1] > ext[0] ? (ext[2] > ext[1] ? 2 : 1) : (ext[2] > ext[0] ? 2 : 0);
       left_n = (int)n / 2;
     }
-    const int from = warp_sort_idx(act ? c[axis] : FLT_MAX, lane);
+    const int from = warp_sort_idx(act ? c[axis] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane);
     const uint32_t sid = __shfl_sync(0xffffffffu, id, from);
     float bl[3], bh[3];
     for (int k = 0; k < 3; k++)

@@ -163,12 +163,14 @@ void free_scene(nova_b200_ctx *c) {
   if (c->d_arena) cudaFreeAsync(c->d_arena, c->stream);
   if (c->d_nodes) cudaFreeAsync(c->d_nodes, c->stream);
   if (c->d_tris) cudaFreeAsync(c->d_tris, c->stream);
+  if (c->d_valid) cudaFreeAsync(c->d_valid, c->stream);
   c->d_arena = nullptr;
   c->d_nodes = nullptr;
   c->d_tris = nullptr;
+  c->d_valid = nullptr;
+  c->n_valid = 0;
   c->scene = nb::DevScene{};
   c->h_instances.clear();
-  c->h_valid.clear();
   c->scene_ready = c->bvh_ready = false;
   c->primal_valid = false;
   c->scene_bytes = 0;
@@ -245,6 +247,100 @@ __global__ void k_interleave(const InterleaveMesh *meshes, uint32_t n_meshes, ui
   attr[4 * (size_t)i + 1] = make_float4(n[3 * i + 1], n[3 * i + 2], t[3 * i], t[3 * i + 1]);
   attr[4 * (size_t)i + 2] = make_float4(t[3 * i + 2], b[3 * i], b[3 * i + 1], b[3 * i + 2]);
   attr[4 * (size_t)i + 3] = make_float4(uv[2 * i], uv[2 * i + 1], 0.f, 0.f);
+}
+
+/* Per global primitive (instance by instance, triangle by triangle): its instance (binary search on
+ * the instances' first primitive ids), a flag for "can be hit" (no repeated vertex index,
+ * Triangle.h:127-132) and the check that its indices name vertices of its mesh (bad[0] |= 1). */
+__global__ void k_scene_tables(const nb::DevInstance *inst, uint32_t n_inst, const nb::DevMesh *meshes, uint32_t n_prims,
+                               uint32_t *prim_inst, uint32_t *can_hit, unsigned *bad) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_prims) return;
+  uint32_t lo = 0, hi = n_inst;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (inst[mid].prim_offset <= p)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const nb::DevMesh &m = meshes[inst[lo].mesh];
+  const uint32_t t = p - inst[lo].prim_offset;
+  const uint32_t a = m.idx[3 * (size_t)t], b = m.idx[3 * (size_t)t + 1], c = m.idx[3 * (size_t)t + 2];
+  if (a >= m.n_verts || b >= m.n_verts || c >= m.n_verts) atomicOr(bad, 1u);
+  prim_inst[p] = lo;
+  can_hit[p] = (a == b || c == b || c == a) ? 0u : 1u;
+}
+
+/* Stable compaction of the primitives that can be hit: per block of kCompactItems flags a count,
+ * one block scans the counts (block offsets and the total), then each block writes its ids. */
+constexpr uint32_t kCompactThreads = 1024, kCompactPer = 4, kCompactItems = kCompactThreads * kCompactPer;
+
+__device__ __forceinline__ uint32_t block_excl_scan1024(uint32_t v, uint32_t *sh /* 32 */, uint32_t *total) {
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t s = sh[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= (uint32_t)o) s += y;
+    }
+    sh[lane] = s; /* inclusive over warps */
+  }
+  __syncthreads();
+  const uint32_t before = (w ? sh[w - 1] : 0u) + x - v;
+  *total = sh[31];
+  __syncthreads();
+  return before;
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_compact_count(const uint32_t *flags, uint32_t n, uint32_t *counts) {
+  __shared__ uint32_t sh[32];
+  const uint32_t base = blockIdx.x * kCompactItems + threadIdx.x * kCompactPer;
+  uint32_t c = 0;
+  for (uint32_t k = 0; k < kCompactPer; k++)
+    if (base + k < n) c += flags[base + k];
+  uint32_t total;
+  block_excl_scan1024(c, sh, &total);
+  if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_compact_offsets(uint32_t *counts, uint32_t n_blocks,
+                                                                     uint32_t *total_out) {
+  __shared__ uint32_t sh[32];
+  const uint32_t per = (n_blocks + kCompactThreads - 1) / kCompactThreads;
+  const uint32_t b = threadIdx.x * per, e = min(b + per, n_blocks);
+  uint32_t sum = 0;
+  for (uint32_t i = b; i < e; i++) sum += counts[i];
+  uint32_t total;
+  uint32_t run = block_excl_scan1024(sum, sh, &total);
+  for (uint32_t i = b; i < e; i++) {
+    const uint32_t cnt = counts[i];
+    counts[i] = run;
+    run += cnt;
+  }
+  if (threadIdx.x == 0) *total_out = total;
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_compact_write(const uint32_t *flags, uint32_t n,
+                                                                   const uint32_t *offsets, uint32_t *out) {
+  __shared__ uint32_t sh[32];
+  const uint32_t base = blockIdx.x * kCompactItems + threadIdx.x * kCompactPer;
+  uint32_t f[kCompactPer], c = 0;
+  for (uint32_t k = 0; k < kCompactPer; k++) {
+    f[k] = base + k < n ? flags[base + k] : 0u;
+    c += f[k];
+  }
+  uint32_t total;
+  uint32_t pos = offsets[blockIdx.x] + block_excl_scan1024(c, sh, &total);
+  for (uint32_t k = 0; k < kCompactPer; k++)
+    if (f[k]) out[pos++] = base + k;
 }
 
 __global__ void k_validate(const float4 *nodes, uint32_t n_nodes, uint32_t n_tris, unsigned *bad) {
@@ -417,8 +513,6 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     const nova_b200_mesh &m = d->meshes[i];
     if (!m.vertices || !m.normals || !m.tangents || !m.bitangents || !m.uv || !m.indices || m.n_tris == 0)
       return fail(c, NOVA_B200_INVALID_ARGUMENT, "mesh needs vertices, normals, tangents, bitangents, uv, indices%s");
-    for (uint64_t k = 0; k < 3ull * m.n_tris; k++)
-      if (m.indices[k] >= m.n_verts) return fail(c, NOVA_B200_INVALID_ARGUMENT, "mesh index out of range%s");
     meshes[i].n_verts = m.n_verts, meshes[i].n_tris = m.n_tris;
     const size_t nv = m.n_verts;
     MeshOffsets &o = moff[i];
@@ -456,22 +550,17 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     return fail(c, NOVA_B200_OUT_OF_MEMORY, "more than 2^27 triangles are not supported by the leaf encoding%s");
   c->n_prims = offset;
   c->n_materials = d->n_materials;
-  std::vector<uint32_t> prim_inst(offset);
-  c->h_valid.clear();
-  c->h_valid.reserve(offset);
-  for (uint32_t i = 0; i < d->n_instances; i++) {
-    const nova_b200_mesh &m = d->meshes[d->instances[i].mesh];
-    const uint32_t base = c->h_instances[i].prim_offset;
-    for (uint32_t t = 0; t < m.n_tris; t++) {
-      prim_inst[base + t] = i;
-      const uint32_t *id = m.indices + 3ull * t;
-      if (!(id[0] == id[1] || id[2] == id[1] || id[2] == id[0])) c->h_valid.push_back(base + t);
-    }
-  }
-  if (c->h_valid.empty()) return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "scene has no non-degenerate triangle%s");
+  /* per-triangle tables (instance of each primitive, which primitives can be hit) and the index
+   * check are built on the device after the copies */
   const size_t off_mats = plan.add(mats.data(), mats.size() * sizeof(nb::DevMaterial));
   const size_t off_inst = plan.add(c->h_instances.data(), c->h_instances.size() * sizeof(nb::DevInstance));
-  const size_t off_pi = plan.add(prim_inst.data(), prim_inst.size() * sizeof(uint32_t));
+  const size_t off_pi = plan.arena;
+  plan.arena += UploadPlan::align(offset * sizeof(uint32_t));
+  const uint32_t n_cblocks = (uint32_t)((offset + kCompactItems - 1) / kCompactItems);
+  const size_t off_flags = plan.add(nullptr, offset * sizeof(uint32_t), true);
+  const size_t off_counts = plan.add(nullptr, (n_cblocks + 2) * sizeof(uint32_t), true);
+  plan.pieces.pop_back();
+  plan.pieces.pop_back();
   /* texture and mesh tables hold device pointers: reserve their space now, fill after allocation */
   const size_t off_tex = plan.arena;
   plan.arena += UploadPlan::align(tex.size() * sizeof(nb::DevTexture));
@@ -504,9 +593,28 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
   if (total_verts)
     k_interleave<<<(unsigned)((total_verts + 255) / 256), 256, 0, c->stream>>>(
         reinterpret_cast<const InterleaveMesh *>(temp + off_ilv), d->n_meshes, (uint32_t)total_verts, temp, arena);
-  const cudaError_t e_launch = cudaGetLastError();
+  uint32_t *flags = reinterpret_cast<uint32_t *>(temp + off_flags), *counts = reinterpret_cast<uint32_t *>(temp + off_counts);
+  unsigned *bad = counts + n_cblocks; /* bad, total */
+  cudaError_t e_launch = cudaGetLastError();
+  if (e_launch == cudaSuccess) e_launch = cudaMallocAsync(&c->d_valid, offset * sizeof(uint32_t), c->stream);
+  if (e_launch == cudaSuccess) e_launch = cudaMemsetAsync(bad, 0, sizeof(unsigned), c->stream);
+  if (e_launch == cudaSuccess) {
+    k_scene_tables<<<(unsigned)((offset + 255) / 256), 256, 0, c->stream>>>(
+        reinterpret_cast<const nb::DevInstance *>(arena + off_inst), d->n_instances,
+        reinterpret_cast<const nb::DevMesh *>(arena + off_mesh), (uint32_t)offset,
+        reinterpret_cast<uint32_t *>(arena + off_pi), flags, bad);
+    k_compact_count<<<n_cblocks, kCompactThreads, 0, c->stream>>>(flags, (uint32_t)offset, counts);
+    k_compact_offsets<<<1, kCompactThreads, 0, c->stream>>>(counts, n_cblocks, bad + 1);
+    k_compact_write<<<n_cblocks, kCompactThreads, 0, c->stream>>>(flags, (uint32_t)offset, counts, c->d_valid);
+    e_launch = cudaGetLastError();
+  }
+  if (e_launch == cudaSuccess)
+    e_launch = cudaMemcpyAsync(c->h_counters, bad, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
   cudaFreeAsync(temp, c->stream);
-  if (e_launch != cudaSuccess) return cuda_fail(c, e_launch, "k_interleave");
+  if (e_launch != cudaSuccess) {
+    free_scene(c);
+    return cuda_fail(c, e_launch, "scene tables");
+  }
   c->scene.textures = reinterpret_cast<const nb::DevTexture *>(arena + off_tex);
   c->scene.materials = reinterpret_cast<const nb::DevMaterial *>(arena + off_mats);
   c->scene.meshes = reinterpret_cast<const nb::DevMesh *>(arena + off_mesh);
@@ -518,6 +626,15 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
   c->scene.n_prims = (uint32_t)offset;
   c->scene.has_emissive = emissive ? 1u : 0u;
   NB_CUDA(c, cudaStreamSynchronize(c->stream), "upload_scene");
+  if (c->h_counters[0] != 0) {
+    free_scene(c);
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "mesh index out of range%s");
+  }
+  c->n_valid = c->h_counters[1];
+  if (c->n_valid == 0) {
+    free_scene(c);
+    return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "scene has no non-degenerate triangle%s");
+  }
   c->scene_ready = true;
   return NOVA_B200_SUCCESS;
 }
@@ -527,7 +644,7 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   if (!c) return NOVA_B200_INVALID_ARGUMENT;
   if (!c->scene_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "upload a scene before building%s");
   cudaSetDevice(c->device);
-  const uint32_t n = (uint32_t)c->h_valid.size();
+  const uint32_t n = c->n_valid;
   const int width = opts && opts->width ? opts->width : 2;
   if (width != 2 && width != 8) return fail(c, NOVA_B200_INVALID_ARGUMENT, "BVH width must be 2 or 8%s");
   nb::BvhBuildParams p;
@@ -546,18 +663,16 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   c->d_tris = nullptr;
   c->bvh_ready = false;
   c->primal_valid = false;
-  uint32_t *d_valid = nullptr, *d_order = nullptr;
+  const uint32_t *d_valid = c->d_valid;
+  uint32_t *d_order = nullptr;
   float4 *d_lo = nullptr, *d_hi = nullptr;
   const size_t max_nodes = std::max<size_t>(2 * (size_t)n, 2);
   NB_CUDA(c, cudaMallocAsync(&c->d_nodes, sizeof(float4) * 4 * max_nodes, c->stream), "cudaMalloc(nodes)");
   NB_CUDA(c, cudaMallocAsync(&c->d_tris, sizeof(float4) * 3 * (size_t)n, c->stream), "cudaMalloc(tris)");
   NB_CUDA(c, cudaMemsetAsync(c->d_nodes, 0, sizeof(float4) * 4 * max_nodes, c->stream), "memset(nodes)");
-  NB_CUDA(c, cudaMallocAsync(&d_valid, sizeof(uint32_t) * n, c->stream), "cudaMalloc(valid)");
   NB_CUDA(c, cudaMallocAsync(&d_order, sizeof(uint32_t) * n, c->stream), "cudaMalloc(order)");
   NB_CUDA(c, cudaMallocAsync(&d_lo, sizeof(float4) * n, c->stream), "cudaMalloc(lo)");
   NB_CUDA(c, cudaMallocAsync(&d_hi, sizeof(float4) * n, c->stream), "cudaMalloc(hi)");
-  NB_CUDA(c, cudaMemcpyAsync(d_valid, c->h_valid.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream),
-          "upload(valid)");
   k_prim_boxes<<<(n + 255) / 256, 256, 0, c->stream>>>(c->scene, d_valid, n, d_lo, d_hi);
   NB_CUDA(c, cudaGetLastError(), "k_prim_boxes");
   nb::BvhBuildResult r{};
@@ -567,7 +682,6 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   NB_CUDA(c, cudaMemsetAsync(c->d_counters, 0, 4, c->stream), "memset");
   k_validate<<<(r.n_nodes + 255) / 256, 256, 0, c->stream>>>(c->d_nodes, r.n_nodes, n, c->d_counters);
   NB_CUDA(c, cudaMemcpyAsync(c->h_counters, c->d_counters, 4, cudaMemcpyDeviceToHost, c->stream), "readback");
-  cudaFreeAsync(d_valid, c->stream);
   cudaFreeAsync(d_order, c->stream);
   cudaFreeAsync(d_lo, c->stream);
   cudaFreeAsync(d_hi, c->stream);
@@ -695,7 +809,7 @@ nova_b200_status nova_b200_scene_info(nova_b200_ctx *c, uint64_t *tris, uint64_t
   if (leaves) *leaves = c->n_leaves;
   if (bytes)
     *bytes = c->scene_bytes + (uint64_t)c->n_nodes * (c->bvh_width == 8 ? 80 : 64) +
-             (uint64_t)c->h_valid.size() * 48 + c->queue_bytes + c->radiance_cap * 16;
+             (uint64_t)c->n_valid * 48 + c->queue_bytes + c->radiance_cap * 16;
   return NOVA_B200_SUCCESS;
 }
 

@@ -23,7 +23,8 @@ struct nova_b200_ctx {
   size_t h_stage_bytes = 0;
   nb::DevScene scene{};
   std::vector<nb::DevInstance> h_instances;
-  std::vector<uint32_t> h_valid; /* global primitive ids that can be hit */
+  uint32_t *d_valid = nullptr;   /* global primitive ids that can be hit, ascending (device) */
+  uint32_t n_valid = 0;
   uint64_t n_prims = 0;
   uint32_t n_materials = 0;
   bool scene_ready = false;

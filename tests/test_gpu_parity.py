@@ -212,6 +212,49 @@ def test_error_paths(ctx):
     assert e.value.status == 4  # INVALID_SCENE_TYPE
 
 
+def test_upload_checks_indices_and_degenerate_triangles(ctx, oracle, torch_cuda):
+    """The per-triangle scene tables are built on the device: an index past its mesh's vertices is
+    rejected (INVALID_ARGUMENT), a scene of only degenerate triangles too (INVALID_SCENE_TYPE, as
+    Triangle.h:127-132 makes them unhittable), and the context stays usable; triangles with a
+    repeated index are left out of the BVH, so hits agree with the oracle."""
+    import copy
+    from axomae_b200 import native, scenes
+    s = scenes.spheres_scene(48, 48, n_spheres=6, seed=4)
+    bad = copy.deepcopy(s)
+    idx = np.array(bad["meshes"][1]["indices"], np.uint32).reshape(-1)
+    idx[7] = len(np.asarray(bad["meshes"][1]["vertices"]).reshape(-1, 3))
+    bad["meshes"][1]["indices"] = idx.reshape(np.shape(s["meshes"][1]["indices"]))
+    with pytest.raises(native.NovaError) as e:
+        ctx.upload(bad)
+    assert e.value.status == 15
+    flat = copy.deepcopy(s)
+    for m in flat["meshes"]:
+        ix = np.array(m["indices"], np.uint32).reshape(-1, 3)
+        ix[:, 1] = ix[:, 0]
+        m["indices"] = ix.reshape(np.shape(m["indices"]))
+    with pytest.raises(native.NovaError) as e:
+        ctx.upload(flat)
+    assert e.value.status == 4
+    half = copy.deepcopy(s)
+    rng = np.random.default_rng(3)
+    for m in half["meshes"]:
+        ix = np.array(m["indices"], np.uint32).reshape(-1, 3)
+        sel = rng.random(len(ix)) < 0.3
+        ix[sel, 2] = ix[sel, 1]
+        m["indices"] = ix.reshape(np.shape(m["indices"]))
+    ctx.upload(half)
+    ctx.build()
+    osc = oracle.OracleScene(half)
+    assert ctx.info()["triangles"] == sum(np.size(half["meshes"][x["mesh"]]["indices"]) // 3 for x in half["instances"])
+    o = rng.uniform([-10, 0.05, -10], [10, 3, 10], (20000, 3)).astype(np.float32)
+    d = rng.normal(size=(20000, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    _check_hits(ctx, torch_cuda, osc, o, d, 1e-4)
+    film, _ = _render(ctx, half, 48, 48, 8, 4)
+    ref, _ = osc.render(oracle.options(48, 48, 8, 4))
+    assert rel_rmse(film, ref) <= REL_RMSE_TOL
+
+
 def test_batch_equals_individual_renders(torch_cuda):
     """nova_b200_render_batch: frames of different scenes, sizes, sample counts and depths rendered
     as one wavefront equal the same frames rendered one by one, bit for bit."""
