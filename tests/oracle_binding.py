@@ -184,6 +184,8 @@ class OracleScene:
                       (C.c_float * 16)(*np.asarray(scene["inv_P"], np.float32).reshape(16)),
                       (C.c_float * 16)(*np.asarray(scene["inv_V"], np.float32).reshape(16)))
         self._keep += [meshes, insts, mats, texs, sc]
+        self.n_tris = sum(meshes[x["mesh"]].n_tris for x in scene["instances"])
+        self.n_materials = len(scene["materials"])
         self.h = lib().orc_build(C.byref(sc))
         if not self.h:
             raise ValueError("oracle rejected the scene")
@@ -275,8 +277,18 @@ class OracleScene:
         if lib().orc_set_perturbation(self.h, kind, index, channel, delta) != 0:
             raise ValueError("bad perturbation")
 
+    def _check_sizes(self, opt, d_image, n_tris, n_materials):
+        """The C side writes 3 * (scene triangles) and (scene materials) gradients and reads W * H * 4
+        image adjoints: refuse buffers of other sizes."""
+        if n_tris != self.n_tris or n_materials != self.n_materials:
+            raise ValueError("gradient sizes %d / %d do not match the scene's %d triangles / %d materials"
+                             % (n_tris, n_materials, self.n_tris, self.n_materials))
+        if np.size(d_image) != opt.width * opt.height * 4:
+            raise ValueError("d_image must hold width * height * 4 floats")
+
     def backward(self, opt, d_image, n_tris, n_materials, threads=0):
         """Replay adjoint on the CPU: (grad_albedo (n_tris, 3), grad_roughness (n_materials,))."""
+        self._check_sizes(opt, d_image, n_tris, n_materials)
         d_image = np.ascontiguousarray(d_image, np.float32)
         ga = np.zeros(3 * n_tris, np.float32)
         gr = np.zeros(n_materials, np.float32)
@@ -287,6 +299,7 @@ class OracleScene:
 
     def backward_range(self, opt, sample_begin, sample_count, d_image, n_tris, n_materials, threads=0):
         """Replay adjoint of the mean over samples [sample_begin, sample_begin + sample_count)."""
+        self._check_sizes(opt, d_image, n_tris, n_materials)
         d_image = np.ascontiguousarray(d_image, np.float32)
         ga = np.zeros(3 * n_tris, np.float32)
         gr = np.zeros(n_materials, np.float32)

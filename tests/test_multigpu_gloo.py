@@ -75,7 +75,7 @@ def _grad_worker(rank, world, port, per, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         s = scenes.spheres_scene(W, H, n_spheres=6, seed=2)
-        n_tris = sum(len(m["indices"]) // 3 for m in s["meshes"])
+        n_tris = sum(np.size(s["meshes"][x["mesh"]]["indices"]) // 3 for x in s["instances"])
         n_mat = len(s["materials"])
         osc = ob.OracleScene(s)
         spp_total, begin, count = multigpu.strong_range(per, rank, world)
