@@ -87,8 +87,9 @@ bool is_identity(const float *m) {
 
 /* Scene uploads go to one device arena per scene (one pool allocation instead of one cudaMalloc per
  * texture / mesh / table; cudaMalloc and cudaFree synchronise the device).  Pieces up to kSmallPiece
- * bytes are gathered in a pinned host buffer and copied with one transfer; larger ones are copied
- * directly from the caller's memory. */
+ * bytes are read by a gather kernel when the caller's memory is pinned, else gathered in a pinned
+ * host buffer and copied with one transfer; larger ones are copied directly from the caller's
+ * memory. */
 constexpr size_t kSmallPiece = 1 << 16;
 
 struct Piece {
@@ -122,14 +123,66 @@ nova_b200_status ensure_pinned_stage(nova_b200_ctx *c, size_t bytes) {
   return NOVA_B200_SUCCESS;
 }
 
-/* Copies the plan's pieces: small ones through the pinned buffer (one transfer per region), large
- * ones directly. */
+/* One small piece read by the device straight from the caller's pinned host memory. */
+struct GatherPiece {
+  const char *src; /* device-accessible address of pinned host memory */
+  char *dst;
+  uint32_t bytes;
+};
+
+/* One block per piece: 16-byte words when both ends are 16-byte aligned, else bytes. */
+__global__ void k_gather_pieces(const GatherPiece *pieces) {
+  const GatherPiece g = pieces[blockIdx.x];
+  if (!((reinterpret_cast<uintptr_t>(g.src) | reinterpret_cast<uintptr_t>(g.dst)) & 15)) {
+    const uint32_t n16 = g.bytes >> 4;
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(g.src);
+    uint4 *d4 = reinterpret_cast<uint4 *>(g.dst);
+    for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) d4[i] = s4[i];
+    for (uint32_t i = (n16 << 4) + threadIdx.x; i < g.bytes; i += blockDim.x) g.dst[i] = g.src[i];
+  } else {
+    for (uint32_t i = threadIdx.x; i < g.bytes; i += blockDim.x) g.dst[i] = g.src[i];
+  }
+}
+
+/* Device-accessible address of pinned (page-locked, mapped) host memory, or null for anything else. */
+const char *pinned_device_address(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? static_cast<const char *>(a.devicePointer) : nullptr;
+}
+
+/* Copies the plan's pieces: large ones with one transfer each; small ones from pinned caller memory
+ * by one gather kernel that reads them over the bus (no host copy, one launch), the rest through
+ * the context's pinned staging buffer (one transfer per run of adjacent pieces). */
 nova_b200_status copy_pieces(nova_b200_ctx *c, const UploadPlan &plan, char *arena, char *temp) {
+  std::vector<GatherPiece> gather;
+  std::vector<char> pinned(plan.pieces.size(), 0);
   size_t small = 0;
-  for (const Piece &p : plan.pieces)
-    if (p.bytes <= kSmallPiece) small += UploadPlan::align(p.bytes);
-  nova_b200_status st = ensure_pinned_stage(c, small);
+  for (size_t k = 0; k < plan.pieces.size(); k++) {
+    const Piece &p = plan.pieces[k];
+    if (p.bytes > kSmallPiece || p.bytes == 0) continue;
+    if (const char *src = pinned_device_address(p.src)) {
+      pinned[k] = 1;
+      gather.push_back(GatherPiece{src, (p.temp ? temp : arena) + p.off, (uint32_t)p.bytes});
+    } else {
+      small += UploadPlan::align(p.bytes);
+    }
+  }
+  const size_t table = gather.size() * sizeof(GatherPiece);
+  nova_b200_status st = ensure_pinned_stage(c, small + table + 256);
   if (st != NOVA_B200_SUCCESS) return st;
+  if (!gather.empty()) {
+    /* the table goes at the end of the staging buffer, read by the kernel over the bus as well */
+    char *tab = static_cast<char *>(c->h_stage) + UploadPlan::align(small);
+    std::memcpy(tab, gather.data(), table);
+    const char *tab_dev = pinned_device_address(tab);
+    if (!tab_dev) return nbctx::fail(c, NOVA_B200_RENDERER_EXCEPTION, "staging buffer is not device-accessible%s");
+    k_gather_pieces<<<(unsigned)gather.size(), 256, 0, c->stream>>>(reinterpret_cast<const GatherPiece *>(tab_dev));
+    NB_CUDA(c, cudaGetLastError(), "k_gather_pieces");
+  }
   /* small pieces are packed per region in plan order; each region's packed pieces are contiguous
    * neither on the host nor on the device in general, so runs of adjacent pieces are merged */
   char *h = static_cast<char *>(c->h_stage);
@@ -139,12 +192,14 @@ nova_b200_status copy_pieces(nova_b200_ctx *c, const UploadPlan &plan, char *are
     size_t hbegin, bytes;
   };
   std::vector<Run> runs;
-  for (const Piece &p : plan.pieces) {
+  for (size_t k = 0; k < plan.pieces.size(); k++) {
+    const Piece &p = plan.pieces[k];
     char *dst = (p.temp ? temp : arena) + p.off;
     if (p.bytes > kSmallPiece) {
       NB_CUDA(c, cudaMemcpyAsync(dst, p.src, p.bytes, cudaMemcpyHostToDevice, c->stream), "upload(scene)");
       continue;
     }
+    if (pinned[k] || p.bytes == 0) continue;
     std::memcpy(h + hoff, p.src, p.bytes);
     const size_t step = UploadPlan::align(p.bytes);
     if (!runs.empty() && runs.back().dst + runs.back().bytes == dst && runs.back().hbegin + runs.back().bytes == hoff)
