@@ -809,6 +809,35 @@ nova_b200_status nova_b200_trace(nova_b200_ctx *c, uint64_t n, const float *o, c
   return nb_trace(c, n, o, d, prim, t, u, v);
 }
 
+nova_b200_status nova_b200_trace_host(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim,
+                                      float *t, float *u, float *v) {
+  using namespace nbctx;
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  if (n == 0) return NOVA_B200_SUCCESS;
+  if (!o || !d || !prim || !t || !u || !v) return fail(c, NOVA_B200_INVALID_ARGUMENT, "null buffer%s");
+  cudaSetDevice(c->device);
+  char *buf = nullptr; /* origins, directions, prim, t, u, v */
+  const size_t b3 = n * 3 * sizeof(float), b1 = n * sizeof(float);
+  NB_CUDA(c, cudaMallocAsync(reinterpret_cast<void **>(&buf), 2 * b3 + 4 * b1, c->stream), "cudaMalloc(rays)");
+  float *d_o = reinterpret_cast<float *>(buf), *d_d = reinterpret_cast<float *>(buf + b3);
+  int32_t *d_p = reinterpret_cast<int32_t *>(buf + 2 * b3);
+  float *d_t = reinterpret_cast<float *>(buf + 2 * b3 + b1), *d_u = d_t + n, *d_v = d_u + n;
+  cudaError_t e = cudaMemcpyAsync(d_o, o, b3, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_d, d, b3, cudaMemcpyHostToDevice, c->stream);
+  nova_b200_status st = e == cudaSuccess ? nb_trace(c, n, d_o, d_d, d_p, d_t, d_u, d_v) : NOVA_B200_SUCCESS;
+  if (e == cudaSuccess && st == NOVA_B200_SUCCESS) {
+    e = cudaMemcpyAsync(prim, d_p, b1, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t, d_t, b1, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(u, d_u, b1, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v, d_v, b1, cudaMemcpyDeviceToHost, c->stream);
+  }
+  cudaFreeAsync(buf, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "trace_host");
+  if (st != NOVA_B200_SUCCESS) return st;
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "trace_host");
+  return NOVA_B200_SUCCESS;
+}
+
 nova_b200_status nova_b200_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *idx, const uint32_t *dim, uint32_t seed,
                                  float *out) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;

@@ -101,7 +101,8 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_set_diff_params", "nova_b200_backward", "nova_b200_upload_scene_batch",
            "nova_b200_build_bvh_batch", "nova_b200_render_aov", "nova_b200_film_accumulate",
            "nova_b200_display_blend", "nova_b200_snapshot", "nova_b200_hdr_info", "nova_b200_hdr_read",
-           "nova_b200_hdr_write", "nova_b200_last_call_ms", "nova_b200_bake_texture"]
+           "nova_b200_hdr_write", "nova_b200_last_call_ms", "nova_b200_bake_texture",
+           "nova_b200_trace_host"]
 
 
 def lib():

@@ -210,6 +210,9 @@ nova_b200_status nova_b200_render_noalloc(nova_b200_ctx *ctx, const nova_b200_fr
  * prim = global primitive index (-1 on miss), t / u / v = Moller-Trumbore distance and barycentrics. */
 nova_b200_status nova_b200_trace(nova_b200_ctx *ctx, uint64_t n, const float *orig_dev, const float *dir_dev,
                                  int32_t *prim_dev, float *t_dev, float *u_dev, float *v_dev);
+/* The same for rays in host memory: copies them to the device, traces, copies the hits back. */
+nova_b200_status nova_b200_trace_host(nova_b200_ctx *ctx, uint64_t n, const float *orig_host, const float *dir_host,
+                                      int32_t *prim_host, float *t_host, float *u_host, float *v_host);
 
 /* One shading event for each of n given hits, all buffers in DEVICE memory: the hit record
  * (Embree fillHitStructure semantics, aggregate/api/embree/embree.cpp:360-412), the principled
