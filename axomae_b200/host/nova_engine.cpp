@@ -885,11 +885,21 @@ class B200Engine final : public Engine {
 
 /* ---- the device accelerator plug-in ------------------------------------------------------- */
 
+/* The accelerator's device context, shared with the intersectors it hands out so that an
+ * intersector stays valid after its accelerator is cleaned up or destroyed. */
+using SharedCtx = std::shared_ptr<nova_b200_ctx>;
+
+SharedCtx make_shared_ctx(int device) {
+  nova_b200_ctx *c = nullptr;
+  if (nova_b200_create(&c, device) != NOVA_B200_SUCCESS) return nullptr;
+  return SharedCtx(c, [](nova_b200_ctx *p) { nova_b200_destroy(p); });
+}
+
 class B200IntersectorImpl final : public aggregate::DeviceIntersectorInterface {
-  nova_b200_ctx *ctx_;
+  SharedCtx ctx_;
 
  public:
-  explicit B200IntersectorImpl(nova_b200_ctx *c) : ctx_(c) {}
+  explicit B200IntersectorImpl(SharedCtx c) : ctx_(std::move(c)) {}
   /* one renderGpu frame (api/engine.cpp:469-481): sample params.sample_index of params.sample_max
    * into render_buffers.partial_buffer */
   void traverse(const device_traversal_param_s &p) const override {
@@ -903,32 +913,32 @@ class B200IntersectorImpl final : public aggregate::DeviceIntersectorInterface {
     f.reset = 1;
     std::memcpy(f.inv_P, p.camera.inv_P, 64);
     std::memcpy(f.inv_V, p.camera.inv_V, 64);
-    nova_b200_render(ctx_, &f, p.render_buffers.partial_buffer, nullptr, nullptr);
+    if (ctx_) nova_b200_render(ctx_.get(), &f, p.render_buffers.partial_buffer, nullptr, nullptr);
   }
 };
 
 class B200AcceleratorImpl final : public aggregate::B200Accelerator {
-  nova_b200_ctx *ctx_ = nullptr;
+  int device_;
+  SharedCtx ctx_;
   ERROR_STATE status_ = RENDER_ENGINE_NOT_INITIALIZED;
   std::string err_;
 
  public:
-  explicit B200AcceleratorImpl(int device) {
-    if (nova_b200_create(&ctx_, device) == NOVA_B200_SUCCESS)
+  explicit B200AcceleratorImpl(int device) : device_(device), ctx_(make_shared_ctx(device)) {
+    if (ctx_)
       status_ = SCENE_NOT_PROCESSED;
     else
-      ctx_ = nullptr, err_ = "no CUDA device " + std::to_string(device);
-  }
-  ~B200AcceleratorImpl() override {
-    if (ctx_) nova_b200_destroy(ctx_);
+      err_ = "no CUDA device " + std::to_string(device);
   }
   void build(aggregate::primitive_aggregate_data_s d) override {
+    if (!ctx_) ctx_ = make_shared_ctx(device_); /* after cleanup() */
     if (!ctx_) return;
-    status_ = upload_views(ctx_, d, &err_);
+    status_ = upload_views(ctx_.get(), d, &err_);
   }
+  /* releases this accelerator's hold on the device scene; intersectors already handed out keep
+   * theirs until they are destroyed */
   void cleanup() override {
-    if (ctx_) nova_b200_destroy(ctx_);
-    ctx_ = nullptr;
+    ctx_.reset();
     status_ = RENDER_ENGINE_NOT_INITIALIZED;
   }
   /* the device traversal stack holds 64 entries; a path scatters up to 255 times */
@@ -946,7 +956,7 @@ class B200AcceleratorImpl final : public aggregate::B200Accelerator {
   ERROR_STATE closestHits(uint64_t n, const float *o, const float *d, int32_t *prim, float *t, float *u,
                           float *v) const override {
     if (status_ != SUCCESS) return status_;
-    return (ERROR_STATE)nova_b200_trace_host(ctx_, n, o, d, prim, t, u, v);
+    return (ERROR_STATE)nova_b200_trace_host(ctx_.get(), n, o, d, prim, t, u, v);
   }
 };
 

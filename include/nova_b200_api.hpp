@@ -480,6 +480,8 @@ class DeviceAcceleratorInterface {
   virtual void cleanup() = 0;
   virtual unsigned getMaxRecursiveDepth() const = 0;
   virtual void copyParamsToDevice(const device_traversal_param_s &params) const = 0;
+  /* The B200 intersector shares the accelerator's device scene and stays valid after the
+   * accelerator's cleanup() or destruction. */
   virtual std::unique_ptr<DeviceIntersectorInterface> getIntersectorObject() const = 0;
   /* The B200 accelerator on device 0 (api/device_accelerator_factory.cpp:9-18). */
   static std::unique_ptr<DeviceAcceleratorInterface> make();

@@ -392,11 +392,19 @@ void test_accel() {
     cam->getInverseViewMatrix(prm.camera.inv_V);
     prm.width = 8, prm.height = 6, prm.depth = 2, prm.sample_index = 0, prm.sample_max = 1;
     c.acc->copyParamsToDevice(prm);
-    c.acc->getIntersectorObject()->traverse(prm);
+    auto intersector = c.acc->getIntersectorObject();
+    intersector->traverse(prm);
     bool all_finite = true, any_written = false;
     for (float x : film) all_finite &= std::isfinite(x), any_written |= x != -1.f;
     CHECK(all_finite && any_written);
     CHECK(c.acc->getMaxRecursiveDepth() >= 16);
+    /* an intersector outlives its accelerator's cleanup: it renders the same frame again */
+    std::vector<float> first = film;
+    c.acc->cleanup();
+    CHECK(c.b200().lastStatus() == nova::RENDER_ENGINE_NOT_INITIALIZED);
+    std::fill(film.begin(), film.end(), -1.f);
+    intersector->traverse(prm);
+    CHECK(std::memcmp(film.data(), first.data(), film.size() * 4) == 0);
   }
   {
     /* nointersect_outside_back_translated: the cube 3 units to the right of the view */
