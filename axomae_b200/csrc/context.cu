@@ -809,6 +809,12 @@ nova_b200_status nova_b200_trace(nova_b200_ctx *c, uint64_t n, const float *o, c
   return nb_trace(c, n, o, d, prim, t, u, v);
 }
 
+nova_b200_status nova_b200_cancel(nova_b200_ctx *c) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  c->cancel.store(true);
+  return NOVA_B200_SUCCESS;
+}
+
 nova_b200_status nova_b200_trace_host(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim,
                                       float *t, float *u, float *v) {
   using namespace nbctx;

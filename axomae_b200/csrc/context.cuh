@@ -1,5 +1,6 @@
 /* The C-ABI context: owns the device, stream, scene buffers, BVH and render buffers. */
 #pragma once
+#include <atomic>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -12,6 +13,7 @@ struct nova_b200_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_a = nullptr, ev_b = nullptr;
   std::string error;
+  std::atomic<bool> cancel{false}; /* set by nova_b200_cancel from any thread, read by the wave loop */
 
   /* tables (allocated once) */
   uint32_t *d_sobol = nullptr;

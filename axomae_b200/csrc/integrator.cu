@@ -889,6 +889,10 @@ nova_b200_status run_waves(nova_b200_ctx *x, uint32_t total, uint32_t cap, Launc
       ls.traced += r.traced;
       break;
     }
+    if (x->cancel.load()) { /* nova_b200_cancel: let the group in flight finish, enqueue nothing more */
+      NB_CUDA(x, cudaEventSynchronize(x->ev_done[slot ^ 1]), "waves");
+      return nbctx::fail(x, NOVA_B200_RENDERER_EXCEPTION, "render cancelled%s");
+    }
     NB_CUDA(x, launch(slot), "wave group");
     slot ^= 1;
   }
@@ -922,6 +926,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
                              const std::vector<const nova_b200_frame *> &frames, float *const *films_host,
                              float *const *films_device, nova_b200_render_stats *stats) {
   using namespace nbctx;
+  x->cancel.store(false); /* a cancel applies to the call in progress */
   const size_t nj = ctxs.size();
   const int width = ctxs[0]->bvh_width;
   uint64_t max_np = 0, total = 0;
@@ -983,6 +988,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   std::vector<Job> hj(kParamJobs);
   ManyJobs many{};
   for (const auto &chunk : chunks) {
+    if (x->cancel.load()) return fail(x, NOVA_B200_RENDERER_EXCEPTION, "render cancelled%s");
     if (chunk.empty()) continue;
     uint32_t pb = 0;
     for (size_t k = 0; k < chunk.size(); k++) {
@@ -1140,6 +1146,8 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
   const bool reuse = (flags & NOVA_B200_BACKWARD_REUSE_PRIMAL) && c->primal_valid &&
                      per_chunk >= (uint32_t)f->sample_count && same_paths(c->primal_frame, *f) &&
                      c->primal_albedo == c->scene.diff_albedo && c->primal_rough == c->scene.diff_rough;
+  if (!reuse) c->primal_valid = false; /* the radiance pass below overwrites the buffer (and may stop midway) */
+  c->cancel.store(false);              /* a cancel applies to the call in progress */
   for (uint32_t s0 = 0; s0 < (uint32_t)f->sample_count; s0 += per_chunk) {
     const uint32_t take = std::min<uint32_t>(per_chunk, (uint32_t)f->sample_count - s0);
     OneJob one{};

@@ -836,6 +836,7 @@ class B200Engine final : public Engine {
   /* api/engine.cpp:577-586: stops, waits for the frame in flight, frame index back to 1 */
   ERROR_STATE stopRender() override {
     rendering_.store(false);
+    if (ctx_) nova_b200_cancel(ctx_); /* a frame in flight stops within a group of waves */
     join();
     frame_index_.store(1);
     return SUCCESS;

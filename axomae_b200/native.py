@@ -102,7 +102,7 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_build_bvh_batch", "nova_b200_render_aov", "nova_b200_film_accumulate",
            "nova_b200_display_blend", "nova_b200_snapshot", "nova_b200_hdr_info", "nova_b200_hdr_read",
            "nova_b200_hdr_write", "nova_b200_last_call_ms", "nova_b200_bake_texture",
-           "nova_b200_trace_host"]
+           "nova_b200_trace_host", "nova_b200_cancel"]
 
 
 def lib():
@@ -144,6 +144,7 @@ def lib():
         L.nova_b200_hdr_read.argtypes = [vp, C.c_char_p, vp, vp, C.c_uint64]
         L.nova_b200_hdr_write.argtypes = [vp, C.c_char_p, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
         L.nova_b200_last_call_ms.argtypes = [vp, C.POINTER(C.c_float)]
+        L.nova_b200_cancel.argtypes = [vp]
         L.nova_b200_bake_texture.argtypes = [vp, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p,
                                              C.c_char_p]
         L.nova_b200_render_batch.argtypes = [C.POINTER(vp), C.POINTER(Frame), C.c_uint32, C.POINTER(vp),
@@ -466,6 +467,10 @@ class Context:
         """The bake command: path_in (.hdr) -> irradiance map path_out + ".hdr"."""
         self._check(lib().nova_b200_bake_texture(self.h, kind.encode(), width, height, samples,
                                                  os.fsencode(path_in), os.fsencode(path_out)))
+
+    def cancel(self):
+        """Stops the render / backward call running on this context in another thread."""
+        self._check(lib().nova_b200_cancel(self.h))
 
     def last_call_ms(self) -> float:
         """Device time of the kernel of the last film / .hdr call."""

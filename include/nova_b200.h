@@ -344,6 +344,15 @@ nova_b200_status nova_b200_bake_texture(nova_b200_ctx *ctx, const char *type, in
  * hdr_read / hdr_write call (CUDA events).  No counterpart in the reference. */
 nova_b200_status nova_b200_last_call_ms(nova_b200_ctx *ctx, float *device_ms);
 
+/* Stops the render, render_batch or backward call running on this context (for a batch: on its
+ * first context) from another thread: NvEngineInstance::stopRender's is_rendering flag
+ * (api/engine.cpp:577-586).  The wave loop checks it after every group of four waves and between
+ * chunks; the call then waits for the group still in flight and returns RENDERER_EXCEPTION
+ * ("render cancelled") without writing the film.  The accumulation film keeps the chunks finished
+ * before the stop, so the next frame should set reset.  A cancel applies to the call in progress:
+ * each render / backward call clears it when it starts.  No counterpart call in the reference. */
+nova_b200_status nova_b200_cancel(nova_b200_ctx *ctx);
+
 /* Last error message: Engine::getRenderEngineError (api_engine.h:185).  buf holds 1024 chars. */
 void nova_b200_get_error(nova_b200_ctx *ctx, char buf[1024], size_t *size);
 

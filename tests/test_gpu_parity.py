@@ -255,6 +255,56 @@ def test_upload_checks_indices_and_degenerate_triangles(ctx, oracle, torch_cuda)
     assert rel_rmse(film, ref) <= REL_RMSE_TOL
 
 
+def test_cancel_stops_a_long_render(torch_cuda):
+    """nova_b200_cancel from another thread stops a long render within a few wave groups with
+    RENDERER_EXCEPTION, and the context renders correctly afterwards."""
+    import threading
+    import time
+    from axomae_b200 import native, scenes
+    torch = torch_cuda
+    s = scenes.spheres_scene(64, 64, n_spheres=8, seed=1)
+    c = native.Context(0)
+    try:
+        c.upload(s)
+        c.build()
+        film = torch.zeros(1024 * 1024 * 4, device="cuda")
+        long_frame = native.make_frame(s, 1024, 1024, 2048, 8)  # 2^31 paths: seconds of work
+        result = {}
+
+        def run():
+            try:
+                c.render(long_frame, film_device_ptr=film.data_ptr())
+                result["done"] = True
+            except native.NovaError as e:
+                result["error"] = e
+
+        t = threading.Thread(target=run)
+        t.start()
+        time.sleep(0.3)
+        t0 = time.perf_counter()
+        c.cancel()
+        t.join(timeout=60)
+        stopped = time.perf_counter() - t0
+        assert not t.is_alive()
+        assert "error" in result, "the render finished before the cancel"
+        assert result["error"].status == 16 and "cancel" in str(result["error"])
+        assert stopped < 2.0
+        small = native.make_frame(s, 64, 64, 4, 4)
+        a = np.zeros((64, 64, 4), np.float32)
+        c.render(small, film_host=a)
+        fresh = native.Context(0)
+        try:
+            fresh.upload(s)
+            fresh.build()
+            b = np.zeros((64, 64, 4), np.float32)
+            fresh.render(small, film_host=b)
+        finally:
+            fresh.close()
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    finally:
+        c.close()
+
+
 def test_upload_from_pinned_memory_equals_pageable(ctx, torch_cuda):
     """Scene arrays in pinned host memory are read by the device's gather kernel, pageable ones go
     through the staging buffer: both uploads give the same BVH and the same image bit for bit."""
