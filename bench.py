@@ -400,6 +400,46 @@ def film_io_timing(local_rank, cpu_baseline=True, reps=10):
     return out
 
 
+BAKE_SAMPLES = 128
+
+
+def bake_timing(local_rank, cpu_baseline=True, reps=5):
+    """The irradiance bake on the heightfield workload's 2048 x 1024 log-normal(0, 1.5) environment
+    map: 64 x 64 (the editor's size) and 512 x 256 outputs, BAKE_SAMPLES samples per texel.  Device
+    side: nova_b200_bake_irradiance on device buffers, wall clock around the call (it synchronises),
+    median of `reps`; CPU side: the oracle's restatement of the reference's CPU bake with its 8
+    worker threads (TextureProcessing.cpp:10-64).  Unit: output texels x samples per second."""
+    import torch
+    from axomae_b200 import native, scenes
+    s = scenes.heightfield_scene(n=8, width=16, height=16, env_w=HF["env_w"], env_h=HF["env_h"], seed=HF["seed"])
+    env = next(t for t in s["textures"] if t["format"] == "f32")
+    src = np.asarray(env["pixels"], np.float32).reshape(env["height"], env["width"], 4)
+    c = native.Context(local_rank)
+    out = {"env": "%dx%d float RGBA" % (env["width"], env["height"]), "samples": BAKE_SAMPLES}
+    try:
+        ts = torch.from_numpy(np.ascontiguousarray(src)).cuda()
+        for ow, oh in ((64, 64), (512, 256)):
+            dst = torch.zeros((oh, ow, 4), device="cuda")
+            walls = []
+            for _ in range(reps + 1):
+                t0 = time.perf_counter()
+                c.bake_irradiance(ts.data_ptr(), env["width"], env["height"], 4, ow, oh, BAKE_SAMPLES, dst.data_ptr())
+                walls.append(time.perf_counter() - t0)
+            w = float(np.median(walls[1:]))
+            rec = {"seconds": w, "gtexel_samples_per_s": ow * oh * BAKE_SAMPLES / w / 1e9}
+            if cpu_baseline:
+                ob = oracle_module()
+                t0 = time.perf_counter()
+                ob.bake_irradiance(src, ow, oh, BAKE_SAMPLES, threads=8)
+                cw = time.perf_counter() - t0
+                rec["cpu"] = {"seconds": cw, "gtexel_samples_per_s": ow * oh * BAKE_SAMPLES / cw / 1e9, "cores": 8,
+                              "kind": "port"}
+            out["%dx%d" % (ow, oh)] = rec
+    finally:
+        c.close()
+    return out
+
+
 def adjoint_timing(local_rank, reps=3):
     """The differentiable configuration: the 64-sphere scene at 256 x 256, 64 spp, depth 4, with
     per-triangle albedo (init 0.5) and per-material roughness (init 0.3) as parameters and an L2
@@ -638,6 +678,11 @@ def run_ours(args, rank, world, local_rank):
         extra["adjoint"] = adjoint_timing(local_rank)
     if batched and not args.no_film_io:
         extra["film_io"] = film_io_timing(local_rank, cpu_baseline=not args.no_cpu and local_rank == 0)
+    if batched and not args.no_bake:
+        try:  # the bake is a side measurement: a failure here is reported, never loses the bench line
+            extra["bake"] = bake_timing(local_rank, cpu_baseline=not args.no_cpu and local_rank == 0)
+        except Exception as e:  # noqa: BLE001
+            extra["bake"] = {"error": repr(e)}
     metric = {"heightfield": HF_METRIC, "instanced": IN_METRIC}.get(args.workload, BATCH_METRIC)
     workload = {"heightfield": HF_WORKLOAD, "instanced": IN_WORKLOAD}.get(args.workload, BATCH_WORKLOAD)
     if args.frame or args.spp:
@@ -674,6 +719,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="batched arm: keep the default launch tuning")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
     ap.add_argument("--no-film-io", action="store_true", help="skip the film output / .hdr timing")
+    ap.add_argument("--no-bake", action="store_true", help="skip the irradiance bake timing")
     ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="heightfield: override the frame size")
     ap.add_argument("--spp", type=int, help="heightfield: override samples per pixel")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8], help="BVH layout (0 = library default)")
