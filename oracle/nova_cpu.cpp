@@ -1174,6 +1174,52 @@ extern "C" int32_t orc_backward_range(void *h, const orc_options *opt, int32_t s
   return 0;
 }
 
+/* The BxDF math the reference's BxDFTest.cpp exercises (:27-125): Fresnel::real, VNDF::sample
+ * (sampleGGXVNDF) and VNDF::G1 of the restatement above, and correct_specular_shading_normal. */
+extern "C" float orc_fresnel_real(float ior, float cos_i, float *new_eta) {
+  float e = 0.f;
+  const float r = fresnel_real(ior, cos_i, e);
+  if (new_eta) *new_eta = e;
+  return r;
+}
+extern "C" void orc_vndf_sample(float anisotropy, float roughness, const float wo[3], const float uc[2], float wm[3]) {
+  const VNDF g(anisotropy, roughness);
+  const V3 m = g.sample(V3{wo[0], wo[1], wo[2]}, uc);
+  wm[0] = m.x, wm[1] = m.y, wm[2] = m.z;
+}
+extern "C" float orc_vndf_g1(float anisotropy, float roughness, const float v[3]) {
+  return VNDF(anisotropy, roughness).G1(V3{v[0], v[1], v[2]});
+}
+extern "C" void orc_correct_specular_normal(const float ng[3], const float wo[3], const float ns[3], float out[3]) {
+  const V3 r = correct_specular_shading_normal(V3{ng[0], ng[1], ng[2]}, V3{wo[0], wo[1], wo[2]}, V3{ns[0], ns[1], ns[2]});
+  out[0] = r.x, out[1] = r.y, out[2] = r.z;
+}
+
+/* EnvmapTexture::sample (env_sample above) of a float texture for n directions: the function the
+ * reference's envmap tests exercise (NovaTextureInterfaceTest.cpp:56-133).  out: 4 floats each. */
+extern "C" void orc_env_sample(const float *pixels, int32_t w, int32_t h, int32_t channels, uint64_t n,
+                               const float *dirs, float *out) {
+  Scene s;
+  Texture t;
+  t.f32.assign(pixels, pixels + (size_t)w * h * channels);
+  t.w = w, t.h = h, t.channels = channels;
+  s.textures.push_back(std::move(t));
+  s.envmap = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    const V4 r = env_sample(s, V3{dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]});
+    out[4 * i] = r.x, out[4 * i + 1] = r.y, out[4 * i + 2] = r.z, out[4 * i + 3] = r.w;
+  }
+}
+
+/* cartesianToSpherical with the fast approximations (math_spherical.h:44-52): (phi, theta) per
+ * direction, the mapping the reference's TextureProcessingTest.cpp:102-110 bounds by 5e-3. */
+extern "C" void orc_cartesian_to_spherical(uint64_t n, const float *xyz, float *phi_theta) {
+  for (uint64_t i = 0; i < n; i++) {
+    phi_theta[2 * i] = atan2_approx(xyz[3 * i + 1], xyz[3 * i]);
+    phi_theta[2 * i + 1] = acos_lt(xyz[3 * i + 2]);
+  }
+}
+
 /* AOV integrators (NormalIntegrator.cpp, DepthIntegrator.cpp, EmissiveIntegrator.cpp): one
  * unjittered camera ray per pixel; out = W*H*4 floats in film layout. */
 extern "C" int32_t orc_render_aov(void *h, const orc_options *opt, int32_t kind, float near_plane, float far_plane,

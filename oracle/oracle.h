@@ -143,6 +143,16 @@ void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int3
 int32_t orc_bake_irradiance(const float *src, int32_t src_w, int32_t src_h, int32_t channels, int32_t out_w,
                             int32_t out_h, int32_t samples, int32_t threads, float *out);
 
+/* BxDF math of the restatement (property tests). */
+float orc_fresnel_real(float ior, float cos_i, float *new_eta);
+void orc_vndf_sample(float anisotropy, float roughness, const float wo[3], const float uc[2], float wm[3]);
+float orc_vndf_g1(float anisotropy, float roughness, const float v[3]);
+void orc_correct_specular_normal(const float ng[3], const float wo[3], const float ns[3], float out[3]);
+/* Environment lookup of a float texture and the fast spherical mapping (property tests). */
+void orc_env_sample(const float *pixels, int32_t w, int32_t h, int32_t channels, uint64_t n, const float *dirs,
+                    float *out);
+void orc_cartesian_to_spherical(uint64_t n, const float *xyz, float *phi_theta);
+
 /* Film outputs and the Radiance .hdr format (film_io.cpp). */
 void orc_film_accumulate(const float *partial, float *accum, float *final_buf, uint64_t n, uint32_t frame_index);
 void orc_display_blend(const float *partial, const float *accum, float *out, uint64_t n, uint32_t current_frame);

@@ -101,6 +101,14 @@ def lib():
         L.orc_bake_irradiance.argtypes = [f32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                           C.c_int32, f32p]
         L.orc_bake_irradiance.restype = C.c_int32
+        L.orc_env_sample.argtypes = [f32p, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, f32p, f32p]
+        L.orc_fresnel_real.argtypes = [C.c_float, C.c_float, f32p]
+        L.orc_fresnel_real.restype = C.c_float
+        L.orc_vndf_sample.argtypes = [C.c_float, C.c_float, f32p, f32p, f32p]
+        L.orc_vndf_g1.argtypes = [C.c_float, C.c_float, f32p]
+        L.orc_vndf_g1.restype = C.c_float
+        L.orc_correct_specular_normal.argtypes = [f32p, f32p, f32p, f32p]
+        L.orc_cartesian_to_spherical.argtypes = [C.c_uint64, f32p, f32p]
         u8p = C.POINTER(C.c_uint8)
         L.orc_film_accumulate.argtypes = [f32p, f32p, f32p, C.c_uint64, C.c_uint32]
         L.orc_display_blend.argtypes = [f32p, f32p, f32p, C.c_uint64, C.c_uint32]
@@ -324,6 +332,52 @@ def bake_irradiance(src: np.ndarray, out_w: int, out_h: int, samples: int, threa
     rc = lib().orc_bake_irradiance(_p(src, f32p), w, h, ch, out_w, out_h, samples, threads, _p(out, f32p))
     if rc != 0:
         raise ValueError("bake rejected")
+    return out
+
+
+def _v(x, n):
+    return np.ascontiguousarray(x, np.float32).reshape(n)
+
+
+def fresnel_real(ior, cos_i):
+    """Fresnel::real: (reflectance, the eta used) for the cosine of incidence."""
+    e = np.zeros(1, np.float32)
+    r = lib().orc_fresnel_real(ior, cos_i, _p(e, f32p))
+    return float(r), float(e[0])
+
+
+def vndf_sample(roughness, wo, uc, anisotropy=0.0):
+    wo, uc, wm = _v(wo, 3), _v(uc, 2), np.zeros(3, np.float32)
+    lib().orc_vndf_sample(anisotropy, roughness, _p(wo, f32p), _p(uc, f32p), _p(wm, f32p))
+    return wm
+
+
+def vndf_g1(roughness, v, anisotropy=0.0):
+    v = _v(v, 3)
+    return float(lib().orc_vndf_g1(anisotropy, roughness, _p(v, f32p)))
+
+
+def correct_specular_normal(ng, wo, ns):
+    ng, wo, ns, out = _v(ng, 3), _v(wo, 3), _v(ns, 3), np.zeros(3, np.float32)
+    lib().orc_correct_specular_normal(_p(ng, f32p), _p(wo, f32p), _p(ns, f32p), _p(out, f32p))
+    return out
+
+
+def env_sample(pixels, dirs):
+    """EnvmapTexture::sample of a float texture (H, W, C) for directions (n, 3): (n, 4)."""
+    px = np.ascontiguousarray(pixels, np.float32)
+    h, w, ch = px.shape
+    d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    out = np.zeros((d.shape[0], 4), np.float32)
+    lib().orc_env_sample(_p(px, f32p), w, h, ch, d.shape[0], _p(d, f32p), _p(out, f32p))
+    return out
+
+
+def cartesian_to_spherical(xyz):
+    """(phi, theta) of unit directions (n, 3) with the reference's fast approximations."""
+    d = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    out = np.zeros((d.shape[0], 2), np.float32)
+    lib().orc_cartesian_to_spherical(d.shape[0], _p(d, f32p), _p(out, f32p))
     return out
 
 

@@ -1,0 +1,101 @@
+"""The reference's own property tests (tests/unit_test/corelib/nova/material/BxDFTest.cpp,
+tests/unit_test/corelib/nova/texturing/NovaTextureInterfaceTest.cpp,
+tests/unit_test/sources/processing/TextureProcessingTest.cpp) restated against the CPU oracle's
+functions, with the reference's inputs and bounds.  The reference pins no numeric results for this
+path; these properties are what it does check, so the oracle is held to them too.  Where the
+reference draws from its own unseeded or library random generator, seeded numpy draws of the same
+distribution stand in.  The device computes the same functions bit for bit (test_scatter_bit_exact
+compares whole shading events, environment lookups included, with the oracle's)."""
+import math
+
+import numpy as np
+
+import oracle_binding as ob
+
+UC_SAMPLES = [(0.0, 0.0), (0.1, 0.5), (0.2, 0.25), (0.3, 0.75), (0.4, 0.125)]
+ROUGHNESS = [1e-4, 0.1, 0.45, 0.75, 1.0, 0.0]  # BxDFTest.cpp:42 (six slots, the last left at 0)
+IOR_VACUUM, IOR_GLASS, IOR_DIAMOND = 1.0, 1.5, 2.417
+
+
+def _n(v):
+    v = np.asarray(v, np.float64)
+    return (v / np.linalg.norm(v)).astype(np.float32)
+
+
+def test_specular_normal_correction(oracle):
+    """BxDF_mathTest.specular_normal_correction: the corrected normal keeps the mirror direction of
+    wo above the geometric normal."""
+    wo, ng, ns = _n([0.8, 0.6, 0.0]), np.array([0.0, 1.0, 0.0], np.float32), _n([0.9, 0.1, 0.0])
+    corrected = ob.correct_specular_normal(ng, wo, ns)
+    r = -wo - 2.0 * np.dot(corrected, -wo) * corrected  # glm::reflect(-wo, corrected)
+    assert np.dot(ng, r) > 0 and np.dot(corrected, ng) > 0
+
+
+def test_fresnel_real(oracle):
+    """FresnelTest.real: eta kept on the upper hemisphere and inverted below; transmission dominates
+    at the reference's first argument for glass, reflection near grazing and for diamond."""
+    r, eta = ob.fresnel_real(IOR_GLASS, 0.5)
+    assert eta == np.float32(IOR_GLASS) and 1 - r > r
+    r, eta = ob.fresnel_real(IOR_GLASS, 0.001)
+    assert eta == np.float32(IOR_GLASS) and r > 1 - r
+    r, eta = ob.fresnel_real(IOR_GLASS, -0.001)
+    assert eta != np.float32(IOR_GLASS)
+    r, eta = ob.fresnel_real(IOR_VACUUM, 0.5)
+    assert eta == np.float32(IOR_VACUUM) and 1 - r > r
+    r, eta = ob.fresnel_real(IOR_DIAMOND, 0.1)
+    assert r > 1 - r
+
+
+def test_ggx_sample_wm(oracle):
+    """GGXTest.SampleWm: sampled microfacet normals are unit length and in the view hemisphere."""
+    wo = np.array([1.2, 0.4, 1.0], np.float32)
+    for rough in ROUGHNESS:
+        for uc in UC_SAMPLES:
+            wm = ob.vndf_sample(rough, wo, uc)
+            assert abs(float(np.dot(wm, wm)) - 1.0) <= 1e-4
+            assert wm[2] * wo[2] > 0
+
+
+def test_ggx_g1_bounds(oracle):
+    """GGXTest.G1_bounds: G1 is ~1 looking straight down and ~0 at grazing angles."""
+    top = ob.vndf_g1(0.75, [0.0, 0.0, 1.0])
+    assert 0 < top <= 1 and abs(top - 1) <= 1e-3
+    grazing = ob.vndf_g1(0.75, [1.0, 1.0, 1e-4])
+    assert 0 <= grazing < 1 and abs(grazing) <= 1e-2
+
+
+def test_envmap_sample_rgba_order(oracle):
+    """EnvmapTextureTest.sample_RGBA_order: a constant 256 x 256 RGB map returns its red, green and
+    blue in order."""
+    tex = np.tile(np.array([0.4, 0.5, 0.6], np.float32), (256, 256, 1))
+    px = ob.env_sample(tex, [[0.0, 1.0, 0.0]])[0]
+    assert px[0] == np.float32(0.4) and px[1] == np.float32(0.5) and px[2] == np.float32(0.6)
+
+
+def test_envmap_sample_direction_encoded(oracle):
+    """EnvmapTextureTest.sample: a 256 x 256 map whose texel (i, j) holds the direction of
+    (u, v) = (i / 255, j / 255) returns, for 100 directions with components in [0, 1), a colour
+    within 0.1 of the normalised direction."""
+    W = H = 256
+    j, i = np.mgrid[0:H, 0:W]
+    phi = 2 * math.pi * (i / (W - 1))
+    theta = math.pi * (j / (H - 1))
+    cart = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)], -1)
+    cart /= np.linalg.norm(cart, axis=-1, keepdims=True)
+    tex = cart.astype(np.float32)
+    dirs = np.random.default_rng(0xDEADBEEF).uniform(0.0, 1.0, (100, 3)).astype(np.float32)
+    px = ob.env_sample(tex, dirs)[:, :3]
+    want = dirs / np.linalg.norm(dirs, axis=1, keepdims=True)
+    assert np.all(np.abs(px - want) < 1e-1)
+
+
+def test_cartesian_to_spherical_approximation(oracle):
+    """TexturingTest.uvCartesianCohesionApproximated: the fast atan2 polynomial and the acos table
+    recover (phi, theta) within 5e-3."""
+    rng = np.random.default_rng(3)
+    phi = rng.uniform(-math.pi + 1e-3, math.pi - 1e-3, 2000)
+    theta = rng.uniform(1e-2, math.pi - 1e-2, 2000)
+    cart = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)], -1)
+    got = ob.cartesian_to_spherical(cart.astype(np.float32))
+    err = np.hypot(got[:, 0] - phi, got[:, 1] - theta)
+    assert err.max() <= 5e-3
