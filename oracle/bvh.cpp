@@ -14,13 +14,6 @@
 
 namespace orc {
 
-namespace {
-
-struct Cache {
-  std::vector<Box> aabbs;
-  std::vector<V3> centroids;
-};
-
 /* Triangle::computeAABB / centroid (Triangle.h:99-114; compute_center Object3D.h:194-199). */
 void prim_bounds(const Scene &s, const Prim &p, Box &box, V3 &centroid) {
   const Mesh &m = s.meshes[s.inst_mesh[p.inst]];
@@ -36,6 +29,13 @@ void prim_bounds(const Scene &s, const Prim &p, Box &box, V3 &centroid) {
        (v[0].z + v[1].z + v[2].z) * 0.333333f};
   centroid = xyz(mul(x.m, V4{c.x, c.y, c.z, 1.f}));
 }
+
+namespace {
+
+struct Cache {
+  std::vector<Box> aabbs;
+  std::vector<V3> centroids;
+};
 
 /* update_aabb, BvhBuilder.cpp:77-99: starts from (INT_MAX, INT_MIN) and unions the prims. */
 void update_aabb(const Cache &c, Scene &s, int32_t node_id) {

@@ -1211,6 +1211,20 @@ extern "C" void orc_env_sample(const float *pixels, int32_t w, int32_t h, int32_
   }
 }
 
+/* Triangle::computeAABB / centroid of every primitive (prim_bounds in bvh.cpp): 6 floats of box
+ * (min, max) and 3 of centroid per primitive, world space. */
+extern "C" void orc_prim_bounds(void *h, float *boxes, float *centroids) {
+  const Scene &s = *static_cast<Scene *>(h);
+  for (size_t k = 0; k < s.prims.size(); k++) {
+    Box b;
+    V3 c;
+    prim_bounds(s, s.prims[k], b, c);
+    float *o = boxes + 6 * k;
+    o[0] = b.mn.x, o[1] = b.mn.y, o[2] = b.mn.z, o[3] = b.mx.x, o[4] = b.mx.y, o[5] = b.mx.z;
+    centroids[3 * k] = c.x, centroids[3 * k + 1] = c.y, centroids[3 * k + 2] = c.z;
+  }
+}
+
 /* cartesianToSpherical with the fast approximations (math_spherical.h:44-52): (phi, theta) per
  * direction, the mapping the reference's TextureProcessingTest.cpp:102-110 bounds by 5e-3. */
 extern "C" void orc_cartesian_to_spherical(uint64_t n, const float *xyz, float *phi_theta) {
@@ -1278,6 +1292,28 @@ extern "C" void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n,
   }
 }
 
+static int32_t tile_split(int W, int H, int ntw, int nth, int32_t *rects) {
+  const int tw = W / ntw, th = H / nth;
+  const int twr = tw + (W % tw), thr = th + (H % th);
+  int32_t n = 0;
+  for (int j = 0; j < nth; j++)
+    for (int i = 0; i < ntw; i++, n++) {
+      int32_t *r = rects + 4 * n;
+      r[0] = i * tw;
+      r[1] = r[0] + ((i == ntw - 1) ? twr : tw);
+      r[2] = j * th;
+      r[3] = r[2] + ((j == nth - 1) ? thr : th);
+    }
+  return n;
+}
+
+/* divideByTiles (utils/nova_utils.h:34-53): ntw x nth tiles of W / ntw x H / nth pixels, the last
+ * column and row taking the remainder; rects gets (x0, x1, y0, y1) per tile, row by row. */
+extern "C" int32_t orc_tile_split(int32_t W, int32_t H, int32_t ntw, int32_t nth, int32_t *rects) {
+  if (W <= 0 || H <= 0 || ntw <= 0 || nth <= 0 || ntw > W || nth > H) return 0;
+  return tile_split(W, H, ntw, nth, rects);
+}
+
 /* Progressive render (api/engine.cpp:498-525, utils/DrawEngine.cpp:57-89): each frame renders 1 spp
  * of every tile on a worker pool, the orchestrating thread waits on the frame fence, then folds the
  * partial buffer into the running mean (writeFramebuffer, engine.cpp:351-363). */
@@ -1296,19 +1332,15 @@ extern "C" int32_t orc_render(void *h, const orc_options *opt, float *out_rgba, 
   };
   std::vector<Task> tasks;
   if (!pixel_ids) {
-    int ntw = std::max(1, W / tile), nth = std::max(1, H / tile);
-    int tw = W / ntw, th = H / nth;
-    int twr = tw + (W % tw), thr = th + (H % th); /* divideByTiles, nova_utils.h:34-53 */
-    for (int j = 0; j < nth; j++)
-      for (int i = 0; i < ntw; i++) {
-        Task t{};
-        t.x0 = i * tw;
-        t.x1 = t.x0 + ((i == ntw - 1) ? twr : tw);
-        t.y0 = j * th;
-        t.y1 = t.y0 + ((j == nth - 1) ? thr : th);
-        t.p0 = t.p1 = -1;
-        tasks.push_back(t);
-      }
+    const int ntw = std::max(1, W / tile), nth = std::max(1, H / tile);
+    std::vector<int32_t> rects((size_t)ntw * nth * 4);
+    tile_split(W, H, ntw, nth, rects.data());
+    for (size_t k = 0; k < rects.size(); k += 4) {
+      Task t{};
+      t.x0 = rects[k], t.x1 = rects[k + 1], t.y0 = rects[k + 2], t.y1 = rects[k + 3];
+      t.p0 = t.p1 = -1;
+      tasks.push_back(t);
+    }
   } else {
     int64_t chunk = (int64_t)tile * tile;
     for (int64_t p = 0; p < n_pixels; p += chunk) tasks.push_back(Task{0, 0, 0, 0, p, std::min(n_pixels, p + chunk)});

@@ -152,6 +152,10 @@ void orc_correct_specular_normal(const float ng[3], const float wo[3], const flo
 void orc_env_sample(const float *pixels, int32_t w, int32_t h, int32_t channels, uint64_t n, const float *dirs,
                     float *out);
 void orc_cartesian_to_spherical(uint64_t n, const float *xyz, float *phi_theta);
+/* Triangle bounds and centroids of every primitive, instance by instance (property tests). */
+void orc_prim_bounds(void *scene, float *boxes, float *centroids);
+/* The frame's tile split: (x0, x1, y0, y1) per tile; returns the tile count, 0 for bad sizes. */
+int32_t orc_tile_split(int32_t width, int32_t height, int32_t tiles_w, int32_t tiles_h, int32_t *rects);
 
 /* Film outputs and the Radiance .hdr format (film_io.cpp). */
 void orc_film_accumulate(const float *partial, float *accum, float *final_buf, uint64_t n, uint32_t frame_index);

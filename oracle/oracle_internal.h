@@ -108,6 +108,7 @@ struct TraceCounters {
 };
 
 void build_bvh(Scene &s);
+void prim_bounds(const Scene &s, const Prim &p, Box &box, V3 &centroid);
 Hit trace(const Scene &s, const Ray &r, TraceCounters *c);
 bool triangle_hit(const Scene &s, const Prim &p, const Ray &r, float tmin, float tmax, float &t, float &u, float &v);
 

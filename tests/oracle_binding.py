@@ -109,6 +109,9 @@ def lib():
         L.orc_vndf_g1.restype = C.c_float
         L.orc_correct_specular_normal.argtypes = [f32p, f32p, f32p, f32p]
         L.orc_cartesian_to_spherical.argtypes = [C.c_uint64, f32p, f32p]
+        L.orc_prim_bounds.argtypes = [C.c_void_p, f32p, f32p]
+        L.orc_tile_split.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p]
+        L.orc_tile_split.restype = C.c_int32
         u8p = C.POINTER(C.c_uint8)
         L.orc_film_accumulate.argtypes = [f32p, f32p, f32p, C.c_uint64, C.c_uint32]
         L.orc_display_blend.argtypes = [f32p, f32p, f32p, C.c_uint64, C.c_uint32]
@@ -208,6 +211,14 @@ class OracleScene:
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
         lib().orc_bvh_info(self.h, C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
+
+    def prim_bounds(self):
+        """(boxes (n, 6) as min then max, centroids (n, 3)) of every triangle, world space, instance
+        by instance and triangle by triangle."""
+        boxes = np.zeros((self.n_tris, 6), np.float32)
+        cents = np.zeros((self.n_tris, 3), np.float32)
+        lib().orc_prim_bounds(self.h, _p(boxes, f32p), _p(cents, f32p))
+        return boxes, cents
 
     def trace(self, orig, dirs):
         orig = np.ascontiguousarray(orig, np.float32)
@@ -379,6 +390,15 @@ def cartesian_to_spherical(xyz):
     out = np.zeros((d.shape[0], 2), np.float32)
     lib().orc_cartesian_to_spherical(d.shape[0], _p(d, f32p), _p(out, f32p))
     return out
+
+
+def tile_split(width, height, tiles_w, tiles_h):
+    """The frame's split into tiles_w x tiles_h tiles: (n, 4) rows of (x0, x1, y0, y1)."""
+    rects = np.zeros((max(tiles_w, 0) * max(tiles_h, 0), 4), np.int32)
+    n = lib().orc_tile_split(width, height, tiles_w, tiles_h, _p(rects, i32p))
+    if n == 0 and rects.size:
+        raise ValueError("bad tile split %dx%d of %dx%d" % (tiles_w, tiles_h, width, height))
+    return rects[:n]
 
 
 # ---- film outputs and the Radiance .hdr format (oracle/film_io.cpp) ----

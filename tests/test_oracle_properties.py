@@ -1,6 +1,8 @@
 """The reference's own property tests (tests/unit_test/corelib/nova/material/BxDFTest.cpp,
 tests/unit_test/corelib/nova/texturing/NovaTextureInterfaceTest.cpp,
-tests/unit_test/sources/processing/TextureProcessingTest.cpp) restated against the CPU oracle's
+tests/unit_test/sources/processing/TextureProcessingTest.cpp,
+tests/unit_test/corelib/nova/shape/TriangleTest.cpp, tests/unit_test/corelib/nova/nova_utilsTest.cpp)
+restated against the CPU oracle's
 functions, with the reference's inputs and bounds.  The reference pins no numeric results for this
 path; these properties are what it does check, so the oracle is held to them too.  Where the
 reference draws from its own unseeded or library random generator, seeded numpy draws of the same
@@ -99,3 +101,44 @@ def test_cartesian_to_spherical_approximation(oracle):
     got = ob.cartesian_to_spherical(cart.astype(np.float32))
     err = np.hypot(got[:, 0] - phi, got[:, 1] - theta)
     assert err.max() <= 5e-3
+
+
+def _cube_scene(offset):
+    from axomae_b200 import scenes
+    b = scenes._Builder()
+    M = np.eye(4)
+    M[:3, 3] = offset
+    b.add(scenes.box((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), np.eye(3)), b.lambert((0.5, 0.5, 0.5)))
+    b.place(0, 0, M)
+    env = b.tex(scenes.f32_texture(np.ones((2, 2, 4), np.float32)))
+    return b.finish(env, scenes.camera((0.0, 0.0, 5.0), (0.0, 0.0, 0.0), 8, 8))
+
+
+def test_triangle_aabb_and_centroid(oracle):
+    """TriangleTest.computeAABB / centroid: a triangle's box is the min / max of its (transformed)
+    vertices and its centroid their mean within 1e-5; here for every face of a cube placed with the
+    identity and with a translation."""
+    offset = np.array([3.0, -1.0, 0.5], np.float32)
+    scene = _cube_scene(offset)
+    boxes, cents = oracle.OracleScene(scene).prim_bounds()
+    mesh = scene["meshes"][0]
+    tri = mesh["vertices"].reshape(-1, 3)[mesh["indices"].reshape(-1, 3)]  # (12, 3, 3)
+    for k, shift in enumerate((np.zeros(3, np.float32), offset)):
+        w = tri + shift
+        sl = slice(12 * k, 12 * (k + 1))
+        np.testing.assert_array_equal(boxes[sl, :3], w.min(axis=1))
+        np.testing.assert_array_equal(boxes[sl, 3:], w.max(axis=1))
+        assert np.abs(cents[sl] - w.mean(axis=1)).max() <= 1e-5
+
+
+def test_divide_by_tiles(oracle):
+    """NovaTests.divideByTiles: a 50 x 50 frame split 5 x 5 gives 25 tiles; they cover the frame
+    once, the last column and row taking the remainder of an uneven split."""
+    rects = oracle.tile_split(50, 50, 5, 5)
+    assert len(rects) == 25
+    for W, H, tw, th in ((50, 50, 5, 5), (97, 61, 6, 4), (1920, 1080, 60, 33)):
+        rects = oracle.tile_split(W, H, tw, th)
+        cover = np.zeros((H, W), np.int32)
+        for x0, x1, y0, y1 in rects:
+            cover[y0:y1, x0:x1] += 1
+        assert len(rects) == tw * th and np.all(cover == 1)
