@@ -256,3 +256,11 @@ Hit trace(const Scene &s, const Ray &r, TraceCounters *cnt) {
 }
 
 }  // namespace orc
+
+/* The traversal's slab test on one box (property tests): the entry distance of the ray (o, d) when
+ * it meets [mn, mx] no farther than dist_min, else MAXFLOAT. */
+extern "C" float orc_box_intersect(const float mn[3], const float mx[3], const float o[3], const float d[3],
+                                   float dist_min) {
+  orc::Node n{{mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, 0, 0};
+  return orc::box_intersect(n, orc::V3{d[0], d[1], d[2]}, orc::V3{o[0], o[1], o[2]}, dist_min);
+}

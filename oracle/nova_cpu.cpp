@@ -450,6 +450,7 @@ struct PrincipledBSDF {
     params.ng = normalize(mul_t(frame, params.ng));
     weights();
   }
+  PrincipledBSDF() = default;
   PrincipledBSDF(const BsdfParams &p, float uc) {
     configure(p);
     float idx = 0.f;
@@ -614,6 +615,47 @@ struct PrincipledBSDF {
     return true;
   }
 };
+
+/* DielectricBxDF::f (BxDF.h:497-524), radiance transport: the evaluator the reference's unit tests
+ * hold the sampler to; the path itself only samples. */
+static Spec dielectric_f(const PrincipledBSDF &b, V3 wo, V3 wi) {
+  if (b.ggx.full_specular() || b.params.eta.x == 1.f) return v3(0.f);
+  const float eta = b.params.eta.x, ci = bx::costheta(wi), co = bx::costheta(wo);
+  float new_eta = 0.f;
+  Spec f;
+  if (bx::same_hemi(wi, wo)) {
+    V3 wm = normalize(wi + wo);
+    float R = fresnel_real(eta, bx::absdot(wo, wm), new_eta);
+    f = b.params.albedo * b.ggx.D(wm) * b.ggx.G(wo, wi) * R / (4 * ci * co);
+  } else {
+    V3 wm = normalize(wi * eta + wo);
+    if (dot(wo, wm) < 0) wm = -wm;
+    float T = 1.f - fresnel_real(eta, bx::absdot(wo, wm), new_eta);
+    float denom = sqr(dot(wi, wm) + dot(wo, wm) / eta);
+    f = b.params.albedo * T * b.ggx.D(wm) * b.ggx.G(wo, wi) * std::fabs(dot(wi, wm) * dot(wo, wm) / (ci * co * denom));
+    f = f / sqr(eta);
+  }
+  return b.lobe_w * f;
+}
+
+/* DielectricBxDF::pdf (BxDF.h:526-557), all flags. */
+static float dielectric_pdf(const PrincipledBSDF &b, V3 wo, V3 wi) {
+  if (b.params.eta.x == 1.f || b.ggx.full_specular()) return 0.f;
+  const float eta = b.params.eta.x;
+  float new_eta = 0.f;
+  if (bx::same_hemi(wi, wo)) {
+    V3 wm = normalize(wi + wo);
+    float wo_dot_wm = bx::absdot(wo, wm);
+    float R = fresnel_real(eta, wo_dot_wm, new_eta), T = 1.f - R;
+    return b.lobe_p * (b.ggx.pdf(wo, wm) / (4 * wo_dot_wm) * R / (R + T));
+  }
+  V3 wm = normalize(wi * eta + wo);
+  if (dot(wo, wm) < 0) wm = -wm;
+  float R = fresnel_real(eta, bx::absdot(wo, wm), new_eta), T = 1.f - R;
+  float denom = sqr(dot(wi, wm) + dot(wo, wm) / eta);
+  float jac = bx::absdot(wi, wm) / denom;
+  return b.lobe_p * (b.ggx.pdf(wo, wm) * jac * T / (T + R));
+}
 
 /* bsdf::correct_specular_shading_normal, BxDF_math.h:26-53 */
 static V3 correct_specular_shading_normal(V3 ng, V3 wo, V3 ns) {
@@ -879,6 +921,16 @@ static V4 render_sample(PathCtx &c, const orc_options &opt, int x, int y, int s)
 
 using namespace orc;
 
+static orc::Texture texture_from(const orc_texture &t) {
+  orc::Texture d;
+  d.w = t.width, d.h = t.height, d.channels = t.channels;
+  d.is_rgba = t.is_rgba != 0, d.invert_u = t.invert_u != 0, d.invert_v = t.invert_v != 0;
+  size_t n = (size_t)t.width * t.height;
+  if (t.u8_pixels) d.u8.assign(t.u8_pixels, t.u8_pixels + n);
+  if (t.f32_pixels) d.f32.assign(t.f32_pixels, t.f32_pixels + n * t.channels);
+  return d;
+}
+
 extern "C" void *orc_build(const orc_scene *in) {
   if (!in || in->n_instances == 0 || in->envmap < 0 || (uint32_t)in->envmap >= in->n_textures) return nullptr;
   Scene *s = new Scene();
@@ -915,14 +967,7 @@ extern "C" void *orc_build(const orc_scene *in) {
     s->materials.push_back(d);
   }
   for (uint32_t i = 0; i < in->n_textures; i++) {
-    const orc_texture &t = in->textures[i];
-    Texture d;
-    d.w = t.width, d.h = t.height, d.channels = t.channels;
-    d.is_rgba = t.is_rgba != 0, d.invert_u = t.invert_u != 0, d.invert_v = t.invert_v != 0;
-    size_t n = (size_t)t.width * t.height;
-    if (t.u8_pixels) d.u8.assign(t.u8_pixels, t.u8_pixels + n);
-    if (t.f32_pixels) d.f32.assign(t.f32_pixels, t.f32_pixels + n * t.channels);
-    s->textures.push_back(std::move(d));
+    s->textures.push_back(texture_from(in->textures[i]));
   }
   s->envmap = in->envmap;
   s->inv_P = m4_from(in->inv_P);
@@ -1209,6 +1254,38 @@ extern "C" void orc_env_sample(const float *pixels, int32_t w, int32_t h, int32_
     const V4 r = env_sample(s, V3{dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]});
     out[4 * i] = r.x, out[4 * i + 1] = r.y, out[4 * i + 2] = r.z, out[4 * i + 3] = r.w;
   }
+}
+
+/* DielectricBxDF on its own (weight and probability 1, radiance transport, all flags), as the
+ * reference's unit tests build it (BxDFTest.cpp:216-270): sample_f at (wo, uc, u), then f and pdf
+ * evaluated at the normalised sampled direction.  out = f[3], pdf, wi[3], costheta, f_eval[3],
+ * pdf_eval.  Returns 1 when a direction was sampled. */
+extern "C" int32_t orc_dielectric_lobe(const float albedo[3], float eta, float roughness, float anisotropy,
+                                       const float wo[3], float uc, const float u[2], float out[12]) {
+  PrincipledBSDF b;
+  b.params.albedo = {albedo[0], albedo[1], albedo[2]};
+  b.params.eta = v3(eta);
+  b.params.roughness = roughness;
+  b.params.anisotropy = anisotropy;
+  b.lobe = L_DIELECTRIC;
+  b.ggx = VNDF(anisotropy, roughness);
+  Sample smp;
+  const V3 w{wo[0], wo[1], wo[2]};
+  const bool ok = b.dielectric_sample(w, uc, u, smp);
+  const V3 wi = ok ? normalize(smp.wi) : smp.wi;
+  const Spec fe = ok ? dielectric_f(b, w, wi) : v3(0.f);
+  const float vals[12] = {smp.f.x, smp.f.y, smp.f.z, smp.pdf, smp.wi.x, smp.wi.y, smp.wi.z, smp.costheta,
+                          fe.x, fe.y, fe.z, ok ? dielectric_pdf(b, w, wi) : 0.f};
+  std::copy(vals, vals + 12, out);
+  return ok ? 1 : 0;
+}
+
+/* One texture lookup (property tests): an 8-bit texture through the bilinear sample, a float one
+ * through the nearest-texel read; out = RGBA (8-bit channels in 0..255). */
+extern "C" void orc_texture_lookup(const orc_texture *t, float u, float v, float out[4]) {
+  const Texture tx = texture_from(*t);
+  const V4 p = t->u8_pixels ? sample_u8(tx, u, v) : f32pixel(tx, u, v);
+  out[0] = p.x, out[1] = p.y, out[2] = p.z, out[3] = p.w;
 }
 
 /* Triangle::computeAABB / centroid of every primitive (prim_bounds in bvh.cpp): 6 floats of box

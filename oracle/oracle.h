@@ -152,6 +152,14 @@ void orc_correct_specular_normal(const float ng[3], const float wo[3], const flo
 void orc_env_sample(const float *pixels, int32_t w, int32_t h, int32_t channels, uint64_t n, const float *dirs,
                     float *out);
 void orc_cartesian_to_spherical(uint64_t n, const float *xyz, float *phi_theta);
+/* The dielectric lobe alone: sample at (wo, uc, u), then f and pdf evaluated at the sampled direction
+ * (property tests); out = f[3], pdf, wi[3], costheta, f_eval[3], pdf_eval. */
+int32_t orc_dielectric_lobe(const float albedo[3], float eta, float roughness, float anisotropy, const float wo[3],
+                            float uc, const float u[2], float out[12]);
+/* The traversal's slab test on one box: entry distance, or MAXFLOAT past dist_min (property tests). */
+float orc_box_intersect(const float mn[3], const float mx[3], const float o[3], const float d[3], float dist_min);
+/* One texture lookup: 8-bit bilinear sample or float nearest texel, RGBA (property tests). */
+void orc_texture_lookup(const orc_texture *texture, float u, float v, float out[4]);
 /* Triangle bounds and centroids of every primitive, instance by instance (property tests). */
 void orc_prim_bounds(void *scene, float *boxes, float *centroids);
 /* The frame's tile split: (x0, x1, y0, y1) per tile; returns the tile count, 0 for bad sizes. */

@@ -110,6 +110,11 @@ def lib():
         L.orc_correct_specular_normal.argtypes = [f32p, f32p, f32p, f32p]
         L.orc_cartesian_to_spherical.argtypes = [C.c_uint64, f32p, f32p]
         L.orc_prim_bounds.argtypes = [C.c_void_p, f32p, f32p]
+        L.orc_texture_lookup.argtypes = [C.POINTER(OrcTexture), C.c_float, C.c_float, f32p]
+        L.orc_box_intersect.argtypes = [f32p, f32p, f32p, f32p, C.c_float]
+        L.orc_box_intersect.restype = C.c_float
+        L.orc_dielectric_lobe.argtypes = [f32p, C.c_float, C.c_float, C.c_float, f32p, C.c_float, f32p, f32p]
+        L.orc_dielectric_lobe.restype = C.c_int32
         L.orc_tile_split.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p]
         L.orc_tile_split.restype = C.c_int32
         u8p = C.POINTER(C.c_uint8)
@@ -382,6 +387,42 @@ def env_sample(pixels, dirs):
     out = np.zeros((d.shape[0], 4), np.float32)
     lib().orc_env_sample(_p(px, f32p), w, h, ch, d.shape[0], _p(d, f32p), _p(out, f32p))
     return out
+
+
+def texture_lookup(tex, u, v):
+    """One lookup of a texture dictionary (scenes layout) at (u, v): RGBA float."""
+    if tex["format"] == "u8":
+        px = np.ascontiguousarray(tex["pixels"], np.uint32)
+        t = OrcTexture(_p(px, u32p), None, tex["width"], tex["height"], tex.get("channels", 4),
+                       int(tex.get("is_rgba", 1)), int(tex.get("invert_u", 0)), int(tex.get("invert_v", 0)))
+    else:
+        px = np.ascontiguousarray(tex["pixels"], np.float32)
+        t = OrcTexture(None, _p(px, f32p), tex["width"], tex["height"], tex.get("channels", 4),
+                       int(tex.get("is_rgba", 1)), int(tex.get("invert_u", 0)), int(tex.get("invert_v", 0)))
+    out = np.zeros(4, np.float32)
+    lib().orc_texture_lookup(C.byref(t), u, v, _p(out, f32p))
+    return out
+
+
+MAXFLOAT = float(np.finfo(np.float32).max)
+
+
+def box_intersect(mn, mx, o, d, dist_min):
+    """The traversal's slab test: entry distance of the ray into [mn, mx], MAXFLOAT for a miss."""
+    a = [np.ascontiguousarray(x, np.float32).reshape(3) for x in (mn, mx, o, d)]
+    return lib().orc_box_intersect(*[_p(x, f32p) for x in a], dist_min)
+
+
+def dielectric_lobe(albedo, eta, roughness, anisotropy, wo, uc, u):
+    """The dielectric lobe alone: (sampled, dict of f, pdf, wi, costheta, f_eval, pdf_eval)."""
+    alb = np.ascontiguousarray(albedo, np.float32).reshape(3)
+    w = np.ascontiguousarray(wo, np.float32).reshape(3)
+    uu = np.ascontiguousarray(u, np.float32).reshape(2)
+    out = np.zeros(12, np.float32)
+    ok = lib().orc_dielectric_lobe(_p(alb, f32p), eta, roughness, anisotropy, _p(w, f32p), uc, _p(uu, f32p),
+                                   _p(out, f32p))
+    return bool(ok), {"f": out[0:3], "pdf": float(out[3]), "wi": out[4:7], "costheta": float(out[7]),
+                      "f_eval": out[8:11], "pdf_eval": float(out[11])}
 
 
 def cartesian_to_spherical(xyz):

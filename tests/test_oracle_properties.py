@@ -1,7 +1,9 @@
 """The reference's own property tests (tests/unit_test/corelib/nova/material/BxDFTest.cpp,
 tests/unit_test/corelib/nova/texturing/NovaTextureInterfaceTest.cpp,
+tests/unit_test/corelib/nova/texturing/TextureContextTest.cpp,
 tests/unit_test/sources/processing/TextureProcessingTest.cpp,
-tests/unit_test/corelib/nova/shape/TriangleTest.cpp, tests/unit_test/corelib/nova/nova_utilsTest.cpp)
+tests/unit_test/corelib/nova/shape/TriangleTest.cpp, tests/unit_test/corelib/nova/shape/BoxTest.cpp,
+tests/unit_test/corelib/nova/nova_utilsTest.cpp)
 restated against the CPU oracle's
 functions, with the reference's inputs and bounds.  The reference pins no numeric results for this
 path; these properties are what it does check, so the oracle is held to them too.  Where the
@@ -91,6 +93,25 @@ def test_envmap_sample_direction_encoded(oracle):
     assert np.all(np.abs(px - want) < 1e-1)
 
 
+CORNERS = [(0.0, 0.0), (1.0, 0.0), (0.0, 1.0), (1.0, 1.0)]
+
+
+def test_texture_context_corners(oracle):
+    """TextureContextTest.sample_texture: on a 2 x 2 texture (BGRA byte order, not inverted) the
+    lookups at (0, 0), (1, 0), (0, 1), (1, 1) return texels 0, 1, 2, 3 in that order, for an 8-bit
+    texture (0xFF000000, 0x00FF0000, 0x0000FF00, 0x000000FF) and for a float one (1 .. 16)."""
+    words = np.array([0xFF000000, 0x00FF0000, 0x0000FF00, 0x000000FF], np.uint32)
+    tex = {"format": "u8", "pixels": words, "width": 2, "height": 2, "channels": 4, "is_rgba": 0}
+    for k, (u, v) in enumerate(CORNERS):
+        b = [(int(words[k]) >> (8 * i)) & 0xFF for i in range(4)]
+        want = np.array([b[2], b[1], b[0], b[3]], np.float32)  # not RGBA: r and b swap
+        np.testing.assert_array_equal(oracle.texture_lookup(tex, u, v), want)
+    vals = np.arange(1, 17, dtype=np.float32)
+    tex = {"format": "f32", "pixels": vals, "width": 2, "height": 2, "channels": 4, "is_rgba": 0}
+    for k, (u, v) in enumerate(CORNERS):
+        np.testing.assert_array_equal(oracle.texture_lookup(tex, u, v), vals[4 * k:4 * k + 4])
+
+
 def test_cartesian_to_spherical_approximation(oracle):
     """TexturingTest.uvCartesianCohesionApproximated: the fast atan2 polynomial and the acos table
     recover (phi, theta) within 5e-3."""
@@ -101,6 +122,74 @@ def test_cartesian_to_spherical_approximation(oracle):
     got = ob.cartesian_to_spherical(cart.astype(np.float32))
     err = np.hypot(got[:, 0] - phi, got[:, 1] - theta)
     assert err.max() <= 5e-3
+
+
+def test_dielectric_specular_transmission(oracle):
+    """DielectricBxDF.sample_f: a smooth dielectric of the vacuum's index passes light straight
+    through (costheta within 1e-5 of 1) with f <= 1.  The reference asks for transmission only; the
+    path samples with every flag, which is the same here since the vacuum reflects nothing."""
+    ok, s = oracle.dielectric_lobe([0.0, 0.0, 0.0], 1.0, 0.0, 0.0, [0.0, 0.0, 1.0], 0.533, [0.33, 1.35])
+    assert ok and abs(s["costheta"] - 1.0) <= 1e-5 and np.all(s["f"] <= 1.0)
+    assert s["wi"][2] < 0  # transmitted below the surface
+
+
+def test_dielectric_sample_matches_f_and_pdf(oracle):
+    """DielectricBxDF.f / pdf: for a rough glass (eta 1.5, roughness 0.1, anisotropy 0.01) the sampled
+    f is within 1e-2 of f evaluated at the sampled direction and the sampled pdf within 1e-1 of pdf;
+    checked at the reference's sample and, to 1e-4 relative, at 64 seeded ones covering both lobes."""
+    albedo = [0.2, 0.1, 0.0]
+    wo = _n([-0.3, 0.5, 1.0])
+    ok, s = oracle.dielectric_lobe(albedo, 1.5, 0.1, 0.01, wo, 0.533, [0.33, 1.35])
+    assert ok
+    assert np.all(np.abs(s["f_eval"] - s["f"]) <= 1e-2) and abs(s["pdf_eval"] - s["pdf"]) <= 1e-1
+    rng = np.random.default_rng(11)
+    lobes = set()
+    for _ in range(64):
+        ok, s = oracle.dielectric_lobe(albedo, 1.5, 0.1, 0.01, wo, float(rng.uniform()), rng.uniform(0, 1, 2))
+        if not ok:
+            continue
+        lobes.add(bool(s["wi"][2] > 0))
+        # f and pdf reach 1e3 to 1e4 at this roughness: the bounds are relative there (float32 rounding)
+        assert np.all(np.abs(s["f_eval"] - s["f"]) <= 1e-4 * max(1.0, float(np.abs(s["f"]).max())))
+        assert abs(s["pdf_eval"] - s["pdf"]) <= 1e-4 * max(1.0, s["pdf"])
+    assert lobes == {True, False}
+
+
+BOX_HALF = 200.0  # tests/unit_test/utils/aabb_utils_test.h: a cube of half extent 200
+AXES = np.concatenate([np.eye(3), -np.eye(3)]).astype(np.float32)
+
+
+def _outside(p):
+    return bool(np.any(np.abs(p) > BOX_HALF))
+
+
+def test_box_hit_from_outside(oracle):
+    """BoxTest.outIntersection: 50 rays from points drawn in [-2000, 2000]^3 outside the box, aimed
+    at its centre, all hit it (within 10000)."""
+    mn, mx = np.full(3, -BOX_HALF), np.full(3, BOX_HALF)
+    rng = np.random.default_rng(5)
+    hits = 0
+    while hits < 50:
+        p = rng.uniform(-2000.0, 2000.0, 3).astype(np.float32)
+        if not _outside(p):
+            continue
+        d = (-p / np.linalg.norm(p)).astype(np.float32)
+        t = oracle.box_intersect(mn, mx, p, d, 10000.0)
+        assert 0 < t < 10000.0
+        hits += 1
+
+
+def test_box_hit_from_inside(oracle):
+    """BoxTest.inIntersection: from 50 points inside the box, rays along the six axis directions
+    (zero components, so infinite slab distances) all hit it."""
+    mn, mx = np.full(3, -BOX_HALF), np.full(3, BOX_HALF)
+    rng = np.random.default_rng(6)
+    for _ in range(50):
+        p = rng.uniform(-BOX_HALF, BOX_HALF, 3).astype(np.float32)
+        for d in AXES:
+            assert oracle.box_intersect(mn, mx, p, d, 10000.0) < oracle.MAXFLOAT
+    # and a box behind the ray is missed
+    assert oracle.box_intersect(mn, mx, [0.0, 0.0, 500.0], [0.0, 0.0, 1.0], 10000.0) == oracle.MAXFLOAT
 
 
 def _cube_scene(offset):
