@@ -682,6 +682,7 @@ class B200Engine final : public Engine {
   std::thread worker_;
   mutable std::mutex err_mu_;
   std::string error_;
+  exception::NovaException errors_; /* the last start's and render's error bits */
 
   void set_error(const std::string &e) {
     std::lock_guard<std::mutex> g(err_mu_);
@@ -747,6 +748,18 @@ class B200Engine final : public Engine {
     }
   }
 
+  /* the exception bit of a failed frame's status */
+  static uint64_t frame_error_bits(ERROR_STATE e) {
+    switch (e) {
+      case OUT_OF_MEMORY:
+      case RENDERER_EXCEPTION:
+      case RENDER_ENGINE_NOT_INITIALIZED: return exception::GENERAL_GPU_ERROR;
+      case INVALID_BUFFER_STATE:
+      case RENDER_BUFFER_NOT_INITIALIZED: return exception::INVALID_RENDERBUFFER_STATE;
+      default: return exception::GENERAL_ERROR;
+    }
+  }
+
   void render_loop() {
     const Camera *cam = scene_->getCamera((unsigned)std::max(0, scene_->getCurrentCameraId()));
     float iP[16], iV[16];
@@ -759,6 +772,7 @@ class B200Engine final : public Engine {
       const ERROR_STATE e = render_frame(frame, iP, iV, near_p, far_p);
       if (callback_) callback_->framePostRenderRoutine();
       if (e != SUCCESS) { /* the error text is kept for getRenderEngineError; the render stops */
+        if (rendering_.load()) errors_.addErrorType(frame_error_bits(e)); /* not a stopRender() */
         rendering_.store(false);
         break;
       }
@@ -849,21 +863,34 @@ class B200Engine final : public Engine {
   }
 
   ERROR_STATE startRender() override {
+    errors_ = exception::NovaException();
     if (!options_) return RENDER_OPTIONS_NOT_INITIALIZED;
-    if (!buffers_) return RENDER_BUFFER_NOT_INITIALIZED;
+    if (!buffers_) {
+      errors_.addErrorType(exception::INVALID_RENDERBUFFER_STATE);
+      return RENDER_BUFFER_NOT_INITIALIZED;
+    }
     if (!scene_built_ || !accel_built_) return SCENE_NOT_PROCESSED; /* the device context comes with the scene */
     if (!ctx_) return RENDER_ENGINE_NOT_INITIALIZED;
     if (!options_->isUsingGpu())
       return fail(INVALID_ENGINE_STATE, "the B200 engine renders on the GPU only: call RenderOptions::useGpu(true)");
     const int flag = options_->getIntegratorFlag();
-    if (!(flag & integrator::PATH)) return fail(RENDERER_EXCEPTION, "invalid integrator: the PATH bit is required");
-    if (!(flag & (integrator::COMBINED | integrator::NORMAL | integrator::DEPTH | integrator::EMISSIVE)))
+    if (!(flag & integrator::PATH)) {
+      errors_.addErrorType(exception::INVALID_INTEGRATOR);
+      return fail(RENDERER_EXCEPTION, "invalid integrator: the PATH bit is required");
+    }
+    if (!(flag & (integrator::COMBINED | integrator::NORMAL | integrator::DEPTH | integrator::EMISSIVE))) {
+      errors_.addErrorType(exception::INVALID_RENDER_MODE);
       return fail(RENDERER_EXCEPTION, "invalid render mode: no COMBINED, NORMAL, DEPTH or EMISSIVE pass");
+    }
     const int cam = scene_->getCurrentCameraId();
     if (cam < 0 || !scene_->getCamera((unsigned)cam)) return fail(INVALID_SCENE_TYPE, "the scene has no current camera");
-    if (buffers_->getWidth() == 0 || buffers_->getHeight() == 0 ||
-        buffers_->getAccumulator().size() != (size_t)buffers_->getWidth() * buffers_->getHeight() * 4)
+    const unsigned bw = buffers_->getWidth(), bh = buffers_->getHeight();
+    if (bw == 0 || bh == 0 || bw > 65536 || bh > 65536 || buffers_->getAccumulator().size() != (size_t)bw * bh * 4) {
+      /* DrawEngine.cpp:44-50: zero or over 65536 pixels a side is a dimension error, else the state */
+      const bool bad_dim = bw == 0 || bh == 0 || bw > 65536 || bh > 65536;
+      errors_.addErrorType(bad_dim ? exception::INVALID_RENDERBUFFER_DIM : exception::INVALID_RENDERBUFFER_STATE);
       return fail(INVALID_BUFFER_STATE, "render buffers are not sized (RenderBuffer::resize)");
+    }
     rendering_.store(false);
     join();
     frame_index_.store(0);
@@ -882,6 +909,7 @@ class B200Engine final : public Engine {
     log[size] = 0;
   }
   unsigned getFrameIndex() const override { return frame_index_.load(); }
+  const exception::NovaException &errors() const { return errors_; }
 };
 
 /* ---- the device accelerator plug-in ------------------------------------------------------- */
@@ -974,6 +1002,15 @@ ScenePtr create_scene() { return std::make_unique<B200Scene>(); }
 EnginePtr create_engine() { return std::make_unique<B200Engine>(0); }
 EnginePtr create_engine(int device) { return std::make_unique<B200Engine>(device); }
 ERROR_STATE init_threads(unsigned n) { return n == 0 ? THREADPOOL_CREATION_ERROR : SUCCESS; }
+
+uint64_t get_error_status(const Engine &engine) {
+  const auto *e = dynamic_cast<const B200Engine *>(&engine);
+  return e ? e->errors().getErrorFlag() : (uint64_t)exception::GENERAL_ERROR;
+}
+std::vector<exception::ERROR> get_error_list(const Engine &engine) {
+  const auto *e = dynamic_cast<const B200Engine *>(&engine);
+  return e ? e->errors().getErrorList() : std::vector<exception::ERROR>{exception::GENERAL_ERROR};
+}
 
 std::unique_ptr<aggregate::DeviceAcceleratorInterface> aggregate::DeviceAcceleratorInterface::make() {
   return std::make_unique<B200AcceleratorImpl>(0);

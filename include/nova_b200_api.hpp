@@ -22,10 +22,12 @@
  */
 #ifndef NOVA_B200_API_HPP
 #define NOVA_B200_API_HPP
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <memory>
 #include <span>
+#include <vector>
 
 namespace nova {
 
@@ -49,6 +51,58 @@ enum ERROR_STATE {
   INVALID_ARGUMENT,
   RENDERER_EXCEPTION,
 };
+
+namespace exception {
+/* engine/nova_exception.h:13-31: one bit per render error, numbered as in the reference. */
+enum ERROR : uint64_t {
+  NOERR = 0,
+  INVALID_INTEGRATOR = 1ULL << 0,
+  INVALID_RENDER_MODE = 1ULL << 1,
+  INVALID_SAMPLER_DIM = 1ULL << 2,
+  SAMPLER_INIT_ERROR = 1ULL << 3,
+  SAMPLER_DOMAIN_EXHAUSTED = 1ULL << 4,
+  SAMPLER_INVALID_ALLOC = 1ULL << 5,
+  SAMPLER_INVALID_ARG = 1ULL << 6,
+  INVALID_RENDERBUFFER_STATE = 1ULL << 7,
+  INVALID_ENGINE_INSTANCE = 1ULL << 8,
+  INVALID_RENDERBUFFER_DIM = 1ULL << 9,
+  GENERAL_GPU_ERROR = 1ULL << 31,
+  GENERAL_ERROR = 1ULL << 32,
+};
+
+/* NovaException (engine/nova_exception.h:33-61, nova_exception.cpp): a set of ERROR bits that any
+ * thread may add to.  A copy carries the bits; a move takes them and leaves the source empty. */
+class NovaException {
+  std::atomic<uint64_t> flags_{NOERR};
+
+ public:
+  NovaException() = default;
+  NovaException(const NovaException &o) noexcept : flags_(o.getErrorFlag()) {}
+  NovaException(NovaException &&o) noexcept : flags_(o.flags_.exchange(NOERR, std::memory_order_relaxed)) {}
+  NovaException &operator=(const NovaException &o) noexcept {
+    if (this != &o) flags_.store(o.getErrorFlag(), std::memory_order_relaxed);
+    return *this;
+  }
+  NovaException &operator=(NovaException &&o) noexcept {
+    if (this != &o) flags_.store(o.flags_.exchange(NOERR, std::memory_order_relaxed), std::memory_order_relaxed);
+    return *this;
+  }
+  [[nodiscard]] bool errorCheck() const { return getErrorFlag() != NOERR; }
+  [[nodiscard]] uint64_t getErrorFlag() const { return flags_.load(std::memory_order_relaxed); }
+  void addErrorType(uint64_t errors) { flags_.fetch_or(errors, std::memory_order_relaxed); }
+  /* adds another exception's bits to these */
+  void merge(uint64_t other_flags) { flags_.fetch_or(other_flags, std::memory_order_relaxed); }
+  /* every set bit as its own ERROR, lowest first ({NOERR} when none is); bits 0 to 62 */
+  [[nodiscard]] std::vector<ERROR> getErrorList() const {
+    const uint64_t f = getErrorFlag();
+    if (f == NOERR) return {NOERR};
+    std::vector<ERROR> out;
+    for (unsigned bit = 0; bit < 63; bit++)
+      if (f & (1ULL << bit)) out.push_back(static_cast<ERROR>(1ULL << bit));
+    return out;
+  }
+};
+}  // namespace exception
 
 namespace integrator {
 /* api_common.h:29-48: integrator bits 0-7, render-pass bits 8-13 */
@@ -421,6 +475,14 @@ class Engine {
 /* The engine on device `device` (the reference's create_engine() takes no argument: device 0). */
 EnginePtr create_engine();
 EnginePtr create_engine(int device);
+/* api_engine.h:193-196 read the engine's exception manager; here the engine holds the errors of its
+ * last startRender() and render: what the start checks found (INVALID_INTEGRATOR without the PATH
+ * bit, INVALID_RENDER_MODE without a pass, INVALID_RENDERBUFFER_DIM / _STATE for unsized buffers),
+ * then the failure of a frame (GENERAL_GPU_ERROR for a device failure, INVALID_RENDERBUFFER_STATE,
+ * GENERAL_ERROR otherwise).  startRender() clears them. */
+uint64_t get_error_status(const Engine &engine);
+std::vector<exception::ERROR> get_error_list(const Engine &engine);
+
 /* The reference sizes its CPU thread pool here; the B200 engine renders on its own host thread and
  * the device, so this only checks the argument (0 -> THREADPOOL_CREATION_ERROR). */
 ERROR_STATE init_threads(unsigned number_threads);

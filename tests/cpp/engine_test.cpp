@@ -13,6 +13,7 @@
  *
  * Exit status 0 when every check passes; each failed check prints its line.
  */
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -294,10 +295,13 @@ void test_engine_errors_without_device() {
   CHECK(e->setRenderOptions(nullptr) == nova::INVALID_ARGUMENT);
   CHECK(e->setRenderOptions(nova::create_renderoptions()) == nova::SUCCESS);
   CHECK(e->startRender() == nova::RENDER_BUFFER_NOT_INITIALIZED);
+  CHECK(nova::get_error_status(*e) == nova::exception::INVALID_RENDERBUFFER_STATE);
   CHECK(e->setRenderBuffers(nullptr) == nova::INVALID_BUFFER_STATE);
   CHECK(e->setRenderBuffers(nova::create_renderbuffer()) == nova::SUCCESS);
   CHECK(e->prepareRender() == nova::SUCCESS);
   CHECK(e->startRender() == nova::SCENE_NOT_PROCESSED);
+  CHECK(nova::get_error_status(*e) == nova::exception::NOERR); /* each start clears the bits */
+  CHECK(nova::get_error_list(*e) == std::vector<nova::exception::ERROR>{nova::exception::NOERR});
   CHECK(!e->isRendering() && e->getFrameIndex() == 0);
   CHECK(e->stopRender() == nova::SUCCESS && e->getFrameIndex() == 1); /* as the reference's stopRender */
   CHECK(e->cleanup() == nova::INVALID_ENGINE_STATE);                  /* no scene */
@@ -306,6 +310,62 @@ void test_engine_errors_without_device() {
   size_t n = 0;
   e->getRenderEngineError(log, n);
   CHECK(n > 0 && std::strstr(log, "buildScene") != nullptr); /* the last failure: buildAcceleration() */
+}
+
+/* The reference's nova_exception tests (tests/unit_test/corelib/nova/engine/nova_exceptionTest.cpp). */
+bool has(const std::vector<nova::exception::ERROR> &list, nova::exception::ERROR e) {
+  return std::find(list.begin(), list.end(), e) != list.end();
+}
+
+void test_nova_exception() {
+  namespace ex = nova::exception;
+  {
+    ex::NovaException e; /* get_error_list */
+    e.addErrorType(ex::SAMPLER_INIT_ERROR | ex::INVALID_SAMPLER_DIM);
+    const auto list = e.getErrorList();
+    CHECK(has(list, ex::SAMPLER_INIT_ERROR) && has(list, ex::INVALID_SAMPLER_DIM) && list.size() == 2);
+  }
+  {
+    ex::NovaException e; /* add_error_type */
+    e.addErrorType(ex::SAMPLER_INIT_ERROR);
+    e.addErrorType(ex::INVALID_SAMPLER_DIM);
+    CHECK((e.getErrorFlag() & ex::SAMPLER_INIT_ERROR) && (e.getErrorFlag() & ex::INVALID_SAMPLER_DIM) && e.errorCheck());
+  }
+  {
+    ex::NovaException origin, target; /* copy_constructor: the copy carries the bits, the source keeps them */
+    origin.addErrorType(ex::INVALID_INTEGRATOR | ex::SAMPLER_INIT_ERROR | ex::INVALID_RENDER_MODE);
+    target = origin;
+    const auto list = target.getErrorList();
+    CHECK(has(list, ex::INVALID_INTEGRATOR) && has(list, ex::SAMPLER_INIT_ERROR) && has(list, ex::INVALID_RENDER_MODE));
+    CHECK(!has(list, ex::INVALID_SAMPLER_DIM) && origin.getErrorFlag() == target.getErrorFlag());
+    ex::NovaException copied(origin);
+    CHECK(copied.getErrorFlag() == origin.getErrorFlag());
+  }
+  {
+    ex::NovaException origin, target; /* move_constructor: the bits move, the source is left empty */
+    origin.addErrorType(ex::INVALID_INTEGRATOR | ex::SAMPLER_INIT_ERROR | ex::INVALID_RENDER_MODE);
+    target = std::move(origin);
+    const auto list = target.getErrorList();
+    CHECK(has(list, ex::INVALID_INTEGRATOR) && has(list, ex::SAMPLER_INIT_ERROR) && has(list, ex::INVALID_RENDER_MODE));
+    CHECK(!has(list, ex::INVALID_SAMPLER_DIM));
+    ex::NovaException moved(std::move(target));
+    CHECK(moved.getErrorList().size() == 3 && !target.errorCheck()); /* NOLINT: use after move is the point */
+  }
+  {
+    ex::NovaException origin, target; /* merge */
+    origin.addErrorType(ex::SAMPLER_INIT_ERROR | ex::INVALID_SAMPLER_DIM);
+    target.addErrorType(ex::SAMPLER_INVALID_ARG | ex::SAMPLER_INVALID_ALLOC);
+    target.merge(origin.getErrorFlag());
+    const auto list = target.getErrorList();
+    CHECK(has(list, ex::SAMPLER_INIT_ERROR) && has(list, ex::INVALID_SAMPLER_DIM) && has(list, ex::SAMPLER_INVALID_ARG) &&
+          has(list, ex::SAMPLER_INVALID_ALLOC) && !has(list, ex::INVALID_RENDER_MODE));
+  }
+  {
+    ex::NovaException e; /* no error: {NOERR}; the two high bits are listed like the others */
+    CHECK(e.getErrorList() == std::vector<ex::ERROR>{ex::NOERR} && !e.errorCheck());
+    e.addErrorType(ex::GENERAL_ERROR | ex::GENERAL_GPU_ERROR);
+    CHECK(e.getErrorList() == (std::vector<ex::ERROR>{ex::GENERAL_GPU_ERROR, ex::GENERAL_ERROR}));
+  }
 }
 
 /* ---- accel --------------------------------------------------------------------------------- */
@@ -537,6 +597,7 @@ void test_render(const std::string &dir) {
     std::this_thread::sleep_for(std::chrono::milliseconds(2));
   CHECK(engine->getFrameIndex() == SPP && engine->isRendering());
   CHECK(engine->stopRender() == nova::SUCCESS && !engine->isRendering());
+  CHECK(nova::get_error_status(*engine) == nova::exception::NOERR);
   CHECK(pre == (int)SPP && post == (int)SPP);
   engine->getRenderEngineError(log, n);
   std::vector<float> image(engine->getRenderBuffers()->frontBuffer().begin(),
@@ -612,6 +673,7 @@ void test_render(const std::string &dir) {
   CHECK(!engine->isRendering() && engine->getFrameIndex() == 0);
   engine->getRenderEngineError(log, n);
   CHECK(n > 0);
+  CHECK(nova::get_error_status(*engine) == nova::exception::GENERAL_ERROR); /* an invalid argument of the frame */
   engine->stopRender();
   CHECK(engine->cleanup() == nova::SUCCESS);
   nova_b200_destroy(ctx);
@@ -647,6 +709,7 @@ int main(int argc, char **argv) {
     test_options_and_buffers();
     test_scene();
     test_engine_errors_without_device();
+    test_nova_exception();
   } else if (mode == "accel") {
     test_accel();
   } else if (mode == "render" && argc > 2) {
