@@ -16,7 +16,17 @@ film (the mean over its samples), so the gradient of the combined film is the co
 
 The path has no other exchange: scenes and BVHs are built on every rank, and nothing crosses
 between ranks while a frame renders.
+
+Failures.  A rank whose render or backward failed still takes part in the reduction, with
+`failed=True` (its film or gradients are replaced by zeros); the reduction carries the failure
+count beside the sample count, and every rank then raises RankFailure, so all ranks take the same
+collective steps and none waits for a peer that gave up.  A rank that dies or never arrives is
+caught by the process group's timeout, which the caller keeps short (the collective then raises).
 """
+
+
+class RankFailure(RuntimeError):
+    """Raised on every rank after a reduction in which at least one rank reported a failure."""
 
 
 def weak_range(spp_per_rank: int, rank: int, world: int):
@@ -37,37 +47,59 @@ def strong_range(spp_total: int, rank: int, world: int):
     return spp_total, begin, end - begin
 
 
-def reduce_films(film, count: int, group=None):
-    """In place: film (a float tensor, this rank's mean over `count` samples) becomes the mean over
-    every rank's samples.  Collective: all ranks call it in the same order."""
+def _counts(count: int, failed: bool, device):
     import torch
+    return torch.tensor([0.0 if failed else float(count), 1.0 if failed else 0.0], dtype=torch.float64,
+                        device=device)
+
+
+def _check(counts):
+    ranks_failed = int(counts[1].item())
+    if ranks_failed:
+        raise RankFailure("%d rank(s) reported a failed render or backward" % ranks_failed)
+    return counts[0].item()
+
+
+def reduce_films(film, count: int, group=None, failed: bool = False):
+    """In place: film (a float tensor, this rank's mean over `count` samples) becomes the mean over
+    every rank's samples.  Collective: all ranks call it in the same order.  A rank whose render
+    failed passes failed=True; then every rank raises RankFailure after the reduction."""
     import torch.distributed as dist
-    total = torch.tensor([float(count)], dtype=torch.float64, device=film.device)
-    film.mul_(float(count))
+    counts = _counts(count, failed, film.device)
+    if failed:
+        film.zero_()
+    else:
+        film.mul_(float(count))
     dist.all_reduce(film, group=group)
-    dist.all_reduce(total, group=group)
-    if total.item() > 0:
-        film.div_(total.item())
+    dist.all_reduce(counts, group=group)
+    total = _check(counts)
+    if total > 0:
+        film.div_(total)
     return film
 
 
-def reduce_gradients(grads, count: int, group=None):
+def reduce_gradients(grads, count: int, group=None, failed: bool = False):
     """In place: each tensor in `grads` (this rank's gradient of the mean over its `count` samples,
     e.g. per-triangle albedo and per-material roughness gradients) becomes the gradient of the mean
     over every rank's samples.  One all-reduce of the concatenated gradients, one of the counts.
-    Collective: all ranks call it in the same order, with the same tensor shapes."""
+    Collective: all ranks call it in the same order, with the same tensor shapes.  failed=True as
+    in reduce_films."""
     import torch
     import torch.distributed as dist
     grads = list(grads)
     if not grads:
         return grads
     flat = torch.cat([g.reshape(-1) for g in grads]).to(torch.float32)
-    total = torch.tensor([float(count)], dtype=torch.float64, device=flat.device)
-    flat.mul_(float(count))
+    counts = _counts(count, failed, flat.device)
+    if failed:
+        flat.zero_()
+    else:
+        flat.mul_(float(count))
     dist.all_reduce(flat, group=group)
-    dist.all_reduce(total, group=group)
-    if total.item() > 0:
-        flat.div_(total.item())
+    dist.all_reduce(counts, group=group)
+    total = _check(counts)
+    if total > 0:
+        flat.div_(total)
     off = 0
     for g in grads:
         n = g.numel()

@@ -32,6 +32,7 @@ import subprocess
 import sys
 import threading
 import time
+import traceback
 
 import numpy as np
 
@@ -521,19 +522,26 @@ def run_ours(args, rank, world, local_rank):
     plain_flat = torch.zeros_like(flat)
     plain_films = [plain_flat[int(offs[k]):int(offs[k + 1])] for k in range(nj)]
 
-    def reduce(buf):
-        if dist:  # every rank rendered the same number of samples of every frame
-            multigpu.reduce_films(buf, 1)
+    def render_and_reduce(buf, render):
+        """This rank's renders, then (several ranks) the film reduction.  A rank whose render fails
+        reports it in the reduction, so every rank raises RankFailure there instead of waiting."""
+        if not dist:
+            return render()
+        try:
+            out, failed = render(), False
+        except RuntimeError:
+            traceback.print_exc()
+            out, failed = [], True
+        multigpu.reduce_films(buf, 1, failed=failed)  # every rank rendered the same sample count
+        return out
 
     def plain_step():
-        sts = [c.render(f, film_device_ptr=p.data_ptr()) for c, f, p in zip(ctxs, frames, plain_films)]
-        reduce(plain_flat)
-        return sts
+        return render_and_reduce(plain_flat, lambda: [c.render(f, film_device_ptr=p.data_ptr())
+                                                      for c, f, p in zip(ctxs, frames, plain_films)])
 
     def batch_step():
-        st = native.render_batch(ctxs, frames, films_device=[p.data_ptr() for p in films])
-        reduce(flat)
-        return [st]
+        return render_and_reduce(flat, lambda: [native.render_batch(ctxs, frames,
+                                                                    films_device=[p.data_ptr() for p in films])])
 
     arms = {"plain": plain_step}
     if batched:

@@ -125,3 +125,83 @@ def test_ranges_cover_the_frame_once():
         multigpu.weak_range(0, 0, 1)
     with pytest.raises(ValueError):
         multigpu.strong_range(4, 2, 2)
+
+
+def _failing_worker(rank, world, port, fail_rank, kind, out_dir):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from axomae_b200 import multigpu
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    try:
+        failed = rank == fail_rank
+        try:
+            if kind == "films":
+                multigpu.reduce_films(torch.full((16,), float("nan") if failed else 1.0), 1, failed=failed)
+            else:
+                multigpu.reduce_gradients([torch.ones(6), torch.ones(2)], 3, failed=failed)
+            outcome = "returned"
+        except multigpu.RankFailure as e:
+            outcome = "raised: %s" % e
+        # the ranks stay in step after the failure: one more reduction succeeds everywhere
+        film = torch.full((4,), float(rank + 1))
+        multigpu.reduce_films(film, 1)
+        with open(os.path.join(out_dir, "rank%d.txt" % rank), "w") as f:
+            f.write("%s\n%s\n" % (outcome, film.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind", ["films", "gradients"])
+def test_failed_rank_raises_on_every_rank(tmp_path, kind):
+    """A rank whose render (or backward) failed reports it in the reduction: every rank raises
+    RankFailure, none waits on a peer, and the next reduction works on all ranks."""
+    import torch.multiprocessing as mp
+    world = 3
+    mp.start_processes(_failing_worker, args=(world, _free_port(), 1, kind, str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    for r in range(world):
+        outcome, film = open(tmp_path / ("rank%d.txt" % r)).read().splitlines()
+        assert outcome.startswith("raised: 1 rank(s)"), outcome
+        assert film == str([2.0] * 4)  # mean of 1, 2, 3
+
+
+def _vanishing_worker(rank, world, port, out_dir):
+    import datetime
+    import time
+    import torch
+    import torch.distributed as dist
+    from axomae_b200 import multigpu
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        os._exit(0)  # the rank is lost between steps, with nothing in flight
+    t0 = time.monotonic()
+    try:
+        multigpu.reduce_films(torch.ones(16), 1)
+        outcome = "returned"
+    except Exception as e:  # the process group reports the lost peer
+        outcome = "raised %s" % type(e).__name__
+    with open(os.path.join(out_dir, "rank0.txt"), "w") as f:
+        f.write("%s\n%.1f\n" % (outcome, time.monotonic() - t0))
+    os._exit(0)  # no destroy_process_group: its peer is gone
+
+
+def test_lost_rank_ends_the_reduction_with_an_error(tmp_path):
+    """A rank that leaves between steps: the survivor's next reduction ends with an error within the
+    process group's short timeout instead of waiting for good."""
+    import multiprocessing
+    ctx = multiprocessing.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_vanishing_worker, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    outcome, secs = open(tmp_path / "rank0.txt").read().splitlines()
+    assert outcome.startswith("raised"), outcome
+    assert float(secs) < 60
