@@ -51,3 +51,14 @@ def test_status_numbering_matches_reference_enum():
     from axomae_b200 import native
     assert native.STATUS[0] == "SUCCESS" and native.STATUS[9] == "SCENE_NOT_PROCESSED"
     assert native.STATUS[15] == "INVALID_ARGUMENT" and native.STATUS[16] == "RENDERER_EXCEPTION"
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """With the library absent the bindings raise at the first call; there is no other path."""
+    from axomae_b200 import native
+    monkeypatch.setattr(native, "_lib", None)
+    monkeypatch.setattr(native, "LIB_PATH", str(tmp_path / "libnova_b200.so"))
+    with pytest.raises(ImportError, match="not built"):
+        native.lib()
+    with pytest.raises(ImportError):
+        native.Context(0)
