@@ -163,14 +163,25 @@ def oracle_scenes(jobs):
     C with the GIL released)."""
     from concurrent.futures import ThreadPoolExecutor
     ob = oracle_module()
-    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+    with ThreadPoolExecutor(max_workers=min(len(jobs), usable_cores())) as ex:
         return list(ex.map(lambda j: ob.OracleScene(j["scene"]), jobs))
+
+
+def usable_cores():
+    """Host cores this process may run on (its CPU affinity, which a container can narrow)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
 
 
 def cpu_sample(jobs, stride, threads=0, oscs=None, films=None):
     """Oracle render of every `stride`-th pixel of every job (all samples): Mrays/s on the host
-    cores, the reference-BVH node visits / triangle tests per ray, and, when GPU films are given,
-    the relative RMSE of those films against the oracle on the sampled pixels."""
+    cores (threads=0: every usable core), the reference-BVH node visits / triangle tests per ray,
+    and, when GPU films are given, the relative RMSE of those films against the oracle on the
+    sampled pixels."""
+    if threads <= 0:
+        threads = usable_cores()
     t0 = time.perf_counter()
     ob = oracle_module()
     if oscs is None:
@@ -195,7 +206,7 @@ def cpu_sample(jobs, stride, threads=0, oscs=None, films=None):
             d = (g - r) / np.maximum(r, 1e-3)
             sq += float((d * d).sum())
             cnt += d.size
-    cores = threads if threads > 0 else os.cpu_count()
+    cores = threads
     return {"mrays": traced / seconds / 1e6, "seconds": seconds, "traced": traced, "pixels": pixels,
             "node_visits_per_ray": nodes / max(1, traced), "tri_tests_per_ray": tris / max(1, traced),
             "cores": cores, "build_s": build_s, "oscs": oscs,
