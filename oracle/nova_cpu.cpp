@@ -35,12 +35,15 @@ static inline float wrap(float uv) {
   return uv;
 }
 
-/* uv2index, TextureContext.h:52-58; uvToPixel = unsigned(coord * dim) (math_texturing.h:19-21). */
+/* uvToPixel, math_texturing.h:19-21: unsigned(coord * dim), the product in float. */
+static inline unsigned uv_to_pixel(float coord, unsigned dim) { return (unsigned)(coord * (float)dim); }
+
+/* uv2index, TextureContext.h:52-58 */
 static inline unsigned uv2index(float t, int dim) {
   float a = std::fabs(t);
   float rem = a - std::floor(a);
   rem = rem == 0 ? a : rem;
-  return (unsigned)(rem * (float)(unsigned)dim);
+  return uv_to_pixel(rem, (unsigned)dim);
 }
 
 /* getPixelFromFormat, NovaTextureInterface.h:60-99 (little-endian byte order r,g,b,a). */
@@ -1286,6 +1289,20 @@ extern "C" void orc_texture_lookup(const orc_texture *t, float u, float v, float
   const Texture tx = texture_from(*t);
   const V4 p = t->u8_pixels ? sample_u8(tx, u, v) : f32pixel(tx, u, v);
   out[0] = p.x, out[1] = p.y, out[2] = p.z, out[3] = p.w;
+}
+
+/* The oracle's restatements of the reference's header-only arithmetic on the texture and
+ * environment path, for the pin against those headers compiled as they are (oracle/_ref):
+ * atan2_approx (math_utils_approx.h:13-40), rgb_uint2float on the bilinear sample's float channels
+ * (math_texturing.h:8-12), uvToPixel (math_texturing.h:19-21). */
+extern "C" void orc_atan2_approx(uint64_t n, const float *y, const float *x, float *out) {
+  for (uint64_t i = 0; i < n; i++) out[i] = atan2_approx(y[i], x[i]);
+}
+extern "C" void orc_rgb_to_unit(uint64_t n, const float *v, float *out) {
+  for (uint64_t i = 0; i < n; i++) out[i] = u8f(v[i]);
+}
+extern "C" void orc_uv_to_pixel(uint64_t n, const float *t, const uint32_t *dim, uint32_t *out) {
+  for (uint64_t i = 0; i < n; i++) out[i] = uv_to_pixel(t[i], dim[i]);
 }
 
 /* Triangle::computeAABB / centroid of every primitive (prim_bounds in bvh.cpp): 6 floats of box

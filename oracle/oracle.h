@@ -5,10 +5,13 @@
  *
  * Parity status: the Sobol direction vectors, the Sobol/Owen sample values and the acos lookup
  * table are pinned against fixtures produced by the reference's own generator scripts
- * (tests/golden/).  Everything downstream (camera, BVH, triangle test, hit record, BSDFs,
- * envmap, integrator) is a restatement of the reference sources cited per function; the
- * reference itself cannot be built here (glm/boost/Embree are empty submodules), so those parts
- * are pinned only by the reference's own property tests and are otherwise "parity unpinned".
+ * (tests/golden/).  The few header-only reference functions that compile without glm (the fast
+ * atan2, the texel conversions, the tile split) are compiled from the reference tree by
+ * ref_pieces.cpp and the restatements below equal them bit for bit.  Everything else downstream
+ * (camera, BVH, triangle test, hit record, BSDFs, envmap, integrator) is a restatement of the
+ * reference sources cited per function; the reference itself cannot be built here (glm/boost/Embree
+ * are empty submodules), so those parts are pinned only by the reference's own property tests and
+ * are otherwise "parity unpinned".
  */
 #pragma once
 #include <stdint.h>
@@ -160,6 +163,10 @@ int32_t orc_dielectric_lobe(const float albedo[3], float eta, float roughness, f
 float orc_box_intersect(const float mn[3], const float mx[3], const float o[3], const float d[3], float dist_min);
 /* One texture lookup: 8-bit bilinear sample or float nearest texel, RGBA (property tests). */
 void orc_texture_lookup(const orc_texture *texture, float u, float v, float out[4]);
+/* Header-only reference arithmetic as the oracle restates it (pinned against oracle/_ref). */
+void orc_atan2_approx(uint64_t n, const float *y, const float *x, float *out);
+void orc_rgb_to_unit(uint64_t n, const float *v, float *out);
+void orc_uv_to_pixel(uint64_t n, const float *t, const uint32_t *dim, uint32_t *out);
 /* Triangle bounds and centroids of every primitive, instance by instance (property tests). */
 void orc_prim_bounds(void *scene, float *boxes, float *centroids);
 /* The frame's tile split: (x0, x1, y0, y1) per tile; returns the tile count, 0 for bad sizes. */

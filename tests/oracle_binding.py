@@ -110,6 +110,9 @@ def lib():
         L.orc_correct_specular_normal.argtypes = [f32p, f32p, f32p, f32p]
         L.orc_cartesian_to_spherical.argtypes = [C.c_uint64, f32p, f32p]
         L.orc_prim_bounds.argtypes = [C.c_void_p, f32p, f32p]
+        L.orc_atan2_approx.argtypes = [C.c_uint64, f32p, f32p, f32p]
+        L.orc_rgb_to_unit.argtypes = [C.c_uint64, f32p, f32p]
+        L.orc_uv_to_pixel.argtypes = [C.c_uint64, f32p, u32p, u32p]
         L.orc_texture_lookup.argtypes = [C.POINTER(OrcTexture), C.c_float, C.c_float, f32p]
         L.orc_box_intersect.argtypes = [f32p, f32p, f32p, f32p, C.c_float]
         L.orc_box_intersect.restype = C.c_float

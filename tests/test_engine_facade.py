@@ -72,3 +72,22 @@ def test_engine_render_matches_c_abi_and_oracle(engine_test, oracle, tmp_path):
     rel = (image[..., :3].astype(np.float64) - ref[..., :3]) / np.maximum(ref[..., :3], 1e-3)
     assert np.isfinite(image).all() and image[..., :3].max() > 0
     assert float(np.sqrt(np.mean(rel * rel))) <= 1e-3
+
+
+def test_api_caller_builds_against_reference_headers_and_here(engine_test):
+    """tests/cpp/api_caller.cpp, a caller of every scene / camera / transform / mesh / material /
+    texture / render-option / render-buffer method and of NovaException, compiles unchanged against
+    the reference's own API headers and against include/nova_b200_api.hpp, runs its checks here,
+    and both builds print the same enum values (ERROR_STATE, integrator flags, texture formats and
+    channels, mesh types, exception bits)."""
+    build = os.path.join(ROOT, "tests", "cpp", "_build")
+    ours = _run(os.path.join(build, "api_caller"))
+    assert "0 failed checks" in ours.stdout
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "tests", "cpp"), "ref"], capture_output=True)
+    ref_exe = os.path.join(build, "api_caller_ref")
+    if not os.path.exists(ref_exe):
+        pytest.skip("the reference's API headers are not here")
+    ref = _run(ref_exe)
+    enum_lines = lambda out: [l for l in out.splitlines() if not l.startswith("api caller")]
+    assert enum_lines(ours.stdout) == enum_lines(ref.stdout)
+    assert len(enum_lines(ref.stdout)) == 5
