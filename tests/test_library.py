@@ -62,3 +62,13 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
         native.lib()
     with pytest.raises(ImportError):
         native.Context(0)
+
+
+def test_c_abi_from_plain_c():
+    """tests/cpp/cabi_caller.c: the header compiles as C99 (-pedantic) and a C program links the
+    library and gets its status codes (no device work)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "tests", "cpp")], check=True)
+    r = subprocess.run([os.path.join(ROOT, "tests", "cpp", "_build", "cabi_caller")], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
