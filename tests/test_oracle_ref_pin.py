@@ -84,3 +84,43 @@ def test_tile_split_matches_reference_header(oracle, pin):
         n = pin.ref_divide_by_tiles(w, h, tw, th, want.ctypes.data_as(C.POINTER(C.c_int32)))
         assert n == tw * th
         np.testing.assert_array_equal(oracle.tile_split(w, h, tw, th), want)
+
+
+def _fixture(pin, shape):
+    """A mesh fixture of the reference's unit tests (geometry_shapes.h), compiled into the pin."""
+    pin.ref_fixture_floats.restype = C.c_int64
+    pin.ref_fixture_indices.restype = C.c_int64
+    out = {}
+    for attr in ("vertices", "normals", "uv", "tangents", "bitangents"):
+        n = pin.ref_fixture_floats(shape.encode(), attr.encode(), None, 0)
+        a = np.zeros(n, np.float32)
+        pin.ref_fixture_floats(shape.encode(), attr.encode(), _p(a, f32p), n)
+        out[attr] = a
+    n = pin.ref_fixture_indices(shape.encode(), None, 0)
+    idx = np.zeros(n, np.uint32)
+    pin.ref_fixture_indices(shape.encode(), _p(idx, u32p), n)
+    out["indices"] = idx
+    return out
+
+
+@pytest.mark.parametrize("shape", ["CUBE", "QUAD", "TRIANGLE"])
+def test_triangle_bounds_on_reference_fixtures(oracle, pin, shape):
+    """TriangleTest.computeAABB / centroid (shape/TriangleTest.cpp:25-62) on the reference's own
+    fixture meshes, every face: the oracle's box is the min / max of the face's vertices and its
+    centroid their mean within 1e-5 (identity transform, as the reference test builds it)."""
+    from axomae_b200 import scenes
+    mesh = _fixture(pin, shape)
+    nv = mesh["vertices"].size // 3
+    for attr in ("normals", "tangents", "bitangents"):  # one record per vertex (CUBE's lists are per face corner)
+        mesh[attr] = mesh[attr][:3 * nv]
+    mesh["uv"] = mesh["uv"][:2 * nv]
+    b = scenes._Builder()
+    b.add(mesh, b.lambert((0.5, 0.5, 0.5)))
+    env = b.tex(scenes.f32_texture(np.ones((2, 2, 4), np.float32)))
+    scene = b.finish(env, scenes.camera((0.0, 0.0, 5.0), (0.0, 0.0, 0.0), 8, 8))
+    boxes, cents = oracle.OracleScene(scene).prim_bounds()
+    tri = mesh["vertices"].reshape(-1, 3)[mesh["indices"].reshape(-1, 3)]
+    assert boxes.shape[0] == tri.shape[0] == mesh["indices"].size // 3
+    np.testing.assert_array_equal(boxes[:, :3], tri.min(axis=1))
+    np.testing.assert_array_equal(boxes[:, 3:], tri.max(axis=1))
+    assert np.abs(cents - tri.mean(axis=1)).max() <= 1e-5
