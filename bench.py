@@ -17,7 +17,8 @@ Metric: Mrays/s = closest-hit rays traced on the device / device render time (CU
 render stream), whole job over all ranks.  `e2e` is the same metric through the C ABI from pinned
 host buffers each step: scene upload + device BVH build + render + film readback.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload batched|heightfield]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload batched|heightfield|instanced]
 
 With N > 1 (torchrun, one rank per GPU) every rank renders its own sample range of every frame
 (frame spp x N in total) and the films are summed with one NCCL all-reduce (weak scaling).
