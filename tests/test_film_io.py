@@ -179,3 +179,57 @@ def test_bake_cli_usage_errors():
     assert r.returncode == 1 and "integers" in r.stderr
     r = subprocess.run([exe, "--bake", "prefilter", "32", "16", "8", "a", "b"], capture_output=True, text=True)
     assert r.returncode == 1 and "only \"irradiance\"" in r.stderr
+
+
+def _rows_strategy():
+    from hypothesis import strategies as st
+    # rows built from runs: (length, value) pieces so long runs, short runs and literals all occur
+    piece = st.tuples(st.integers(1, 140), st.integers(0, 255))
+    return st.tuples(st.integers(8, 300), st.integers(1, 4), st.lists(piece, min_size=1, max_size=12),
+                     st.integers(0, 2**32 - 1))
+
+
+def test_hdr_rle_round_trip_fuzz(oracle):
+    """Random run structures (runs up to 140 bytes, so past the 127-byte packet limit, literals,
+    widths 8..300): the test-side packer's file parses back to the same pixels, flat files too,
+    and the oracle's own writer emits files its parser reads back to the encoder's bytes."""
+    from hypothesis import given, settings, HealthCheck
+
+    @settings(max_examples=60, deadline=None, derandomize=True,
+              suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(_rows_strategy())
+    def check(case):
+        w, h, pieces, seed = case
+        rng = np.random.default_rng(seed)
+        rgbe = np.zeros((h, w, 4), np.uint8)
+        for j in range(h):
+            for k in range(4):
+                plane, x = [], 0
+                order = rng.permutation(len(pieces))
+                while len(plane) < w:
+                    n, v = pieces[order[x % len(pieces)]]
+                    plane += [v] * n if rng.random() < 0.7 else list(rng.integers(0, 256, n))
+                    x += 1
+                rgbe[j, :, k] = plane[:w]
+        # a flat file's first pixel must not read as a run-length row header (2, 2, < 128): a
+        # normalised RGBE pixel never does (its largest mantissa byte is >= 128)
+        rgbe[0, 0, 0] = max(rgbe[0, 0, 0], 128)
+        for rle in (True, False):
+            code, gw, gh, got = ob.hdr_parse(make_file(rgbe, rle=rle))
+            assert (code, gw, gh) == (0, w, h)
+            np.testing.assert_array_equal(got, rgbe)
+
+    check()
+
+
+def test_hdr_writer_output_parses_back(oracle, tmp_path):
+    rng = np.random.default_rng(9)
+    for w, h in ((8, 3), (37, 5), (300, 2), (5, 4)):
+        px = rng.lognormal(0.0, 2.0, (h, w, 4)).astype(np.float32)
+        px[0, : w // 2] = 1.5  # a run
+        base = str(tmp_path / ("img%dx%d" % (w, h)))
+        ob.hdr_write(base, px, w, h, 4)
+        data = open(base + ".hdr", "rb").read()
+        code, gw, gh, got = ob.hdr_parse(data)
+        assert (code, gw, gh) == (0, w, h)
+        np.testing.assert_array_equal(got.reshape(-1, 4), ob.rgbe_encode(px, 4))
