@@ -233,3 +233,50 @@ def test_hdr_writer_output_parses_back(oracle, tmp_path):
         code, gw, gh, got = ob.hdr_parse(data)
         assert (code, gw, gh) == (0, w, h)
         np.testing.assert_array_equal(got.reshape(-1, 4), ob.rgbe_encode(px, 4))
+
+
+def test_hdr_info_header_fuzz(tmp_path):
+    """Random headers (magic lines, extra lines, FORMAT lines, resolution strings with odd spacing,
+    signs and sizes): the library's host-only header parse accepts exactly what the oracle's
+    header rules accept, with the same size.  The body is valid, so only the header decides."""
+    from hypothesis import given, settings, HealthCheck, strategies as st
+    from axomae_b200 import native
+    line = st.sampled_from(["# comment", "EXPOSURE=1.0", "GAMMA=2.2", "FORMAT=32-bit_rle_xyze", "", "x" * 300,
+                            "FORMAT=32-bit_rle_rgbe"])
+    size = st.one_of(st.integers(1, 64), st.integers(-2, 70000))
+    res = st.tuples(st.sampled_from(["-Y", "-Y", "-Y", "+Y", "-X", "Y"]), size, st.sampled_from([" ", " ", "  ", ""]),
+                    st.sampled_from(["+X", "+X", "-X", "X"]), size)
+    lines = st.one_of(st.just(["FORMAT=32-bit_rle_rgbe"]), st.lists(line, max_size=5))
+    case = st.tuples(st.sampled_from(["#?RADIANCE", "#?RADIANCE", "#?RGBE", "#?RADIANCE ", "#?radiance"]), lines, res)
+    counter = [0]
+
+    @settings(max_examples=120, deadline=None, derandomize=True,
+              suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(case)
+    def check(c):
+        first, lines, (ys, h, sp, xs, w) = c
+        head = (first + "\n" + "".join(l + "\n" for l in lines if l) + "\n" + "%s %d%s%s %d\n" % (ys, h, sp, xs, w))
+        body = bytes(4 * 8 * 2)  # enough flat zeros for the smallest valid sizes; larger ones read zeros
+        data = head.encode() + body
+        small = w <= 64 and h <= 64  # the oracle decodes what it accepts: keep its images small
+        code, ow, oh, _ = ob.hdr_parse(data) if small or "-Y" not in ys else (None, 0, 0, None)
+        p = tmp_path / ("h%d.hdr" % counter[0])
+        counter[0] += 1
+        p.write_bytes(data)
+        try:
+            got = native.hdr_info(str(p))
+        except native.NovaError as e:
+            assert e.status == 15
+            got = None
+        if code is None:  # a large image: the oracle is not asked to decode it, only the header matters
+            return
+        assert (got is not None) == (code == 0), (head, code, got)
+        if got is not None:
+            assert got == (ow, oh)
+            accepted[0] += 1
+        else:
+            rejected[0] += 1
+
+    accepted, rejected = [0], [0]
+    check()
+    assert accepted[0] > 0 and rejected[0] > 0
