@@ -146,7 +146,8 @@ typedef struct {
   uint64_t kernels;    /* kernels launched */
 } nova_b200_render_stats;
 
-/* Context lifecycle: DeviceAcceleratorInterface::make (api/device_accelerator_factory.cpp:9) and cleanup. */
+/* Context lifecycle: DeviceAcceleratorInterface::make (api/device_accelerator_factory.cpp:9) and
+ * cleanup (aggregate/device_acceleration_interface.h:25); destroy frees everything the context holds. */
 nova_b200_status nova_b200_create(nova_b200_ctx **ctx, int32_t device);
 nova_b200_status nova_b200_destroy(nova_b200_ctx *ctx);
 
@@ -154,7 +155,7 @@ nova_b200_status nova_b200_destroy(nova_b200_ctx *ctx);
 nova_b200_status nova_b200_upload_scene(nova_b200_ctx *ctx, const nova_b200_scene_desc *scene);
 
 /* Builds the device BVH (binned SAH on the GPU): Engine::buildAcceleration (api/engine.cpp:235)
- * and DeviceAcceleratorInterface::build (aggregate/device_acceleration_interface.h:25). */
+ * and DeviceAcceleratorInterface::build (aggregate/device_acceleration_interface.h:24). */
 nova_b200_status nova_b200_build_bvh(nova_b200_ctx *ctx, const nova_b200_bvh_options *opts);
 
 /* AOV integrators (integrator/NormalIntegrator.cpp, DepthIntegrator.cpp, EmissiveIntegrator.cpp;
@@ -206,7 +207,8 @@ nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b
 nova_b200_status nova_b200_render_noalloc(nova_b200_ctx *ctx, const nova_b200_frame *frame, float *film_device);
 
 /* Closest-hit queries for n world-space rays held in DEVICE memory (3 floats each): the intersector
- * of DeviceIntersectorInterface::traverse / GenericHostAccelerator::hit (aggregate/acceleration_interface.h).
+ * of DeviceIntersectorInterface::traverse (aggregate/device_acceleration_interface.h:14) /
+ * GenericHostAccelerator::hit (aggregate/acceleration_interface.h:29).
  * prim = global primitive index (-1 on miss), t / u / v = Moller-Trumbore distance and barycentrics. */
 nova_b200_status nova_b200_trace(nova_b200_ctx *ctx, uint64_t n, const float *orig_dev, const float *dir_dev,
                                  int32_t *prim_dev, float *t_dev, float *u_dev, float *v_dev);
