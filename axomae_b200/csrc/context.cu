@@ -478,6 +478,13 @@ nova_b200_status nova_b200_create(nova_b200_ctx **out, int32_t device) {
   }
   cudaMemcpy(c->d_sobol, sob.data(), sob.size() * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(c->d_acos, ac.data(), ac.size() * 4, cudaMemcpyHostToDevice);
+  /* the allocation-free render's device memory (its static scratch array and its kernel's local
+   * memory) is taken here, so that nova_b200_render_noalloc itself never allocates */
+  const nova_b200_status st = nb_noalloc_prepare(c);
+  if (st != NOVA_B200_SUCCESS) {
+    nova_b200_destroy(c);
+    return st;
+  }
   *out = c;
   return NOVA_B200_SUCCESS;
 }

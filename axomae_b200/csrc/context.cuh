@@ -115,3 +115,6 @@ nova_b200_status nb_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *idx, con
                           float *out);
 nova_b200_status nb_bake(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh, int32_t ch, int32_t ow,
                          int32_t oh, int32_t samples, float *out);
+/* Defined in render_noalloc.cu: loads the no-alloc kernels' module on the context's device, takes
+ * the scratch array's address and reserves the path kernel's local memory (called at create). */
+nova_b200_status nb_noalloc_prepare(nova_b200_ctx *c);

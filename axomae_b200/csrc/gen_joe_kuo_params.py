@@ -18,7 +18,9 @@ ROWS = 255
 
 
 def main() -> None:
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/scripts/joe_kuo.txt"
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_joe_kuo_params.py <path to joe_kuo.txt>")
+    src = sys.argv[1]
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "joe_kuo_params.inc")
     lines = []
     with open(src) as f:

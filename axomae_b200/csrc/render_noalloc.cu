@@ -4,9 +4,8 @@
  * reserved by another allocator (for example a framework's caching allocator that has claimed the
  * GPU), or a real-time viewport that must not risk a device-wide synchronisation or an allocation
  * failure in the middle of a frame.  This entry point renders with no allocation at all: its only
- * scratch is the file-scope device array below, kNoAllocScratchBytes = 32 MiB, which every GPU that
- * loads the library holds until the process exits.  The caller passes the output film (device
- * memory); the scene and BVH are the ones the context already holds.
+ * scratch is the file-scope device array below, kNoAllocScratchBytes = 32 MiB.  The caller passes
+ * the output film (device memory); the scene and BVH are the ones the context already holds.
  *
  * The scratch holds the radiance of one chunk of paths (pixels x samples, at most
  * kNoAllocPaths = 2 Mi paths): one thread traces one path through every bounce, then a second
@@ -15,9 +14,13 @@
  * keeps the last call's contents.  All calls share the one array, so calls that overlap on the GPU
  * (two contexts, or two streams, rendering at the same time) race on it.
  *
- * Set-up: the first call on a device, with that device current, looks up the array's device address
- * with cudaGetSymbolAddress (the host-side name is only a stand-in, not a device address) and caches
- * it for that device; make that first call before any stream capture.
+ * Set-up happens in nova_b200_create, on the context's device with that device current
+ * (nb_noalloc_prepare below): it makes the CUDA runtime load this file's module (under lazy module
+ * loading the 32 MiB array is only allocated then), looks up the array's device address with
+ * cudaGetSymbolAddress (in host code the array's name is only a stand-in, not a device address),
+ * caches it for that device, and launches the path kernel once over no paths so that the driver
+ * reserves the kernel's per-thread local memory (its traversal stack) at that point too.  After
+ * that a nova_b200_render_noalloc call launches two kernels and allocates nothing.
  *
  * The per-path arithmetic is the same sequence of device functions as the wavefront kernels
  * (integrator.cu), so the film equals nova_b200_render's for the same sample range.
@@ -149,9 +152,12 @@ __global__ void k_resolve_noalloc(const float4 *radiance, Params rp, float *film
       make_float4(a.x / denom, a.y / denom, a.z / denom, a.w / denom);
 }
 
-/* Once per device, with that device current: the scratch array's device address. */
+/* The scratch array's device address on the current device, looked up once per device. */
 nova_b200_status scratch_for_device(nova_b200_ctx *c, float4 **out) {
   if (c->device < 0 || c->device >= kMaxDevices) return nbctx::fail(c, NOVA_B200_INVALID_ARGUMENT, "device id%s");
+  int current = -1;
+  NB_CUDA(c, cudaGetDevice(&current), "cudaGetDevice");
+  if (current != c->device) return nbctx::fail(c, NOVA_B200_RENDERER_EXCEPTION, "no-alloc set-up on the wrong device%s");
   std::lock_guard<std::mutex> lk(g_setup_mutex);
   if (!g_scratch_ptr[c->device]) {
     void *p = nullptr;
@@ -163,7 +169,36 @@ nova_b200_status scratch_for_device(nova_b200_ctx *c, float4 **out) {
   return NOVA_B200_SUCCESS;
 }
 
+/* Makes the caller's current device the context's for one call and restores it on return. */
+struct DeviceScope {
+  int previous = -1;
+  cudaError_t status = cudaSuccess;
+  explicit DeviceScope(int device) {
+    if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+    status = cudaSetDevice(device);
+  }
+  ~DeviceScope() {
+    if (previous >= 0) cudaSetDevice(previous);
+  }
+};
+
 }  // namespace
+
+/* Called by nova_b200_create with the context's device current: module load, scratch address and
+ * the driver's local-memory reservation for the path kernel all happen here, not in a render. */
+nova_b200_status nb_noalloc_prepare(nova_b200_ctx *c) {
+  float4 *scratch = nullptr;
+  nova_b200_status st = scratch_for_device(c, &scratch);
+  if (st != NOVA_B200_SUCCESS) return st;
+  cudaFuncAttributes attr;
+  NB_CUDA(c, cudaFuncGetAttributes(&attr, k_path_noalloc), "no-alloc path kernel");
+  NB_CUDA(c, cudaFuncGetAttributes(&attr, k_resolve_noalloc), "no-alloc resolve kernel");
+  Params none{};  /* n_pix * count = 0: every thread returns before reading the scene */
+  k_path_noalloc<<<1, 128, 0, c->stream>>>(c->scene, none, scratch);
+  NB_CUDA(c, cudaGetLastError(), "no-alloc set-up launch");
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "no-alloc set-up");
+  return NOVA_B200_SUCCESS;
+}
 
 extern "C" nova_b200_status nova_b200_render_noalloc(nova_b200_ctx *c, const nova_b200_frame *f, float *film_device) {
   using namespace nbctx;
@@ -181,7 +216,8 @@ extern "C" nova_b200_status nova_b200_render_noalloc(nova_b200_ctx *c, const nov
   if ((uint64_t)f->sample_count > kNoAllocPaths)
     return fail(c, NOVA_B200_INVALID_ARGUMENT,
                 "sample_count exceeds the no-alloc scratch limit of 2097152 paths per pixel chunk%s");
-  cudaSetDevice(c->device);
+  DeviceScope on_device(c->device);
+  NB_CUDA(c, on_device.status, "cudaSetDevice");
   float4 *scratch = nullptr;
   nova_b200_status st = scratch_for_device(c, &scratch);
   if (st != NOVA_B200_SUCCESS) return st;

@@ -147,7 +147,11 @@ typedef struct {
 } nova_b200_render_stats;
 
 /* Context lifecycle: DeviceAcceleratorInterface::make (api/device_accelerator_factory.cpp:9) and
- * cleanup (aggregate/device_acceleration_interface.h:25); destroy frees everything the context holds. */
+ * cleanup (aggregate/device_acceleration_interface.h:25); destroy frees everything the context holds.
+ * create also loads the allocation-free render's kernels on that device, which takes their static
+ * 32 MiB scratch array and the path kernel's local memory once per device (see
+ * nova_b200_render_noalloc).  Entry points make the context's device current and leave it so, except
+ * nova_b200_render_noalloc, which restores the caller's current device. */
 nova_b200_status nova_b200_create(nova_b200_ctx **ctx, int32_t device);
 nova_b200_status nova_b200_destroy(nova_b200_ctx *ctx);
 
@@ -197,13 +201,18 @@ nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b
                                         nova_b200_render_stats *stats);
 
 /* Allocation-free variant of nova_b200_render, for callers that cannot call cudaMalloc during a
- * frame (device memory fully reserved by another allocator, or a real-time loop that must not risk
- * an allocation or a device-wide synchronisation).  No counterpart in the reference.  Renders
+ * frame: a host loop whose device memory is entirely reserved by another allocator (a framework's
+ * caching allocator that has claimed the GPU), or a real-time loop that must not risk an allocation
+ * failure or a device-wide synchronisation mid-frame.  No counterpart in the reference.  Renders
  * samples [sample_begin, sample_begin + sample_count) of every pixel and writes their mean RGBA
  * to film_device (width*height*4 floats, device memory); the context's accumulation film and
  * frame->reset are not used.  Its only scratch is a static 32 MiB device array shared by every
- * call, so calls that overlap on the GPU race.  sample_count is limited to 2097152.  The first
- * call on a device looks up the array's address; make it before any stream capture. */
+ * call, so calls that overlap on the GPU race; sample_count is limited to 2097152 and larger
+ * values are rejected with INVALID_ARGUMENT.  The array, the kernels and the path kernel's local
+ * memory are all taken by nova_b200_create on the context's device, so this call allocates
+ * nothing.  It runs on the context's stream and returns after that stream has finished: the caller
+ * must finish its own work on film_device (on any other stream) before the call.  The caller's
+ * current device is restored on return. */
 nova_b200_status nova_b200_render_noalloc(nova_b200_ctx *ctx, const nova_b200_frame *frame, float *film_device);
 
 /* Closest-hit queries for n world-space rays held in DEVICE memory (3 floats each): the intersector

@@ -19,7 +19,7 @@ Outputs (next to this script):
                                        owen_scramble().
   acos_lut.json       sha256 of the float32 table of generate_acos(500000) plus sample entries.
 
-Usage: python make_golden.py [reference_root]   (default /root/reference)
+Usage: python make_golden.py <reference_root>   (or set AXOMAE_REFERENCE to the reference checkout)
 """
 import ast
 import copy
@@ -46,7 +46,9 @@ def load_functions(path: str) -> dict:
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("AXOMAE_REFERENCE", "")
+    if not ref or not os.path.isdir(os.path.join(ref, "scripts")):
+        sys.exit("usage: make_golden.py <reference_root> (or AXOMAE_REFERENCE=<reference_root>)")
     sob = load_functions(os.path.join(ref, "scripts", "generate_luts_sobol.py"))
     trig = load_functions(os.path.join(ref, "scripts", "generate_luts_trigonometrics.py"))
 
