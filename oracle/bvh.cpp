@@ -170,19 +170,13 @@ void build_bvh(Scene &s) {
   subdivide_all(c, s);
 }
 
-/* Triangle::hit (Triangle.h:146-177): degenerate check, ray to object space, Moller-Trumbore with
- * inv_det computed before the det == 0 test; edges inclusive; no culling. */
-bool triangle_hit(const Scene &s, const Prim &p, const Ray &in, float tmin, float tmax, float &t_out, float &u_out,
-                  float &v_out) {
-  const Mesh &m = s.meshes[s.inst_mesh[p.inst]];
-  const uint32_t *id = &m.idx[3 * p.tri];
-  if (id[0] == id[1] || id[2] == id[1] || id[2] == id[0]) return false;
-  const Xform &x = s.xf[p.inst];
-  const V3 o = xyz(mul(x.inv, V4{in.o.x, in.o.y, in.o.z, 1.f}));
-  const V3 d = xyz(mul(x.inv, V4{in.d.x, in.d.y, in.d.z, 0.f}));
-  V3 v0{m.v[3 * id[0]], m.v[3 * id[0] + 1], m.v[3 * id[0] + 2]};
-  V3 v1{m.v[3 * id[1]], m.v[3 * id[1] + 1], m.v[3 * id[1] + 2]};
-  V3 v2{m.v[3 * id[2]], m.v[3 * id[2] + 1], m.v[3 * id[2] + 2]};
+/* Triangle::hit's intersection (Triangle.h:150-177): ray to object space through the inverse
+ * transform, Moller-Trumbore with inv_det computed before the det == 0 test; edges inclusive; no
+ * culling. */
+bool moller_trumbore(const M4 &inv, V3 v0, V3 v1, V3 v2, const Ray &in, float tmin, float tmax, float &t_out,
+                     float &u_out, float &v_out) {
+  const V3 o = xyz(mul(inv, V4{in.o.x, in.o.y, in.o.z, 1.f}));
+  const V3 d = xyz(mul(inv, V4{in.d.x, in.d.y, in.d.z, 0.f}));
   const V3 e1 = v1 - v0, e2 = v2 - v0;
   const V3 P = cross(d, e2);
   const float det = dot(P, e1);
@@ -200,6 +194,20 @@ bool triangle_hit(const Scene &s, const Prim &p, const Ray &in, float tmin, floa
   u_out = u;
   v_out = v;
   return true;
+}
+
+/* Triangle::hit (Triangle.h:146-177): degenerate check (isDegenerate, :127-132), then the
+ * intersection above. */
+bool triangle_hit(const Scene &s, const Prim &p, const Ray &in, float tmin, float tmax, float &t_out, float &u_out,
+                  float &v_out) {
+  const Mesh &m = s.meshes[s.inst_mesh[p.inst]];
+  const uint32_t *id = &m.idx[3 * p.tri];
+  if (id[0] == id[1] || id[2] == id[1] || id[2] == id[0]) return false;
+  const Xform &x = s.xf[p.inst];
+  const V3 v0{m.v[3 * id[0]], m.v[3 * id[0] + 1], m.v[3 * id[0] + 2]};
+  const V3 v1{m.v[3 * id[1]], m.v[3 * id[1] + 1], m.v[3 * id[1] + 2]};
+  const V3 v2{m.v[3 * id[2]], m.v[3 * id[2] + 1], m.v[3 * id[2] + 2]};
+  return moller_trumbore(x.inv, v0, v1, v2, in, tmin, tmax, t_out, u_out, v_out);
 }
 
 /* iter_traverse, native.cpp:56-114.  Stack of 2048 node pointers; both children slab-tested;

@@ -1283,6 +1283,116 @@ extern "C" int32_t orc_dielectric_lobe(const float albedo[3], float eta, float r
   return ok ? 1 : 0;
 }
 
+/* ---- pin entry points: the oracle's BSDF, triangle and spawn arithmetic on given inputs, held bit
+ * for bit to the reference's own headers compiled in oracle/_ref (tests only). ---- */
+static BsdfParams bsdf_params_of(const orc_bsdf_case &c) {
+  BsdfParams p;
+  p.ns = {c.ns[0], c.ns[1], c.ns[2]};
+  p.ng = {c.ng[0], c.ng[1], c.ng[2]};
+  p.dpdu = {c.dpdu[0], c.dpdu[1], c.dpdu[2]};
+  p.dpdv = {c.dpdv[0], c.dpdv[1], c.dpdv[2]};
+  p.wo_dot_ng = c.wo_dot_ng;
+  p.roughness = c.roughness;
+  p.metal = c.metal;
+  p.transmission = c.transmission;
+  p.anisotropy = c.anisotropy;
+  p.thin = c.thin != 0;
+  p.eta = v3(c.eta);
+  p.albedo = {c.albedo[0], c.albedo[1], c.albedo[2]};
+  return p;
+}
+
+static void store_sample(bool ok, const Sample &smp, orc_bsdf_result &r) {
+  r.f[0] = smp.f.x, r.f[1] = smp.f.y, r.f[2] = smp.f.z;
+  r.wi[0] = smp.wi.x, r.wi[1] = smp.wi.y, r.wi[2] = smp.wi.z;
+  r.pdf = smp.pdf, r.costheta = smp.costheta, r.flags = smp.flags, r.valid = ok ? 1 : 0;
+}
+
+extern "C" void orc_principled_sample(uint64_t n, const orc_bsdf_case *cases, orc_bsdf_result *out) {
+  for (uint64_t i = 0; i < n; i++) {
+    const orc_bsdf_case &c = cases[i];
+    const PrincipledBSDF b(bsdf_params_of(c), c.uc);
+    Sample smp;
+    const bool ok = b.sample_f(V3{c.wo[0], c.wo[1], c.wo[2]}, c.uc, c.u, smp);
+    store_sample(ok, smp, out[i]);
+  }
+}
+
+extern "C" void orc_lobe_sample(int32_t lobe, uint64_t n, const orc_bsdf_case *cases, orc_bsdf_result *out) {
+  for (uint64_t i = 0; i < n; i++) {
+    const orc_bsdf_case &c = cases[i];
+    PrincipledBSDF b;
+    b.params = bsdf_params_of(c);
+    b.lobe_w = c.weight, b.lobe_p = c.probability;
+    b.ggx = VNDF(c.anisotropy, c.roughness);
+    Sample smp;
+    const V3 wo{c.wo[0], c.wo[1], c.wo[2]};
+    bool ok = false;
+    if (lobe == 1) b.lobe = L_DIFFUSE, ok = b.diffuse_sample(wo, c.u, smp);
+    if (lobe == 2) b.lobe = L_SPECULAR, ok = b.specular_sample(wo, c.u, smp);
+    if (lobe == 3) b.lobe = L_DIELECTRIC, ok = b.dielectric_sample(wo, c.uc, c.u, smp);
+    store_sample(ok, smp, out[i]);
+  }
+}
+
+extern "C" void orc_dielectric_eval(uint64_t n, const orc_bsdf_case *cases, const float *wi, float *f, float *pdf) {
+  for (uint64_t i = 0; i < n; i++) {
+    const orc_bsdf_case &c = cases[i];
+    PrincipledBSDF b;
+    b.params = bsdf_params_of(c);
+    b.lobe = L_DIELECTRIC, b.lobe_w = c.weight, b.lobe_p = c.probability;
+    b.ggx = VNDF(c.anisotropy, c.roughness);
+    const V3 wo{c.wo[0], c.wo[1], c.wo[2]}, w{wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
+    const Spec fe = dielectric_f(b, wo, w);
+    f[3 * i] = fe.x, f[3 * i + 1] = fe.y, f[3 * i + 2] = fe.z;
+    pdf[i] = dielectric_pdf(b, wo, w);
+  }
+}
+
+extern "C" void orc_triangle_hits(uint64_t n, const float *tri, const float *inv, const float *o, const float *d,
+                                  float tmin, float tmax, int32_t *hit, float *t, float *u, float *v) {
+  for (uint64_t i = 0; i < n; i++) {
+    const float *q = tri + 9 * i;
+    const M4 m = m4_from(inv + 16 * i);
+    Ray r;
+    r.o = {o[3 * i], o[3 * i + 1], o[3 * i + 2]};
+    r.d = {d[3 * i], d[3 * i + 1], d[3 * i + 2]};
+    float tt = 0.f, uu = 0.f, vv = 0.f;
+    hit[i] = moller_trumbore(m, V3{q[0], q[1], q[2]}, V3{q[3], q[4], q[5]}, V3{q[6], q[7], q[8]}, r, tmin, tmax, tt, uu,
+                             vv)
+                 ? 1
+                 : 0;
+    t[i] = tt, u[i] = uu, v[i] = vv;
+  }
+}
+
+extern "C" void orc_spawn(uint64_t n, const float *wi, const float *nrm, const float *pos, float *out_o, float *out_d) {
+  for (uint64_t i = 0; i < n; i++) {
+    const Ray r = spawn(V3{wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]}, V3{nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]},
+                        V3{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]});
+    out_o[3 * i] = r.o.x, out_o[3 * i + 1] = r.o.y, out_o[3 * i + 2] = r.o.z;
+    out_d[3 * i] = r.d.x, out_d[3 * i + 1] = r.d.y, out_d[3 * i + 2] = r.d.z;
+  }
+}
+
+extern "C" void orc_gram_shmidt(uint64_t n, const float *nrm, const float *tan, const float *bit, float *out) {
+  for (uint64_t i = 0; i < n; i++) {
+    const M3 m = gram_shmidt(V3{nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]}, V3{tan[3 * i], tan[3 * i + 1], tan[3 * i + 2]},
+                             V3{bit[3 * i], bit[3 * i + 1], bit[3 * i + 2]});
+    for (int c = 0; c < 3; c++)
+      for (int k = 0; k < 3; k++) out[9 * i + 3 * c + k] = m.c[c][k];
+  }
+}
+
+extern "C" void orc_make_onb(uint64_t n, const float *nrm, float *out) {
+  for (uint64_t i = 0; i < n; i++) {
+    V3 b1, b2;
+    make_onb(V3{nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]}, b1, b2);
+    const float vals[6] = {b1.x, b1.y, b1.z, b2.x, b2.y, b2.z};
+    std::copy(vals, vals + 6, out + 6 * i);
+  }
+}
+
 /* One texture lookup (property tests): an 8-bit texture through the bilinear sample, a float one
  * through the nearest-texel read; out = RGBA (8-bit channels in 0..255). */
 extern "C" void orc_texture_lookup(const orc_texture *t, float u, float v, float out[4]) {

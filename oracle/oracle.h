@@ -172,6 +172,44 @@ void orc_prim_bounds(void *scene, float *boxes, float *centroids);
 /* The frame's tile split: (x0, x1, y0, y1) per tile; returns the tile count, 0 for bad sizes. */
 int32_t orc_tile_split(int32_t width, int32_t height, int32_t tiles_w, int32_t tiles_h, int32_t *rects);
 
+/* One BSDF query for the pin against the reference's own BxDF / BSDF code (tests only): the
+ * bsdf_params_s fields the path fills (BxDF.h:22-39; eta uniform over RGB), the outgoing direction,
+ * the random numbers, and for a single lobe its weight and probability.  Directions are in world
+ * space for orc_principled_sample and in the local shading frame for the single lobes. */
+typedef struct {
+  float ns[3], ng[3], dpdu[3], dpdv[3];
+  float wo_dot_ng, roughness, metal, transmission, anisotropy, eta;
+  float albedo[3];
+  float wo[3];
+  float uc, u[2];
+  float weight, probability;
+  int32_t thin;
+} orc_bsdf_case;
+/* BSDFSample fields the integrator reads (BxDF_flags.h:26-35) and whether sampling succeeded. */
+typedef struct {
+  float f[3], wi[3];
+  float pdf, costheta;
+  uint32_t flags;
+  int32_t valid;
+} orc_bsdf_result;
+/* PrincipledBSDF(params, uc).sample_f(wo, uc, u) (BSDF.h:87-130). */
+void orc_principled_sample(uint64_t n, const orc_bsdf_case *cases, orc_bsdf_result *out);
+/* One lobe's sample_f in the local frame: lobe 1 DisneyDiffuseBxDF, 2 SpecularBxDF, 3 DielectricBxDF
+ * (BxDF.h:252-594). */
+void orc_lobe_sample(int32_t lobe, uint64_t n, const orc_bsdf_case *cases, orc_bsdf_result *out);
+/* DielectricBxDF::f / ::pdf at wi (3 floats per case) in the local frame (BxDF.h:497-545). */
+void orc_dielectric_eval(uint64_t n, const orc_bsdf_case *cases, const float *wi, float *f, float *pdf);
+/* Triangle::hit's Moller-Trumbore on one triangle per query (Triangle.h:146-177): tri = 9 floats of
+ * object-space vertices, inv = 16 floats (column-major inverse transform), ray in world space;
+ * returns hit flags, t, u, v. */
+void orc_triangle_hits(uint64_t n, const float *tri, const float *inv, const float *o, const float *d, float tmin,
+                       float tmax, int32_t *hit, float *t, float *u, float *v);
+/* Ray::spawn(wi, n, position) (Ray.h:22-27): next origin and direction. */
+void orc_spawn(uint64_t n, const float *wi, const float *nrm, const float *pos, float *out_o, float *out_d);
+/* math::geometry::gram_shmidt and make_onb (utils_3D.h:52-81): 9 floats (T, B, N) / 6 floats (b1, b2). */
+void orc_gram_shmidt(uint64_t n, const float *nrm, const float *tan, const float *bit, float *out);
+void orc_make_onb(uint64_t n, const float *nrm, float *out);
+
 /* Film outputs and the Radiance .hdr format (film_io.cpp). */
 void orc_film_accumulate(const float *partial, float *accum, float *final_buf, uint64_t n, uint32_t frame_index);
 void orc_display_blend(const float *partial, const float *accum, float *out, uint64_t n, uint32_t current_frame);

@@ -111,5 +111,7 @@ void build_bvh(Scene &s);
 void prim_bounds(const Scene &s, const Prim &p, Box &box, V3 &centroid);
 Hit trace(const Scene &s, const Ray &r, TraceCounters *c);
 bool triangle_hit(const Scene &s, const Prim &p, const Ray &r, float tmin, float tmax, float &t, float &u, float &v);
+bool moller_trumbore(const M4 &inv, V3 v0, V3 v1, V3 v2, const Ray &in, float tmin, float tmax, float &t, float &u,
+                     float &v);
 
 }  // namespace orc
