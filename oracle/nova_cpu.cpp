@@ -1087,6 +1087,27 @@ extern "C" void orc_scatter(void *h, uint64_t n, const float *o, const float *d,
   }
 }
 
+/* The hit record scatter() starts from, for the pin of PrincipledMaterial::scatter (tests only). */
+extern "C" void orc_hit_record(void *h, uint64_t n, const float *o, const float *d, const int32_t *prim, const float *t,
+                               const float *u, const float *v, float *out) {
+  const Scene &s = *static_cast<Scene *>(h);
+  for (uint64_t i = 0; i < n; i++) {
+    float *r = out + 23 * i;
+    std::fill(r, r + 23, 0.f);
+    if (prim[i] < 0 || (size_t)prim[i] >= s.prims.size()) continue;
+    Ray ray;
+    ray.o = {o[3 * i], o[3 * i + 1], o[3 * i + 2]};
+    ray.d = {d[3 * i], d[3 * i + 1], d[3 * i + 2]};
+    Hit hit;
+    hit.is_hit = true, hit.prim = prim[i], hit.t = t[i], hit.u = u[i], hit.v = v[i];
+    const HitRecord hr = make_record(s, ray, hit);
+    const V3 vs[4] = {hr.ng, hr.dpdu, hr.dpdv, hr.position};
+    for (int k = 0; k < 4; k++) r[3 * k] = vs[k].x, r[3 * k + 1] = vs[k].y, r[3 * k + 2] = vs[k].z;
+    r[12] = hr.u, r[13] = hr.v;
+    for (int c = 0; c < 3; c++) r[14 + 3 * c] = hr.frame.c[c].x, r[15 + 3 * c] = hr.frame.c[c].y, r[16 + 3 * c] = hr.frame.c[c].z;
+  }
+}
+
 extern "C" int32_t orc_set_diff_params(void *h, const float *albedo, const float *roughness) {
   Scene &s = *static_cast<Scene *>(h);
   if (albedo)

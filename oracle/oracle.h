@@ -210,6 +210,11 @@ void orc_spawn(uint64_t n, const float *wi, const float *nrm, const float *pos, 
 void orc_gram_shmidt(uint64_t n, const float *nrm, const float *tan, const float *bit, float *out);
 void orc_make_onb(uint64_t n, const float *nrm, float *out);
 
+/* The Embree-semantics hit record the oracle builds for a hit (prim, t, u, v) of a ray (embree.cpp:287-412):
+ * 23 floats per hit: ng[3], dpdu[3], dpdv[3], position[3], u, v, shading frame columns T[3], B[3], N[3]. */
+void orc_hit_record(void *h, uint64_t n, const float *o, const float *d, const int32_t *prim, const float *t,
+                    const float *u, const float *v, float *out);
+
 /* Film outputs and the Radiance .hdr format (film_io.cpp). */
 void orc_film_accumulate(const float *partial, float *accum, float *final_buf, uint64_t n, uint32_t frame_index);
 void orc_display_blend(const float *partial, const float *accum, float *out, uint64_t n, uint32_t current_frame);

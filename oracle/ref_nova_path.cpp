@@ -8,10 +8,17 @@
  *   nova/ray/Ray.h              Ray::spawn
  *   internal/common/math/utils_3D.h   gram_shmidt, make_onb
  *   internal/geometry/BoundingBox.cpp BoundingBox::intersect (the traversal's slab test)
+ *   internal/common/math/math_random.h SobolGenerator (gray code, Owen scramble, direction vectors
+ *                               from the header the reference's own generator script writes)
+ *   nova/texturing/NovaTextureInterface.h + TextureContext.h  EnvmapTexture::sample (spherical map,
+ *                               acos table of math_acos_lt.cpp, nearest texel) and ImageTexture<u32>
+ *   nova/material/NovaMaterials.h  PrincipledMaterial::scatter (texture pack, normal map, channel
+ *                               mapping, specular-normal correction, sampler dimensions), with
+ *                               nova/sampler/Sampler.h's SobolSampler
  * Those headers need glm, an empty submodule in the reference tree; oracle/glm_shim stands in for
  * it with glm's evaluation order.  The float transcendentals they call come from ref_libm.cpp
  * (correctly rounded, the oracle's and the device's convention).  The entry points below take the
- * same inputs as the oracle's orc_* pin functions, and tests/test_oracle_ref_pin.py compares the two
+ * same inputs as the oracle's orc_* pin functions, and tests/test_oracle_ref_pin_path.py compares the two
  * bit for bit.  No reference code is copied: it is compiled where it lies. */
 #include <cstdint>
 #include <cstring>
@@ -20,9 +27,14 @@
 #include <internal/common/math/utils_3D.h>
 #include <internal/geometry/BoundingBox.h>
 #include <internal/geometry/Object3D.h>
+#include <internal/common/math/math_random.h>
 #include <material/BSDF.h>
 #include <material/BxDF.h>
 #include <material/BxDF_math.h>
+#include <material/NovaMaterials.h>
+#include <sampler/Sampler.h>
+#include <texturing/NovaTextureInterface.h>
+#include <texturing/TextureContext.h>
 #include <ray/Ray.h>
 #include <shape/MeshContext.h>
 #include <shape/Triangle.h>
@@ -203,4 +215,115 @@ extern "C" void ref_vndf(uint64_t n, const float *aniso, const float *rough, con
 extern "C" void ref_correct_specular_normal(uint64_t n, const float *ng, const float *wo, const float *ns, float *out) {
   for (uint64_t i = 0; i < n; i++)
     put3(out + 3 * i, bsdf::correct_specular_shading_normal(v3(ng + 3 * i), v3(wo + 3 * i), v3(ns + 3 * i)));
+}
+
+/* SobolGenerator(seed).generate(index, dim), math_random.h:73-98. */
+extern "C" void ref_sobol(uint64_t n, const uint32_t *index, const uint32_t *dim, uint32_t seed, float *out) {
+  const math::random::SobolGenerator gen(seed);
+  for (uint64_t i = 0; i < n; i++) out[i] = gen.generate(index[i], dim[i]);
+}
+
+namespace {
+
+/* The scene's textures as the reference's texture context sees them: one 8-bit and one float slot per
+ * texture index (the unused one left empty), the CPU fetch path (no interop). */
+struct TextureSet {
+  std::vector<U32Texture> u32;
+  std::vector<F32Texture> f32;
+  nova::texturing::TextureCtx ctx;
+  explicit TextureSet(const orc_texture *tex, uint32_t n) : u32(n), f32(n), ctx(make(tex, n)) {}
+
+  nova::texturing::TextureBundleViews make(const orc_texture *tex, uint32_t n) {
+    for (uint32_t k = 0; k < n; k++) {
+      const orc_texture &t = tex[k];
+      const size_t texels = (size_t)t.width * t.height;
+      U32Texture &a = u32[k];
+      F32Texture &b = f32[k];
+      a.width = b.width = (uint32_t)t.width;
+      a.height = b.height = (uint32_t)t.height;
+      a.channels = b.channels = (uint32_t)t.channels;
+      a.is_rgba = b.is_rgba = t.is_rgba != 0;
+      a.invert_u = b.invert_u = t.invert_u != 0;
+      a.invert_v = b.invert_v = t.invert_v != 0;
+      if (t.u8_pixels) a.raw_data = axstd::span<const uint32_t>(t.u8_pixels, texels);
+      if (t.f32_pixels) b.raw_data = axstd::span<const float>(t.f32_pixels, texels * t.channels);
+    }
+    nova::texturing::u32tex_shared_views_s uv{};
+    uv.managed_tex_view = CstU32ImgTexView(u32.data(), u32.size());
+    nova::texturing::f32tex_shared_views_s fv{};
+    fv.managed_tex_view = CstF32ImgTexView(f32.data(), f32.size());
+    return nova::texturing::TextureBundleViews(uv, fv);
+  }
+};
+
+}  // namespace
+
+/* EnvmapTexture(envmap).sample for n directions (NovaTextureInterface.h:152-174): 4 floats each. */
+extern "C" void ref_env_sample(const orc_texture *tex, uint32_t n_tex, int32_t envmap, uint64_t n, const float *dirs,
+                               float *out) {
+  const TextureSet set(tex, n_tex);
+  const nova::texturing::EnvmapTexture env((std::size_t)envmap);
+  nova::texturing::texture_data_aggregate_s data{};
+  data.texture_ctx = &set.ctx;
+  for (uint64_t i = 0; i < n; i++) {
+    data.geometric_data.sampling_vector = v3(dirs + 3 * i);
+    const glm::vec4 p = env.sample(0.f, 0.f, data);
+    for (int k = 0; k < 4; k++) out[4 * i + k] = p[k];
+  }
+}
+
+/* PrincipledMaterial::scatter (NovaMaterials.h:89-137) from a hit record (23 floats, as
+ * orc_hit_record writes it) and the incoming direction, with a SobolSampler at (index, 2 + 4 * bounce)
+ * (the integrator's dimension schedule), then Ray::spawn and the integrator's path weight
+ * f * costheta / pdf (Integrator.cpp:80-87).  Outputs as orc_scatter. */
+extern "C" void ref_material_scatter(uint64_t n, const float *records, const float *dirs, const uint32_t *material,
+                                     const orc_material *mats, uint32_t n_mats, const orc_texture *tex, uint32_t n_tex,
+                                     const uint32_t *index, const int32_t *bounce, uint32_t seed, float *out_o,
+                                     float *out_d, float *weight, float *emissive, int32_t *valid) {
+  const TextureSet set(tex, n_tex);
+  std::vector<nova::texturing::ImageTexture<uint32_t>> images(n_tex);
+  for (uint32_t k = 0; k < n_tex; k++) images[k] = nova::texturing::ImageTexture<uint32_t>(k);
+  auto handle = [&](int32_t k) {
+    return k >= 0 ? nova::texturing::NovaTextureInterface(&images[k]) : nova::texturing::NovaTextureInterface();
+  };
+  std::vector<nova::material::PrincipledMaterial> materials;
+  for (uint32_t m = 0; m < n_mats; m++) {
+    nova::material::texture_pack pack{};
+    pack.albedo = handle(mats[m].albedo);
+    pack.metallic = handle(mats[m].metallic);
+    pack.normalmap = handle(mats[m].normalmap);
+    pack.emissive = handle(mats[m].emissive);
+    float eta[3] = {mats[m].eta[0], mats[m].eta[1], mats[m].eta[2]}, k[3] = {mats[m].k[0], mats[m].k[1], mats[m].k[2]};
+    materials.emplace_back(pack, eta, k, mats[m].anisotropy);
+  }
+  nova::texturing::texture_data_aggregate_s aggregate{};
+  aggregate.texture_ctx = &set.ctx;
+  nova::material::shading_data_s shading{};
+  shading.texture_aggregate = &aggregate;
+  StackAllocator allocator;
+  for (uint64_t i = 0; i < n; i++) {
+    const float *r = records + 23 * i;
+    nova::intersection_record_s hit{};
+    hit.geometry.ng = v3(r);
+    hit.geometry.dpdu = v3(r + 3);
+    hit.geometry.dpdv = v3(r + 6);
+    hit.geometry.position = v3(r + 9);
+    hit.geometry.u = r[12], hit.geometry.v = r[13];
+    hit.shading.frame = IntersectFrame(glm::mat3(v3(r + 14), v3(r + 17), v3(r + 20)));
+    nova::sampler::SobolSampler<math::random::SobolGenerator> sobol{math::random::SobolGenerator(seed)};
+    nova::sampler::SamplerInterface sampler(&sobol);
+    sampler.reset(index[i]);
+    for (int k = 0; k < 2 + 4 * bounce[i]; k++) sampler.next1D();
+    const nova::Ray in(glm::vec3(0.f), v3(dirs + 3 * i));
+    material_record_s rec{};
+    allocator.reset();
+    const bool ok = materials[material[i]].scatter(in, hit, rec, sampler, allocator, shading);
+    const nova::Ray next = nova::Ray::spawn(rec.lobe.wi, hit.geometry.ng, hit.geometry.position);
+    const nova::Spectrum w = rec.lobe.pdf_cosine_weighted ? rec.attenuation / rec.lobe.pdf
+                                                          : rec.attenuation * rec.lobe.costheta / rec.lobe.pdf;
+    put3(out_o + 3 * i, next.origin);
+    put3(out_d + 3 * i, next.direction);
+    for (int k = 0; k < 3; k++) weight[3 * i + k] = w[k], emissive[3 * i + k] = rec.emissive[k];
+    valid[i] = ok ? 1 : 0;
+  }
 }

@@ -162,6 +162,33 @@ def options(width, height, spp, max_depth, seed=0, index_mode=0, rr_start=-1, th
     return OrcOptions(width, height, spp, max_depth, seed, index_mode, rr_start, threads, tile, vertical_invert)
 
 
+def material_table(scene: dict):
+    """The scene's materials as an orc_material array."""
+    mats = (OrcMaterial * len(scene["materials"]))()
+    for i, m in enumerate(scene["materials"]):
+        mats[i] = OrcMaterial(m.get("albedo", -1), m.get("metallic", -1), m.get("normalmap", -1),
+                              m.get("emissive", -1), (C.c_float * 3)(*m.get("eta", (0, 0, 0))),
+                              (C.c_float * 3)(*m.get("k", (0, 0, 0))), m.get("anisotropy", 0.0))
+    return mats
+
+
+def texture_table(scene: dict):
+    """The scene's textures as an orc_texture array, and the pixel arrays it points into."""
+    texs = (OrcTexture * len(scene["textures"]))()
+    keep = []
+    for i, t in enumerate(scene["textures"]):
+        if t["format"] == "u8":
+            px = np.ascontiguousarray(t["pixels"], np.uint32)
+            texs[i] = OrcTexture(_p(px, u32p), None, t["width"], t["height"], t.get("channels", 4),
+                                 int(t.get("is_rgba", 1)), int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+        else:
+            px = np.ascontiguousarray(t["pixels"], np.float32)
+            texs[i] = OrcTexture(None, _p(px, f32p), t["width"], t["height"], t.get("channels", 4),
+                                 int(t.get("is_rgba", 1)), int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
+        keep.append(px)
+    return texs, keep
+
+
 class OracleScene:
     """Builds the oracle's scene + reference binary SAH BVH from a scene dictionary
     (see axomae_b200.scenes for the layout)."""
@@ -182,22 +209,8 @@ class OracleScene:
             n = np.asarray(x["n"], np.float32).reshape(9)
             insts[i] = OrcInstance(x["mesh"], x["material"], (C.c_float * 16)(*m), (C.c_float * 16)(*inv),
                                    (C.c_float * 9)(*n))
-        mats = (OrcMaterial * len(scene["materials"]))()
-        for i, m in enumerate(scene["materials"]):
-            mats[i] = OrcMaterial(m.get("albedo", -1), m.get("metallic", -1), m.get("normalmap", -1),
-                                  m.get("emissive", -1), (C.c_float * 3)(*m.get("eta", (0, 0, 0))),
-                                  (C.c_float * 3)(*m.get("k", (0, 0, 0))), m.get("anisotropy", 0.0))
-        texs = (OrcTexture * len(scene["textures"]))()
-        for i, t in enumerate(scene["textures"]):
-            if t["format"] == "u8":
-                px = np.ascontiguousarray(t["pixels"], np.uint32)
-                texs[i] = OrcTexture(_p(px, u32p), None, t["width"], t["height"], t.get("channels", 4),
-                                     int(t.get("is_rgba", 1)), int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
-            else:
-                px = np.ascontiguousarray(t["pixels"], np.float32)
-                texs[i] = OrcTexture(None, _p(px, f32p), t["width"], t["height"], t.get("channels", 4),
-                                     int(t.get("is_rgba", 1)), int(t.get("invert_u", 0)), int(t.get("invert_v", 0)))
-            self._keep.append(px)
+        mats, texs, keep = material_table(scene), *texture_table(scene)
+        self._keep += keep
         sc = OrcScene(meshes, len(scene["meshes"]), insts, len(scene["instances"]), mats, len(scene["materials"]),
                       texs, len(scene["textures"]), scene["envmap"],
                       (C.c_float * 16)(*np.asarray(scene["inv_P"], np.float32).reshape(16)),

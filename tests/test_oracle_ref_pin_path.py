@@ -350,3 +350,142 @@ def test_glibc_transcendentals_move_few_samples(pin, orc):
     fin = np.isfinite(fw).all(axis=1) & np.isfinite(fg).all(axis=1)  # non-finite f: DENANed by the path
     rel = np.abs(fw[fin] - fg[fin]) / np.maximum(np.abs(fg[fin]), 1e-30)
     assert np.quantile(rel, 0.999) < 1e-5
+
+
+def _lib_pin_extra(pin):
+    u32p = C.POINTER(C.c_uint32)
+    pin.ref_sobol.argtypes = [C.c_uint64, u32p, u32p, C.c_uint32, f32p]
+    pin.ref_env_sample.argtypes = [vp, C.c_uint32, C.c_int32, C.c_uint64, f32p, f32p]
+    pin.ref_material_scatter.argtypes = [C.c_uint64, f32p, f32p, u32p, vp, C.c_uint32, vp, C.c_uint32, u32p, i32p,
+                                         C.c_uint32, f32p, f32p, f32p, f32p, i32p]
+    return u32p
+
+
+@pytest.mark.parametrize("seed", [0, 0xDEADBEEF, 12345])
+def test_sobol_generator_matches_reference(pin, oracle, seed):
+    """SobolGenerator(seed).generate(index, dim) (math_random.h:37-98) with the direction-vector table
+    the reference's generator script writes, for every dimension the path uses and indices up to 2^32-2."""
+    u32p = _lib_pin_extra(pin)
+    rng = np.random.default_rng(180)
+    n = 300000
+    idx = np.concatenate([np.arange(4096, dtype=np.uint32), rng.integers(0, 2 ** 32 - 1, n - 4096, dtype=np.uint32)])
+    idx[-3:] = [2 ** 32 - 2, 2 ** 31, 2 ** 31 - 1]
+    dim = rng.integers(0, 255, n).astype(np.uint32)
+    want, got = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    pin.ref_sobol(n, _p(idx, u32p), _p(dim, u32p), seed, _p(want))
+    oracle.lib().orc_sobol_samples(_p(idx, u32p), _p(dim, u32p), n, seed, _p(got))
+    assert _same(want, got).all()
+
+
+def test_env_lookup_matches_reference(pin, oracle):
+    """EnvmapTexture::sample (NovaTextureInterface.h:152-174): cartesianToSpherical with the fast
+    atan2 and the acos table of math_acos_lt.cpp, sphericalToUv, wrap, the nearest-texel float fetch
+    (TextureContext.h:196-223), on a 2048 x 1024 map, incl. the poles and the seam."""
+    _lib_pin_extra(pin)
+    rng = np.random.default_rng(190)
+    h, w = 1024, 2048
+    px = rng.lognormal(0.0, 1.5, (h, w, 4)).astype(np.float32)
+    scene = {"textures": [{"format": "f32", "pixels": px, "width": w, "height": h, "channels": 4}]}
+    texs, keep = oracle.texture_table(scene)
+    n = 200000
+    d = _unit(rng, n)
+    d[:6] = [[0, 1, 0], [0, -1, 0], [0, 0, -1], [0, 0, 1], [-1, 0, 0], [1e-8, 0.3, -1]]
+    d[6:1000] *= rng.uniform(0.1, 10, (994, 1)).astype(np.float32)  # not normalised
+    want, got = np.zeros((n, 4), np.float32), np.zeros((n, 4), np.float32)
+    pin.ref_env_sample(C.cast(texs, vp), 1, 0, n, _p(d), _p(want))
+    oracle.lib().orc_env_sample(_p(px), w, h, 4, n, _p(d), _p(got))
+    assert _same(want, got).all()
+
+
+def _scatter_scene():
+    """40 small spheres and boxes on a tessellated ground, materials cycling through Lambert, GGX
+    conductor, GGX dielectric and Burley diffuse; every third with a bumpy normal map, every fourth
+    emissive."""
+    from axomae_b200 import scenes
+    rng = np.random.default_rng(41)
+    b = scenes._Builder()
+    b.add(scenes.grid_quad(30.0, 16), b.lambert((0.6, 0.6, 0.6)))
+    for i in range(40):
+        kind = i % 4
+        if kind == 0:
+            mat = b.lambert(rng.uniform(0.1, 0.9, 3))
+        elif kind == 1:
+            mat = b.conductor(rng.uniform(0.5, 1.0, 3), rng.uniform(0.0, 0.8))
+        elif kind == 2:
+            mat = b.dielectric(rng.uniform(0.0, 0.5))
+        else:
+            mat = b.burley(rng.uniform(0.1, 0.9, 3), rng.uniform(0.2, 1.0))
+        c = np.array([rng.uniform(-8, 8), rng.uniform(0.5, 2.5), rng.uniform(-8, 8)])
+        mesh = (scenes.uv_sphere(c, rng.uniform(0.4, 1.2), 16, 8) if rng.uniform() < 0.6
+                else scenes.box(c, rng.uniform(0.3, 1.0, 3), scenes.random_rotation(rng)))
+        b.add(mesh, mat)
+    mats = b.materials
+    for i, m in enumerate(mats):
+        if i % 4 == 1:
+            m["emissive"] = b.tex(scenes.solid_u8(rng.uniform(0.2, 1.0, 3)))
+        if i % 3 == 2:
+            nm = np.concatenate([rng.integers(90, 166, (8, 8, 2)), rng.integers(200, 256, (8, 8, 1)),
+                                 np.full((8, 8, 1), 255)], -1).astype(np.uint8)
+            m["normalmap"] = b.tex(scenes.u8_texture(nm))
+    env = np.concatenate([rng.lognormal(0.0, 1.0, (64, 128, 3)), np.ones((64, 128, 1))], -1).astype(np.float32)
+    return b.finish(b.tex(scenes.f32_texture(env)), scenes.camera((0.0, 10.0, 18.0), (0.0, 0.0, 0.0), 64, 48))
+
+
+def test_material_scatter_matches_reference(pin, oracle):
+    """PrincipledMaterial::scatter (NovaMaterials.h:89-137) on traced hits of a mixed Lambert / GGX
+    conductor / dielectric scene with normal maps and emissive textures: the textures through
+    ImageTexture<u32>'s bilinear CPU fetch, roughness = metallic.g and metal = .b, transmission when eta
+    is set and k is not, the sampler's dimension order (uc, u0, u1, then uc again after the
+    specular-normal correction) from a SobolSampler at the integrator's dimension 2 + 4 * bounce, then
+    Ray::spawn and the path weight f * costheta / pdf.  The hit record (Embree semantics, the one step
+    whose reference code needs Embree) comes from the oracle and is fed to both."""
+    u32p = _lib_pin_extra(pin)
+    scene = _scatter_scene()
+    osc = oracle.OracleScene(scene)
+    lib = oracle.lib()
+    lib.orc_hit_record.argtypes = [vp, C.c_uint64, f32p, f32p, i32p, f32p, f32p, f32p, f32p]
+    rng = np.random.default_rng(200)
+    W, H = 64, 48
+    opt = oracle.options(W, H, 4, 6)
+    n = 60000
+    px, py, ps = rng.integers(0, W, n), rng.integers(0, H, n), rng.integers(0, 4, n)
+    o, d = osc.camera_rays(opt, px, py, ps)
+    # second half: random rays from above the scene, so grazing and backface hits are in the mix
+    o[n // 2:] = rng.uniform(-8, 8, (n - n // 2, 3)).astype(np.float32) + np.float32([0, 6, 0])
+    d[n // 2:] = _unit(rng, n - n // 2)
+    prim, t, u, v, _ = osc.trace(o, d)
+    keep = prim >= 0
+    o, d, prim, t, u, v = o[keep], d[keep], prim[keep], t[keep], u[keep], v[keep]
+    m = prim.size
+    assert m > 20000
+    # material of each primitive: primitives are numbered instance by instance
+    tri_counts = [np.asarray(scene["meshes"][x["mesh"]]["indices"]).size // 3 for x in scene["instances"]]
+    first = np.cumsum([0] + tri_counts)
+    inst = np.searchsorted(first, prim, side="right") - 1
+    mat_of = np.array([x["material"] for x in scene["instances"]], np.uint32)[inst]
+    index = rng.integers(0, 2 ** 31, m).astype(np.uint32)
+    bounce = rng.integers(0, 8, m).astype(np.int32)
+    seed = 7
+    rec = np.zeros((m, 23), np.float32)
+    lib.orc_hit_record(osc.h, m, _p(o), _p(d), _p(prim, i32p), _p(t), _p(u), _p(v), _p(rec))
+    outs_ref = [np.zeros((m, 3), np.float32) for _ in range(4)] + [np.zeros(m, np.int32)]
+    mats = oracle.material_table(scene)
+    texs, keep_px = oracle.texture_table(scene)
+    pin.ref_material_scatter(m, _p(rec), _p(d), _p(mat_of, u32p), C.cast(mats, vp), len(scene["materials"]),
+                             C.cast(texs, vp), len(scene["textures"]), _p(index, u32p), _p(bounce, i32p), seed,
+                             *[_p(a) for a in outs_ref[:4]], _p(outs_ref[4], i32p))
+    no, nd, w, e, ok = osc.scatter(o, d, prim, t, u, v, index, bounce, seed=seed)
+    assert (ok == outs_ref[4]).all(), np.flatnonzero(ok != outs_ref[4])[:10]
+    valid = ok == 1
+    assert 0.5 < valid.mean() < 1.0
+    for got, want in zip((no, nd, w), outs_ref[:3]):
+        assert _same(got[valid], want[valid]).all()
+    assert _same(e, outs_ref[3]).all()
+    # every material feature is exercised: emissive, normal-mapped, dielectric (eta set, k not)
+    mm = scene["materials"]
+    feats = {"emissive": [x.get("emissive", -1) >= 0 for x in mm],
+             "normalmap": [i % 3 == 2 for i in range(len(mm))],
+             "dielectric": [any(x.get("eta", (0, 0, 0))) and not any(x.get("k", (0, 0, 0))) for x in mm]}
+    for name, flag in feats.items():
+        assert np.asarray(flag)[mat_of].sum() > 100, name
+    assert (e.max(axis=1) > 0).sum() > 100
