@@ -23,8 +23,9 @@ host buffers each step: scene upload + device BVH build + render + film readback
 With N > 1 (torchrun, one rank per GPU) every rank renders its own sample range of every frame
 (frame spp x N in total) and the films are summed with one NCCL all-reduce (weak scaling).
 --impl reference times the CPU implementation of the path (the oracle restatement of the
-reference's CPU Nova path; the reference itself cannot be built) on the host cores on a bounded
-pixel sample of the same workload.
+reference's CPU Nova path; the reference itself cannot be built as a whole) on the host cores: whole
+frames of one sample per pixel, the reference's tiles and worker pool, each job's frame time
+extrapolated to its spp (8 jobs per step, rotating); the instanced workload on a pixel subset.
 """
 import argparse
 import json
@@ -214,46 +215,126 @@ def cpu_sample(jobs, stride, threads=0, oscs=None, films=None):
             "rel_rmse": float(np.sqrt(sq / cnt)) if cnt else None}
 
 
-def cpu_stride(workload, kind):
+def cpu_frames(jobs, subset=None, threads=0, oscs=None):
+    """The reference's own frame loop on whole frames: one frame of one sample per pixel of each job in
+    `subset` (all jobs by default), every pixel in the reference's 20x20 tiles on a worker pool of
+    every usable core, the running-mean film.  Every frame of a job costs the same in expectation
+    (only the sample index differs), so each job's frame is extrapolated to its spp: Mrays/s =
+    sum(rays_j * spp_j) / sum(seconds_j * spp_j), the full workload's rate.  Returns per-job
+    (rays, seconds, node visits, triangle tests, pixels), so that rotating subsets (the reference
+    arm's steps) add up to the same estimate."""
+    if threads <= 0:
+        threads = usable_cores()
+    ob = oracle_module()
+    if oscs is None:
+        oscs = oracle_scenes(jobs)
+    subset = range(len(jobs)) if subset is None else subset
+    per_job = {}
+    for k in subset:
+        j = jobs[k]
+        W, H = j["width"], j["height"]
+        opt = ob.options(W, H, 1, j["depth"], seed=0, rr_start=j["rr_start"], threads=threads)
+        _, st = oscs[k].render(opt)
+        per_job[k] = (st.traced, st.seconds, st.node_visits, st.tri_tests, W * H)
+    return per_job
+
+
+def frames_rate(jobs, per_job, threads):
+    """Full-workload estimate from per-job whole-frame timings (see cpu_frames)."""
+    rays = sum(v[0] * jobs[k]["spp"] for k, v in per_job.items())
+    secs = sum(v[1] * jobs[k]["spp"] for k, v in per_job.items())
+    nodes = sum(v[2] * jobs[k]["spp"] for k, v in per_job.items())
+    tris = sum(v[3] * jobs[k]["spp"] for k, v in per_job.items())
+    return {"mrays": rays / secs / 1e6, "seconds": sum(v[1] for v in per_job.values()),
+            "traced": sum(v[0] for v in per_job.values()), "pixels": sum(v[4] for v in per_job.values()),
+            "node_visits_per_ray": nodes / max(1, rays), "tri_tests_per_ray": tris / max(1, rays),
+            "cores": threads, "jobs_timed": len(per_job)}
+
+
+def cpu_sampling(workload):
+    """How the CPU legs sample the workload: whole frames, except the instanced scene, whose
+    reference BVH leaves one 5.25 M-triangle leaf (a CPU ray costs ~5 M triangle tests), where a
+    pixel subset is all that fits in a bounded sample."""
+    return "pixels" if workload == "instanced" else "frames"
+
+
+def frames_sample_text(jobs, threads):
+    return ("oracle (CPU restatement of the reference Nova path) rendering whole frames the way the reference does: "
+            "one frame of 1 sample per pixel per job, 20x20 tiles on a pool of %d workers, running-mean film; each "
+            "job's frame time extrapolated to its spp (sum rays*spp / sum seconds*spp over %d jobs)" % (threads, len(jobs)))
+
+
+def cpu_stride(workload):
+    """Pixel stride of the pixel-subset sample (the instanced workload's CPU timing and, for the
+    others, the untimed film-vs-oracle check)."""
     env = os.environ.get("NOVA_BENCH_CPU_STRIDE")
     if env:
         return int(env)
-    # baseline sample (our arm, once): about 10-30 s of oracle work on a 16-core host;
-    # reference arm: a few seconds per step
-    if workload == "heightfield":
-        return 2 if kind == "baseline" else 8
     if workload == "instanced":
         # the reference builder leaves this scene in one 5.25 M-triangle leaf (its SAH starts from
         # (float)INT_MAX and no split of a node this large scores below it), so a CPU ray costs
         # ~5 M triangle tests
-        return 12288 if kind == "baseline" else 49152
-    return 16 if kind == "baseline" else 64
+        return 49152
+    if workload == "heightfield":
+        return 16
+    return 64
+
+
+CONFIG_L2 = "inputs larger than L2 (no flush): the scenes' triangles and BVHs exceed the 126 MB L2"
+
+
+def bench_config(workload, nj):
+    """The config both arms print (identical, so the two lines describe the same workload)."""
+    return {"workload": workload, "jobs": nj, "l2": CONFIG_L2}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     jobs = make_jobs(args.workload)
-    stride = cpu_stride(args.workload, "reference")
     oscs = oracle_scenes(jobs)
-    for _ in range(min(args.warmup, 1)):
-        cpu_sample(jobs, stride * 4, oscs=oscs)
-    vals, secs = [], []
-    last = None
-    for _ in range(args.steps):
-        last = cpu_sample(jobs, stride, oscs=oscs)
-        vals.append(last["mrays"])
-        secs.append(last["seconds"])
-    v = float(np.median(vals))
+    threads = usable_cores()
     metric = {"heightfield": HF_METRIC, "instanced": IN_METRIC}.get(args.workload, BATCH_METRIC)
     workload = {"heightfield": HF_WORKLOAD, "instanced": IN_WORKLOAD}.get(args.workload, BATCH_WORKLOAD)
-    sample = ("oracle (CPU restatement of the reference Nova path, thread pool of %d workers, 20x20 tiles) on every "
-              "%dth pixel of every frame, all samples: %d pixels" % (last["cores"], stride, last["pixels"]))
+    secs = []
+    if cpu_sampling(args.workload) == "frames":
+        # each step: one whole frame of each of 8 jobs, rotating through all of them
+        per_step = min(8, len(jobs))
+        for _ in range(min(args.warmup, 1)):
+            cpu_frames(jobs, subset=[0], oscs=oscs)
+        per_job = {}
+        for step in range(args.steps):
+            sub = [(step * per_step + q) % len(jobs) for q in range(per_step)]
+            t0 = time.perf_counter()
+            got = cpu_frames(jobs, subset=sub, oscs=oscs)
+            secs.append(time.perf_counter() - t0)
+            for k, v in got.items():  # a job timed again adds its frame to the job's totals
+                if k in per_job:
+                    a = per_job[k]
+                    per_job[k] = tuple(x + y for x, y in zip(a[:4], v[:4])) + (a[4],)
+                else:
+                    per_job[k] = v
+        v = frames_rate(jobs, per_job, threads)["mrays"]
+        sample = frames_sample_text(jobs, threads) + "; 8 jobs per step, rotating"
+    else:
+        stride = cpu_stride(args.workload)
+        for _ in range(min(args.warmup, 1)):
+            cpu_sample(jobs, stride * 4, oscs=oscs)
+        vals = []
+        last = None
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            last = cpu_sample(jobs, stride, oscs=oscs)
+            secs.append(time.perf_counter() - t0)
+            vals.append(last["mrays"])
+        v = float(np.median(vals))
+        sample = ("oracle (CPU restatement of the reference Nova path, thread pool of %d workers) on every %dth pixel "
+                  "of the frame, all samples: %d pixels" % (last["cores"], stride, last["pixels"]))
     line = {"impl": "reference", "metric": metric, "value": v, "unit": "Mrays/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(secs)) * 1000.0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(secs)) * 1000.0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)", "config": {"workload": workload, "pixel_sample": sample},
-            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": last["cores"], "kind": "port", "sample": sample},
+            "data": "synthetic (seeded scenes and env maps)", "config": bench_config(workload, len(jobs)),
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -593,7 +674,7 @@ def run_ours(args, rank, world, local_rank):
         host_films = [torch.empty(s, dtype=torch.float32).pin_memory() for s in sizes]
         e_frames = [native.make_frame(j["scene"], j["width"], j["height"], j["spp"], j["depth"], seed=0,
                                       rr_start=j["rr_start"]) for j in jobs]
-        e_steps = max(1, min(args.steps, 3))
+        e_steps = args.steps
 
         def e2e_step():
             t0 = time.perf_counter()
@@ -646,9 +727,21 @@ def run_ours(args, rank, world, local_rank):
         return
 
     cpu = None
+    check = None
     if not args.no_cpu:
         host = [f.cpu().numpy() for f in films] if batched else [f.cpu().numpy() for f in plain_films]
-        cpu = cpu_sample(jobs, cpu_stride(args.workload, "baseline"), films=host if world == 1 else None)
+        threads = usable_cores()
+        if cpu_sampling(args.workload) == "frames":
+            oscs = oracle_scenes(jobs)
+            cpu = frames_rate(jobs, cpu_frames(jobs, oscs=oscs, threads=threads), threads)
+            cpu["sample"] = frames_sample_text(jobs, threads)
+            # untimed: the device films against the oracle on a pixel subset with all samples
+            check = cpu_sample(jobs, cpu_stride(args.workload), oscs=oscs, films=host if world == 1 else None)
+        else:
+            cpu = cpu_sample(jobs, cpu_stride(args.workload), films=host if world == 1 else None)
+            check = cpu
+            cpu["sample"] = ("oracle on every %dth pixel of the frame, all samples (%d pixels, %.1f s)"
+                             % (cpu_stride(args.workload), cpu["pixels"], cpu["seconds"]))
     pk = peaks()
     hbm = pk.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
@@ -678,7 +771,9 @@ def run_ours(args, rank, world, local_rank):
              "paths_per_step": acc.paths / args.steps, "trace_ms_per_step": acc.trace_ms / args.steps,
              "shade_ms_per_step": acc.shade_ms / args.steps, "bvh_build_s": build_s, "upload_s": upload_s,
              "bvh_nodes": sum(i["nodes"] for i in infos), "triangles": sum(i["triangles"] for i in infos),
-             "device_bytes": sum(i["device_bytes"] for i in infos)}
+             "device_bytes": sum(i["device_bytes"] for i in infos), "bvh_width": args.bvh_width or 2,
+             "parallelism": "sample-range partition + NCCL film all-reduce" if world > 1 else "single GPU",
+             "films_mb": int(sum(sizes) * 4 / 1e6)}
     if batched:
         pacc, pms, ptraced = res["plain"]
         pval = ptraced / args.steps / (pms / 1e3) / 1e6
@@ -692,8 +787,9 @@ def run_ours(args, rank, world, local_rank):
         extra["equal_rmse"] = ("batched and plain films compared bit for bit after the timed steps; "
                                "rel_rmse_vs_cpu is the per-pixel relative RMSE of the film against the oracle "
                                "on the CPU sample's pixels")
-    if cpu:
-        extra["rel_rmse_vs_cpu"] = cpu["rel_rmse"]
+    if check:
+        extra["rel_rmse_vs_cpu"] = check["rel_rmse"]
+        extra["rel_rmse_pixels"] = "every %dth pixel of every frame, all samples" % cpu_stride(args.workload)
     if batched and not args.no_adjoint:
         extra["adjoint"] = adjoint_timing(local_rank)
     if batched and not args.no_film_io:
@@ -710,15 +806,11 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": metric, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and env maps)",
-            "config": {"workload": workload, "jobs": nj, "bvh_width": args.bvh_width or 2,
-                       "parallelism": "sample-range partition + NCCL film all-reduce" if world > 1 else "single GPU",
-                       "l2": "working set larger than L2 (%d BVH nodes + %d tris over %d scenes, films %d MB)" % (
-                           extra["bvh_nodes"], extra["triangles"], nj, int(sum(sizes) * 4 / 1e6))},
+            "config": bench_config(workload, nj),
             "e2e": e2e, "roofline": roof,
             "cpu_baseline": None if not cpu else {
                 "value": cpu["mrays"], "unit": "Mrays/s", "cores": cpu["cores"], "kind": "port",
-                "sample": "oracle on every %dth pixel of every frame, all samples (%d pixels, %.1f s)" % (
-                    cpu_stride(args.workload, "baseline"), cpu["pixels"], cpu["seconds"])},
+                "sample": cpu["sample"]},
             "clocks": clk_summary, "gpu_launches": acc.kernels, "extra": extra}
     print(json.dumps(line), flush=True)
     for c in ctxs:

@@ -1550,7 +1550,10 @@ extern "C" int32_t orc_render(void *h, const orc_options *opt, float *out_rgba, 
   const int tile = opt->tile > 0 ? opt->tile : 20;
   unsigned nthreads = opt->threads > 0 ? (unsigned)opt->threads : std::max(1u, std::thread::hardware_concurrency());
 
-  /* Work items: tiles of the full frame, or chunks of tile*tile pixels of the subset. */
+  /* Work items: tiles of the full frame (the reference's 20 x 20 tiles, DrawEngine.cpp:57-89), or, for
+   * a pixel subset, chunks of at most tile*tile pixels, small enough that every worker gets about four
+   * per frame: a sparse subset of a small frame must not leave cores idle that a full frame of the
+   * reference would keep busy. */
   struct Task {
     int x0, y0, x1, y1;
     int64_t p0, p1;
@@ -1567,7 +1570,8 @@ extern "C" int32_t orc_render(void *h, const orc_options *opt, float *out_rgba, 
       tasks.push_back(t);
     }
   } else {
-    int64_t chunk = (int64_t)tile * tile;
+    const int64_t per_worker = (n_pixels + 4 * (int64_t)nthreads - 1) / (4 * (int64_t)nthreads);
+    const int64_t chunk = std::min<int64_t>((int64_t)tile * tile, std::max<int64_t>(16, per_worker));
     for (int64_t p = 0; p < n_pixels; p += chunk) tasks.push_back(Task{0, 0, 0, 0, p, std::min(n_pixels, p + chunk)});
   }
 

@@ -1,5 +1,5 @@
 """bench.py's reference arm runs on the host alone (the oracle restatement of the reference's CPU
-path on a bounded pixel sample) and prints the one JSON line of the bench contract with
+path on whole frames of one sample per pixel, extrapolated to each job's spp) and prints the one JSON line of the bench contract with
 "impl": "reference", its cpu_baseline and an e2e block that moves no bytes."""
 import json
 import os
