@@ -686,6 +686,8 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
   c->scene.acos_lut = c->d_acos;
   c->scene.envmap = d->envmap;
   c->scene.n_prims = (uint32_t)offset;
+  c->scene.n_instances = d->n_instances;
+  c->scene.n_materials = d->n_materials;
   c->scene.has_emissive = emissive ? 1u : 0u;
   NB_CUDA(c, cudaStreamSynchronize(c->stream), "upload_scene");
   if (c->h_counters[0] != 0) {

@@ -69,6 +69,7 @@ struct DevScene {
   const float *acos_lut;     /* 500000 entries */
   int32_t envmap;
   uint32_t n_prims;
+  uint32_t n_instances, n_materials; /* table sizes: the shading kernels check every index against them */
   uint32_t has_emissive;
   const float *diff_albedo;  /* differentiable parameters (NULL: textures): 3 x n_prims RGB albedo */
   const float *diff_rough;   /* and n_materials roughness values */

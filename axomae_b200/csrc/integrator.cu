@@ -87,6 +87,10 @@ struct WaveCounters {
   uint32_t done;
   uint32_t waves; /* waves that did work */
   uint32_t trace_next; /* next queued ray handed out by the persistent trace kernel */
+  /* device status of the whole loop (never reset between waves): path radiance values that were not
+   * finite and were written as 0 (the reference's DENAN, Integrator.cpp:92), and hits whose
+   * primitive, instance or material id is out of range (the path ends black, the render fails) */
+  uint32_t nonfinite, bad_index;
   unsigned long long traced;
 };
 
@@ -216,21 +220,36 @@ __global__ void __launch_bounds__(256) k_refill(Queue q, const WaveCounters *wcp
   }
 }
 
-__device__ __forceinline__ float4 finite_or_zero(V3 L, float alpha) {
-  if (!finite3(L)) return make_float4(0.f, 0.f, 0.f, 0.f);
+/* Non-finite radiance becomes 0 (DENAN), counted in *nonfinite (rare: a plain atomic). */
+__device__ __forceinline__ float4 finite_or_zero(V3 L, float alpha, unsigned *nonfinite) {
+  if (!finite3(L)) {
+    atomicAdd(nonfinite, 1u);
+    return make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   return make_float4(L.x, L.y, L.z, alpha);
 }
 
 /* Writes a finished path's radiance (adds the emission gathered so far when the scene has any). */
-__device__ __forceinline__ void finish_path(const DevScene &sc, float4 *L, uint32_t g, float4 result) {
+__device__ __forceinline__ void finish_path(const DevScene &sc, float4 *L, uint32_t g, float4 result,
+                                            unsigned *nonfinite) {
   if (sc.has_emissive) {
     const float4 acc = L[g];
     float4 r = make_float4(acc.x + result.x, acc.y + result.y, acc.z + result.z, result.w);
-    if (!isfinite(r.x) || !isfinite(r.y) || !isfinite(r.z)) r = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!isfinite(r.x) || !isfinite(r.y) || !isfinite(r.z)) {
+      atomicAdd(nonfinite, 1u);
+      r = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     L[g] = r;
   } else {
     L[g] = result;
   }
+}
+
+/* The hit's primitive, its instance and the instance's material all index their tables. */
+__device__ __forceinline__ bool hit_ids_valid(const DevScene &sc, int prim, uint32_t &inst) {
+  if (prim < 0 || (uint32_t)prim >= sc.n_prims) return false;
+  inst = __ldg(sc.prim_inst + prim);
+  return inst < sc.n_instances && sc.instances[inst].material < sc.n_materials;
 }
 
 /* Warp-aggregated append: returns the slot of every lane with `flag` set. */
@@ -269,7 +288,8 @@ __global__ void __launch_bounds__(128, 10) k_trace(Queue q, WaveCounters *wcp, f
         const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
         finish_path(sc, L, __float_as_uint(o.w),
                     finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z},
-                                   (float)(__float_as_uint(d.w) & 0xffu) + e.w));
+                                   (float)(__float_as_uint(d.w) & 0xffu) + e.w, &wcp->nonfinite),
+                    &wcp->nonfinite);
       }
     }
     const unsigned slot = warp_append(is_hit, &wcp->hit_count);
@@ -327,7 +347,9 @@ __global__ void __launch_bounds__(128) k_trace_dyn(Queue q, WaveCounters *wcp, f
       const float4 o = q.o[ray], b4 = q.beta[ray], d = q.d[ray];
       const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
       finish_path(sc, L, __float_as_uint(o.w),
-                  finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z}, (float)(__float_as_uint(d.w) & 0xffu) + e.w));
+                  finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z}, (float)(__float_as_uint(d.w) & 0xffu) + e.w,
+                                 &wcp->nonfinite),
+                  &wcp->nonfinite);
     }
     const unsigned slot = warp_append(is_hit, &wcp->hit_count);
     if (is_hit) {
@@ -362,7 +384,13 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
       const int prim = __float_as_int(h.w);
       bool done = false;
       float4 result = make_float4(0.f, 0.f, 0.f, 0.f);
-      const uint32_t inst = __ldg(sc.prim_inst + prim);
+      uint32_t inst = 0;
+      if (!hit_ids_valid(sc, prim, inst)) {
+        atomicAdd(&wcp->bad_index, 1u);
+        L[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        goto append;
+      }
+      {
       const DevInstance &I = sc.instances[inst];
       const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)prim - I.prim_offset, h.x, h.y, h.z);
       const ScatterResult sr = scatter(sc, rd, hr, sc.materials[I.material], index, 2u + 4u * (unsigned)bounce, rp.seed,
@@ -398,7 +426,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
           const V3 no3 = hr.position + hr.ng * (eps + eps * fsign(dot(hr.ng, sr.wi)));
           if (bounce + 1 > rp.max_depth) {
             const V4 e = env_sample(sc, nd3);
-            result = finite_or_zero(beta * V3{e.x, e.y, e.z}, (float)bounce + 1.f + e.w);
+            result = finite_or_zero(beta * V3{e.x, e.y, e.z}, (float)bounce + 1.f + e.w, &wcp->nonfinite);
             done = true;
           } else {
             enq = true;
@@ -408,8 +436,10 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
           }
         }
       }
-      if (done) finish_path(sc, L, g, result);
+      if (done) finish_path(sc, L, g, result, &wcp->nonfinite);
+      }
     }
+  append:
     const unsigned slot = warp_append(enq, &wcp->out_count);
     if (enq) {
       out.o[slot] = no;
@@ -519,7 +549,12 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
     V3 rem{r4.x, r4.y, r4.z};
     const V3 dl{l4.x, l4.y, l4.z};
     const int prim = __float_as_int(h.w);
-    const uint32_t inst = __ldg(sc.prim_inst + prim);
+    uint32_t inst = 0;
+    if (!hit_ids_valid(sc, prim, inst)) {
+      atomicAdd(&wcp->bad_index, 1u);
+      goto gather;
+    }
+    {
     const DevInstance &I = sc.instances[inst];
     const HitRecord hr = make_record(sc, ro, rd, I, (uint32_t)prim - I.prim_offset, h.x, h.y, h.z);
     Scores scs;
@@ -560,7 +595,9 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
         ndl = l4;
       }
     }
+    }
   }
+gather:
   if (g_alb) warp_add_by_key<3>(g_act, g_prim, va, g_alb);
   if (g_rough) warp_add_by_key<1>(g_act, g_mat, vr, g_rough);
   const unsigned slot = warp_append(enq, &wcp->out_count);
@@ -844,8 +881,11 @@ nova_b200_status capture_graphs(nova_b200_ctx *c, const ManyJobs &js, const Laun
 struct LoopStats {
   float t_trace = 0.f, t_shade = 0.f;
   uint64_t kernels = 0, traced = 0;
+  uint64_t nonfinite = 0, bad_index = 0;
   uint32_t waves = 0;
   void add_to(nova_b200_render_stats &s) const {
+    s.nonfinite += nonfinite;
+    s.bad_index += bad_index;
     s.traced += traced;
     s.segments += traced;
     s.waves += waves;
@@ -884,9 +924,21 @@ nova_b200_status run_waves(nova_b200_ctx *x, uint32_t total, uint32_t cap, Launc
     }
     ls.kernels += 4 * kWavesPerGraph;
     const WaveCounters r = hw[slot];
+    if (r.bad_index) { /* the device status word: stop after this group, as the reference aborts a tile
+                        * once its exception manager holds an error (integrator/Integrator.h:74-78) */
+      NB_CUDA(x, cudaEventSynchronize(x->ev_done[slot ^ 1]), "waves");
+      const WaveCounters last = hw[slot ^ 1];
+      ls.bad_index += std::max(r.bad_index, last.bad_index);
+      ls.nonfinite += std::max(r.nonfinite, last.nonfinite);
+      char msg[160];
+      std::snprintf(msg, sizeof(msg), "device status: %u hits with an out-of-range primitive, instance or material id",
+                    (unsigned)std::max(r.bad_index, last.bad_index));
+      return nbctx::fail(x, NOVA_B200_RENDERER_EXCEPTION, "%s", msg);
+    }
     if (r.done) {
       ls.waves += r.waves;
       ls.traced += r.traced;
+      ls.nonfinite += r.nonfinite;
       break;
     }
     if (x->cancel.load()) { /* nova_b200_cancel: let the group in flight finish, enqueue nothing more */

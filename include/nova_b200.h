@@ -144,6 +144,14 @@ typedef struct {
   double trace_ms;     /* device time inside the closest-hit kernel */
   double shade_ms;     /* device time inside the shading kernel */
   uint64_t kernels;    /* kernels launched */
+  /* The device status word of the call.  nonfinite: path radiance values that came out NaN or
+   * infinite and were written as 0, as the reference's DENAN does (integrator/Integrator.cpp:92); the
+   * render succeeds.  bad_index: hits whose primitive, instance or material id lies outside the
+   * scene's tables (not reachable through validated uploads; it guards against corrupted device
+   * memory): the path ends black, the loop stops after the current wave group and the call returns
+   * RENDERER_EXCEPTION, which the engine facade reports as exception::GENERAL_GPU_ERROR. */
+  uint64_t nonfinite;
+  uint64_t bad_index;
 } nova_b200_render_stats;
 
 /* Context lifecycle: DeviceAcceleratorInterface::make (api/device_accelerator_factory.cpp:9) and

@@ -536,3 +536,45 @@ def test_aov_matches_oracle(ctx, oracle, emissive_scene, kind, name, vinv):
     assert same.mean() >= 0.999, (name, same.mean())
     if kind == 4:
         assert (out[..., :3].max(-1) > 0).any()
+
+
+def test_device_status_counts_nonfinite_radiance(ctx, oracle, torch_cuda):
+    """The device status word, from a host-made bad input: every 7th triangle gets a NaN albedo (per-
+    triangle albedo of the differentiable parameters).  Paths through those triangles carry NaN
+    weights; the device writes their radiance as 0 (the reference's DENAN, Integrator.cpp:92), counts
+    them in the stats' `nonfinite`, and the film stays finite and equal to the oracle's, which applies
+    DENAN at every level.  A clean render reports zero, and no index error either way."""
+    from axomae_b200 import native, scenes
+    W = H = 48
+    s = scenes.spheres_scene(W, H, n_spheres=8, seed=2)
+    ctx.upload(s)
+    ctx.build()
+    ntri = ctx.info()["triangles"]
+    nmat = len(s["materials"])
+    alb = np.full((ntri, 3), 0.5, np.float32)
+    rough = np.full(nmat, 0.3, np.float32)
+    fr = native.make_frame(s, W, H, 8, 4)
+    osc = oracle.OracleScene(s)
+    results = {}
+    for name in ("clean", "nan"):
+        a = alb.copy()
+        if name == "nan":
+            a[::7] = np.nan
+        ta, tr = torch_cuda.from_numpy(a).cuda(), torch_cuda.from_numpy(rough).cuda()
+        ctx.set_diff_params(ta.data_ptr(), tr.data_ptr())
+        film = np.zeros((H, W, 4), np.float32)
+        try:
+            st = ctx.render(fr, film_host=film)
+        finally:
+            ctx.set_diff_params(None, None)
+        osc.set_diff_params(a, rough)
+        ref, _ = osc.render(oracle.options(W, H, 8, 4))
+        results[name] = (st, film, ref)
+    st, film, ref = results["clean"]
+    assert st.nonfinite == 0 and st.bad_index == 0
+    st, film, ref = results["nan"]
+    assert st.bad_index == 0
+    assert st.nonfinite > 100, st.nonfinite
+    assert np.isfinite(film).all()
+    assert rel_rmse(film, ref) <= REL_RMSE_TOL
+    assert film[..., :3].mean() < results["clean"][1][..., :3].mean()  # the zeroed paths darken the image
