@@ -873,6 +873,12 @@ nova_b200_status nova_b200_bake_irradiance(nova_b200_ctx *c, const float *src, i
   return nb_bake(c, src, sw, sh, ch, ow, oh, samples, out);
 }
 
+nova_b200_status nova_b200_bake_irradiance_texunit(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh,
+                                                   int32_t ch, int32_t ow, int32_t oh, int32_t samples, float *out) {
+  if (!c) return NOVA_B200_INVALID_ARGUMENT;
+  return nb_bake_texunit(c, src, sw, sh, ch, ow, oh, samples, out);
+}
+
 void nova_b200_get_error(nova_b200_ctx *c, char buf[1024], size_t *size) {
   if (!buf) return;
   const std::string &e = c ? c->error : std::string("null context");

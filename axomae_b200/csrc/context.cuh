@@ -113,6 +113,8 @@ nova_b200_status nb_scatter(nova_b200_ctx *c, uint64_t n, const float *o, const 
                             float *emissive, int32_t *valid);
 nova_b200_status nb_sobol(nova_b200_ctx *c, uint64_t n, const uint32_t *idx, const uint32_t *dim, uint32_t seed,
                           float *out);
+nova_b200_status nb_bake_texunit(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh, int32_t ch, int32_t ow,
+                                 int32_t oh, int32_t samples, float *out);
 nova_b200_status nb_bake(nova_b200_ctx *c, const float *src, int32_t sw, int32_t sh, int32_t ch, int32_t ow,
                          int32_t oh, int32_t samples, float *out);
 /* Defined in render_noalloc.cu: loads the no-alloc kernels' module on the context's device, takes

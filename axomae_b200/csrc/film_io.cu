@@ -700,6 +700,12 @@ extern "C" nova_b200_status nova_b200_hdr_write(nova_b200_ctx *c, const char *pa
 
 extern "C" nova_b200_status nova_b200_bake_texture(nova_b200_ctx *c, const char *type, int32_t out_w, int32_t out_h,
                                                    int32_t samples, const char *path_in, const char *path_out) {
+  return nova_b200_bake_texture_flags(c, type, out_w, out_h, samples, path_in, path_out, 0u);
+}
+
+extern "C" nova_b200_status nova_b200_bake_texture_flags(nova_b200_ctx *c, const char *type, int32_t out_w,
+                                                         int32_t out_h, int32_t samples, const char *path_in,
+                                                         const char *path_out, uint32_t flags) {
   using namespace nbctx;
   if (check_ctx(c)) return NOVA_B200_INVALID_ARGUMENT;
   if (!type || std::strcmp(type, "irradiance") != 0)
@@ -724,7 +730,9 @@ extern "C" nova_b200_status nova_b200_bake_texture(nova_b200_ctx *c, const char 
     return cuda_fail(c, e, "cudaMalloc(irradiance map)");
   }
   st = nova_b200_hdr_read(c, path_in, nullptr, src, src_n);
-  if (!st) st = nb_bake(c, src, w, h, 4, out_w, out_h, samples, out);
+  if (!st)
+    st = (flags & NOVA_B200_BAKE_GPU_KERNEL) ? nb_bake_texunit(c, src, w, h, 4, out_w, out_h, samples, out)
+                                             : nb_bake(c, src, w, h, 4, out_w, out_h, samples, out);
   if (!st) st = nova_b200_hdr_write(c, path_out, nullptr, out, out_w, out_h, 4, 0);
   cudaFreeAsync(src, c->stream);
   cudaFreeAsync(out, c->stream);

@@ -102,7 +102,8 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_build_bvh_batch", "nova_b200_render_aov", "nova_b200_film_accumulate",
            "nova_b200_display_blend", "nova_b200_snapshot", "nova_b200_hdr_info", "nova_b200_hdr_read",
            "nova_b200_hdr_write", "nova_b200_last_call_ms", "nova_b200_bake_texture",
-           "nova_b200_trace_host", "nova_b200_cancel"]
+           "nova_b200_trace_host", "nova_b200_cancel", "nova_b200_bake_irradiance_texunit",
+           "nova_b200_bake_texture_flags"]
 
 
 def lib():
@@ -147,6 +148,10 @@ def lib():
         L.nova_b200_cancel.argtypes = [vp]
         L.nova_b200_bake_texture.argtypes = [vp, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p,
                                              C.c_char_p]
+        L.nova_b200_bake_texture_flags.argtypes = [vp, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p,
+                                                   C.c_char_p, C.c_uint32]
+        L.nova_b200_bake_irradiance_texunit.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                                        C.c_int32, C.c_int32, vp]
         L.nova_b200_render_batch.argtypes = [C.POINTER(vp), C.POINTER(Frame), C.c_uint32, C.POINTER(vp),
                                              C.POINTER(vp), C.POINTER(RenderStats)]
         for name in EXPORTS:
@@ -426,6 +431,11 @@ class Context:
         self._check(lib().nova_b200_bake_irradiance(self.h, C.c_void_p(src_ptr), sw, sh, ch, ow, oh, samples,
                                                     C.c_void_p(out_ptr)))
 
+    def bake_irradiance_texunit(self, src_ptr, sw, sh, ch, ow, oh, samples, out_ptr):
+        """The bake of the reference's CUDA kernel (texture-unit filtering); out: ow * oh * 4 floats."""
+        self._check(lib().nova_b200_bake_irradiance_texunit(self.h, C.c_void_p(src_ptr), sw, sh, ch, ow, oh, samples,
+                                                            C.c_void_p(out_ptr)))
+
     def film_accumulate(self, partial_ptr, accum_ptr, final_ptr, n, frame_index):
         """accum += partial; final = accum / (frame_index + 1) over n device floats."""
         self._check(lib().nova_b200_film_accumulate(self.h, C.c_void_p(partial_ptr), C.c_void_p(accum_ptr),
@@ -463,10 +473,12 @@ class Context:
         self._check(lib().nova_b200_hdr_write(self.h, os.fsencode(path), fh, fd, width, height, channels,
                                               1 if flip else 0))
 
-    def bake_texture(self, kind, width, height, samples, path_in, path_out):
-        """The bake command: path_in (.hdr) -> irradiance map path_out + ".hdr"."""
-        self._check(lib().nova_b200_bake_texture(self.h, kind.encode(), width, height, samples,
-                                                 os.fsencode(path_in), os.fsencode(path_out)))
+    def bake_texture(self, kind, width, height, samples, path_in, path_out, gpu_kernel=False):
+        """The bake command: path_in (.hdr) -> irradiance map path_out + ".hdr" (gpu_kernel: the
+        reference's --gpu bake)."""
+        self._check(lib().nova_b200_bake_texture_flags(self.h, kind.encode(), width, height, samples,
+                                                       os.fsencode(path_in), os.fsencode(path_out),
+                                                       1 if gpu_kernel else 0))
 
     def cancel(self):
         """Stops the render / backward call running on this context in another thread."""

@@ -315,6 +315,16 @@ nova_b200_status nova_b200_sobol(nova_b200_ctx *ctx, uint64_t n, const uint32_t 
 nova_b200_status nova_b200_bake_irradiance(nova_b200_ctx *ctx, const float *src_dev, int32_t src_w, int32_t src_h,
                                            int32_t channels, int32_t out_w, int32_t out_h, int32_t samples,
                                            float *out_dev);
+/* The same bake with the semantics of the reference's CUDA kernel, the path its command line takes
+ * with --gpu: GPU_compute_irradiance (sources/processing/cuda/CubemapProcessing.cu:244-284, kernel
+ * :129-175).  The hash is seeded with the output texel's indices, directions map to uv with the
+ * exact acos / atan2f, and the source (RGB or RGBA, made RGBA with alpha 1 as
+ * TextureProcessing.cpp:24-32 does) is read through a float4 texture object with hardware bilinear
+ * filtering and wrap addressing.  out_dev: out_w*out_h*4 floats, alpha 1.  Power-of-two output
+ * sizes; the source must fit a 2D texture. */
+nova_b200_status nova_b200_bake_irradiance_texunit(nova_b200_ctx *ctx, const float *src_dev, int32_t src_w,
+                                                   int32_t src_h, int32_t channels, int32_t out_w, int32_t out_h,
+                                                   int32_t samples, float *out_dev);
 
 /* ---- Film outputs (device buffers, the context's device and stream) ---------------------------
  *
@@ -359,6 +369,13 @@ nova_b200_status nova_b200_hdr_write(nova_b200_ctx *ctx, const char *path, const
  * reference leaves it).  type must be "irradiance" (the only type the reference bakes). */
 nova_b200_status nova_b200_bake_texture(nova_b200_ctx *ctx, const char *type, int32_t out_width, int32_t out_height,
                                         int32_t samples, const char *path_in, const char *path_out);
+/* The same with flags: NOVA_B200_BAKE_GPU_KERNEL bakes with nova_b200_bake_irradiance_texunit, the
+ * reference's `--gpu` path (ProgramOptionsManager.cpp:39-40,69 sets CONF_USE_CUDA, which
+ * API.cpp:52 passes to computeDiffuseIrradiance); its output alpha is 1. */
+#define NOVA_B200_BAKE_GPU_KERNEL 1u
+nova_b200_status nova_b200_bake_texture_flags(nova_b200_ctx *ctx, const char *type, int32_t out_width,
+                                              int32_t out_height, int32_t samples, const char *path_in,
+                                              const char *path_out, uint32_t flags);
 /* Device time in ms of the kernel of the last film_accumulate / display_blend / snapshot /
  * hdr_read / hdr_write call (CUDA events).  No counterpart in the reference. */
 nova_b200_status nova_b200_last_call_ms(nova_b200_ctx *ctx, float *device_ms);

@@ -7,6 +7,18 @@
  *                                                       sources/processing/TextureProcessing.h:174-303
  *   pgc3d                                                corelib/internal/common/math/math_importance_sampling.h:7-22
  * The spherical mapping uses the reference's fast approximations (atan2 polynomial, acos table).
+ *
+ * The reference's CUDA bake (the --gpu path), orc_bake_irradiance_texunit:
+ *   gpgpu_device_compute_diffuse_irradiance             sources/processing/cuda/CubemapProcessing.cu:129-175
+ *   spherical_math::*, gpu_pgc3d, dot / cross / normalize :12-105
+ *   texture descriptor (wrap, linear, normalised)        :216-230
+ * Its tex2D<float4> fetch is restated from the texture unit's published bilinear filter (CUDA C++
+ * Programming Guide, "Texture Fetching", linear filtering): x_B = x * W - 0.5, i = floor(x_B),
+ * alpha = frac(x_B) held in 9-bit fixed point with 8 fractional bits (rounded to nearest here; the
+ * guide does not state the rounding), wrap addressing on the texel indices, and
+ * T = (1-a)(1-b) T[i,j] + a(1-b) T[i+1,j] + (1-a) b T[i,j+1] + a b T[i+1,j+1].  The float
+ * trigonometry is correctly rounded here where the device uses its own functions (within a few ulp),
+ * so the two agree to a tolerance, not bit for bit.
  */
 #include "oracle_internal.h"
 #include <algorithm>
@@ -139,6 +151,94 @@ V3 texel_irradiance(const Src &src, float x, float y, float z, unsigned W, unsig
 }  // namespace orc
 
 using namespace orc;
+
+/* ---- the reference's CUDA kernel ---- */
+namespace orc {
+namespace {
+
+struct F3 {
+  float x, y, z;
+};
+inline F3 sph_to_cart(float phi, float theta) {
+  return F3{sin_rn(theta) * cos_rn(phi), sin_rn(theta) * sin_rn(phi), cos_rn(theta)};
+}
+inline F3 cross3(F3 a, F3 b) { return F3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+
+/* tex2D<float4> with linear filtering, wrap addressing and normalised coordinates. */
+struct TexUnit {
+  const float *rgba;
+  int w, h;
+  static int wrap(int i, int n) { return ((i % n) + n) % n; }
+  static float weight(float f) { return std::nearbyint(f * 256.f) / 256.f; }
+  V4 fetch(float u, float v) const {
+    u = u - std::floor(u), v = v - std::floor(v);
+    const float xb = u * (float)w - 0.5f, yb = v * (float)h - 0.5f;
+    const float fx = std::floor(xb), fy = std::floor(yb);
+    const float a = weight(xb - fx), b = weight(yb - fy);
+    const int i0 = wrap((int)fx, w), i1 = wrap((int)fx + 1, w), j0 = wrap((int)fy, h), j1 = wrap((int)fy + 1, h);
+    auto T = [&](int i, int j) {
+      const float *p = rgba + ((size_t)j * w + i) * 4;
+      return V4{p[0], p[1], p[2], p[3]};
+    };
+    const V4 t00 = T(i0, j0), t10 = T(i1, j0), t01 = T(i0, j1), t11 = T(i1, j1);
+    const float w00 = (1 - a) * (1 - b), w10 = a * (1 - b), w01 = (1 - a) * b, w11 = a * b;
+    return V4{w00 * t00.x + w10 * t10.x + w01 * t01.x + w11 * t11.x, w00 * t00.y + w10 * t10.y + w01 * t01.y + w11 * t11.y,
+              w00 * t00.z + w10 * t10.z + w01 * t01.z + w11 * t11.z, w00 * t00.w + w10 * t10.w + w01 * t01.w + w11 * t11.w};
+  }
+};
+
+}  // namespace
+}  // namespace orc
+
+using namespace orc;
+
+/* The reference's CUDA bake (CubemapProcessing.cu:129-175) on an RGBA source: out = out_w * out_h
+ * * 4 floats, alpha 1.  Returns 1 for non-power-of-two sizes or no samples. */
+extern "C" int32_t orc_bake_irradiance_texunit(const float *rgba, int32_t src_w, int32_t src_h, int32_t out_w,
+                                               int32_t out_h, int32_t samples, int32_t threads, float *out) {
+  auto pow2 = [](int32_t v) { return v > 0 && (v & (v - 1)) == 0; };
+  if (!pow2(out_w) || !pow2(out_h) || samples <= 0) return 1;
+  const TexUnit tex{rgba, src_w, src_h};
+  const unsigned W = (unsigned)out_w, H = (unsigned)out_h, nt = threads > 0 ? (unsigned)threads : 8u;
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nt; t++)
+    pool.emplace_back([=, &tex] {
+      for (unsigned j = t; j < H; j += nt)
+        for (unsigned i = 0; i < W; i++) {
+          const float u = (float)i / (float)W, v = (float)j / (float)H;
+          const F3 normal = sph_to_cart((float)(2 * PI_D * u), (float)(PI_D * v));
+          const F3 some{1.f, 0.f, 0.f};
+          const float dd = some.x * normal.x + some.y * normal.y + some.z * normal.z;
+          F3 tangent{0.f, 1.f, 0.f};
+          if (1.0 - std::fabs(dd) > 1e-6) {
+            const F3 c = cross3(some, normal);
+            const float d = std::sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
+            tangent = F3{c.x / d, c.y / d, c.z / d};
+          }
+          const F3 bit = cross3(normal, tangent);
+          float irr[3] = {0.f, 0.f, 0.f};
+          for (unsigned s = 0; s < (unsigned)samples; s++) {
+            float r[3];
+            pgc3d(i, j, s, r);
+            const float phi = (float)(2 * PI_D * r[0]);
+            const float theta = asin_rn(std::sqrt(r[1]));
+            const F3 c = sph_to_cart(phi, theta);
+            const F3 w{c.x * tangent.x + c.y * bit.x + c.z * normal.x, c.x * tangent.y + c.y * bit.y + c.z * normal.y,
+                       c.x * tangent.z + c.y * bit.z + c.z * normal.z};
+            const float th = (float)std::acos((double)w.z), ph = (float)std::atan2((double)w.y, (double)w.x);
+            const V4 px = tex.fetch((float)(ph / (2 * PI_D)), (float)(th / PI_D));
+            irr[0] += px.x, irr[1] += px.y, irr[2] += px.z;
+          }
+          float *o = out + ((size_t)j * W + i) * 4;
+          o[0] = irr[0] / (float)samples;
+          o[1] = irr[1] / (float)samples;
+          o[2] = irr[2] / (float)samples;
+          o[3] = 1.f;
+        }
+    });
+  for (auto &t : pool) t.join();
+  return 0;
+}
 
 extern "C" int32_t orc_bake_irradiance(const float *src, int32_t src_w, int32_t src_h, int32_t channels, int32_t out_w,
                                        int32_t out_h, int32_t samples, int32_t threads, float *out) {

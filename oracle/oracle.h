@@ -142,6 +142,10 @@ int32_t orc_render_aov(void *h, const orc_options *opt, int32_t kind, float near
 void orc_sample_radiance(void *h, const orc_options *opt, uint64_t n, const int32_t *px, const int32_t *py,
                          const int32_t *s, float *out);
 
+/* The reference's CUDA irradiance bake (sources/processing/cuda/CubemapProcessing.cu:129-175) with the
+ * texture unit's bilinear filter restated; rgba source, out = out_w * out_h * 4 floats (alpha 1). */
+int32_t orc_bake_irradiance_texunit(const float *rgba, int32_t src_w, int32_t src_h, int32_t out_w, int32_t out_h,
+                                    int32_t samples, int32_t threads, float *out);
 /* Diffuse irradiance bake, CPU path (sources/processing/TextureProcessing.cpp:10-64). */
 int32_t orc_bake_irradiance(const float *src, int32_t src_w, int32_t src_h, int32_t channels, int32_t out_w,
                             int32_t out_h, int32_t samples, int32_t threads, float *out);

@@ -367,6 +367,23 @@ def bake_irradiance(src: np.ndarray, out_w: int, out_h: int, samples: int, threa
     return out
 
 
+def bake_irradiance_texunit(src: np.ndarray, out_w: int, out_h: int, samples: int, threads: int = 8) -> np.ndarray:
+    """The reference's CUDA bake (CubemapProcessing.cu:129-175) restated, texture filter included:
+    (out_h, out_w, 4), alpha 1.  The source is made RGBA with alpha 1 first, as the reference does."""
+    src = np.asarray(src, np.float32)
+    h, w, ch = src.shape
+    rgba = np.ones((h, w, 4), np.float32)
+    rgba[..., :3] = src[..., :3]
+    out = np.zeros((out_h, out_w, 4), np.float32)
+    L = lib()
+    L.orc_bake_irradiance_texunit.argtypes = [f32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                              f32p]
+    L.orc_bake_irradiance_texunit.restype = C.c_int32
+    if L.orc_bake_irradiance_texunit(_p(rgba, f32p), w, h, out_w, out_h, samples, threads, _p(out, f32p)) != 0:
+        raise ValueError("bake rejected")
+    return out
+
+
 def _v(x, n):
     return np.ascontiguousarray(x, np.float32).reshape(n)
 

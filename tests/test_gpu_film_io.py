@@ -216,3 +216,29 @@ def test_bake_cli_matches_oracle(oracle, torch_cuda, tmp_path):
     r = subprocess.run([exe, "--bake", "irradiance", "32", "16", "64", str(tmp_path / "none.hdr"),
                         str(tmp_path / "bad")], capture_output=True, text=True, timeout=300)
     assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+def test_bake_cli_gpu_flag_uses_the_cuda_kernel(oracle, torch_cuda, tmp_path):
+    """nova_b200_bake --gpu bakes with the reference's CUDA kernel, as the reference's --gpu option
+    selects it (ProgramOptionsManager.cpp:39-40): the file agrees with the oracle's restatement of that
+    kernel within the RGBE encoding and the texture filter's tolerance, and differs from the CPU-path
+    bake of the same map."""
+    rng = np.random.default_rng(14)
+    env = np.concatenate([rng.lognormal(0, 1, (64, 128, 3)), np.ones((64, 128, 1))], -1).astype(np.float32)
+    src = tmp_path / "env.hdr"
+    src.write_bytes(make_file(oracle.rgbe_encode(env, 4).reshape(64, 128, 4)))
+    exe = os.path.join(ROOT, "axomae_b200", "nova_b200_bake")
+    r = subprocess.run([exe, "--bake", "irradiance", "32", "16", "64", str(src), str(tmp_path / "irr"), "--gpu"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    code, w, h, q = oracle.hdr_parse((tmp_path / "irr.hdr").read_bytes())
+    assert (code, w, h) == (0, 32, 16)
+    got = oracle.rgbe_decode(q.reshape(-1, 4)).reshape(h, w, 4)
+    _, _, _, qin = oracle.hdr_parse(src.read_bytes())
+    env_dec = oracle.rgbe_decode(qin.reshape(-1, 4)).reshape(64, 128, 4)
+    ref = oracle.bake_irradiance_texunit(env_dec, 32, 16, 64)
+    d = (got[..., :3].astype(np.float64) - ref[..., :3]) / np.maximum(ref[..., :3], 1e-3)
+    assert float(np.sqrt(np.mean(d * d))) <= 1e-2
+    cpu = oracle.bake_irradiance(env_dec, 32, 16, 64)
+    d2 = (got[..., :3].astype(np.float64) - cpu[..., :3]) / np.maximum(cpu[..., :3], 1e-3)
+    assert float(np.sqrt(np.mean(d2 * d2))) > 2e-2
