@@ -92,6 +92,7 @@ struct WaveCounters {
    * primitive, instance or material id is out of range (the path ends black, the render fails) */
   uint32_t nonfinite, bad_index;
   unsigned long long traced;
+  unsigned long long node_visits, tri_tests; /* trace_mode 2 only: the traversal's own work */
 };
 
 /* The chunk's job table as a kernel parameter. */
@@ -268,7 +269,7 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
  * Integrator.cpp:94-98); hits are appended to a compact hit list so the shading kernel only runs
  * on rays that hit.  At least 10 resident blocks of 128 (48 registers): the walk is latency-bound,
  * and 40 warps per SM beat 32 (-4% on the batched scenes); 12 blocks spill the walk state. */
-template <int WIDTH, class JS, bool ADJ = false>
+template <int WIDTH, class JS, bool ADJ = false, bool COUNT = false>
 __global__ void __launch_bounds__(128, 10) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
                                                const __grid_constant__ JS js) {
   const uint32_t n = wcp->n_active + wave_new(*wcp);
@@ -277,10 +278,12 @@ __global__ void __launch_bounds__(128, 10) k_trace(Queue q, WaveCounters *wcp, f
   {
     bool is_hit = false;
     TraceResult r{-1, 0.f, 0.f, 0.f};
+    uint64_t nv = 0, tt = 0;
     if (i < n) {
       const float4 o = q.o[i], d = q.d[i];
       const DevScene &sc = js.at(__float_as_uint(d.w) >> 8).sc;
-      r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z});
+      r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, COUNT ? &nv : nullptr,
+                                 COUNT ? &tt : nullptr);
       if (r.prim >= 0) {
         is_hit = true;
       } else if (!ADJ) { /* a replayed path's radiance is already known */
@@ -290,6 +293,16 @@ __global__ void __launch_bounds__(128, 10) k_trace(Queue q, WaveCounters *wcp, f
                     finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z},
                                    (float)(__float_as_uint(d.w) & 0xffu) + e.w, &wcp->nonfinite),
                     &wcp->nonfinite);
+      }
+    }
+    if constexpr (COUNT) { /* one atomic per warp for each counter */
+      for (int off = 16; off > 0; off >>= 1) {
+        nv += __shfl_down_sync(0xffffffffu, nv, off);
+        tt += __shfl_down_sync(0xffffffffu, tt, off);
+      }
+      if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(&wcp->node_visits, (unsigned long long)nv);
+        atomicAdd(&wcp->tri_tests, (unsigned long long)tt);
       }
     }
     const unsigned slot = warp_append(is_hit, &wcp->hit_count);
@@ -754,7 +767,8 @@ nova_b200_status ensure_wave_buffers(nova_b200_ctx *c, uint32_t cap, size_t radi
 struct LaunchShape {
   uint32_t cap;
   uint32_t trace_block, shade_block;
-  uint32_t trace_mode; /* 0: one ray per thread, 1: persistent warps with ray hand-out (binary BVH) */
+  uint32_t trace_mode; /* 0: one ray per thread, 1: persistent warps with ray hand-out (binary BVH),
+                         2: one ray per thread, counting node visits and triangle tests */
 };
 
 struct WaveBuffers {
@@ -823,6 +837,9 @@ void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int sl
       cudaEventRecordWithFlags(ev[3 * w + 0], c->stream, flags);
       if (WIDTH == 2 && ls.trace_mode == 1)
         k_trace_dyn<JS><<<g_dyn, 128, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+      else if (ls.trace_mode == 2)
+        k_trace<WIDTH, JS, false, true>
+            <<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
       else
         k_trace<WIDTH, JS><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
       cudaEventRecordWithFlags(ev[3 * w + 1], c->stream, flags);
@@ -881,9 +898,11 @@ nova_b200_status capture_graphs(nova_b200_ctx *c, const ManyJobs &js, const Laun
 struct LoopStats {
   float t_trace = 0.f, t_shade = 0.f;
   uint64_t kernels = 0, traced = 0;
-  uint64_t nonfinite = 0, bad_index = 0;
+  uint64_t nonfinite = 0, bad_index = 0, node_visits = 0, tri_tests = 0;
   uint32_t waves = 0;
   void add_to(nova_b200_render_stats &s) const {
+    s.node_visits += node_visits;
+    s.tri_tests += tri_tests;
     s.nonfinite += nonfinite;
     s.bad_index += bad_index;
     s.traced += traced;
@@ -939,6 +958,8 @@ nova_b200_status run_waves(nova_b200_ctx *x, uint32_t total, uint32_t cap, Launc
       ls.waves += r.waves;
       ls.traced += r.traced;
       ls.nonfinite += r.nonfinite;
+      ls.node_visits += r.node_visits;
+      ls.tri_tests += r.tri_tests;
       break;
     }
     if (x->cancel.load()) { /* nova_b200_cancel: let the group in flight finish, enqueue nothing more */

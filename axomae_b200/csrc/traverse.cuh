@@ -149,6 +149,7 @@ NB_D TraceResult trace_closest2(const DevScene &sc, V3 o, V3 d, uint64_t *node_v
 /* Triangle tests of one leaf range with the instance-transform cache (Triangle.h:146-153). */
 NB_D void test_triangles(const DevScene &sc, uint32_t first, uint32_t count, V3 o, V3 d, int32_t &cached_inst, V3 &lo_o,
                          V3 &lo_d, float &tmax, TraceResult &r) {
+  /* count: the caller counts triangle tests (trace_closest8's tri_tests) */
   for (uint32_t k = first; k < first + count; k++) {
     const float4 t0 = __ldg(&sc.tris[3 * k + 0]);
     const float4 t1 = __ldg(&sc.tris[3 * k + 1]);
@@ -251,8 +252,10 @@ struct Walk2 {
  * eight quantised child boxes, tests the triangles of hit leaf children in slot order, then
  * descends into the first hit inner child; the other hit inner children stay on a stack as one
  * (child_base, hit mask, inner mask) group.  Child slots are visited in increasing (slot ^ oct)
- * order, oct being the ray's direction-sign bits, which is near-to-far for the slot assignment. */
-NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d) {
+ * order, oct being the ray's direction-sign bits, which is near-to-far for the slot assignment.
+ * node_visits / tri_tests (optional) add the nodes visited and the triangles tested. */
+NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
+                               uint64_t *tri_tests = nullptr) {
   TraceResult r{-1, 0.f, 0.f, 0.f};
   float tmax = FLT_MAX;
   const float ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
@@ -262,7 +265,9 @@ NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d) {
   uint32_t node = 0;
   int32_t cached_inst = -1;
   V3 lo_o = o, lo_d = d;
+  uint32_t nv = 0, tt = 0;
   for (;;) {
+    nv++;
     const float4 *np = sc.nodes + 5 * (size_t)node;
     const float4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
     const uint32_t hdr = __float_as_uint(w0.w);
@@ -310,6 +315,7 @@ NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d) {
       const uint32_t slot = (uint32_t)(__ffs(leaf_hits) - 1) ^ oct;
       leaf_hits &= leaf_hits - 1;
       const uint32_t m = (meta[slot >> 2] >> (8 * (slot & 3))) & 0xffu;
+      tt += ((m >> 5) & 3u) + 1u;
       test_triangles(sc, tri_base + (m & 31u), ((m >> 5) & 3u) + 1u, o, d, cached_inst, lo_o, lo_d, tmax, r);
     }
     if (inner_hits) {
@@ -328,15 +334,18 @@ NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d) {
     if (hits) stack[sp++] = make_uint2(g.x, hits | (gmask << 8));
     node = g.x + __popc(gmask & ((1u << slot) - 1u));
   }
+  if (node_visits) *node_visits += nv;
+  if (tri_tests) *tri_tests += tt;
   return r;
 }
 
 template <int WIDTH>
-NB_D TraceResult trace_closest_w(const DevScene &sc, V3 o, V3 d) {
+NB_D TraceResult trace_closest_w(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
+                                 uint64_t *tri_tests = nullptr) {
   if constexpr (WIDTH == 8)
-    return trace_closest8(sc, o, d);
+    return trace_closest8(sc, o, d, node_visits, tri_tests);
   else
-    return trace_closest2(sc, o, d);
+    return trace_closest2(sc, o, d, node_visits, tri_tests);
 }
 
 NB_D TraceResult trace_closest(const DevScene &sc, V3 o, V3 d) {

@@ -86,7 +86,8 @@ class Frame(C.Structure):
 class RenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("traced", C.c_uint64), ("waves", C.c_uint64),
                 ("device_ms", C.c_double), ("trace_ms", C.c_double), ("shade_ms", C.c_double),
-                ("kernels", C.c_uint64), ("nonfinite", C.c_uint64), ("bad_index", C.c_uint64)]
+                ("kernels", C.c_uint64), ("nonfinite", C.c_uint64), ("bad_index", C.c_uint64),
+                ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

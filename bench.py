@@ -665,6 +665,27 @@ def run_ours(args, rank, world, local_rank):
     if batched:
         films_identical = bool(torch.equal(flat, plain_flat))
 
+    # untimed: the same step once more in the counting trace mode (tuning.trace_mode 2), for the
+    # closest-hit kernel's own work per ray (node visits, triangle tests) on this workload's rays
+    counted = None
+    saved = [c.get_tuning() for c in ctxs]
+    try:
+        for c, t in zip(ctxs, saved):
+            tc = native.Tuning.from_buffer_copy(t)
+            tc.trace_mode = 2
+            tc.bvh_width = 0
+            c.set_tuning(tc)
+        sts = batch_step() if batched else plain_step()
+        nodes = sum(s.node_visits for s in sts)
+        tris = sum(s.tri_tests for s in sts)
+        traced = sum(s.traced for s in sts)
+        counted = {"node_visits_per_ray": nodes / max(1, traced), "tri_tests_per_ray": tris / max(1, traced)}
+    finally:
+        for c, t in zip(ctxs, saved):
+            t2 = native.Tuning.from_buffer_copy(t)
+            t2.bvh_width = 0
+            c.set_tuning(t2)
+
     # end to end through the C ABI from pinned host buffers: upload + build + render + readback
     e2e = None
     if rank == 0 and not args.no_e2e:
@@ -749,13 +770,20 @@ def run_ours(args, rank, world, local_rank):
     # Algorithmic bytes per traced ray (reference binary BVH node/triangle counts measured by the
     # oracle on this workload's rays): 32 B ray + 16 B hit + 64 B per inner-node visit + 36 B per
     # triangle test.
-    b_ray = 32 + 16 + 64 * cpu["node_visits_per_ray"] + 36 * cpu["tri_tests_per_ray"] if cpu else None
+    # reference-BVH model: 32 B ray + 16 B hit + 64 B per inner-node visit + 36 B per triangle test,
+    # with the visit counts the oracle measured on the reference's binary SAH BVH
+    b_ref = 32 + 16 + 64 * cpu["node_visits_per_ray"] + 36 * cpu["tri_tests_per_ray"] if cpu else None
+    if args.workload == "instanced":
+        b_ref = None  # reference-BVH visit counts of a degenerate tree say nothing about k_trace
+    # this kernel's own work: 32 B ray in, 16 B hit + 4 B queue slot out, one node record per visit
+    # (binary 64 B, 8-wide 80 B) and 48 B per triangle tested, counted by the kernel itself
+    node_bytes = 80 if (args.bvh_width or 2) == 8 else 64
+    b_dev = (32 + 20 + node_bytes * counted["node_visits_per_ray"] + 48 * counted["tri_tests_per_ray"]
+             if counted else None)
     trace_rate = acc.traced / (acc.trace_ms / 1e3) if acc.trace_ms > 0 else None
     roof = None
-    if args.workload == "instanced":
-        b_ray = None  # reference-BVH visit counts of a degenerate tree say nothing about k_trace
-    if b_ray and trace_rate:
-        achieved = trace_rate * b_ray / 1e9
+    if b_dev and trace_rate:
+        achieved = trace_rate * b_dev / 1e9
         rays_per_wave = acc.traced / max(1, acc.waves)
         dram_ray = K_TRACE_DRAM_BYTES_PER_RAY[args.workload] or 0.0
         roof = {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -763,10 +791,15 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": dram_ray * rays_per_wave if dram_ray else None,
                 "traffic_note": "DRAM bytes of one full wave (%.0f rays) at %.0f B/ray measured by ncu "
                                 "(dram__bytes_read.sum + dram__bytes_write.sum) on this workload's k_trace waves; "
-                                "achieved uses the algorithmic bytes (reference-BVH node/triangle visits)"
-                                % (rays_per_wave, dram_ray),
+                                "achieved uses this kernel's algorithmic bytes: its own node visits and triangle "
+                                "tests per ray, counted on this workload (trace_mode 2)" % (rays_per_wave, dram_ray),
                 "dram_gbs_from_traffic": trace_rate * dram_ray / 1e9,
-                "bytes_per_ray": b_ray, "trace_ms_per_step": acc.trace_ms / args.steps}
+                "bytes_per_ray": b_dev, "node_visits_per_ray": counted["node_visits_per_ray"],
+                "tri_tests_per_ray": counted["tri_tests_per_ray"], "trace_ms_per_step": acc.trace_ms / args.steps,
+                "reference_bvh_model": None if not b_ref else {
+                    "bytes_per_ray": b_ref, "node_visits_per_ray": cpu["node_visits_per_ray"],
+                    "tri_tests_per_ray": cpu["tri_tests_per_ray"], "achieved": trace_rate * b_ref / 1e9,
+                    "frac": trace_rate * b_ref / 1e9 / hbm}}
     extra = {"waves_per_step": acc.waves / args.steps, "traced_per_step": acc.traced / args.steps,
              "paths_per_step": acc.paths / args.steps, "trace_ms_per_step": acc.trace_ms / args.steps,
              "shade_ms_per_step": acc.shade_ms / args.steps, "bvh_build_s": build_s, "upload_s": upload_s,

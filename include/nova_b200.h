@@ -152,6 +152,10 @@ typedef struct {
    * RENDERER_EXCEPTION, which the engine facade reports as exception::GENERAL_GPU_ERROR. */
   uint64_t nonfinite;
   uint64_t bad_index;
+  /* With tuning.trace_mode 2: inner nodes visited and triangles tested by the closest-hit kernel
+   * (binary BVH: one 64-byte node per visit; 8-wide: one 80-byte node; 48 bytes per triangle). */
+  uint64_t node_visits;
+  uint64_t tri_tests;
 } nova_b200_render_stats;
 
 /* Context lifecycle: DeviceAcceleratorInterface::make (api/device_accelerator_factory.cpp:9) and
@@ -286,7 +290,9 @@ typedef struct {
   int32_t bvh_width;       /* reported by nova_b200_autotune: the BVH width it left the contexts
                               built with (0: not tuned); ignored by nova_b200_set_tuning */
   uint32_t trace_mode;     /* 0: one ray per thread (default); 1: persistent warps that hand out rays
-                              as their lanes finish (binary BVH only; the 8-wide BVH ignores it) */
+                              as their lanes finish (binary BVH only; the 8-wide BVH ignores it);
+                              2: as 0, and the render stats count the traversal's node visits and
+                              triangle tests (a measurement mode; the autotuner never picks it) */
 } nova_b200_tuning;
 
 /* tuning = NULL restores the defaults. */
