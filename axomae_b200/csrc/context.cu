@@ -219,6 +219,9 @@ void free_scene(nova_b200_ctx *c) {
   if (c->d_nodes) cudaFreeAsync(c->d_nodes, c->stream);
   if (c->d_tris) cudaFreeAsync(c->d_tris, c->stream);
   if (c->d_valid) cudaFreeAsync(c->d_valid, c->stream);
+  if (c->d_blas_root) cudaFreeAsync(c->d_blas_root, c->stream);
+  c->d_blas_root = nullptr;
+  c->h_meshes.clear();
   c->d_arena = nullptr;
   c->d_nodes = nullptr;
   c->d_tris = nullptr;
@@ -411,6 +414,254 @@ __global__ void k_validate(const float4 *nodes, uint32_t n_nodes, uint32_t n_tri
       if (f + cnt > n_tris) atomicAdd(bad, 1u);
     }
   }
+}
+
+/* ------------------------------------------------------------------ two-level BVH (width 1)
+ *
+ * The reference's Embree accelerator keeps one sub-scene per mesh under its instances
+ * (aggregate/api/embree/embree.cpp:236-254).  Here: a binary BVH per mesh over its object-space
+ * triangles that can be hit (bottom level, built once however many instances use the mesh), and a
+ * binary BVH over the instances' world-space boxes with one instance per leaf (top level), in one
+ * node array: the top level first, then each mesh's nodes with their references relocated.  Bottom
+ * triangle records hold the mesh-local triangle id; the hit's primitive id is the instance's first
+ * primitive id plus it, the reference's numbering (api/engine.cpp:159-175). */
+
+/* 1 where a mesh triangle can be hit (no repeated vertex index, Triangle.h:127-132). */
+__global__ void k_mesh_flags(nb::DevMesh m, uint32_t *flags) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m.n_tris) return;
+  const uint32_t a = m.idx[3 * (size_t)t], b = m.idx[3 * (size_t)t + 1], c = m.idx[3 * (size_t)t + 2];
+  flags[t] = (a == b || c == b || c == a) ? 0u : 1u;
+}
+
+__global__ void k_mesh_boxes(nb::DevMesh m, const uint32_t *ids, uint32_t n, float4 *lo, float4 *hi) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t t = ids[i];
+  nb::V3 w[3];
+  for (int k = 0; k < 3; k++) w[k] = nb::vertex_position(m, m.idx[3 * (size_t)t + k]);
+  lo[i] = make_float4(fminf(w[0].x, fminf(w[1].x, w[2].x)), fminf(w[0].y, fminf(w[1].y, w[2].y)),
+                      fminf(w[0].z, fminf(w[1].z, w[2].z)), 0.f);
+  hi[i] = make_float4(fmaxf(w[0].x, fmaxf(w[1].x, w[2].x)), fmaxf(w[0].y, fmaxf(w[1].y, w[2].y)),
+                      fmaxf(w[0].z, fmaxf(w[1].z, w[2].z)), 0.f);
+}
+
+/* Bottom-level triangle records in leaf order: (v0, mesh-local triangle id), (v1 - v0, 0), (v2 - v0, 0). */
+__global__ void k_write_blas_tris(nb::DevMesh m, const uint32_t *ids, const uint32_t *order, uint32_t n, float4 *tris) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t t = ids[order[k]];
+  const uint32_t a = m.idx[3 * (size_t)t], b = m.idx[3 * (size_t)t + 1], cc = m.idx[3 * (size_t)t + 2];
+  const nb::V3 v0 = nb::vertex_position(m, a), v1 = nb::vertex_position(m, b), v2 = nb::vertex_position(m, cc);
+  const nb::V3 e1 = v1 - v0, e2 = v2 - v0;
+  tris[3 * k + 0] = make_float4(v0.x, v0.y, v0.z, __int_as_float((int)t));
+  tris[3 * k + 1] = make_float4(e1.x, e1.y, e1.z, 0.f);
+  tris[3 * k + 2] = make_float4(e2.x, e2.y, e2.z, 0.f);
+}
+
+/* A bottom level built at node 0 moved to node_base, its triangles to tri_base. */
+__global__ void k_relocate(float4 *nodes, uint32_t n_nodes, uint32_t node_base, uint32_t tri_base) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_nodes) return;
+  float4 &n3 = nodes[4 * (size_t)(node_base + i) + 3];
+  int32_t r[2] = {__float_as_int(n3.x), __float_as_int(n3.y)};
+  for (int s = 0; s < 2; s++)
+    r[s] = r[s] >= 0 ? r[s] + (int32_t)node_base : nb::leaf_ref(nb::leaf_first(r[s]) + tri_base, nb::leaf_count(r[s]));
+  n3.x = __int_as_float(r[0]);
+  n3.y = __int_as_float(r[1]);
+}
+
+/* World box of each instance: the eight corners of its mesh's bottom-level root box, transformed. */
+__global__ void k_instance_boxes(const nb::DevInstance *inst, uint32_t n, const float4 *nodes, const uint32_t *blas_root,
+                                 float4 *lo, float4 *hi) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const nb::DevInstance &I = inst[i];
+  const float4 *rn = nodes + 4 * (size_t)blas_root[I.mesh];
+  const float4 n0 = rn[0], n1 = rn[1], n2 = rn[2];
+  /* union of the root's two child boxes (an empty child box is inverted and drops out) */
+  const nb::V3 bl{fminf(n0.x, n1.x), fminf(n0.z, n1.z), fminf(n2.x, n2.z)};
+  const nb::V3 bh{fmaxf(n0.y, n1.y), fmaxf(n0.w, n1.w), fmaxf(n2.y, n2.w)};
+  nb::V3 wl{FLT_MAX, FLT_MAX, FLT_MAX}, wh{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int k = 0; k < 8; k++) {
+    const nb::V3 p{(k & 1) ? bh.x : bl.x, (k & 2) ? bh.y : bl.y, (k & 4) ? bh.z : bl.z};
+    const nb::V3 w = I.identity ? p : nb::xform_point(I.m, p);
+    wl = nb::V3{fminf(wl.x, w.x), fminf(wl.y, w.y), fminf(wl.z, w.z)};
+    wh = nb::V3{fmaxf(wh.x, w.x), fmaxf(wh.y, w.y), fmaxf(wh.z, w.z)};
+  }
+  lo[i] = make_float4(wl.x, wl.y, wl.z, 0.f);
+  hi[i] = make_float4(wh.x, wh.y, wh.z, 0.f);
+}
+
+/* Top-level leaves (one instance each) name the instance itself instead of its slot in `order`. */
+__global__ void k_top_leaves(float4 *nodes, uint32_t n_nodes, const uint32_t *order) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_nodes) return;
+  float4 &n3 = nodes[4 * (size_t)i + 3];
+  int32_t r[2] = {__float_as_int(n3.x), __float_as_int(n3.y)};
+  for (int s = 0; s < 2; s++)
+    if (r[s] < 0) r[s] = nb::leaf_ref(order[nb::leaf_first(r[s])], 1u);
+  n3.x = __int_as_float(r[0]);
+  n3.y = __int_as_float(r[1]);
+}
+
+/* Builds the two-level BVH into c->d_nodes / c->d_tris / c->d_blas_root.  res: total nodes, leaves,
+ * and the deepest top + bottom path (for the traversal stack). */
+nova_b200_status build_two_level(nova_b200_ctx *c, const nb::BvhBuildParams &p, nb::BvhBuildResult &res) {
+  using namespace nbctx;
+  const uint32_t n_inst = (uint32_t)c->h_instances.size(), n_meshes = (uint32_t)c->h_meshes.size();
+  std::vector<char> used(n_meshes, 0);
+  for (const nb::DevInstance &I : c->h_instances) used[I.mesh] = 1;
+  /* per used mesh: the triangles that can be hit, compacted on the device */
+  std::vector<uint32_t *> ids(n_meshes, nullptr);
+  std::vector<uint32_t> count(n_meshes, 0);
+  uint32_t *counts_h = c->h_counters; /* 16 pinned words: done in batches of 8 meshes (count, bad) */
+  auto free_ids = [&] {
+    for (uint32_t *q : ids)
+      if (q) cudaFreeAsync(q, c->stream);
+  };
+  for (uint32_t m0 = 0; m0 < n_meshes; m0 += 8) {
+    const uint32_t m1 = std::min(n_meshes, m0 + 8);
+    for (uint32_t m = m0; m < m1; m++) {
+      if (!used[m]) continue;
+      const nb::DevMesh &M = c->h_meshes[m];
+      const uint32_t T = M.n_tris, nb_ = (T + kCompactItems - 1) / kCompactItems;
+      uint32_t *flags = nullptr, *cnts = nullptr;
+      cudaError_t e = cudaMallocAsync(&ids[m], sizeof(uint32_t) * T, c->stream);
+      if (e == cudaSuccess) e = cudaMallocAsync(&flags, sizeof(uint32_t) * T, c->stream);
+      if (e == cudaSuccess) e = cudaMallocAsync(&cnts, sizeof(uint32_t) * (nb_ + 1), c->stream);
+      if (e == cudaSuccess) {
+        k_mesh_flags<<<(T + 255) / 256, 256, 0, c->stream>>>(M, flags);
+        k_compact_count<<<nb_, kCompactThreads, 0, c->stream>>>(flags, T, cnts);
+        k_compact_offsets<<<1, kCompactThreads, 0, c->stream>>>(cnts, nb_, c->d_counters + (m - m0));
+        k_compact_write<<<nb_, kCompactThreads, 0, c->stream>>>(flags, T, cnts, ids[m]);
+        e = cudaGetLastError();
+      }
+      if (flags) cudaFreeAsync(flags, c->stream);
+      if (cnts) cudaFreeAsync(cnts, c->stream);
+      if (e != cudaSuccess) {
+        free_ids();
+        return cuda_fail(c, e, "two-level BVH: triangle lists");
+      }
+    }
+    NB_CUDA(c, cudaMemcpyAsync(counts_h, c->d_counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream),
+            "readback");
+    NB_CUDA(c, cudaStreamSynchronize(c->stream), "two-level BVH");
+    for (uint32_t m = m0; m < m1; m++)
+      if (used[m]) count[m] = counts_h[m - m0];
+  }
+  /* node and triangle offsets: top level first */
+  const size_t top_nodes = std::max<size_t>(2 * (size_t)n_inst, 2);
+  std::vector<uint32_t> node_off(n_meshes, 0), tri_off(n_meshes, 0);
+  size_t total_nodes = top_nodes, total_tris = 0;
+  size_t real_tris = 0;
+  for (uint32_t m = 0; m < n_meshes; m++) {
+    if (!used[m]) continue;
+    node_off[m] = (uint32_t)total_nodes;
+    tri_off[m] = (uint32_t)total_tris;
+    /* a mesh of degenerate triangles only gets one node over one zero triangle (never hit) */
+    total_nodes += std::max<size_t>(2 * (size_t)count[m], 2);
+    total_tris += std::max<uint32_t>(count[m], 1u);
+    real_tris += count[m];
+  }
+  if (real_tris == 0 || total_nodes >= (1ull << 31) || total_tris >= (1ull << 27)) {
+    free_ids();
+    return fail(c, NOVA_B200_INVALID_SCENE_TYPE, "two-level BVH: no triangle can be hit, or too many%s");
+  }
+  float4 *lo = nullptr, *hi = nullptr;
+  uint32_t *order = nullptr;
+  size_t scratch = n_inst;
+  for (uint32_t m = 0; m < n_meshes; m++) scratch = std::max<size_t>(scratch, count[m]);
+  cudaError_t e = cudaMallocAsync(&c->d_nodes, sizeof(float4) * 4 * total_nodes, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&c->d_tris, sizeof(float4) * 3 * total_tris, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&c->d_blas_root, sizeof(uint32_t) * n_meshes, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_nodes, 0, sizeof(float4) * 4 * total_nodes, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_tris, 0, sizeof(float4) * 3 * total_tris, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&lo, sizeof(float4) * scratch, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&hi, sizeof(float4) * scratch, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&order, sizeof(uint32_t) * scratch, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_counters, 0, 4, c->stream);
+  auto cleanup = [&] {
+    free_ids();
+    if (lo) cudaFreeAsync(lo, c->stream);
+    if (hi) cudaFreeAsync(hi, c->stream);
+    if (order) cudaFreeAsync(order, c->stream);
+  };
+  if (e != cudaSuccess) {
+    cleanup();
+    return cuda_fail(c, e, "cudaMalloc(two-level BVH)");
+  }
+  /* bottom levels */
+  std::vector<uint32_t> roots(n_meshes, 0);
+  nb::BvhBuildResult r{};
+  int bottom_depth = 0;
+  res = nb::BvhBuildResult{};
+  for (uint32_t m = 0; m < n_meshes; m++) {
+    if (!used[m]) continue;
+    if (count[m] == 0) { /* the placeholder: a point box at the origin over a zero triangle */
+      float4 node[4] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
+                        make_float4(0.f, 0.f, 0.f, 0.f)};
+      const int32_t ref = nb::leaf_ref(tri_off[m], 1u);
+      node[3].x = node[3].y = *reinterpret_cast<const float *>(&ref);
+      e = cudaMemcpyAsync(c->d_nodes + 4 * (size_t)node_off[m], node, sizeof(node), cudaMemcpyHostToDevice, c->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream); /* `node` is a stack array */
+      if (e != cudaSuccess) {
+        cleanup();
+        return cuda_fail(c, e, "two-level BVH: placeholder");
+      }
+      roots[m] = node_off[m]; /* its triangle record stays zero (the array was cleared) */
+      continue;
+    }
+    const uint32_t n = count[m];
+    const nb::DevMesh &M = c->h_meshes[m];
+    float4 *nodes = c->d_nodes + 4 * (size_t)node_off[m];
+    float4 *tris = c->d_tris + 3 * (size_t)tri_off[m];
+    k_mesh_boxes<<<(n + 255) / 256, 256, 0, c->stream>>>(M, ids[m], n, lo, hi);
+    e = nb::build_bvh(lo, hi, n, p, nodes, order, c->stream, &r);
+    if (e == cudaSuccess) {
+      k_write_blas_tris<<<(n + 255) / 256, 256, 0, c->stream>>>(M, ids[m], order, n, tris);
+      k_validate<<<(r.n_nodes + 255) / 256, 256, 0, c->stream>>>(nodes, r.n_nodes, n, c->d_counters);
+      k_relocate<<<(r.n_nodes + 255) / 256, 256, 0, c->stream>>>(c->d_nodes, r.n_nodes, node_off[m], tri_off[m]);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess || r.n_nodes > std::max<uint32_t>(2 * n, 2)) {
+      cleanup();
+      return e != cudaSuccess ? cuda_fail(c, e, "two-level BVH: bottom level")
+                              : fail(c, NOVA_B200_RENDERER_EXCEPTION, "BVH validation failed%s");
+    }
+    roots[m] = node_off[m];
+    res.n_nodes += r.n_nodes;
+    res.n_leaves += r.n_leaves;
+    res.ms += r.ms;
+    bottom_depth = std::max(bottom_depth, r.max_depth);
+  }
+  NB_CUDA(c, cudaMemcpyAsync(c->d_blas_root, roots.data(), sizeof(uint32_t) * n_meshes, cudaMemcpyHostToDevice,
+                             c->stream),
+          "upload(bottom-level roots)");
+  /* top level: one instance per leaf */
+  nb::BvhBuildParams pt = p;
+  pt.max_leaf = 1;
+  pt.hard_leaf = 1;
+  const nb::DevInstance *d_inst = c->scene.instances;
+  k_instance_boxes<<<(n_inst + 255) / 256, 256, 0, c->stream>>>(d_inst, n_inst, c->d_nodes, c->d_blas_root, lo, hi);
+  e = nb::build_bvh(lo, hi, n_inst, pt, c->d_nodes, order, c->stream, &r);
+  if (e == cudaSuccess) {
+    k_validate<<<(r.n_nodes + 255) / 256, 256, 0, c->stream>>>(c->d_nodes, r.n_nodes, n_inst, c->d_counters);
+    k_top_leaves<<<(r.n_nodes + 255) / 256, 256, 0, c->stream>>>(c->d_nodes, r.n_nodes, order);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->h_counters, c->d_counters, 4, cudaMemcpyDeviceToHost, c->stream);
+  cleanup();
+  if (e != cudaSuccess) return cuda_fail(c, e, "two-level BVH: top level");
+  NB_CUDA(c, cudaStreamSynchronize(c->stream), "two-level BVH");
+  res.n_nodes += r.n_nodes;
+  res.n_leaves += r.n_leaves;
+  res.ms += r.ms;
+  res.max_depth = r.max_depth + bottom_depth + 1; /* + the stack entry that leaves an instance */
+  if (c->h_counters[0] != 0 || r.n_nodes == 0 || r.n_nodes > top_nodes || res.max_depth >= nb::kTraversalStack)
+    return fail(c, NOVA_B200_RENDERER_EXCEPTION, "BVH validation failed%s");
+  return NOVA_B200_SUCCESS;
 }
 
 /* Runs op(k) for k < n on up to 16 host threads; returns the first failing status (its message is
@@ -647,6 +898,7 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
   }
   plan.pieces.push_back(Piece{tex.data(), tex.size() * sizeof(nb::DevTexture), off_tex, false});
   plan.pieces.push_back(Piece{meshes.data(), meshes.size() * sizeof(nb::DevMesh), off_mesh, false});
+  c->h_meshes = meshes;
   nova_b200_status st = copy_pieces(c, plan, arena, temp);
   if (st != NOVA_B200_SUCCESS) {
     cudaFreeAsync(temp, c->stream);
@@ -710,7 +962,8 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
   cudaSetDevice(c->device);
   const uint32_t n = c->n_valid;
   const int width = opts && opts->width ? opts->width : 2;
-  if (width != 2 && width != 8) return fail(c, NOVA_B200_INVALID_ARGUMENT, "BVH width must be 2 or 8%s");
+  if (width != 1 && width != 2 && width != 8)
+    return fail(c, NOVA_B200_INVALID_ARGUMENT, "BVH width must be 1 (two-level), 2 or 8%s");
   nb::BvhBuildParams p;
   p.max_leaf = opts && opts->max_leaf_size > 0 ? opts->max_leaf_size : (width == 8 ? nb::kWideLeafMax : 8);
   p.hard_leaf = width == 8 ? nb::kWideLeafMax : 16;
@@ -723,10 +976,29 @@ nova_b200_status nova_b200_build_bvh(nova_b200_ctx *c, const nova_b200_bvh_optio
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "max_leaf_size must be 1..16 (1..4 for width 8) and bins 4..32%s");
   if (c->d_nodes) cudaFreeAsync(c->d_nodes, c->stream);
   if (c->d_tris) cudaFreeAsync(c->d_tris, c->stream);
+  if (c->d_blas_root) cudaFreeAsync(c->d_blas_root, c->stream);
   c->d_nodes = nullptr;
   c->d_tris = nullptr;
+  c->d_blas_root = nullptr;
+  c->scene.blas_root = nullptr;
   c->bvh_ready = false;
   c->primal_valid = false;
+  if (width == 1) {
+    nb::BvhBuildResult r{};
+    const nova_b200_status st = build_two_level(c, p, r);
+    if (st != NOVA_B200_SUCCESS) return st;
+    c->scene.nodes = c->d_nodes;
+    c->scene.tris = c->d_tris;
+    c->scene.blas_root = c->d_blas_root;
+    c->scene.width = 1;
+    c->bvh_width = 1;
+    c->n_nodes = r.n_nodes;
+    c->n_leaves = r.n_leaves;
+    c->bvh_depth = r.max_depth;
+    c->bvh_ms = r.ms;
+    c->bvh_ready = true;
+    return NOVA_B200_SUCCESS;
+  }
   const uint32_t *d_valid = c->d_valid;
   uint32_t *d_order = nullptr;
   float4 *d_lo = nullptr, *d_hi = nullptr;

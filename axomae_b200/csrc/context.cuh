@@ -25,6 +25,8 @@ struct nova_b200_ctx {
   size_t h_stage_bytes = 0;
   nb::DevScene scene{};
   std::vector<nb::DevInstance> h_instances;
+  std::vector<nb::DevMesh> h_meshes;      /* device pointers, host copy of the mesh table */
+  uint32_t *d_blas_root = nullptr;        /* two-level BVH: per mesh, its bottom-level root node */
   uint32_t *d_valid = nullptr;   /* global primitive ids that can be hit, ascending (device) */
   uint32_t n_valid = 0;
   uint64_t n_prims = 0;

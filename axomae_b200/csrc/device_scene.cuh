@@ -73,6 +73,7 @@ struct DevScene {
   uint32_t has_emissive;
   const float *diff_albedo;  /* differentiable parameters (NULL: textures): 3 x n_prims RGB albedo */
   const float *diff_rough;   /* and n_materials roughness values */
+  const uint32_t *blas_root; /* two-level BVH (width 1): per mesh, the node index of its bottom-level root */
 };
 
 constexpr int kAcosPrecision = 500000;

@@ -857,6 +857,8 @@ template <class JS>
 void enqueue_group(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int width, int slot, bool external) {
   if (width == 8)
     enqueue_waves<JS, 8>(c, js, ls, slot, external);
+  else if (width == 1)
+    enqueue_waves<JS, 1>(c, js, ls, slot, external);
   else
     enqueue_waves<JS, 2>(c, js, ls, slot, external);
 }
@@ -1250,6 +1252,8 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
     auto bwd = [&](int slot) {
       if (width == 8)
         enqueue_waves<OneJob, 8, true>(c, one, ls, slot, false, &adj);
+      else if (width == 1)
+        enqueue_waves<OneJob, 1, true>(c, one, ls, slot, false, &adj);
       else
         enqueue_waves<OneJob, 2, true>(c, one, ls, slot, false, &adj);
       return cudaGetLastError();

@@ -13,6 +13,8 @@
  * Moller-Trumbore test would hit.
  *
  * Node layout and leaf encoding: see device_scene.cuh.  Leaf reference = ~((first << 4) | (count - 1)).
+ * Three layouts: binary (width 2), compressed 8-wide (width 8) and two-level binary (width 1: a top
+ * level over instances, a bottom level per mesh).
  */
 #pragma once
 #include <cfloat>
@@ -339,17 +341,122 @@ NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d, uint64_t *node_v
   return r;
 }
 
+/* Closest hit on the two-level BVH (width 1): the top level's binary nodes over instance boxes, one
+ * instance per leaf; at a top leaf the ray is brought into the instance's object space (its
+ * inverse transform, Triangle.h:150-153; identity instances keep the world ray bit for bit) and the
+ * walk goes on in the mesh's bottom-level BVH, with a marker on the stack that restores the world
+ * ray when that subtree is done.  t is the same in both spaces (the direction is not renormalised),
+ * so the closest distance found so far prunes both levels.  Node tests, ordering and the triangle
+ * test are trace_closest2's. */
+constexpr int32_t kLeaveInstance = 0x7fffffff; /* stack marker: back to the top level */
+
+NB_D TraceResult trace_closest_tl(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
+                                  uint64_t *tri_tests = nullptr) {
+  TraceResult r{-1, 0.f, 0.f, 0.f};
+  float tmax = FLT_MAX;
+  V3 ro = o, rd = d;
+  float ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
+  int32_t stack[kTraversalStack];
+  int sp = 0;
+  int32_t cur = 0;
+  uint32_t prim_base = 0;
+  bool inside = false;
+  uint32_t nv = 0, tt = 0;
+  for (;;) {
+    if (cur >= 0) {
+      nv++;
+      const float4 n0 = __ldg(&sc.nodes[4 * cur + 0]);
+      const float4 n1 = __ldg(&sc.nodes[4 * cur + 1]);
+      const float4 n2 = __ldg(&sc.nodes[4 * cur + 2]);
+      const float4 n3 = __ldg(&sc.nodes[4 * cur + 3]);
+      float a0 = (n0.x - ro.x) * ix, b0 = (n0.y - ro.x) * ix;
+      float a1 = (n0.z - ro.y) * iy, b1 = (n0.w - ro.y) * iy;
+      float a2 = (n2.x - ro.z) * iz, b2 = (n2.y - ro.z) * iz;
+      float c0n = fmaxf(fmaxf(fminf(a0, b0), fminf(a1, b1)), fmaxf(fminf(a2, b2), 0.f));
+      float c0f = fminf(fminf(fminf(fmaxf(a0, b0), fmaxf(a1, b1)), fmaxf(a2, b2)) * kFarScale, tmax);
+      float d0 = (n1.x - ro.x) * ix, e0 = (n1.y - ro.x) * ix;
+      float d1 = (n1.z - ro.y) * iy, e1 = (n1.w - ro.y) * iy;
+      float d2 = (n2.z - ro.z) * iz, e2 = (n2.w - ro.z) * iz;
+      float c1n = fmaxf(fmaxf(fminf(d0, e0), fminf(d1, e1)), fmaxf(fminf(d2, e2), 0.f));
+      float c1f = fminf(fminf(fminf(fmaxf(d0, e0), fmaxf(d1, e1)), fmaxf(d2, e2)) * kFarScale, tmax);
+      const bool h0 = c0n <= c0f, h1 = c1n <= c1f;
+      const int32_t r0 = __float_as_int(n3.x), r1 = __float_as_int(n3.y);
+      if (h0 && h1) {
+        int32_t first = r0, second = r1;
+        if (c1n < c0n) {
+          first = r1;
+          second = r0;
+        }
+        if (sp < kTraversalStack) stack[sp++] = second;
+        cur = first;
+        continue;
+      } else if (h0) {
+        cur = r0;
+        continue;
+      } else if (h1) {
+        cur = r1;
+        continue;
+      }
+    } else if (!inside) { /* top-level leaf: enter the instance */
+      const DevInstance &I = sc.instances[leaf_first(cur)];
+      if (!I.identity) {
+        ro = xform_point(I.inv, o);
+        rd = xform_dir(I.inv, d);
+        ix = safe_rcp(rd.x), iy = safe_rcp(rd.y), iz = safe_rcp(rd.z);
+      }
+      prim_base = I.prim_offset;
+      inside = true;
+      if (sp < kTraversalStack) stack[sp++] = kLeaveInstance;
+      cur = (int32_t)sc.blas_root[I.mesh];
+      continue;
+    } else { /* bottom-level leaf: object-space triangles, mesh-local ids */
+      const uint32_t first = leaf_first(cur), count = leaf_count(cur);
+      for (uint32_t k = first; k < first + count; k++) {
+        const float4 t0 = __ldg(&sc.tris[3 * k + 0]);
+        const float4 t1 = __ldg(&sc.tris[3 * k + 1]);
+        const float4 t2 = __ldg(&sc.tris[3 * k + 2]);
+        tt++;
+        float ht, hu, hv;
+        if (mt_hit(ro, rd, V3{t0.x, t0.y, t0.z}, V3{t1.x, t1.y, t1.z}, V3{t2.x, t2.y, t2.z}, kRayTNear, tmax, ht, hu,
+                   hv)) {
+          tmax = ht;
+          r.prim = (int32_t)(prim_base + (uint32_t)__float_as_int(t0.w));
+          r.t = ht;
+          r.u = hu;
+          r.v = hv;
+        }
+      }
+    }
+    /* pop; the marker returns the walk to the top level and the world ray */
+    for (;;) {
+      if (sp == 0) {
+        if (node_visits) *node_visits += nv;
+        if (tri_tests) *tri_tests += tt;
+        return r;
+      }
+      cur = stack[--sp];
+      if (cur != kLeaveInstance) break;
+      inside = false;
+      ro = o;
+      rd = d;
+      ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
+    }
+  }
+}
+
 template <int WIDTH>
 NB_D TraceResult trace_closest_w(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
                                  uint64_t *tri_tests = nullptr) {
   if constexpr (WIDTH == 8)
     return trace_closest8(sc, o, d, node_visits, tri_tests);
+  else if constexpr (WIDTH == 1)
+    return trace_closest_tl(sc, o, d, node_visits, tri_tests);
   else
     return trace_closest2(sc, o, d, node_visits, tri_tests);
 }
 
 NB_D TraceResult trace_closest(const DevScene &sc, V3 o, V3 d) {
-  return sc.width == 8 ? trace_closest8(sc, o, d) : trace_closest2(sc, o, d);
+  return sc.width == 8 ? trace_closest8(sc, o, d) : sc.width == 1 ? trace_closest_tl(sc, o, d) : trace_closest2(sc, o, d);
 }
 
 }  // namespace nb

@@ -434,10 +434,12 @@ def test_batch_workload_scene_matches_oracle(job, ctx, oracle, batch_jobs):
     assert err <= REL_RMSE_TOL, err
 
 
-@pytest.mark.parametrize("width", [2, 8], ids=["bvh2", "bvh8"])
+@pytest.mark.parametrize("width", [2, 8, 1], ids=["bvh2", "bvh8", "two_level"])
 def test_instanced_scene_matches_oracle(ctx, oracle, torch_cuda, width):
     """Seeded meshes placed many times with random rigid transforms: rays are brought into each
-    instance's object space (Triangle.h:150-153) exactly as the reference does."""
+    instance's object space (Triangle.h:150-153) exactly as the reference does, with the flat BVHs
+    over every instanced triangle and with the two-level one (a BVH per mesh under a BVH over the
+    instances, as the reference's Embree scene keeps them, embree.cpp:236-254)."""
     from axomae_b200 import scenes
     s = scenes.instanced_scene(n_meshes=3, n_instances=40, tris_per_mesh=1500, width=64, height=48, seed=8,
                                box_size=20.0, env_w=64, env_h=32)
@@ -601,3 +603,46 @@ def test_bake_texunit_matches_oracle(ctx, oracle, torch_cuda, channels):
         assert rel_rmse(dev, ref) <= 1e-3, rel_rmse(dev, ref)
         cpu_path = oracle.bake_irradiance(np.concatenate([src[..., :3], np.ones_like(src[..., :1])], -1), ow, oh, 128)
         assert rel_rmse(dev, cpu_path) > 1e-2  # a different estimator from the CPU path's, as in the reference
+
+
+def test_two_level_bvh_edge_cases(ctx, oracle, torch_cuda):
+    """The two-level BVH with one mesh under many instances (shared bottom level), an identity
+    instance (the world ray kept bit for bit), an unused mesh, and a mesh whose triangles are all
+    degenerate (never hit, Triangle.h:127-132): hits equal the oracle's except exact ties, images
+    within 1e-3, and the same closest primitives as the flat BVH."""
+    from axomae_b200 import scenes
+    s = scenes.instanced_scene(n_meshes=3, n_instances=30, tris_per_mesh=800, width=48, height=40, seed=12,
+                               box_size=16.0, env_w=64, env_h=32)
+    meshes = list(s["meshes"])
+    deg = dict(meshes[0])
+    deg["indices"] = np.repeat(np.asarray(meshes[0]["indices"]).reshape(-1, 3)[:, :1], 3, axis=1)
+    meshes.append(deg)                      # all-degenerate mesh, placed once
+    meshes.append(dict(meshes[1]))          # unused mesh
+    insts = list(s["instances"])
+    ident = dict(insts[0])
+    eye = np.eye(4, dtype=np.float32)
+    ident.update(m=scenes.col_major(eye), inv=scenes.col_major(eye), n=np.eye(3, dtype=np.float32).reshape(9))
+    insts.append(ident)
+    placed = dict(insts[1])
+    placed["mesh"] = len(meshes) - 2
+    insts.append(placed)
+    s = dict(s, meshes=meshes, instances=insts)
+    osc = oracle.OracleScene(s)
+    rng = np.random.default_rng(5)
+    n = 40000
+    o = rng.uniform(-10, 10, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    ctx.upload(s)
+    ctx.build(width=2)
+    flat = _trace(ctx, torch_cuda, o, d)
+    ctx.build(width=1)
+    info = ctx.info()
+    assert info["nodes"] > 0
+    _check_hits(ctx, torch_cuda, osc, o, d, 1e-4)
+    two = _trace(ctx, torch_cuda, o, d)
+    same = (two[0] == flat[0]) | ((two[0] >= 0) & (flat[0] >= 0) & (two[1] == flat[1]))
+    assert same.all()
+    film, _ = _render(ctx, s, 48, 40, 8, 6)
+    ref, _ = osc.render(oracle.options(48, 40, 8, 6))
+    assert rel_rmse(film, ref) <= REL_RMSE_TOL
