@@ -580,6 +580,73 @@ def adjoint_timing(local_rank, reps=3):
                     "reusing variant takes the per-path radiance the forward render left in the radiance buffer"}
 
 
+def instanced_bvh_forms(ctx, job, frame, reps=2):
+    """The instanced scene (1000 instances of 10 meshes) with each BVH form: the flat binary BVH over
+    every instanced triangle's world box (width 2) and the two-level one, a BVH per mesh under a
+    BVH over the instances (width 1, as the reference's Embree scene keeps them).  Per form: the
+    build's wall clock (one synchronous call), the device memory, and the render's Mrays/s (device
+    time, median of `reps` after one warm-up)."""
+    import torch
+    out = {}
+    for name, width in (("flat", 2), ("two_level", 1)):
+        t0 = time.perf_counter()
+        ctx.build(width=width)
+        build_s = time.perf_counter() - t0
+        info = ctx.info()
+        film = torch.zeros((job["height"], job["width"], 4), device="cuda")
+        vals = []
+        for _ in range(reps + 1):
+            st = ctx.render(frame, film_device_ptr=film.data_ptr())
+            vals.append(st.traced / st.device_ms / 1e3)
+        out[name] = {"width": width, "build_ms": build_s * 1e3, "nodes": info["nodes"],
+                     "device_bytes": info["device_bytes"], "mrays": float(np.median(vals[1:])),
+                     "trace_ms": st.trace_ms}
+    return out
+
+
+def instanced_gradients(local_rank, width, reps=2):
+    """Roughness gradients of the instanced scene at 512 x 512 (16 spp, depth 12): per-material
+    roughness (8 materials, init 0.3) against a target rendered with seeded roughness U[0.1, 0.6],
+    L2 loss; device times of one forward render and one replay-adjoint backward (roughness only)."""
+    import torch
+    from axomae_b200 import native, scenes
+    W = H = 512
+    spp, depth = IN["spp"], IN["depth"]
+    s = scenes.instanced_scene(n_meshes=10, n_instances=1000, tris_per_mesh=10000, width=W, height=H, seed=0,
+                               env_w=4096, env_h=2048)
+    c = native.Context(local_rank)
+    try:
+        c.upload(s)
+        c.build(width=width)
+        nmat = len(s["materials"])
+        rng = np.random.default_rng(1)
+        rough_t = torch.tensor(rng.uniform(0.1, 0.6, nmat), dtype=torch.float32, device="cuda")
+        rough = torch.full((nmat,), 0.3, device="cuda")
+        fr = native.make_frame(s, W, H, spp, depth)
+        T = torch.zeros((H, W, 4), device="cuda")
+        c.set_diff_params(None, rough_t.data_ptr())
+        c.render(fr, film_device_ptr=T.data_ptr())
+        c.set_diff_params(None, rough.data_ptr())
+        img = torch.zeros((H, W, 4), device="cuda")
+        gr = torch.zeros_like(rough)
+        fwd, bwd = [], []
+        for _ in range(reps + 1):
+            st = c.render(fr, film_device_ptr=img.data_ptr())
+            dI = torch.zeros_like(img)
+            dI[..., :3] = 2.0 * (img[..., :3] - T[..., :3])
+            gr.zero_()
+            bst = c.backward(fr, dI.data_ptr(), None, gr.data_ptr())
+            fwd.append(st.device_ms)
+            bwd.append(bst.device_ms)
+        f, b = float(np.median(fwd[1:])), float(np.median(bwd[1:]))
+        return {"workload": "instanced scene at 512x512, 16 spp, depth 12; params: %d material roughnesses" % nmat,
+                "bvh_width": width, "forward_ms": f, "backward_ms": b, "backward_over_forward": b / f,
+                "grad_roughness": [float(x) for x in gr.cpu().numpy()],
+                "note": "device time (CUDA events); backward = radiance replay + adjoint replay"}
+    finally:
+        c.close()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from axomae_b200 import native
@@ -825,6 +892,10 @@ def run_ours(args, rank, world, local_rank):
         extra["rel_rmse_pixels"] = "every %dth pixel of every frame, all samples" % cpu_stride(args.workload)
     if batched and not args.no_adjoint:
         extra["adjoint"] = adjoint_timing(local_rank)
+    if args.workload == "instanced":
+        extra["bvh_forms"] = instanced_bvh_forms(ctxs[0], jobs[0], frames[0])
+        if not args.no_adjoint:
+            extra["gradients_512"] = instanced_gradients(local_rank, args.bvh_width or 2)
     if batched and not args.no_film_io:
         extra["film_io"] = film_io_timing(local_rank, cpu_baseline=not args.no_cpu and local_rank == 0)
     if batched and not args.no_bake:
@@ -867,7 +938,8 @@ def main():
     ap.add_argument("--no-bake", action="store_true", help="skip the irradiance bake timing")
     ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="heightfield: override the frame size")
     ap.add_argument("--spp", type=int, help="heightfield: override samples per pixel")
-    ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 8], help="BVH layout (0 = library default)")
+    ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 1, 2, 8],
+                    help="BVH layout: 2 binary, 8 compressed 8-wide, 1 two-level (0 = library default)")
     args = ap.parse_args()
     if args.frame:
         HF["width"], HF["height"] = args.frame
