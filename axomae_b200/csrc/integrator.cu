@@ -269,8 +269,17 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
  * Integrator.cpp:94-98); hits are appended to a compact hit list so the shading kernel only runs
  * on rays that hit.  At least 10 resident blocks of 128 (48 registers): the walk is latency-bound,
  * and 40 warps per SM beat 32 (-4% on the batched scenes); 12 blocks spill the walk state. */
+/* Resident blocks of 128 threads per SM that k_trace is compiled for (the register bound is
+ * 65536 / (128 * blocks)): binary layouts and the 8-wide one separately. */
+#ifndef NB_TRACE_MIN_BLOCKS
+#define NB_TRACE_MIN_BLOCKS 10
+#endif
+#ifndef NB_TRACE8_MIN_BLOCKS
+#define NB_TRACE8_MIN_BLOCKS 10
+#endif
+
 template <int WIDTH, class JS, bool ADJ = false, bool COUNT = false>
-__global__ void __launch_bounds__(128, 10) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
+__global__ void __launch_bounds__(128, WIDTH == 8 ? NB_TRACE8_MIN_BLOCKS : NB_TRACE_MIN_BLOCKS) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
                                                const __grid_constant__ JS js) {
   const uint32_t n = wcp->n_active + wave_new(*wcp);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
