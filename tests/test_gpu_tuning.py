@@ -34,7 +34,9 @@ def _film(c, s, W=61, H=47, spp=32, depth=6):
     dict(tile_w=1, tile_h=1),                                  # image rows
     dict(trace_mode=1),                                        # persistent trace warps
     dict(trace_mode=1, queue_capacity=65536, tile_w=8, tile_h=4),
-], ids=["small-waves", "blocks", "tile8x4", "mixed", "tile64", "rows", "persistent", "persistent-small-waves"])
+    dict(trace_mode=2),                                        # counting node visits and triangle tests
+], ids=["small-waves", "blocks", "tile8x4", "mixed", "tile64", "rows", "persistent", "persistent-small-waves",
+        "counting"])
 def test_tuning_does_not_change_results(scene_ctx, tuning):
     s, c = scene_ctx
     c.set_tuning()
@@ -48,13 +50,17 @@ def test_tuning_does_not_change_results(scene_ctx, tuning):
     assert st1.traced == st0.traced
     if tuning.get("queue_capacity") == 65536:
         assert st1.waves > st0.waves
+    if tuning.get("trace_mode") == 2:  # at least the root per ray; a triangle test for most rays
+        assert st1.node_visits >= st1.traced and 0 < st1.tri_tests < 64 * st1.traced
+    else:
+        assert st1.node_visits == 0 and st1.tri_tests == 0
 
 
 def test_invalid_tuning_rejected(scene_ctx):
     from axomae_b200 import native
     _, c = scene_ctx
     for bad in (dict(queue_capacity=100), dict(trace_block=256), dict(tile_w=8), dict(tile_w=5, tile_h=5),
-                dict(trace_mode=2)):
+                dict(trace_mode=7)):
         with pytest.raises(native.NovaError) as e:
             c.set_tuning(**bad)
         assert e.value.status == 15
