@@ -646,3 +646,18 @@ def test_two_level_bvh_edge_cases(ctx, oracle, torch_cuda):
     film, _ = _render(ctx, s, 48, 40, 8, 6)
     ref, _ = osc.render(oracle.options(48, 40, 8, 6))
     assert rel_rmse(film, ref) <= REL_RMSE_TOL
+
+
+def test_bake_bench_size_matches_oracle(ctx, oracle, torch_cuda):
+    """The bake at the benchmark's size: the heightfield workload's 2048 x 1024 log-normal(0, 1.5)
+    environment map to a 512 x 256 irradiance map, 128 samples per texel, against the oracle's CPU
+    bake (rtol 1e-4)."""
+    from axomae_b200 import scenes
+    s = scenes.heightfield_scene(n=8, width=16, height=16, env_w=2048, env_h=1024, seed=0)
+    env = next(t for t in s["textures"] if t["format"] == "f32")
+    src = np.asarray(env["pixels"], np.float32).reshape(1024, 2048, 4)
+    ts = torch_cuda.from_numpy(np.ascontiguousarray(src)).cuda()
+    out = torch_cuda.zeros((256, 512, 4), dtype=torch_cuda.float32, device="cuda")
+    ctx.bake_irradiance(ts.data_ptr(), 2048, 1024, 4, 512, 256, 128, out.data_ptr())
+    ref = oracle.bake_irradiance(src, 512, 256, 128)
+    np.testing.assert_allclose(out.cpu().numpy()[..., :3], ref[..., :3], rtol=1e-4, atol=1e-6)
