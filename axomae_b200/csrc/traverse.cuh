@@ -24,6 +24,17 @@
 namespace nb {
 
 constexpr int kTraversalStack = 64;
+
+/* When both children of a binary node are hit, the deferred one's node record is prefetched into L1
+ * (NB_TRACE_PREFETCH=1) so the pop later finds it near. */
+#ifndef NB_TRACE_PREFETCH
+#define NB_TRACE_PREFETCH 0
+#endif
+NB_D void prefetch_node(const float4 *nodes, int32_t ref) {
+#if NB_TRACE_PREFETCH
+  if (ref >= 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(nodes + 4 * (size_t)ref));
+#endif
+}
 constexpr float kRayTNear = 0.000001f; /* Ray::tnear, ray/Ray.h:14 */
 constexpr float kFarScale = 1.000000477f; /* 1 + 2^-21: covers the rounding of the slab distances */
 
@@ -100,6 +111,7 @@ NB_D TraceResult trace_closest2(const DevScene &sc, V3 o, V3 d, uint64_t *node_v
           first = r1;
           second = r0;
         }
+        prefetch_node(sc.nodes, second);
         if (sp < kTraversalStack) stack[sp++] = second;
         cur = first;
         continue;
