@@ -34,7 +34,7 @@ nova_b200_status check_tuning(nova_b200_ctx *c, const nova_b200_tuning &t) {
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "block sizes must be 0, 32, 64, 96 or 128%s");
   if ((t.tile_w == 0) != (t.tile_h == 0))
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "tile_w and tile_h must both be 0 or both be set%s");
-  if (t.trace_mode > 2) return fail(c, NOVA_B200_INVALID_ARGUMENT, "trace_mode must be 0, 1 or 2%s");
+  if (t.trace_mode > 3) return fail(c, NOVA_B200_INVALID_ARGUMENT, "trace_mode must be 0, 1, 2 or 3%s");
   if (t.tile_w && !(t.tile_w == 1 && t.tile_h == 1) &&
       (t.tile_w > 64 || t.tile_h > 64 || (t.tile_w * t.tile_h) % 32 != 0))
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "tiles must be 1 x 1 or at most 64 x 64 with a multiple of 32 pixels%s");

@@ -755,6 +755,8 @@ nova_b200_status nova_b200_destroy(nova_b200_ctx *c) {
   cudaFree(c->d_radiance);
   cudaFree(c->d_film_out);
   cudaFree(c->d_wave);
+  cudaFree(c->d_persist);
+  if (c->h_cancel_map) cudaFreeHost(const_cast<int *>(c->h_cancel_map));
   if (c->h_wave) cudaFreeHost(c->h_wave);
   for (cudaGraphExec_t g : c->graph_exec)
     if (g) cudaGraphExecDestroy(g);
@@ -1093,6 +1095,7 @@ nova_b200_status nova_b200_trace(nova_b200_ctx *c, uint64_t n, const float *o, c
 nova_b200_status nova_b200_cancel(nova_b200_ctx *c) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;
   c->cancel.store(true);
+  if (c->h_cancel_map) *c->h_cancel_map = 1; /* the persistent wavefront reads this one */
   return NOVA_B200_SUCCESS;
 }
 

@@ -65,6 +65,11 @@ struct nova_b200_ctx {
   std::vector<char> graph_key;               /* job table, launch shape and width of the graphs */
   nova_b200_tuning tuning{};                 /* launch parameters (zeros: defaults) */
 
+  /* persistent wavefront (tuning.trace_mode 3): its grid barrier, and the cancel flag in mapped host
+   * memory that its wave-end step reads */
+  void *d_persist = nullptr;
+  volatile int *h_cancel_map = nullptr;
+
   /* adjoint: the replay queues' extra path state (remaining radiance, image adjoint) */
   float4 *d_adj = nullptr;
   uint32_t adj_cap = 0;

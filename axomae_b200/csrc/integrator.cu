@@ -87,6 +87,7 @@ struct WaveCounters {
   uint32_t done;
   uint32_t waves; /* waves that did work */
   uint32_t trace_next; /* next queued ray handed out by the persistent trace kernel */
+  uint32_t shade_next; /* next hit handed out in the persistent wavefront */
   /* device status of the whole loop (never reset between waves): path radiance values that were not
    * finite and were written as 0 (the reference's DENAN, Integrator.cpp:92), and hits whose
    * primitive, instance or material id is out of range (the path ends black, the render fails) */
@@ -206,19 +207,25 @@ __device__ __forceinline__ CameraPath camera_path(const JS &js, uint32_t g) {
   return c;
 }
 
+/* Camera ray of new path `next + i` into queue slot `n_active + i`. */
+template <class JS>
+__device__ __forceinline__ void refill_one(const Queue &q, uint32_t next, uint32_t n_active, float4 *L, const JS &js,
+                                           uint32_t i) {
+  const CameraPath c = camera_path(js, next + i);
+  const uint32_t slot = n_active + i;
+  q.o[slot] = make_float4(c.o.x, c.o.y, c.o.z, __uint_as_float(c.rslot));
+  q.d[slot] = make_float4(c.d.x, c.d.y, c.d.z, __uint_as_float(c.job << 8));
+  q.beta[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(c.index));
+  if (js.at(c.job).sc.has_emissive) L[c.rslot] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 template <class JS>
 __global__ void __launch_bounds__(256) k_refill(Queue q, const WaveCounters *wcp, float4 *L,
                                                 const __grid_constant__ JS js) {
   const WaveCounters wc = *wcp;
   const uint32_t n_new = wave_new(wc);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
-    const CameraPath c = camera_path(js, wc.next + i);
-    const uint32_t slot = wc.n_active + i;
-    q.o[slot] = make_float4(c.o.x, c.o.y, c.o.z, __uint_as_float(c.rslot));
-    q.d[slot] = make_float4(c.d.x, c.d.y, c.d.z, __uint_as_float(c.job << 8));
-    q.beta[slot] = make_float4(1.f, 1.f, 1.f, __uint_as_float(c.index));
-    if (js.at(c.job).sc.has_emissive) L[c.rslot] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x)
+    refill_one(q, wc.next, wc.n_active, L, js, i);
 }
 
 /* Non-finite radiance becomes 0 (DENAN), counted in *nonfinite (rare: a plain atomic). */
@@ -230,11 +237,22 @@ __device__ __forceinline__ float4 finite_or_zero(V3 L, float alpha, unsigned *no
   return make_float4(L.x, L.y, L.z, alpha);
 }
 
+/* Loads of data written earlier in the same launch by other blocks: through L2 (ld.global.cg) when P,
+ * the persistent wavefront; plain loads otherwise (a kernel boundary orders them). */
+template <bool P, class T>
+__device__ __forceinline__ T ldq(const T *p) {
+  if constexpr (P)
+    return __ldcg(p);
+  else
+    return *p;
+}
+
 /* Writes a finished path's radiance (adds the emission gathered so far when the scene has any). */
+template <bool P = false>
 __device__ __forceinline__ void finish_path(const DevScene &sc, float4 *L, uint32_t g, float4 result,
                                             unsigned *nonfinite) {
   if (sc.has_emissive) {
-    const float4 acc = L[g];
+    const float4 acc = ldq<P>(&L[g]);
     float4 r = make_float4(acc.x + result.x, acc.y + result.y, acc.z + result.z, result.w);
     if (!isfinite(r.x) || !isfinite(r.y) || !isfinite(r.z)) {
       atomicAdd(nonfinite, 1u);
@@ -278,27 +296,26 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
 #define NB_TRACE8_MIN_BLOCKS 10
 #endif
 
-template <int WIDTH, class JS, bool ADJ = false, bool COUNT = false>
-__global__ void __launch_bounds__(128, WIDTH == 8 ? NB_TRACE8_MIN_BLOCKS : NB_TRACE_MIN_BLOCKS) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
-                                               const __grid_constant__ JS js) {
-  const uint32_t n = wcp->n_active + wave_new(*wcp);
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if ((i & ~31u) >= n) return; /* whole warps leave together (the append below is a warp ballot) */
+/* The closest-hit pass for one warp's lanes (ray i of n queued; the warp's lanes call together: the
+ * hit append is a warp ballot). */
+template <int WIDTH, class JS, bool ADJ, bool COUNT, bool P>
+__device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot,
+                                           float4 *L, const JS &js, uint32_t i, uint32_t n) {
   {
     bool is_hit = false;
     TraceResult r{-1, 0.f, 0.f, 0.f};
     uint64_t nv = 0, tt = 0;
     if (i < n) {
-      const float4 o = q.o[i], d = q.d[i];
+      const float4 o = ldq<P>(&q.o[i]), d = ldq<P>(&q.d[i]);
       const DevScene &sc = js.at(__float_as_uint(d.w) >> 8).sc;
       r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, COUNT ? &nv : nullptr,
                                  COUNT ? &tt : nullptr);
       if (r.prim >= 0) {
         is_hit = true;
       } else if (!ADJ) { /* a replayed path's radiance is already known */
-        const float4 b4 = q.beta[i];
+        const float4 b4 = ldq<P>(&q.beta[i]);
         const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
-        finish_path(sc, L, __float_as_uint(o.w),
+        finish_path<P>(sc, L, __float_as_uint(o.w),
                     finite_or_zero(V3{b4.x, b4.y, b4.z} * V3{e.x, e.y, e.z},
                                    (float)(__float_as_uint(d.w) & 0xffu) + e.w, &wcp->nonfinite),
                     &wcp->nonfinite);
@@ -320,6 +337,15 @@ __global__ void __launch_bounds__(128, WIDTH == 8 ? NB_TRACE8_MIN_BLOCKS : NB_TR
       hit_slot[slot] = i;
     }
   }
+}
+
+template <int WIDTH, class JS, bool ADJ = false, bool COUNT = false>
+__global__ void __launch_bounds__(128, WIDTH == 8 ? NB_TRACE8_MIN_BLOCKS : NB_TRACE_MIN_BLOCKS) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
+                                               const __grid_constant__ JS js) {
+  const uint32_t n = wcp->n_active + wave_new(*wcp);
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i & ~31u) >= n) return; /* whole warps leave together (the append below is a warp ballot) */
+  trace_warp<WIDTH, JS, ADJ, COUNT, false>(q, wcp, hits, hit_slot, L, js, i, n);
 }
 
 /* Persistent variant of k_trace (binary BVH): a fixed grid of warps hands out the queued rays with
@@ -382,18 +408,18 @@ __global__ void __launch_bounds__(128) k_trace_dyn(Queue q, WaveCounters *wcp, f
   }
 }
 
-template <class JS>
-__global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
-                                               const uint32_t *hit_slot, float4 *L, const __grid_constant__ JS js) {
-  const uint32_t n = wcp->hit_count;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if ((i & ~31u) >= n) return;
+/* The shading pass for one warp's lanes (hit i of n; the warp's lanes call together: the continuation
+ * append is a warp ballot). */
+template <class JS, bool P>
+__device__ __forceinline__ void shade_warp(const Queue &in, const Queue &out, WaveCounters *wcp, const float4 *hits,
+                                           const uint32_t *hit_slot, float4 *L, const JS &js, uint32_t i, uint32_t n) {
   {
     bool enq = false;
     float4 no{}, nd{}, nbeta{};
     if (i < n) {
-      const uint32_t slot_in = hit_slot[i];
-      const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
+      const uint32_t slot_in = ldq<P>(&hit_slot[i]);
+      const float4 o4 = ldq<P>(&in.o[slot_in]), d4 = ldq<P>(&in.d[slot_in]), b4 = ldq<P>(&in.beta[slot_in]),
+                   h = ldq<P>(&hits[i]);
       const uint32_t g = __float_as_uint(o4.w);
       const uint32_t tag = __float_as_uint(d4.w);
       const int bounce = (int)(tag & 0xffu);
@@ -420,7 +446,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
       /* a failed scatter returns black, emission included (Integrator.cpp:73-79) */
       if (sr.valid && sc.has_emissive && any_nonzero(sr.emissive)) {
         const V3 em = beta * sr.emissive;
-        const float4 acc = L[g];
+        const float4 acc = ldq<P>(&L[g]);
         L[g] = make_float4(acc.x + em.x, acc.y + em.y, acc.z + em.z, acc.w);
       }
       if (!sr.valid) {
@@ -458,7 +484,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
           }
         }
       }
-      if (done) finish_path(sc, L, g, result, &wcp->nonfinite);
+      if (done) finish_path<P>(sc, L, g, result, &wcp->nonfinite);
       }
     }
   append:
@@ -469,6 +495,15 @@ __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCount
       out.beta[slot] = nbeta;
     }
   }
+}
+
+template <class JS>
+__global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
+                                               const uint32_t *hit_slot, float4 *L, const __grid_constant__ JS js) {
+  const uint32_t n = wcp->hit_count;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((i & ~31u) >= n) return;
+  shade_warp<JS, false>(in, out, wcp, hits, hit_slot, L, js, i, n);
 }
 
 /* ---------------------------------------------------------------- replay adjoint
@@ -644,7 +679,129 @@ __global__ void k_wave_end(WaveCounters *wc) {
   wc->out_count = 0;
   wc->hit_count = 0;
   wc->trace_next = 0;
+  wc->shade_next = 0;
   wc->done = (wc->n_active == 0 && wc->next == wc->total) ? 1u : 0u;
+}
+
+/* ---------------------------------------------------------------- persistent wavefront (trace_mode 3)
+ *
+ * One cooperative launch runs every wave of a chunk: refill -> trace -> shade -> wave end, the same
+ * device functions as the per-wave kernels, separated by a grid barrier.  Warps take 32 rays (hits)
+ * at a time from a counter, so the block scheduler's balancing of the per-wave kernels is kept.
+ * Data one phase writes and a later phase reads on another SM is loaded through L2 (ldq<true>).
+ *
+ * The barrier is this file's own and its wait is bounded: block leaders arrive on a counter and
+ * spin on a generation word with a time limit (globaltimer); a leader that waits past the limit sets
+ * the status word to 1 and every block leaves at its next barrier, so the kernel always ends and the
+ * host reports RENDERER_EXCEPTION.  A cancel (the context's mapped flag) sets status 2 the same way. */
+struct PersistSync {
+  unsigned arrive, gen, status, pad;
+  unsigned long long trace_ns, shade_ns; /* phase times seen by block 0 */
+};
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+/* false once any block gave up waiting (or the render was cancelled): the caller returns.  The leader's
+ * reading of the status word is shared through shared memory, so a block leaves as a whole. */
+__device__ bool grid_barrier(PersistSync *s, unsigned long long limit_ns) {
+  __shared__ unsigned s_status;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned gen = ld_volatile(&s->gen);
+    __threadfence();
+    if (atomicAdd(&s->arrive, 1u) == gridDim.x - 1u) {
+      atomicExch(&s->arrive, 0u);
+      __threadfence();
+      atomicAdd(&s->gen, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (ld_volatile(&s->gen) == gen) {
+        if (ld_volatile(&s->status) != 0u) break;
+        if (global_ns() - t0 > limit_ns) {
+          atomicCAS(&s->status, 0u, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_status = ld_volatile(&s->status);
+  }
+  __syncthreads();
+  return s_status == 0u;
+}
+
+/* A warp's next 32 items from a counter (lane 0 takes them, the warp shares the base). */
+__device__ __forceinline__ uint32_t warp_take(unsigned *counter) {
+  uint32_t base = 0;
+  if ((threadIdx.x & 31u) == 0) base = atomicAdd(counter, 32u);
+  return __shfl_sync(0xffffffffu, base, 0);
+}
+
+/* Resident blocks of 128 per SM that k_persist is compiled for: it holds both the walk and the
+ * shading state, so fewer blocks than k_shade's 8 keep it from spilling. */
+#ifndef NB_PERSIST_MIN_BLOCKS
+#define NB_PERSIST_MIN_BLOCKS 5
+#endif
+
+template <int WIDTH, class JS>
+__global__ void __launch_bounds__(128, NB_PERSIST_MIN_BLOCKS) k_persist(Queue qa, Queue qb, WaveCounters *wcp, float4 *hits,
+                                                 uint32_t *hit_slot, float4 *L, PersistSync *sync,
+                                                 const volatile int *cancel, unsigned long long limit_ns,
+                                                 const __grid_constant__ JS js) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool leader = tid == 0;
+  for (uint32_t w = 0;; w++) {
+    const Queue &in = (w & 1u) ? qb : qa;
+    const Queue &out = (w & 1u) ? qa : qb;
+    const uint32_t n_active = __ldcg(&wcp->n_active), next = __ldcg(&wcp->next);
+    const uint32_t total = __ldcg(&wcp->total), cap = __ldcg(&wcp->cap);
+    if (__ldcg(&wcp->done)) return;
+    const uint32_t n_new = min(cap - n_active, total - next), n = n_active + n_new;
+    for (uint32_t i = tid; i < n_new; i += nthreads) refill_one(in, next, n_active, L, js, i);
+    if (!grid_barrier(sync, limit_ns)) return;
+    const unsigned long long t0 = leader ? global_ns() : 0ull;
+    for (;;) {
+      const uint32_t base = warp_take(&wcp->trace_next);
+      if (base >= n) break;
+      trace_warp<WIDTH, JS, false, false, true>(in, wcp, hits, hit_slot, L, js, base + lane, n);
+    }
+    if (!grid_barrier(sync, limit_ns)) return;
+    const unsigned long long t1 = leader ? global_ns() : 0ull;
+    const uint32_t nh = __ldcg(&wcp->hit_count);
+    for (;;) {
+      const uint32_t base = warp_take(&wcp->shade_next);
+      if (base >= nh) break;
+      shade_warp<JS, true>(in, out, wcp, hits, hit_slot, L, js, base + lane, nh);
+    }
+    if (!grid_barrier(sync, limit_ns)) return;
+    if (leader) { /* k_wave_end's update */
+      sync->trace_ns += t1 - t0;
+      sync->shade_ns += global_ns() - t1;
+      WaveCounters *wc = wcp;
+      if (n) {
+        wc->waves++;
+        wc->traced += n;
+      }
+      wc->next = next + n_new;
+      wc->n_active = __ldcg(&wcp->out_count);
+      wc->out_count = 0;
+      wc->hit_count = 0;
+      wc->trace_next = 0;
+      wc->shade_next = 0;
+      wc->done = (wc->n_active == 0 && wc->next == total) ? 1u : 0u;
+      if (*cancel) atomicCAS(&sync->status, 0u, 2u);
+      __threadfence();
+    }
+    if (!grid_barrier(sync, limit_ns)) return;
+  }
 }
 
 __global__ void k_resolve(const float4 *L, uint32_t NP, uint32_t count, float4 *acc, float denom, float *out, int W,
@@ -777,7 +934,9 @@ struct LaunchShape {
   uint32_t cap;
   uint32_t trace_block, shade_block;
   uint32_t trace_mode; /* 0: one ray per thread, 1: persistent warps with ray hand-out (binary BVH),
-                         2: one ray per thread, counting node visits and triangle tests */
+                         2: one ray per thread, counting node visits and triangle tests,
+                         3: the persistent wavefront (one cooperative launch per chunk) */
+  uint32_t wait_limit_us; /* trace_mode 3: longest grid-barrier wait before the render fails */
 };
 
 struct WaveBuffers {
@@ -984,6 +1143,83 @@ nova_b200_status run_waves(nova_b200_ctx *x, uint32_t total, uint32_t cap, Launc
   return NOVA_B200_SUCCESS;
 }
 
+/* The persistent wavefront over `total` paths: counters and barrier reset, one cooperative launch of
+ * k_persist with every block resident (the occupancy calculator's count per SM), then the counters'
+ * read-back.  Status 1 (a barrier wait ran out) and 2 (cancelled) fail the call; the context stays
+ * usable either way (the kernel has returned). */
+template <int WIDTH, class JS>
+nova_b200_status run_persistent(nova_b200_ctx *x, const JS &js, const LaunchShape &ls, uint32_t total, uint32_t cap,
+                                LoopStats &st) {
+  using namespace nbctx;
+  WaveCounters *hw = static_cast<WaveCounters *>(x->h_wave);
+  if (!x->d_persist) {
+    NB_CUDA(x, cudaMalloc(&x->d_persist, sizeof(PersistSync)), "cudaMalloc(persistent barrier)");
+    void *flag = nullptr;
+    NB_CUDA(x, cudaHostAlloc(&flag, sizeof(int), cudaHostAllocMapped), "cudaHostAlloc(cancel flag)");
+    x->h_cancel_map = static_cast<volatile int *>(flag);
+    *x->h_cancel_map = x->cancel.load() ? 1 : 0;
+  }
+  void *d_cancel_v = nullptr;
+  NB_CUDA(x, cudaHostGetDevicePointer(&d_cancel_v, const_cast<int *>(x->h_cancel_map), 0), "cancel flag");
+  int *d_cancel = static_cast<int *>(d_cancel_v);
+  hw[2] = WaveCounters{};
+  hw[2].total = total;
+  hw[2].cap = cap;
+  NB_CUDA(x, cudaMemcpyAsync(x->d_wave, hw + 2, sizeof(WaveCounters), cudaMemcpyHostToDevice, x->stream),
+          "upload(wave counters)");
+  NB_CUDA(x, cudaMemsetAsync(x->d_persist, 0, sizeof(PersistSync), x->stream), "reset(barrier)");
+  int sms = 148, occ = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device);
+  NB_CUDA(x, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persist<WIDTH, JS>, 128, 0), "occupancy");
+  if (occ < 1) return fail(x, NOVA_B200_RENDERER_EXCEPTION, "persistent wavefront: no resident block fits%s");
+  const WaveBuffers b = wave_buffers(x);
+  PersistSync *sync = static_cast<PersistSync *>(x->d_persist);
+  float4 *L = x->d_radiance;
+  const volatile int *cancel = d_cancel;
+  const unsigned long long limit_ns = 1000ull * ls.wait_limit_us;
+  void *args[] = {const_cast<Queue *>(&b.qa), const_cast<Queue *>(&b.qb), const_cast<WaveCounters **>(&b.wc),
+                  const_cast<float4 **>(&b.hits), const_cast<uint32_t **>(&b.hit_slot), &L, &sync,
+                  const_cast<const volatile int **>(&cancel), const_cast<unsigned long long *>(&limit_ns),
+                  const_cast<JS *>(&js)};
+  NB_CUDA(x, cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(k_persist<WIDTH, JS>), dim3(sms * occ),
+                                         dim3(128), args, 0, x->stream),
+          "persistent wavefront launch");
+  PersistSync hs{};
+  NB_CUDA(x, cudaMemcpyAsync(hw, x->d_wave, sizeof(WaveCounters), cudaMemcpyDeviceToHost, x->stream), "readback");
+  NB_CUDA(x, cudaMemcpyAsync(&hs, x->d_persist, sizeof(PersistSync), cudaMemcpyDeviceToHost, x->stream), "readback");
+  NB_CUDA(x, cudaStreamSynchronize(x->stream), "persistent wavefront");
+  const WaveCounters r = hw[0];
+  st.kernels += 1;
+  st.t_trace += (float)(hs.trace_ns * 1e-6);
+  st.t_shade += (float)(hs.shade_ns * 1e-6);
+  st.waves += r.waves;
+  st.traced += r.traced;
+  st.nonfinite += r.nonfinite;
+  st.bad_index += r.bad_index;
+  if (hs.status == 2u) return fail(x, NOVA_B200_RENDERER_EXCEPTION, "render cancelled%s");
+  if (hs.status != 0u) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "persistent wavefront: a grid barrier waited longer than %u us", ls.wait_limit_us);
+    return fail(x, NOVA_B200_RENDERER_EXCEPTION, "%s", msg);
+  }
+  if (r.bad_index) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "device status: %u hits with an out-of-range primitive, instance or material id",
+                  (unsigned)r.bad_index);
+    return fail(x, NOVA_B200_RENDERER_EXCEPTION, "%s", msg);
+  }
+  if (!r.done) return fail(x, NOVA_B200_RENDERER_EXCEPTION, "persistent wavefront ended before its paths%s");
+  return NOVA_B200_SUCCESS;
+}
+
+template <class JS>
+nova_b200_status run_persistent_w(nova_b200_ctx *x, const JS &js, const LaunchShape &ls, int width, uint32_t total,
+                                  uint32_t cap, LoopStats &st) {
+  if (width == 8) return run_persistent<8>(x, js, ls, total, cap, st);
+  if (width == 1) return run_persistent<1>(x, js, ls, total, cap, st);
+  return run_persistent<2>(x, js, ls, total, cap, st);
+}
+
 struct Piece {
   nova_b200_ctx *ctx; /* the job's context: scene, BVH, film */
   const nova_b200_frame *f;
@@ -1011,6 +1247,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
                              float *const *films_device, nova_b200_render_stats *stats) {
   using namespace nbctx;
   x->cancel.store(false); /* a cancel applies to the call in progress */
+  if (x->h_cancel_map) *x->h_cancel_map = 0;
   const size_t nj = ctxs.size();
   const int width = ctxs[0]->bvh_width;
   uint64_t max_np = 0, total = 0;
@@ -1029,7 +1266,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   const uint32_t qc = tu.queue_capacity ? tu.queue_capacity : kQueueCapDefault;
   const uint32_t cap = (uint32_t)std::min<uint64_t>(qc, std::max<uint64_t>(radiance, 1024));
   const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u,
-                       tu.trace_mode};
+                       tu.trace_mode, tu.wait_limit_us ? tu.wait_limit_us : 1000000u};
   nova_b200_status st = ensure_wave_buffers(x, cap, radiance);
   if (st != NOVA_B200_SUCCESS) return st;
   x->primal_valid = false; /* this render overwrites the radiance buffer */
@@ -1104,14 +1341,19 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
       many = ManyJobs{};
       many.n = (uint32_t)chunk.size();
       std::copy(hj.begin(), hj.begin() + chunk.size(), many.j);
-      if ((st = capture_graphs(x, many, ls, width)) != NOVA_B200_SUCCESS) return st;
     }
-    auto launch = [&](int slot) {
-      if (!single) return cudaGraphLaunch(x->graph_exec[slot], x->stream);
-      enqueue_group(x, one, ls, width, slot, false);
-      return cudaGetLastError();
-    };
-    if ((st = run_waves(x, pb, cap, launch, loop)) != NOVA_B200_SUCCESS) return st;
+    if (ls.trace_mode == 3) { /* the persistent wavefront: one launch runs every wave of the chunk */
+      st = single ? run_persistent_w(x, one, ls, width, pb, cap, loop) : run_persistent_w(x, many, ls, width, pb, cap, loop);
+      if (st != NOVA_B200_SUCCESS) return st;
+    } else {
+      if (!single && (st = capture_graphs(x, many, ls, width)) != NOVA_B200_SUCCESS) return st;
+      auto launch = [&](int slot) {
+        if (!single) return cudaGraphLaunch(x->graph_exec[slot], x->stream);
+        enqueue_group(x, one, ls, width, slot, false);
+        return cudaGetLastError();
+      };
+      if ((st = run_waves(x, pb, cap, launch, loop)) != NOVA_B200_SUCCESS) return st;
+    }
     sum.paths += pb;
     for (size_t k = 0; k < chunk.size(); k++) {
       const Piece &P = chunk[k];
@@ -1206,7 +1448,7 @@ nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const f
   const uint32_t qc = tu.queue_capacity ? tu.queue_capacity : kQueueCapDefault;
   const uint32_t cap = (uint32_t)std::min<uint64_t>(qc, std::max<uint64_t>(radiance, 1024));
   const LaunchShape ls{cap, tu.trace_block ? tu.trace_block : 128u, tu.shade_block ? tu.shade_block : 128u,
-                       tu.trace_mode};
+                       tu.trace_mode == 3 ? 0u : tu.trace_mode, 0u}; /* the replay keeps the per-wave kernels */
   if ((st = ensure_wave_buffers(c, cap, radiance)) != NOVA_B200_SUCCESS) return st;
   if (c->adj_cap < c->queue_cap) {
     cudaFree(c->d_adj);

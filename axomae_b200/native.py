@@ -60,7 +60,7 @@ class SceneDesc(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("queue_capacity", C.c_uint32), ("trace_block", C.c_uint32), ("shade_block", C.c_uint32),
                 ("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("bvh_width", C.c_int32),
-                ("trace_mode", C.c_uint32)]
+                ("trace_mode", C.c_uint32), ("wait_limit_us", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -292,7 +292,12 @@ typedef struct {
   uint32_t trace_mode;     /* 0: one ray per thread (default); 1: persistent warps that hand out rays
                               as their lanes finish (binary BVH only; the 8-wide BVH ignores it);
                               2: as 0, and the render stats count the traversal's node visits and
-                              triangle tests (a measurement mode; the autotuner never picks it) */
+                              triangle tests (a measurement mode; the autotuner never picks it);
+                              3: the persistent wavefront: one cooperative launch runs every wave of a
+                              chunk (refill, trace, shade, wave end) with grid barriers between the
+                              phases; the backward pass keeps the per-wave kernels */
+  uint32_t wait_limit_us;  /* trace_mode 3: the longest a grid barrier may wait, in microseconds (0 =
+                              1000000); a wait past it ends the render with RENDERER_EXCEPTION */
 } nova_b200_tuning;
 
 /* tuning = NULL restores the defaults. */
