@@ -46,10 +46,16 @@ __device__ __forceinline__ void pgc3d(unsigned x, unsigned y, unsigned z, float 
 struct Src {
   const float *data;
   int w, h, ch;
+  bool vec4; /* 4 channels on a 16-byte aligned base: one 16-byte load per texel instead of three */
   __device__ V3 texel(int x, int y) const {
     int xc = x >= w ? x % w : (x < 0 ? w + (x % w) : x);
     int yc = y >= h ? y % h : (y < 0 ? h + (y % h) : y);
-    const float *p = data + ((size_t)yc * w + xc) * ch;
+    const size_t i = (size_t)yc * w + xc;
+    if (vec4) { /* the lookups scatter (each texel hashes its own directions): fewer L1 wavefronts */
+      const float4 q = __ldg(reinterpret_cast<const float4 *>(data) + i);
+      return {q.x, q.y, q.z};
+    }
+    const float *p = data + i * ch;
     return {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
   }
   __device__ V3 uv_sample(float u, float v) const {
@@ -93,6 +99,9 @@ __global__ void k_bake(Src src, const float *lut, int W, int H, int samples, flo
   if (1.0 - (double)fabsf(dd) > 1e-6) tangent = normalize(cross(right, normal));
   const V3 bitangent = cross(normal, tangent);
   V3 irr{0.f, 0.f, 0.f};
+  /* 512 x 256 texels are only 4096 warps (43 % of the GPU's warp slots): unrolling lets the hash,
+   * direction and lookups of neighbouring samples overlap; the sum keeps its sample order */
+#pragma unroll 4
   for (int s = 0; s < samples; s++) {
     float r[3];
     pgc3d(px, py, (unsigned)s, r);
@@ -124,8 +133,11 @@ nova_b200_status nb_bake(nova_b200_ctx *c, const float *src, int32_t sw, int32_t
   if (sw < 1 || sh < 1 || ch < 3 || ch > 4 || samples <= 0)
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "invalid source map or sample count%s");
   cudaSetDevice(c->device);
-  dim3 block(16, 16), grid((ow + 15) / 16, (oh + 15) / 16);
-  k_bake<<<grid, block, 0, c->stream>>>(Src{src, sw, sh, ch}, c->d_acos, ow, oh, samples, out);
+  /* 64-thread blocks: a 512 x 256 bake is 2048 blocks, which spread over 148 SMs within 2%, where
+   * 256-thread blocks (512) leave some SMs a quarter more work than others */
+  dim3 block(16, 4), grid((ow + 15) / 16, (oh + 3) / 4);
+  const bool vec4 = ch == 4 && (reinterpret_cast<uintptr_t>(src) & 15u) == 0;
+  k_bake<<<grid, block, 0, c->stream>>>(Src{src, sw, sh, ch, vec4}, c->d_acos, ow, oh, samples, out);
   NB_CUDA(c, cudaGetLastError(), "k_bake");
   NB_CUDA(c, cudaStreamSynchronize(c->stream), "bake");
   return NOVA_B200_SUCCESS;

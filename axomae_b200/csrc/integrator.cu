@@ -300,12 +300,14 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
  * hit append is a warp ballot). */
 template <int WIDTH, class JS, bool ADJ, bool COUNT, bool P>
 __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot,
-                                           float4 *L, const JS &js, uint32_t i, uint32_t n) {
+                                           float4 *L, const JS &js, uint32_t i, uint32_t n,
+                                           const uint32_t *order = nullptr) {
   {
     bool is_hit = false;
     TraceResult r{-1, 0.f, 0.f, 0.f};
     uint64_t nv = 0, tt = 0;
     if (i < n) {
+      if (order) i = order[i]; /* the queue slot this lane traces (k_order_rays) */
       const float4 o = ldq<P>(&q.o[i]), d = ldq<P>(&q.d[i]);
       const DevScene &sc = js.at(__float_as_uint(d.w) >> 8).sc;
       r = trace_closest_w<WIDTH>(sc, V3{o.x, o.y, o.z}, V3{d.x, d.y, d.z}, COUNT ? &nv : nullptr,
@@ -341,11 +343,72 @@ __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, fl
 
 template <int WIDTH, class JS, bool ADJ = false, bool COUNT = false>
 __global__ void __launch_bounds__(128, WIDTH == 8 ? NB_TRACE8_MIN_BLOCKS : NB_TRACE_MIN_BLOCKS) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
-                                               const __grid_constant__ JS js) {
+                                               const __grid_constant__ JS js, const uint32_t *order = nullptr) {
   const uint32_t n = wcp->n_active + wave_new(*wcp);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if ((i & ~31u) >= n) return; /* whole warps leave together (the append below is a warp ballot) */
-  trace_warp<WIDTH, JS, ADJ, COUNT, false>(q, wcp, hits, hit_slot, L, js, i, n);
+  trace_warp<WIDTH, JS, ADJ, COUNT, false>(q, wcp, hits, hit_slot, L, js, i, n, order);
+}
+
+/* Ray ordering before the trace (NB_RAY_ORDER = window of queue slots, 0 = off): each window of
+ * consecutive slots, whose rays come from neighbouring pixel tiles, is counting-sorted by direction
+ * (8 x 8 octahedral bins), and k_trace's warps take the window's rays in that order, so a warp's
+ * rays start out alike.  Only the order in which rays are traced and appended changes; a path's
+ * result does not depend on it. */
+#ifndef NB_RAY_ORDER
+#define NB_RAY_ORDER 0
+#endif
+constexpr int kOrderThreads = 1024;
+
+__device__ __forceinline__ uint32_t direction_bin(float4 d) {
+  const float s = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+  float x = d.x / s, y = d.y / s;
+  if (d.z < 0.f) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    x = copysignf(1.f - ay, x);
+    y = copysignf(1.f - ax, y);
+  }
+  const int bx = min(7, max(0, (int)((x + 1.f) * 4.f))), by = min(7, max(0, (int)((y + 1.f) * 4.f)));
+  return (uint32_t)(bx + 8 * by);
+}
+
+template <int WINDOW>
+__global__ void __launch_bounds__(kOrderThreads) k_order_rays(Queue q, const WaveCounters *wcp, uint32_t *order) {
+  constexpr int kPer = WINDOW / kOrderThreads;
+  __shared__ uint32_t s_bin[64];
+  const uint32_t n = wcp->n_active + wave_new(*wcp);
+  const uint32_t start = blockIdx.x * (uint32_t)WINDOW;
+  if (start >= n) return;
+  if (threadIdx.x < 64) s_bin[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t key[kPer];
+#pragma unroll
+  for (int k = 0; k < kPer; k++) {
+    const uint32_t slot = start + (uint32_t)k * kOrderThreads + threadIdx.x;
+    key[k] = 64u;
+    if (slot < n) {
+      key[k] = direction_bin(q.d[slot]);
+      atomicAdd(&s_bin[key[k]], 1u);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) { /* exclusive scan of the 64 bins by one warp, two bins a lane */
+    const uint32_t a = s_bin[2 * threadIdx.x], b = s_bin[2 * threadIdx.x + 1];
+    uint32_t x = a + b;
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+      if ((int)threadIdx.x >= off) x += y;
+    }
+    const uint32_t excl = x - a - b;
+    s_bin[2 * threadIdx.x] = excl;
+    s_bin[2 * threadIdx.x + 1] = excl + a;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kPer; k++) {
+    const uint32_t slot = start + (uint32_t)k * kOrderThreads + threadIdx.x;
+    if (key[k] < 64u) order[start + atomicAdd(&s_bin[key[k]], 1u)] = slot;
+  }
 }
 
 /* Persistent variant of k_trace (binary BVH): a fixed grid of warps hands out the queued rays with
@@ -497,12 +560,61 @@ __device__ __forceinline__ void shade_warp(const Queue &in, const Queue &out, Wa
   }
 }
 
+/* Lobe class of hit i, the key k_shade groups a block's hits by (BSDF.h:69-79 picks the lobe from
+ * the material's transmission and metallic inputs): 0 diffuse-only material, 1 a material with a
+ * metallic/roughness texture, 2 a transmissive one (eta set, no absorption), 3 no hit / bad index. */
+template <class JS>
+__device__ __forceinline__ uint32_t lobe_class(const Queue &in, const float4 *hits, const uint32_t *hit_slot,
+                                               const JS &js, uint32_t i, uint32_t n) {
+  if (i >= n) return 3u;
+  const uint32_t tag = __float_as_uint(in.d[hit_slot[i]].w);
+  const DevScene &sc = js.at(tag >> 8).sc;
+  const int prim = __float_as_int(hits[i].w);
+  uint32_t inst = 0;
+  if (!hit_ids_valid(sc, prim, inst)) return 3u;
+  const DevMaterial &m = sc.materials[sc.instances[inst].material];
+  const bool eta = m.eta[0] != 0.f || m.eta[1] != 0.f || m.eta[2] != 0.f;
+  const bool k = m.k[0] != 0.f || m.k[1] != 0.f || m.k[2] != 0.f;
+  return (eta && !k) ? 2u : (m.metallic >= 0 ? 1u : 0u);
+}
+
+#ifndef NB_SHADE_SORT
+#define NB_SHADE_SORT 0
+#endif
+
 template <class JS>
 __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
                                                const uint32_t *hit_slot, float4 *L, const __grid_constant__ JS js) {
   const uint32_t n = wcp->hit_count;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+#if NB_SHADE_SORT
+  /* The block's 128 hits are permuted so that each lobe class runs contiguously (a counting sort of
+   * four keys with warp ballots): warps then take one lobe's code path.  Only the order of the
+   * continuation rays changes, never a path's result. */
+  if (blockIdx.x * blockDim.x >= n) return; /* whole blocks leave together (barriers below) */
+  __shared__ uint32_t s_cnt[4][4];
+  __shared__ uint8_t s_perm[128];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t cls = lobe_class(in, hits, hit_slot, js, i, n);
+  const unsigned mine = __ballot_sync(0xffffffffu, cls == 0u) * (cls == 0u) |
+                        __ballot_sync(0xffffffffu, cls == 1u) * (cls == 1u) |
+                        __ballot_sync(0xffffffffu, cls == 2u) * (cls == 2u) |
+                        __ballot_sync(0xffffffffu, cls == 3u) * (cls == 3u);
+  if (threadIdx.x < 16u) (&s_cnt[0][0])[threadIdx.x] = 0; /* blocks of fewer than 4 warps count 0 for the rest */
+  __syncthreads();
+  if (lane == (uint32_t)(__ffs(mine) - 1)) s_cnt[warp][cls] = (uint32_t)__popc(mine);
+  __syncthreads();
+  uint32_t pos = (uint32_t)__popc(mine & ((1u << lane) - 1u));
+  for (uint32_t c = 0; c < cls; c++)
+    pos += s_cnt[0][c] + s_cnt[1][c] + s_cnt[2][c] + s_cnt[3][c];
+  for (uint32_t w = 0; w < warp; w++) pos += s_cnt[w][cls];
+  s_perm[pos] = (uint8_t)threadIdx.x;
+  __syncthreads();
+  i = blockIdx.x * blockDim.x + s_perm[threadIdx.x];
+  if (__all_sync(0xffffffffu, i >= n)) return;
+#else
   if ((i & ~31u) >= n) return;
+#endif
   shade_warp<JS, false>(in, out, wcp, hits, hit_slot, L, js, i, n);
 }
 
@@ -744,10 +856,12 @@ __device__ __forceinline__ uint32_t warp_take(unsigned *counter) {
   return __shfl_sync(0xffffffffu, base, 0);
 }
 
-/* Resident blocks of 128 per SM that k_persist is compiled for: it holds both the walk and the
- * shading state, so fewer blocks than k_shade's 8 keep it from spilling. */
+/* Resident blocks of 128 per SM that k_persist is compiled for.  It holds both the walk and the
+ * shading state, so its register budget is the larger of the two phases': on the 32-job batch, 6
+ * blocks (80 registers) took 379 ms per step, 5 (96) 408 ms and 4 (128, no spills) 465 ms, against
+ * 316 ms for the per-wave kernels (40 resident warps for k_trace, 32 for k_shade). */
 #ifndef NB_PERSIST_MIN_BLOCKS
-#define NB_PERSIST_MIN_BLOCKS 5
+#define NB_PERSIST_MIN_BLOCKS 6
 #endif
 
 template <int WIDTH, class JS>
@@ -899,7 +1013,7 @@ nova_b200_status ensure_wave_buffers(nova_b200_ctx *c, uint32_t cap, size_t radi
     c->d_queue = nullptr;
     c->queue_cap = 0;
     c->queue_bytes = 0;
-    const size_t bytes = (size_t)cap * (16 * 7 + 4);
+    const size_t bytes = (size_t)cap * (16 * 7 + 4 + (NB_RAY_ORDER ? 4 : 0));
     NB_CUDA(c, cudaMalloc(&c->d_queue, bytes), "cudaMalloc(queue)");
     c->queue_cap = cap;
     c->queue_bytes = bytes;
@@ -943,6 +1057,7 @@ struct WaveBuffers {
   Queue qa, qb;
   float4 *hits;
   uint32_t *hit_slot;
+  uint32_t *order; /* k_order_rays' slot order (NB_RAY_ORDER builds only) */
   WaveCounters *wc;
 };
 
@@ -954,6 +1069,7 @@ WaveBuffers wave_buffers(nova_b200_ctx *c) {
   b.qb = Queue{base + 3 * (size_t)cap, base + 4 * (size_t)cap, base + 5 * (size_t)cap};
   b.hits = base + 6 * (size_t)cap;
   b.hit_slot = reinterpret_cast<uint32_t *>(base + 7 * (size_t)cap);
+  b.order = NB_RAY_ORDER ? b.hit_slot + cap : nullptr;
   b.wc = static_cast<WaveCounters *>(c->d_wave);
   return b;
 }
@@ -1002,14 +1118,22 @@ void enqueue_waves(nova_b200_ctx *c, const JS &js, const LaunchShape &ls, int sl
       cudaEventRecordWithFlags(ev[3 * w + 2], c->stream, flags);
     } else {
       k_refill<JS><<<g_refill, 256, 0, c->stream>>>(in, b.wc, c->d_radiance, js);
+      const bool ordered = NB_RAY_ORDER && !(WIDTH == 2 && ls.trace_mode == 1);
+#if NB_RAY_ORDER
+      if (ordered)
+        k_order_rays<NB_RAY_ORDER><<<(ls.cap + NB_RAY_ORDER - 1) / NB_RAY_ORDER, kOrderThreads, 0, c->stream>>>(
+            in, b.wc, b.order);
+#endif
+      const uint32_t *order = ordered ? b.order : nullptr;
       cudaEventRecordWithFlags(ev[3 * w + 0], c->stream, flags);
       if (WIDTH == 2 && ls.trace_mode == 1)
         k_trace_dyn<JS><<<g_dyn, 128, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
       else if (ls.trace_mode == 2)
         k_trace<WIDTH, JS, false, true>
-            <<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+            <<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js, order);
       else
-        k_trace<WIDTH, JS><<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
+        k_trace<WIDTH, JS>
+            <<<g_trace, ls.trace_block, 0, c->stream>>>(in, b.wc, b.hits, b.hit_slot, c->d_radiance, js, order);
       cudaEventRecordWithFlags(ev[3 * w + 1], c->stream, flags);
       k_shade<JS><<<g_shade, ls.shade_block, 0, c->stream>>>(in, out, b.wc, b.hits, b.hit_slot, c->d_radiance, js);
       cudaEventRecordWithFlags(ev[3 * w + 2], c->stream, flags);

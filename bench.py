@@ -60,6 +60,9 @@ BATCH_METRIC = ("Mrays/s batched wavefront (32-job batch; plain wavefront on the
 # dram__bytes_write.sum over full waves of 8,388,608 rays): batched workload waves 1-2, and the
 # heightfield's first wave (camera rays only).
 K_TRACE_DRAM_BYTES_PER_RAY = {"batched": 72.0, "heightfield": 238.4, "instanced": None}
+# L2 bytes per traced ray (lts__t_bytes.sum) ncu measured for the binary-BVH k_trace on the
+# batched workload's full waves 6-8: L1 serves ~2/3 of the requests, L2 ~90 % of the rest.
+K_TRACE_L2_BYTES_PER_RAY = {"batched": 521.0, "heightfield": None, "instanced": None}
 
 
 def peaks():
@@ -710,8 +713,11 @@ def run_ours(args, rank, world, local_rank):
     clk_summary = None
     tuning = None
     tune_s = None
+    if args.trace_mode is not None:  # a fixed trace mode for both arms (no autotuning)
+        for c in ctxs:
+            c.set_tuning(trace_mode=args.trace_mode)
     for name, step in arms.items():
-        if name == "batched" and not args.no_autotune:
+        if name == "batched" and not args.no_autotune and args.trace_mode is None:
             # the batched system picks its launch tuning (queue capacity, block sizes, pixel tiles)
             # with the library's autotuner; the plain arm above ran with the library defaults
             t0 = time.perf_counter()
@@ -852,7 +858,9 @@ def run_ours(args, rank, world, local_rank):
     if b_dev and trace_rate:
         achieved = trace_rate * b_dev / 1e9
         rays_per_wave = acc.traced / max(1, acc.waves)
-        dram_ray = K_TRACE_DRAM_BYTES_PER_RAY[args.workload] or 0.0
+        binary = (args.bvh_width or 2) == 2  # the ncu figures are the binary layout's
+        dram_ray = (K_TRACE_DRAM_BYTES_PER_RAY[args.workload] or 0.0) if binary else 0.0
+        l2_ray = K_TRACE_L2_BYTES_PER_RAY[args.workload] if binary else None
         roof = {"bound": "hbm", "kernel": "k_trace", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_src,
                 "traffic": dram_ray * rays_per_wave if dram_ray else None,
@@ -860,7 +868,8 @@ def run_ours(args, rank, world, local_rank):
                                 "(dram__bytes_read.sum + dram__bytes_write.sum) on this workload's k_trace waves; "
                                 "achieved uses this kernel's algorithmic bytes: its own node visits and triangle "
                                 "tests per ray, counted on this workload (trace_mode 2)" % (rays_per_wave, dram_ray),
-                "dram_gbs_from_traffic": trace_rate * dram_ray / 1e9,
+                "dram_gbs_from_traffic": trace_rate * dram_ray / 1e9 if dram_ray else None,
+                "l2_bytes_per_ray": l2_ray, "l2_gbs_from_traffic": trace_rate * l2_ray / 1e9 if l2_ray else None,
                 "bytes_per_ray": b_dev, "node_visits_per_ray": counted["node_visits_per_ray"],
                 "tri_tests_per_ray": counted["tri_tests_per_ray"], "trace_ms_per_step": acc.trace_ms / args.steps,
                 "reference_bvh_model": None if not b_ref else {
@@ -883,6 +892,8 @@ def run_ours(args, rank, world, local_rank):
         extra["batched_over_plain"] = value / pval
         extra["autotune"] = {"tuning": tuning, "seconds": tune_s,
                              "note": "batched arm only; the plain arm uses the default tuning"}
+    if args.trace_mode is not None:
+        extra["trace_mode"] = args.trace_mode
         extra["films_identical"] = films_identical
         extra["equal_rmse"] = ("batched and plain films compared bit for bit after the timed steps; "
                                "rel_rmse_vs_cpu is the per-pixel relative RMSE of the film against the oracle "
@@ -938,6 +949,9 @@ def main():
     ap.add_argument("--no-bake", action="store_true", help="skip the irradiance bake timing")
     ap.add_argument("--frame", type=int, nargs=2, metavar=("W", "H"), help="heightfield: override the frame size")
     ap.add_argument("--spp", type=int, help="heightfield: override samples per pixel")
+    ap.add_argument("--trace-mode", type=int, choices=[0, 1, 3],
+                    help="launch tuning's trace mode for both arms: 0 per-wave kernels, 1 persistent trace warps, "
+                         "3 the persistent wavefront (one cooperative launch per chunk); default: autotuned")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 1, 2, 8],
                     help="BVH layout: 2 binary, 8 compressed 8-wide, 1 two-level (0 = library default)")
     args = ap.parse_args()

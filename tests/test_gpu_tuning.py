@@ -57,8 +57,10 @@ def test_tuning_does_not_change_results(scene_ctx, tuning):
             c.build()
     assert np.array_equal(out, ref)
     assert st1.traced == st0.traced
-    if tuning.get("trace_mode") == 3:  # the same waves, one launch for all of them
-        assert st1.waves == st0.waves and st1.kernels < st0.kernels
+    if tuning.get("trace_mode") == 3:  # one launch per chunk for all of its waves
+        assert st1.kernels < st0.kernels
+        if "queue_capacity" not in tuning:
+            assert st1.waves == st0.waves
     if tuning.get("queue_capacity") == 65536:
         assert st1.waves > st0.waves
     if tuning.get("trace_mode") == 2:  # at least the root per ray; a triangle test for most rays
