@@ -99,9 +99,6 @@ __global__ void k_bake(Src src, const float *lut, int W, int H, int samples, flo
   if (1.0 - (double)fabsf(dd) > 1e-6) tangent = normalize(cross(right, normal));
   const V3 bitangent = cross(normal, tangent);
   V3 irr{0.f, 0.f, 0.f};
-  /* 512 x 256 texels are only 4096 warps (43 % of the GPU's warp slots): unrolling lets the hash,
-   * direction and lookups of neighbouring samples overlap; the sum keeps its sample order */
-#pragma unroll 4
   for (int s = 0; s < samples; s++) {
     float r[3];
     pgc3d(px, py, (unsigned)s, r);
