@@ -161,7 +161,8 @@ NB_D TraceResult trace_closest2(const DevScene &sc, V3 o, V3 d, uint64_t *node_v
 }
 
 /* Triangle tests of one leaf range with the instance-transform cache (Triangle.h:146-153). */
-NB_D void test_triangles(const DevScene &sc, uint32_t first, uint32_t count, V3 o, V3 d, int32_t &cached_inst, V3 &lo_o,
+template <class S>
+NB_D void test_triangles(const S &sc, uint32_t first, uint32_t count, V3 o, V3 d, int32_t &cached_inst, V3 &lo_o,
                          V3 &lo_d, float &tmax, TraceResult &r) {
   /* count: the caller counts triangle tests (trace_closest8's tri_tests) */
   for (uint32_t k = first; k < first + count; k++) {
@@ -197,6 +198,14 @@ NB_D void test_triangles(const DevScene &sc, uint32_t first, uint32_t count, V3 
  * to the end reports exactly trace_closest2's hit.  Used where a thread interleaves several rays.
  * The traversal stack (kTraversalStack entries) is the caller's, so the scalar state can stay in
  * registers. */
+/* The three tables a binary walk reads, held in registers by a thread that switches between rays
+ * of different jobs. */
+struct WalkScene {
+  const float4 *nodes;
+  const float4 *tris;
+  const DevInstance *instances;
+};
+
 struct Walk2 {
   V3 o, d;
   float ix, iy, iz, tmax;
@@ -218,8 +227,10 @@ struct Walk2 {
     lo_d = d;
   }
 
-  /* false once the walk is over (r holds the closest hit) */
-  NB_D bool step(const DevScene &sc, int32_t *stack) {
+  /* false once the walk is over (r holds the closest hit); S is any scene view with the nodes,
+   * tris and instances tables (DevScene, WalkScene) */
+  template <class S>
+  NB_D bool step(const S &sc, int32_t *stack) {
     if (cur >= 0) {
       const float4 n0 = __ldg(&sc.nodes[4 * cur + 0]);
       const float4 n1 = __ldg(&sc.nodes[4 * cur + 1]);
