@@ -266,7 +266,9 @@ nova_b200_status nova_b200_set_diff_params(nova_b200_ctx *ctx, const float *albe
  * triangle) to grad_albedo_dev and dLoss/dRoughness (1 float per material) to grad_roughness_dev
  * (either may be NULL).  No tape is stored: each path is recomputed from its Sobol index, once
  * for its radiance and once to push the adjoint through its vertices, where the derivative of the
- * sampled lobe's f (its sampling density held fixed) is applied.  The film is not touched. */
+ * sampled lobe's f (its sampling density held fixed) is applied.  The film is not touched.  The
+ * call runs on the context's own stream: the caller finishes its writes of d_image and of the
+ * gradient buffers (on its own streams) before the call. */
 #define NOVA_B200_BACKWARD_REUSE_PRIMAL 1u /* see nova_b200_backward */
 
 /* flags: NOVA_B200_BACKWARD_REUSE_PRIMAL skips the radiance pass when the context's last render was
