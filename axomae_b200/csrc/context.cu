@@ -898,6 +898,11 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     meshes[i].idx = reinterpret_cast<const uint32_t *>(arena + moff[i].idx);
     meshes[i].attr = reinterpret_cast<const float4 *>(arena + moff[i].attr);
   }
+  for (nb::DevInstance &I : c->h_instances) { /* copied with the pieces below */
+    I.attr = meshes[I.mesh].attr;
+    I.idx = meshes[I.mesh].idx;
+    I.n_tris = meshes[I.mesh].n_tris;
+  }
   plan.pieces.push_back(Piece{tex.data(), tex.size() * sizeof(nb::DevTexture), off_tex, false});
   plan.pieces.push_back(Piece{meshes.data(), meshes.size() * sizeof(nb::DevMesh), off_mesh, false});
   c->h_meshes = meshes;

@@ -264,11 +264,12 @@ __device__ __forceinline__ void finish_path(const DevScene &sc, float4 *L, uint3
   }
 }
 
-/* The hit's primitive, its instance and the instance's material all index their tables. */
-__device__ __forceinline__ bool hit_ids_valid(const DevScene &sc, int prim, uint32_t &inst) {
-  if (prim < 0 || (uint32_t)prim >= sc.n_prims) return false;
-  inst = __ldg(sc.prim_inst + prim);
-  return inst < sc.n_instances && sc.instances[inst].material < sc.n_materials;
+/* The hit's primitive, its instance (from the hit list) and the instance's material all index their
+ * tables, and the primitive is one of the instance's triangles. */
+__device__ __forceinline__ bool hit_ids_valid(const DevScene &sc, int prim, uint32_t inst) {
+  if (prim < 0 || (uint32_t)prim >= sc.n_prims || inst >= sc.n_instances) return false;
+  const DevInstance &I = sc.instances[inst];
+  return (uint32_t)prim - I.prim_offset < I.n_tris && I.material < sc.n_materials;
 }
 
 /* Warp-aggregated append: returns the slot of every lane with `flag` set. */
@@ -299,12 +300,12 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
 /* The closest-hit pass for one warp's lanes (ray i of n queued; the warp's lanes call together: the
  * hit append is a warp ballot). */
 template <int WIDTH, class JS, bool ADJ, bool COUNT, bool P>
-__device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot,
+__device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, float4 *hits, uint2 *hit_slot,
                                            float4 *L, const JS &js, uint32_t i, uint32_t n,
                                            const uint32_t *order = nullptr) {
   {
     bool is_hit = false;
-    TraceResult r{-1, 0.f, 0.f, 0.f};
+    TraceResult r{-1, 0.f, 0.f, 0.f, 0u};
     uint64_t nv = 0, tt = 0;
     if (i < n) {
       if (order) i = order[i]; /* the queue slot this lane traces (k_order_rays) */
@@ -336,13 +337,13 @@ __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, fl
     const unsigned slot = warp_append(is_hit, &wcp->hit_count);
     if (is_hit) {
       hits[slot] = make_float4(r.t, r.u, r.v, __int_as_float(r.prim));
-      hit_slot[slot] = i;
+      hit_slot[slot] = make_uint2(i, r.inst);
     }
   }
 }
 
 template <int WIDTH, class JS, bool ADJ = false, bool COUNT = false>
-__global__ void __launch_bounds__(128, WIDTH == 8 ? NB_TRACE8_MIN_BLOCKS : NB_TRACE_MIN_BLOCKS) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint32_t *hit_slot, float4 *L,
+__global__ void __launch_bounds__(128, WIDTH == 8 ? NB_TRACE8_MIN_BLOCKS : NB_TRACE_MIN_BLOCKS) k_trace(Queue q, WaveCounters *wcp, float4 *hits, uint2 *hit_slot, float4 *L,
                                                const __grid_constant__ JS js, const uint32_t *order = nullptr) {
   const uint32_t n = wcp->n_active + wave_new(*wcp);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -435,7 +436,7 @@ constexpr int kRefillLanes = 8;
 
 template <class JS>
 __global__ void __launch_bounds__(128, NB_DYN_MIN_BLOCKS) k_trace_dyn(Queue q, WaveCounters *wcp, float4 *hits,
-                                                                      uint32_t *hit_slot, float4 *L,
+                                                                      uint2 *hit_slot, float4 *L,
                                                                       const __grid_constant__ JS js) {
   const uint32_t n = wcp->n_active + wave_new(*wcp);
   const unsigned full = 0xffffffffu, lane = threadIdx.x & 31u;
@@ -486,7 +487,7 @@ __global__ void __launch_bounds__(128, NB_DYN_MIN_BLOCKS) k_trace_dyn(Queue q, W
       const unsigned slot = warp_append(is_hit, &wcp->hit_count);
       if (is_hit) {
         hits[slot] = make_float4(w.r.t, w.r.u, w.r.v, __int_as_float(w.r.prim));
-        hit_slot[slot] = (uint32_t)ray;
+        hit_slot[slot] = make_uint2((uint32_t)ray, w.r.inst);
       }
     }
     if (fin) ray = -1;
@@ -497,12 +498,13 @@ __global__ void __launch_bounds__(128, NB_DYN_MIN_BLOCKS) k_trace_dyn(Queue q, W
  * append is a warp ballot). */
 template <class JS, bool P>
 __device__ __forceinline__ void shade_warp(const Queue &in, const Queue &out, WaveCounters *wcp, const float4 *hits,
-                                           const uint32_t *hit_slot, float4 *L, const JS &js, uint32_t i, uint32_t n) {
+                                           const uint2 *hit_slot, float4 *L, const JS &js, uint32_t i, uint32_t n) {
   {
     bool enq = false;
     float4 no{}, nd{}, nbeta{};
     if (i < n) {
-      const uint32_t slot_in = ldq<P>(&hit_slot[i]);
+      const uint2 hs = ldq<P>(&hit_slot[i]);
+      const uint32_t slot_in = hs.x, inst = hs.y;
       const float4 o4 = ldq<P>(&in.o[slot_in]), d4 = ldq<P>(&in.d[slot_in]), b4 = ldq<P>(&in.beta[slot_in]),
                    h = ldq<P>(&hits[i]);
       const uint32_t g = __float_as_uint(o4.w);
@@ -517,7 +519,6 @@ __device__ __forceinline__ void shade_warp(const Queue &in, const Queue &out, Wa
       const int prim = __float_as_int(h.w);
       bool done = false;
       float4 result = make_float4(0.f, 0.f, 0.f, 0.f);
-      uint32_t inst = 0;
       if (!hit_ids_valid(sc, prim, inst)) {
         atomicAdd(&wcp->bad_index, 1u);
         L[g] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -586,13 +587,13 @@ __device__ __forceinline__ void shade_warp(const Queue &in, const Queue &out, Wa
  * the material's transmission and metallic inputs): 0 diffuse-only material, 1 a material with a
  * metallic/roughness texture, 2 a transmissive one (eta set, no absorption), 3 no hit / bad index. */
 template <class JS>
-__device__ __forceinline__ uint32_t lobe_class(const Queue &in, const float4 *hits, const uint32_t *hit_slot,
+__device__ __forceinline__ uint32_t lobe_class(const Queue &in, const float4 *hits, const uint2 *hit_slot,
                                                const JS &js, uint32_t i, uint32_t n) {
   if (i >= n) return 3u;
-  const uint32_t tag = __float_as_uint(in.d[hit_slot[i]].w);
+  const uint2 hs = hit_slot[i];
+  const uint32_t tag = __float_as_uint(in.d[hs.x].w), inst = hs.y;
   const DevScene &sc = js.at(tag >> 8).sc;
   const int prim = __float_as_int(hits[i].w);
-  uint32_t inst = 0;
   if (!hit_ids_valid(sc, prim, inst)) return 3u;
   const DevMaterial &m = sc.materials[sc.instances[inst].material];
   const bool eta = m.eta[0] != 0.f || m.eta[1] != 0.f || m.eta[2] != 0.f;
@@ -606,7 +607,7 @@ __device__ __forceinline__ uint32_t lobe_class(const Queue &in, const float4 *hi
 
 template <class JS>
 __global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
-                                               const uint32_t *hit_slot, float4 *L, const __grid_constant__ JS js) {
+                                               const uint2 *hit_slot, float4 *L, const __grid_constant__ JS js) {
   const uint32_t n = wcp->hit_count;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 #if NB_SHADE_SORT
@@ -716,7 +717,7 @@ __global__ void __launch_bounds__(256) k_refill_adj(Queue q, AdjQueue a, const W
 
 template <class JS>
 __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQueue ain, AdjQueue aout,
-                                                      WaveCounters *wcp, const float4 *hits, const uint32_t *hit_slot,
+                                                      WaveCounters *wcp, const float4 *hits, const uint2 *hit_slot,
                                                       float *g_alb, float *g_rough, const __grid_constant__ JS js) {
   const uint32_t n = wcp->hit_count;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -726,7 +727,8 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
   uint32_t g_prim = 0, g_mat = 0;
   float va[3] = {0.f, 0.f, 0.f}, vr[1] = {0.f};
   if (i < n) {
-    const uint32_t slot_in = hit_slot[i];
+    const uint2 hs = hit_slot[i];
+    const uint32_t slot_in = hs.x, inst = hs.y;
     const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
     const float4 r4 = ain.rem[slot_in], l4 = ain.dl[slot_in];
     const uint32_t tag = __float_as_uint(d4.w);
@@ -740,7 +742,6 @@ __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQu
     V3 rem{r4.x, r4.y, r4.z};
     const V3 dl{l4.x, l4.y, l4.z};
     const int prim = __float_as_int(h.w);
-    uint32_t inst = 0;
     if (!hit_ids_valid(sc, prim, inst)) {
       atomicAdd(&wcp->bad_index, 1u);
       goto gather;
@@ -888,7 +889,7 @@ __device__ __forceinline__ uint32_t warp_take(unsigned *counter) {
 
 template <int WIDTH, class JS>
 __global__ void __launch_bounds__(128, NB_PERSIST_MIN_BLOCKS) k_persist(Queue qa, Queue qb, WaveCounters *wcp, float4 *hits,
-                                                 uint32_t *hit_slot, float4 *L, PersistSync *sync,
+                                                 uint2 *hit_slot, float4 *L, PersistSync *sync,
                                                  const volatile int *cancel, unsigned long long limit_ns,
                                                  const __grid_constant__ JS js) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
@@ -1035,7 +1036,7 @@ nova_b200_status ensure_wave_buffers(nova_b200_ctx *c, uint32_t cap, size_t radi
     c->d_queue = nullptr;
     c->queue_cap = 0;
     c->queue_bytes = 0;
-    const size_t bytes = (size_t)cap * (16 * 7 + 4 + (NB_RAY_ORDER ? 4 : 0));
+    const size_t bytes = (size_t)cap * (16 * 7 + 8 + (NB_RAY_ORDER ? 4 : 0));
     NB_CUDA(c, cudaMalloc(&c->d_queue, bytes), "cudaMalloc(queue)");
     c->queue_cap = cap;
     c->queue_bytes = bytes;
@@ -1078,7 +1079,7 @@ struct LaunchShape {
 struct WaveBuffers {
   Queue qa, qb;
   float4 *hits;
-  uint32_t *hit_slot;
+  uint2 *hit_slot; /* per hit: its ray's queue slot and the hit triangle's instance */
   uint32_t *order; /* k_order_rays' slot order (NB_RAY_ORDER builds only) */
   WaveCounters *wc;
 };
@@ -1090,8 +1091,8 @@ WaveBuffers wave_buffers(nova_b200_ctx *c) {
   b.qa = Queue{base, base + cap, base + 2 * (size_t)cap};
   b.qb = Queue{base + 3 * (size_t)cap, base + 4 * (size_t)cap, base + 5 * (size_t)cap};
   b.hits = base + 6 * (size_t)cap;
-  b.hit_slot = reinterpret_cast<uint32_t *>(base + 7 * (size_t)cap);
-  b.order = NB_RAY_ORDER ? b.hit_slot + cap : nullptr;
+  b.hit_slot = reinterpret_cast<uint2 *>(base + 7 * (size_t)cap);
+  b.order = NB_RAY_ORDER ? reinterpret_cast<uint32_t *>(b.hit_slot + cap) : nullptr;
   b.wc = static_cast<WaveCounters *>(c->d_wave);
   return b;
 }
@@ -1324,7 +1325,7 @@ nova_b200_status run_persistent(nova_b200_ctx *x, const JS &js, const LaunchShap
   const volatile int *cancel = d_cancel;
   const unsigned long long limit_ns = 1000ull * ls.wait_limit_us;
   void *args[] = {const_cast<Queue *>(&b.qa), const_cast<Queue *>(&b.qb), const_cast<WaveCounters **>(&b.wc),
-                  const_cast<float4 **>(&b.hits), const_cast<uint32_t **>(&b.hit_slot), &L, &sync,
+                  const_cast<float4 **>(&b.hits), const_cast<uint2 **>(&b.hit_slot), &L, &sync,
                   const_cast<const volatile int **>(&cancel), const_cast<unsigned long long *>(&limit_ns),
                   const_cast<JS *>(&js)};
   NB_CUDA(x, cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(k_persist<WIDTH, JS>), dim3(sms * occ),

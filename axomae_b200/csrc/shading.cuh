@@ -166,17 +166,17 @@ struct VertexAttr {
   V3 p, n, t, b;
   float u, v;
 };
-NB_D VertexAttr load_vertex(const DevMesh &m, uint32_t i) {
-  const float4 *a = m.attr + 4 * (size_t)i;
+NB_D VertexAttr load_vertex(const float4 *attr, uint32_t i) {
+  const float4 *a = attr + 4 * (size_t)i;
   const float4 a0 = __ldg(a), a1 = __ldg(a + 1), a2 = __ldg(a + 2), a3 = __ldg(a + 3);
   return {{a0.x, a0.y, a0.z}, {a0.w, a1.x, a1.y}, {a1.z, a1.w, a2.x}, {a2.y, a2.z, a2.w}, a3.x, a3.y};
 }
 
 NB_D HitRecord make_record(const DevScene &sc, V3 ro, V3 rd, const DevInstance &I, uint32_t tri, float t, float bu,
                            float bv) {
-  const DevMesh &m = sc.meshes[I.mesh];
-  const uint32_t i0 = __ldg(m.idx + 3 * tri), i1 = __ldg(m.idx + 3 * tri + 1), i2 = __ldg(m.idx + 3 * tri + 2);
-  const VertexAttr A = load_vertex(m, i0), B = load_vertex(m, i1), C = load_vertex(m, i2);
+  const uint32_t *idx = I.idx;
+  const uint32_t i0 = __ldg(idx + 3 * tri), i1 = __ldg(idx + 3 * tri + 1), i2 = __ldg(idx + 3 * tri + 2);
+  const VertexAttr A = load_vertex(I.attr, i0), B = load_vertex(I.attr, i1), C = load_vertex(I.attr, i2);
   HitRecord r;
   const float w = 1 - (bu + bv);
   r.u = A.u * w + B.u * bu + C.u * bv;

@@ -65,6 +65,7 @@ NB_D bool mt_hit(V3 o, V3 d, V3 v0, V3 e1, V3 e2, float tmin, float tmax, float 
 struct TraceResult {
   int32_t prim;
   float t, u, v;
+  uint32_t inst; /* the hit triangle's instance (valid when prim >= 0) */
 };
 
 NB_D float safe_rcp(float d) {
@@ -76,7 +77,7 @@ NB_D float safe_rcp(float d) {
 /* Closest hit of one world-space ray on the binary BVH. */
 NB_D TraceResult trace_closest2(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
                                uint64_t *tri_tests = nullptr) {
-  TraceResult r{-1, 0.f, 0.f, 0.f};
+  TraceResult r{-1, 0.f, 0.f, 0.f, 0u};
   float tmax = FLT_MAX; /* native.cpp:57 starts from MAXFLOAT */
   const float ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
   int32_t stack[kTraversalStack];
@@ -146,6 +147,7 @@ NB_D TraceResult trace_closest2(const DevScene &sc, V3 o, V3 d, uint64_t *node_v
                    hu, hv)) {
           tmax = ht;
           r.prim = __float_as_int(t0.w);
+          r.inst = (uint32_t)inst;
           r.t = ht;
           r.u = hu;
           r.v = hv;
@@ -186,6 +188,7 @@ NB_D void test_triangles(const S &sc, uint32_t first, uint32_t count, V3 o, V3 d
                hv)) {
       tmax = ht;
       r.prim = __float_as_int(t0.w);
+      r.inst = (uint32_t)inst;
       r.t = ht;
       r.u = hu;
       r.v = hv;
@@ -219,7 +222,7 @@ struct Walk2 {
     d = rd;
     ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
     tmax = FLT_MAX;
-    r = TraceResult{-1, 0.f, 0.f, 0.f};
+    r = TraceResult{-1, 0.f, 0.f, 0.f, 0u};
     cur = 0;
     cached_inst = -1;
     sp = 0;
@@ -281,7 +284,7 @@ struct Walk2 {
  * node_visits / tri_tests (optional) add the nodes visited and the triangles tested. */
 NB_D TraceResult trace_closest8(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
                                uint64_t *tri_tests = nullptr) {
-  TraceResult r{-1, 0.f, 0.f, 0.f};
+  TraceResult r{-1, 0.f, 0.f, 0.f, 0u};
   float tmax = FLT_MAX;
   const float ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
   const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
@@ -375,14 +378,14 @@ constexpr int32_t kLeaveInstance = 0x7fffffff; /* stack marker: back to the top 
 
 NB_D TraceResult trace_closest_tl(const DevScene &sc, V3 o, V3 d, uint64_t *node_visits = nullptr,
                                   uint64_t *tri_tests = nullptr) {
-  TraceResult r{-1, 0.f, 0.f, 0.f};
+  TraceResult r{-1, 0.f, 0.f, 0.f, 0u};
   float tmax = FLT_MAX;
   V3 ro = o, rd = d;
   float ix = safe_rcp(d.x), iy = safe_rcp(d.y), iz = safe_rcp(d.z);
   int32_t stack[kTraversalStack];
   int sp = 0;
   int32_t cur = 0;
-  uint32_t prim_base = 0;
+  uint32_t prim_base = 0, inst_in = 0;
   bool inside = false;
   uint32_t nv = 0, tt = 0;
   for (;;) {
@@ -428,6 +431,7 @@ NB_D TraceResult trace_closest_tl(const DevScene &sc, V3 o, V3 d, uint64_t *node
         ix = safe_rcp(rd.x), iy = safe_rcp(rd.y), iz = safe_rcp(rd.z);
       }
       prim_base = I.prim_offset;
+      inst_in = leaf_first(cur);
       inside = true;
       if (sp < kTraversalStack) stack[sp++] = kLeaveInstance;
       cur = (int32_t)sc.blas_root[I.mesh];
@@ -444,6 +448,7 @@ NB_D TraceResult trace_closest_tl(const DevScene &sc, V3 o, V3 d, uint64_t *node
                    hv)) {
           tmax = ht;
           r.prim = (int32_t)(prim_base + (uint32_t)__float_as_int(t0.w));
+          r.inst = inst_in;
           r.t = ht;
           r.u = hu;
           r.v = hv;
