@@ -1079,6 +1079,16 @@ nova_b200_status nova_b200_build_bvh_batch(nova_b200_ctx *const *ctxs, uint32_t 
   return for_each_context(ctxs, n, [&](uint32_t k) { return nova_b200_build_bvh(ctxs[k], opts); });
 }
 
+nova_b200_status nova_b200_upload_build_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                              uint32_t n, const nova_b200_bvh_options *opts) {
+  if (!descs) return ctxs && n && ctxs[0] ? nbctx::fail(ctxs[0], NOVA_B200_INVALID_ARGUMENT, "descs is null%s")
+                                          : NOVA_B200_INVALID_ARGUMENT;
+  return for_each_context(ctxs, n, [&](uint32_t k) {
+    const nova_b200_status st = nova_b200_upload_scene(ctxs[k], &descs[k]);
+    return st != NOVA_B200_SUCCESS ? st : nova_b200_build_bvh(ctxs[k], opts);
+  });
+}
+
 nova_b200_status nova_b200_render(nova_b200_ctx *c, const nova_b200_frame *f, float *film_host, float *film_device,
                                   nova_b200_render_stats *stats) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;

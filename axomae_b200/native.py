@@ -100,7 +100,8 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
            "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune",
            "nova_b200_set_diff_params", "nova_b200_backward", "nova_b200_upload_scene_batch",
-           "nova_b200_build_bvh_batch", "nova_b200_render_aov", "nova_b200_film_accumulate",
+           "nova_b200_build_bvh_batch", "nova_b200_upload_build_batch", "nova_b200_render_aov",
+           "nova_b200_film_accumulate",
            "nova_b200_display_blend", "nova_b200_snapshot", "nova_b200_hdr_info", "nova_b200_hdr_read",
            "nova_b200_hdr_write", "nova_b200_last_call_ms", "nova_b200_bake_texture",
            "nova_b200_trace_host", "nova_b200_cancel", "nova_b200_bake_irradiance_texunit",
@@ -125,6 +126,8 @@ def lib():
         L.nova_b200_render_aov.argtypes = [vp, C.POINTER(Frame), C.c_int32, C.c_float, C.c_float, vp, vp]
         L.nova_b200_upload_scene_batch.argtypes = [C.POINTER(vp), C.POINTER(SceneDesc), C.c_uint32]
         L.nova_b200_build_bvh_batch.argtypes = [C.POINTER(vp), C.c_uint32, C.POINTER(BvhOptions)]
+        L.nova_b200_upload_build_batch.argtypes = [C.POINTER(vp), C.POINTER(SceneDesc), C.c_uint32,
+                                                   C.POINTER(BvhOptions)]
         L.nova_b200_set_diff_params.argtypes = [vp, vp, vp]
         L.nova_b200_backward.argtypes = [vp, C.POINTER(Frame), vp, vp, vp, C.c_uint32, C.POINTER(RenderStats)]
         L.nova_b200_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
@@ -308,6 +311,22 @@ def build_batch(contexts, max_leaf=0, bins=0, width=0, small_subtree=0):
     n = len(contexts)
     hs = (C.c_void_p * n)(*[c.h for c in contexts])
     rc = lib().nova_b200_build_bvh_batch(hs, n, C.byref(BvhOptions(max_leaf, bins, width, small_subtree)))
+    if rc != 0:
+        raise NovaError(rc, contexts[0].error())
+
+
+def upload_build_batch(contexts, scenes, max_leaf=0, bins=0, width=0, small_subtree=0):
+    """nova_b200_upload_build_batch: uploads scenes[k] to contexts[k] and builds its BVH, the
+    contexts concurrently (one scene's copies overlap another's build)."""
+    n = len(contexts)
+    keep, descs = [], (SceneDesc * n)()
+    for k, sc in enumerate(scenes):
+        d, kp = _desc_of(sc)
+        descs[k] = d
+        keep.append(kp)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    rc = lib().nova_b200_upload_build_batch(hs, descs, n, C.byref(BvhOptions(max_leaf, bins, width, small_subtree)))
+    del keep
     if rc != 0:
         raise NovaError(rc, contexts[0].error())
 

@@ -195,6 +195,11 @@ nova_b200_status nova_b200_render_aov(nova_b200_ctx *ctx, const nova_b200_frame 
 nova_b200_status nova_b200_upload_scene_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
                                               uint32_t n);
 nova_b200_status nova_b200_build_bvh_batch(nova_b200_ctx *const *ctxs, uint32_t n, const nova_b200_bvh_options *opts);
+/* Both at once: each host thread uploads a context's scene and then builds its BVH, so the copies of
+ * one scene overlap the build kernels of another.  Equal to nova_b200_upload_scene_batch followed by
+ * nova_b200_build_bvh_batch; opts may be NULL (defaults). */
+nova_b200_status nova_b200_upload_build_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                              uint32_t n, const nova_b200_bvh_options *opts);
 
 /* Renders one frame batch (renderGpu, api/engine.cpp:457-496).  film_host (width*height*4 floats,
  * pageable or pinned) and/or film_device (a device pointer) receive the running-mean RGBA image;

@@ -458,29 +458,34 @@ def test_instanced_scene_matches_oracle(ctx, oracle, torch_cuda, width):
 
 
 def test_batch_upload_and_build_equal_single_calls(torch_cuda):
-    """nova_b200_upload_scene_batch / nova_b200_build_bvh_batch (contexts concurrently) give the
-    same BVHs and images as one call per context."""
+    """nova_b200_upload_scene_batch / nova_b200_build_bvh_batch and nova_b200_upload_build_batch
+    (contexts concurrently) give the same BVHs and images as one call per context."""
     from axomae_b200 import native, scenes
     specs = [scenes.mixed_scene(6000 + 3000 * k, 24, 20, seed=20 + k) for k in range(5)]
     a = [native.Context(0) for _ in specs]
     b = [native.Context(0) for _ in specs]
+    f = [native.Context(0) for _ in specs]
     try:
         native.upload_batch(a, specs)
         native.build_batch(a)
+        native.upload_build_batch(f, specs)
         for c, s in zip(b, specs):
             c.upload(s)
             c.build()
-        for ca, cb, s in zip(a, b, specs):
-            assert ca.info() == cb.info()
-            fa, fb = np.zeros((20, 24, 4), np.float32), np.zeros((20, 24, 4), np.float32)
+        for ca, cb, cf, s in zip(a, b, f, specs):
+            assert ca.info() == cb.info() == cf.info()
+            fa, fb, ff = (np.zeros((20, 24, 4), np.float32) for _ in range(3))
             fr = native.make_frame(s, 24, 20, 4, 5)
             ca.render(fr, film_host=fa)
             cb.render(fr, film_host=fb)
-            assert np.array_equal(fa, fb)
+            cf.render(fr, film_host=ff)
+            assert np.array_equal(fa, fb) and np.array_equal(ff, fb)
         with pytest.raises(native.NovaError):
             native.build_batch([a[0], a[0]])
+        with pytest.raises(native.NovaError):
+            native.upload_build_batch([f[0], f[0]], specs[:2])
     finally:
-        for c in a + b:
+        for c in a + b + f:
             c.close()
 
 
