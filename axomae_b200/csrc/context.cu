@@ -769,6 +769,8 @@ nova_b200_status nova_b200_destroy(nova_b200_ctx *c) {
   if (c->ev_end) cudaEventDestroy(c->ev_end);
   if (c->ev_a) cudaEventDestroy(c->ev_a);
   if (c->ev_b) cudaEventDestroy(c->ev_b);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream), cudaStreamDestroy(c->copy_stream);
+  if (c->ev_copy) cudaEventDestroy(c->ev_copy);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NOVA_B200_SUCCESS;

@@ -11,6 +11,8 @@
 struct nova_b200_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr; /* batch renders: films of finished frames go out on it */
+  cudaEvent_t ev_copy = nullptr;
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_a = nullptr, ev_b = nullptr;
   std::string error;
   std::atomic<bool> cancel{false}; /* set by nova_b200_cancel from any thread, read by the wave loop */

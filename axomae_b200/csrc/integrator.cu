@@ -1450,12 +1450,56 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
       s += take;
     }
   }
+  /* A frame's film is final after its last chunk: with several chunks, device films and pinned host
+   * films of finished frames are copied out on a second stream while later chunks render. */
+  const size_t nc = chunks.size();
+  std::vector<size_t> last_chunk(nj, 0);
+  std::vector<char> early(nj, 0);
+  if (nc > 1) {
+    for (size_t ci = 0; ci < nc; ci++)
+      for (const Piece &P : chunks[ci])
+        for (size_t j = 0; j < nj; j++)
+          if (ctxs[j] == P.ctx) last_chunk[j] = ci;
+    for (size_t j = 0; j < nj; j++) {
+      bool pinned = false;
+      if (films_host && films_host[j]) {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, films_host[j]) == cudaSuccess)
+          pinned = pa.type == cudaMemoryTypeHost;
+        else
+          cudaGetLastError(); /* not a pointer the runtime knows: treated as pageable */
+      }
+      const bool host_ok = !(films_host && films_host[j]) || pinned;
+      early[j] = host_ok && last_chunk[j] + 1 < nc ? 1 : 0;
+    }
+    if (!x->copy_stream) {
+      NB_CUDA(x, cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking), "film copy stream");
+      NB_CUDA(x, cudaEventCreateWithFlags(&x->ev_copy, cudaEventDisableTiming), "film copy event");
+    }
+  }
+  struct CopiesDone { /* every return waits for the film copies already issued */
+    cudaStream_t s;
+    ~CopiesDone() {
+      if (s) cudaStreamSynchronize(s);
+    }
+  } copies_done{nc > 1 ? x->copy_stream : nullptr};
+  auto copy_film = [&](size_t j, cudaStream_t stream) -> nova_b200_status {
+    const size_t bytes = (size_t)frames[j]->width * frames[j]->height * 4 * sizeof(float);
+    if (films_device && films_device[j])
+      NB_CUDA(x, cudaMemcpyAsync(films_device[j], ctxs[j]->d_film_out, bytes, cudaMemcpyDeviceToDevice, stream),
+              "copy film");
+    if (films_host && films_host[j])
+      NB_CUDA(x, cudaMemcpyAsync(films_host[j], ctxs[j]->d_film_out, bytes, cudaMemcpyDeviceToHost, stream),
+              "copy film");
+    return NOVA_B200_SUCCESS;
+  };
   nova_b200_render_stats sum{};
   LoopStats loop;
   NB_CUDA(x, cudaEventRecord(x->ev_begin, x->stream), "event");
   std::vector<Job> hj(kParamJobs);
   ManyJobs many{};
-  for (const auto &chunk : chunks) {
+  for (size_t ci = 0; ci < nc; ci++) {
+    const auto &chunk = chunks[ci];
     if (x->cancel.load()) return fail(x, NOVA_B200_RENDERER_EXCEPTION, "render cancelled%s");
     if (chunk.empty()) continue;
     uint32_t pb = 0;
@@ -1512,19 +1556,21 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
                                                          P.f->height, P.f->vertical_invert);
       sum.kernels++;
     }
+    bool any = false;
+    for (size_t j = 0; j < nj; j++) any = any || (early[j] && last_chunk[j] == ci);
+    if (any) {
+      NB_CUDA(x, cudaEventRecord(x->ev_copy, x->stream), "event");
+      NB_CUDA(x, cudaStreamWaitEvent(x->copy_stream, x->ev_copy, 0), "event");
+      for (size_t j = 0; j < nj; j++)
+        if (early[j] && last_chunk[j] == ci && (st = copy_film(j, x->copy_stream)) != NOVA_B200_SUCCESS) return st;
+    }
   }
   NB_CUDA(x, cudaGetLastError(), "render kernels");
   NB_CUDA(x, cudaEventRecord(x->ev_end, x->stream), "event");
-  for (size_t j = 0; j < nj; j++) {
-    const size_t bytes = (size_t)frames[j]->width * frames[j]->height * 4 * sizeof(float);
-    if (films_device && films_device[j])
-      NB_CUDA(x, cudaMemcpyAsync(films_device[j], ctxs[j]->d_film_out, bytes, cudaMemcpyDeviceToDevice, x->stream),
-              "copy film");
-    if (films_host && films_host[j])
-      NB_CUDA(x, cudaMemcpyAsync(films_host[j], ctxs[j]->d_film_out, bytes, cudaMemcpyDeviceToHost, x->stream),
-              "copy film");
-  }
+  for (size_t j = 0; j < nj; j++)
+    if (!early[j] && (st = copy_film(j, x->stream)) != NOVA_B200_SUCCESS) return st;
   NB_CUDA(x, cudaStreamSynchronize(x->stream), "render");
+  if (x->copy_stream) NB_CUDA(x, cudaStreamSynchronize(x->copy_stream), "film copies");
   if (nj == 1 && chunks.size() == 1 && chunks[0].size() == 1) {
     x->primal_valid = true;
     x->primal_frame = *frames[0];

@@ -212,7 +212,11 @@ nova_b200_status nova_b200_render(nova_b200_ctx *ctx, const nova_b200_frame *fra
  * count and depth (no counterpart in the reference, which renders one engine at a time).  Every
  * frame follows the semantics of nova_b200_render on its own context (sample range, running-mean
  * film, reset) and produces the same film bit for bit.  films_host / films_device may be NULL or
- * hold n pointers (entries may be NULL).  All contexts must share a device and a BVH width. */
+ * hold n pointers (entries may be NULL).  All contexts must share a device and a BVH width.  When
+ * the batch takes several chunks (more than 104 frames, or more paths than one radiance buffer
+ * holds), the films of frames finished in an earlier chunk are copied out on a second stream while
+ * later chunks render, if they are device or pinned host buffers; pageable ones are written at the
+ * end.  The call returns after every copy. */
 nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
                                         float *const *films_host, float *const *films_device,
                                         nova_b200_render_stats *stats);
@@ -402,8 +406,10 @@ nova_b200_status nova_b200_last_call_ms(nova_b200_ctx *ctx, float *device_ms);
  * first context) from another thread: NvEngineInstance::stopRender's is_rendering flag
  * (api/engine.cpp:577-586).  The wave loop checks it after every group of four waves and between
  * chunks; the call then waits for the group still in flight and returns RENDERER_EXCEPTION
- * ("render cancelled") without writing the film.  The accumulation film keeps the chunks finished
- * before the stop, so the next frame should set reset.  A cancel applies to the call in progress:
+ * ("render cancelled") without writing the film (a batch spanning several chunks has already
+ * written the films of frames that finished in an earlier chunk, when they are device or pinned
+ * host buffers).  The accumulation film keeps the chunks finished before the stop, so the next
+ * frame should set reset.  A cancel applies to the call in progress:
  * each render / backward call clears it when it starts.  No counterpart call in the reference. */
 nova_b200_status nova_b200_cancel(nova_b200_ctx *ctx);
 

@@ -358,6 +358,38 @@ def test_batch_equals_individual_renders(torch_cuda):
             c.close()
 
 
+def test_batch_of_several_chunks_copies_every_film(torch_cuda):
+    """A batch of 110 frames spans two chunks (104 jobs per chunk): the films of the first chunk's
+    frames go out while the second chunk renders (pinned host and device films), pageable host films
+    after the render; every film equals the frame rendered alone, bit for bit."""
+    from axomae_b200 import native, scenes
+    torch = torch_cuda
+    n, W, H = 110, 16, 12
+    specs = [scenes.spheres_scene(W, H, n_spheres=2 + k % 4, seed=100 + k) for k in range(n)]
+    ctxs = [native.Context(0) for _ in range(n)]
+    try:
+        native.upload_build_batch(ctxs, specs)
+        frames = [native.make_frame(s, W, H, 4, 4) for s in specs]
+        refs = []
+        for c, fr in zip(ctxs, frames):
+            ref = np.zeros((H, W, 4), np.float32)
+            c.render(fr, film_host=ref)
+            refs.append(ref)
+        pinned = [torch.zeros((H, W, 4), dtype=torch.float32).pin_memory() for _ in range(n)]
+        device = [torch.zeros((H, W, 4), dtype=torch.float32, device="cuda") for _ in range(n)]
+        pageable = [np.zeros((H, W, 4), np.float32) for _ in range(n)]
+        hosts = [pinned[j].numpy() if j % 3 == 0 else (pageable[j] if j % 3 == 2 else None) for j in range(n)]
+        devs = [device[j].data_ptr() if j % 3 == 1 else None for j in range(n)]
+        st = native.render_batch(ctxs, frames, films_host=hosts, films_device=devs)
+        assert st.paths == n * W * H * 4
+        for j in range(n):
+            got = hosts[j] if j % 3 != 1 else device[j].cpu().numpy()
+            assert np.array_equal(got, refs[j]), j
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_scatter_bit_exact(ctx, oracle, torch_cuda):
     """nova_b200_scatter (hit record + principled scatter + spawn) equals the oracle bit for bit on
     the hits of oracle paths through a mixed Lambert / GGX conductor / GGX dielectric scene."""
