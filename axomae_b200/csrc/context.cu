@@ -1103,6 +1103,13 @@ nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b
   return nb_render_batch(ctxs, frames, n, films_host, films_device, stats);
 }
 
+nova_b200_status nova_b200_upload_build_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                                     const nova_b200_frame *frames, uint32_t n,
+                                                     const nova_b200_bvh_options *opts, float *const *films_host,
+                                                     float *const *films_device, nova_b200_render_stats *stats) {
+  return nb_upload_build_render_batch(ctxs, descs, frames, n, opts, films_host, films_device, stats);
+}
+
 nova_b200_status nova_b200_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,
                                  float *u, float *v) {
   if (!c) return NOVA_B200_INVALID_ARGUMENT;

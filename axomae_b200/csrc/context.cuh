@@ -112,6 +112,10 @@ nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *fi
                            nova_b200_render_stats *stats);
 nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
                                  float *const *films_host, float *const *films_device, nova_b200_render_stats *stats);
+nova_b200_status nb_upload_build_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                              const nova_b200_frame *frames, uint32_t n,
+                                              const nova_b200_bvh_options *opts, float *const *films_host,
+                                              float *const *films_device, nova_b200_render_stats *stats);
 nova_b200_status nb_backward(nova_b200_ctx *c, const nova_b200_frame *f, const float *d_image, float *grad_albedo,
                              float *grad_roughness, uint32_t flags, nova_b200_render_stats *stats);
 nova_b200_status nb_trace(nova_b200_ctx *c, uint64_t n, const float *o, const float *d, int32_t *prim, float *t,

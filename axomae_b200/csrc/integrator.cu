@@ -40,7 +40,11 @@
  */
 #include <algorithm>
 #include <cfloat>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "context.cuh"
@@ -1373,10 +1377,10 @@ struct Piece {
   uint32_t begin, count;
 };
 
-nova_b200_status validate_frame(nova_b200_ctx *c, const nova_b200_frame *f) {
+/* The frame's own fields (the scene and BVH are checked by validate_frame). */
+nova_b200_status validate_frame_fields(nova_b200_ctx *c, const nova_b200_frame *f) {
   using namespace nbctx;
   if (!f) return fail(c, NOVA_B200_INVALID_ARGUMENT, "frame is null%s");
-  if (!c->bvh_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "build the acceleration structure first%s");
   if (f->width <= 0 || f->height <= 0 || f->spp_total <= 0 || f->sample_begin < 0 || f->sample_count <= 0 ||
       f->sample_begin + f->sample_count > f->spp_total)
     return fail(c, NOVA_B200_INVALID_ARGUMENT, "invalid frame size or sample range%s");
@@ -1387,21 +1391,33 @@ nova_b200_status validate_frame(nova_b200_ctx *c, const nova_b200_frame *f) {
   return NOVA_B200_SUCCESS;
 }
 
+nova_b200_status validate_frame(nova_b200_ctx *c, const nova_b200_frame *f) {
+  using namespace nbctx;
+  if (f && !c->bvh_ready) return fail(c, NOVA_B200_SCENE_NOT_PROCESSED, "build the acceleration structure first%s");
+  return validate_frame_fields(c, f);
+}
+
+/* Pipelined batches: called before a chunk uses job j's scene; blocks until that context's upload
+ * and build are done and returns their status. */
+using WaitReady = std::function<nova_b200_status(size_t)>;
+
 /* Renders frames (one per job) as one wavefront on the executing context `x`.  Jobs are cut into
  * chunks whose per-path radiance fits the radiance buffer; a job's samples stay in order. */
 nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *> &ctxs,
                              const std::vector<const nova_b200_frame *> &frames, float *const *films_host,
-                             float *const *films_device, nova_b200_render_stats *stats) {
+                             float *const *films_device, nova_b200_render_stats *stats,
+                             const WaitReady *wait_ready = nullptr, int pipelined_width = 0,
+                             uint32_t first_chunk_jobs = kParamJobs) {
   using namespace nbctx;
   x->cancel.store(false); /* a cancel applies to the call in progress */
   if (x->h_cancel_map) *x->h_cancel_map = 0;
   const size_t nj = ctxs.size();
-  const int width = ctxs[0]->bvh_width;
+  const int width = wait_ready ? pipelined_width : ctxs[0]->bvh_width;
   uint64_t max_np = 0, total = 0;
   for (size_t j = 0; j < nj; j++) {
     if (ctxs[j]->device != x->device)
       return fail(x, NOVA_B200_INVALID_ARGUMENT, "all contexts of a batch must use the same device%s");
-    if (ctxs[j]->bvh_width != width)
+    if (!wait_ready && ctxs[j]->bvh_width != width)
       return fail(x, NOVA_B200_INVALID_ARGUMENT, "all scenes of a batch must use the same BVH width%s");
     const uint64_t np = (uint64_t)frames[j]->width * frames[j]->height;
     max_np = std::max(max_np, np);
@@ -1427,9 +1443,12 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
       c->film_samples = 0;
     }
   }
-  /* scene uploads and film clears of other contexts ran on their own streams */
-  for (size_t j = 0; j < nj; j++)
-    if (ctxs[j] != x) NB_CUDA(x, cudaStreamSynchronize(ctxs[j]->stream), "sync batch context");
+  /* scene uploads and film clears of other contexts ran on their own streams (pipelined: each
+   * context's upload and build end with a synchronisation of its stream, and the chunk loop waits
+   * for them) */
+  if (!wait_ready)
+    for (size_t j = 0; j < nj; j++)
+      if (ctxs[j] != x) NB_CUDA(x, cudaStreamSynchronize(ctxs[j]->stream), "sync batch context");
   /* cut the work into chunks of at most `radiance` paths and kParamJobs frame pieces */
   std::vector<std::vector<Piece>> chunks(1);
   uint64_t in_chunk = 0;
@@ -1439,7 +1458,7 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
     uint32_t s = 0;
     while (s < (uint32_t)f->sample_count) {
       uint64_t room = (radiance - in_chunk) / np;
-      if (room == 0 || chunks.back().size() == kParamJobs) {
+      if (room == 0 || chunks.back().size() == (chunks.size() == 1 ? first_chunk_jobs : kParamJobs)) {
         chunks.emplace_back();
         in_chunk = 0;
         room = radiance / np;
@@ -1502,6 +1521,10 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
     const auto &chunk = chunks[ci];
     if (x->cancel.load()) return fail(x, NOVA_B200_RENDERER_EXCEPTION, "render cancelled%s");
     if (chunk.empty()) continue;
+    if (wait_ready)
+      for (const Piece &P : chunk)
+        for (size_t j = 0; j < nj; j++)
+          if (ctxs[j] == P.ctx && (st = (*wait_ready)(j)) != NOVA_B200_SUCCESS) return st;
     uint32_t pb = 0;
     for (size_t k = 0; k < chunk.size(); k++) {
       const Piece &P = chunk[k];
@@ -1593,6 +1616,89 @@ nova_b200_status nb_render(nova_b200_ctx *c, const nova_b200_frame *f, float *fi
   if (st != NOVA_B200_SUCCESS) return st;
   cudaSetDevice(c->device);
   return render_jobs(c, {c}, {f}, &film_host, &film_device, stats);
+}
+
+/* Upload, build and render a batch in one pipelined call: up to 16 host threads upload and build
+ * the contexts in batch order (each on its own stream), and the calling thread renders on ctxs[0],
+ * starting each chunk as soon as the contexts of its frames are built, so the later scenes' copies
+ * and builds overlap the first chunks' waves.  Same result as the three calls one after another. */
+nova_b200_status nb_upload_build_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                              const nova_b200_frame *frames, uint32_t n,
+                                              const nova_b200_bvh_options *opts, float *const *films_host,
+                                              float *const *films_device, nova_b200_render_stats *stats) {
+  using namespace nbctx;
+  if (!ctxs || !ctxs[0]) return NOVA_B200_INVALID_ARGUMENT;
+  nova_b200_ctx *x = ctxs[0];
+  if (!descs || !frames || n == 0) return fail(x, NOVA_B200_INVALID_ARGUMENT, "empty batch%s");
+  const int width = opts && opts->width ? opts->width : 2;
+  std::vector<nova_b200_ctx *> cs(n);
+  std::vector<const nova_b200_frame *> fs(n);
+  for (uint32_t j = 0; j < n; j++) {
+    if (!ctxs[j]) return fail(x, NOVA_B200_INVALID_ARGUMENT, "null context in batch%s");
+    if (ctxs[j]->device != x->device)
+      return fail(x, NOVA_B200_INVALID_ARGUMENT, "all contexts of a batch must use the same device%s");
+    nova_b200_status st = validate_frame_fields(ctxs[j], &frames[j]);
+    if (st != NOVA_B200_SUCCESS) {
+      x->error = ctxs[j]->error;
+      return st;
+    }
+    for (uint32_t k = 0; k < j; k++)
+      if (ctxs[k] == ctxs[j]) return fail(x, NOVA_B200_INVALID_ARGUMENT, "a context appears twice in a batch%s");
+    cs[j] = ctxs[j];
+    fs[j] = &frames[j];
+  }
+  constexpr int kPending = -1;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<int> done(n, kPending);
+  std::atomic<uint32_t> next{0};
+  std::atomic<bool> stop{false};
+  auto work = [&] {
+    for (uint32_t k; (k = next.fetch_add(1)) < n;) {
+      nova_b200_status st = stop.load() ? NOVA_B200_RENDERER_EXCEPTION : nova_b200_upload_scene(cs[k], &descs[k]);
+      if (st == NOVA_B200_SUCCESS) st = nova_b200_build_bvh(cs[k], opts);
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        done[k] = (int)st;
+      }
+      cv.notify_all();
+    }
+  };
+  const unsigned nt = std::max(1u, std::min(std::min(n, 16u), std::max(1u, std::thread::hardware_concurrency())));
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nt; t++) pool.emplace_back(work);
+  const WaitReady wait_ready = [&](size_t j) -> nova_b200_status {
+    nova_b200_status st;
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      cv.wait(lock, [&] { return done[j] != kPending; });
+      st = (nova_b200_status)done[j];
+    }
+    if (st != NOVA_B200_SUCCESS) {
+      if (cs[j] != x) x->error = cs[j]->error;
+      return st;
+    }
+    if (cs[j]->bvh_width != width)
+      return fail(x, NOVA_B200_INVALID_ARGUMENT, "all scenes of a batch must use the same BVH width%s");
+    return NOVA_B200_SUCCESS;
+  };
+  /* the executing context's own scene must be in place before its stream renders */
+  nova_b200_status st = wait_ready(0);
+  if (st == NOVA_B200_SUCCESS) {
+    cudaSetDevice(x->device);
+    /* the first chunk holds only the frames whose scenes the first round of threads builds, so its
+     * waves start while the rest build */
+    st = render_jobs(x, cs, fs, films_host, films_device, stats, &wait_ready, width, std::min<uint32_t>(nt, kParamJobs));
+  }
+  stop.store(st != NOVA_B200_SUCCESS); /* a failed render skips the uploads not started yet */
+  for (auto &t : pool) t.join();
+  if (st == NOVA_B200_SUCCESS)
+    for (uint32_t k = 0; k < n; k++)
+      if (done[k] != (int)NOVA_B200_SUCCESS) {
+        if (k != 0) x->error = cs[k]->error;
+        return (nova_b200_status)done[k];
+      }
+  return st;
 }
 
 nova_b200_status nb_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,

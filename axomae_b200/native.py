@@ -100,7 +100,8 @@ EXPORTS = ["nova_b200_create", "nova_b200_destroy", "nova_b200_upload_scene", "n
            "nova_b200_get_error", "nova_b200_scene_info", "nova_b200_synchronize", "nova_b200_render_noalloc", "nova_b200_render_batch",
            "nova_b200_scatter", "nova_b200_set_tuning", "nova_b200_get_tuning", "nova_b200_autotune",
            "nova_b200_set_diff_params", "nova_b200_backward", "nova_b200_upload_scene_batch",
-           "nova_b200_build_bvh_batch", "nova_b200_upload_build_batch", "nova_b200_render_aov",
+           "nova_b200_build_bvh_batch", "nova_b200_upload_build_batch", "nova_b200_upload_build_render_batch",
+           "nova_b200_render_aov",
            "nova_b200_film_accumulate",
            "nova_b200_display_blend", "nova_b200_snapshot", "nova_b200_hdr_info", "nova_b200_hdr_read",
            "nova_b200_hdr_write", "nova_b200_last_call_ms", "nova_b200_bake_texture",
@@ -128,6 +129,9 @@ def lib():
         L.nova_b200_build_bvh_batch.argtypes = [C.POINTER(vp), C.c_uint32, C.POINTER(BvhOptions)]
         L.nova_b200_upload_build_batch.argtypes = [C.POINTER(vp), C.POINTER(SceneDesc), C.c_uint32,
                                                    C.POINTER(BvhOptions)]
+        L.nova_b200_upload_build_render_batch.argtypes = [C.POINTER(vp), C.POINTER(SceneDesc), C.POINTER(Frame),
+                                                          C.c_uint32, C.POINTER(BvhOptions), C.POINTER(vp),
+                                                          C.POINTER(vp), C.POINTER(RenderStats)]
         L.nova_b200_set_diff_params.argtypes = [vp, vp, vp]
         L.nova_b200_backward.argtypes = [vp, C.POINTER(Frame), vp, vp, vp, C.c_uint32, C.POINTER(RenderStats)]
         L.nova_b200_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
@@ -329,6 +333,31 @@ def upload_build_batch(contexts, scenes, max_leaf=0, bins=0, width=0, small_subt
     del keep
     if rc != 0:
         raise NovaError(rc, contexts[0].error())
+
+
+def upload_build_render_batch(contexts, scenes, frames, films_host=None, films_device=None, max_leaf=0, bins=0,
+                              width=0, small_subtree=0) -> "RenderStats":
+    """nova_b200_upload_build_render_batch: uploads and builds every context's scene on host threads
+    while the calling thread renders frames[j] of contexts[j], each chunk starting once its scenes
+    are built."""
+    n = len(contexts)
+    keep, descs = [], (SceneDesc * n)()
+    for k, sc in enumerate(scenes):
+        d, kp = _desc_of(sc)
+        descs[k] = d
+        keep.append(kp)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    fs = (Frame * n)(*frames)
+    fh = None if films_host is None else (C.c_void_p * n)(*[None if a is None else a.ctypes.data for a in films_host])
+    fd = None if films_device is None else (C.c_void_p * n)(*films_device)
+    st = RenderStats()
+    rc = lib().nova_b200_upload_build_render_batch(hs, descs, fs, n, C.byref(BvhOptions(max_leaf, bins, width,
+                                                                                          small_subtree)),
+                                                   fh, fd, C.byref(st))
+    del keep
+    if rc != 0:
+        raise NovaError(rc, contexts[0].error())
+    return st
 
 
 def autotune(contexts, frames, cache_path=None, flags=0) -> Tuning:

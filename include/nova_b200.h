@@ -221,6 +221,18 @@ nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b
                                         float *const *films_host, float *const *films_device,
                                         nova_b200_render_stats *stats);
 
+/* Upload, build and render in one call (no counterpart in the reference): up to 16 host threads
+ * upload each context's scene and build its BVH (opts may be NULL) in batch order, while the calling
+ * thread renders the frames as nova_b200_render_batch does, starting each chunk of the wavefront as
+ * soon as the scenes of its frames are built; the later scenes' copies and builds overlap the first
+ * chunks.  Scenes, BVHs and films equal those of nova_b200_upload_scene_batch,
+ * nova_b200_build_bvh_batch and nova_b200_render_batch called one after another.  The first failing
+ * status is returned (its message from ctxs[0]); an upload or build that fails fails the call. */
+nova_b200_status nova_b200_upload_build_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_scene_desc *descs,
+                                                     const nova_b200_frame *frames, uint32_t n,
+                                                     const nova_b200_bvh_options *opts, float *const *films_host,
+                                                     float *const *films_device, nova_b200_render_stats *stats);
+
 /* Allocation-free variant of nova_b200_render, for callers that cannot call cudaMalloc during a
  * frame: a host loop whose device memory is entirely reserved by another allocator (a framework's
  * caching allocator that has claimed the GPU), or a real-time loop that must not risk an allocation

@@ -390,6 +390,47 @@ def test_batch_of_several_chunks_copies_every_film(torch_cuda):
             c.close()
 
 
+def test_pipelined_upload_build_render_equals_separate_calls(torch_cuda):
+    """nova_b200_upload_build_render_batch (uploads and builds on host threads while the chunks whose
+    scenes are ready render) gives the films of the three separate batch calls, bit for bit, over a
+    110-frame batch of two chunks; a scene that fails to upload fails the call without a hang, and
+    the contexts render normally afterwards."""
+    from axomae_b200 import native, scenes
+    torch = torch_cuda
+    n, W, H = 110, 16, 12
+    specs = [scenes.spheres_scene(W, H, n_spheres=2 + k % 4, seed=300 + k) for k in range(n)]
+    frames = [native.make_frame(s, W, H, 4, 4) for s in specs]
+    a = [native.Context(0) for _ in range(n)]
+    b = [native.Context(0) for _ in range(n)]
+    try:
+        native.upload_batch(a, specs)
+        native.build_batch(a)
+        refs = [np.zeros((H, W, 4), np.float32) for _ in range(n)]
+        native.render_batch(a, frames, films_host=refs)
+        pinned = [torch.zeros((H, W, 4), dtype=torch.float32).pin_memory() for _ in range(n)]
+        outs = [p.numpy() for p in pinned]
+        st = native.upload_build_render_batch(b, specs, frames, films_host=outs)
+        assert st.paths == n * W * H * 4
+        for ca, cb in zip(a, b):
+            assert ca.info() == cb.info()
+        for o, r in zip(outs, refs):
+            assert np.array_equal(o, r)
+        bad = list(specs)
+        broken = dict(specs[57])
+        broken["instances"] = [dict(x) for x in specs[57]["instances"]]
+        broken["instances"][0]["mesh"] = len(broken["meshes"]) + 5
+        bad[57] = broken
+        with pytest.raises(native.NovaError) as e:
+            native.upload_build_render_batch(b, bad, frames, films_host=outs)
+        assert e.value.status == 15 and "missing mesh" in str(e.value)
+        again = np.zeros((H, W, 4), np.float32)
+        b[3].render(frames[3], film_host=again)
+        assert np.array_equal(again, refs[3])
+    finally:
+        for c in a + b:
+            c.close()
+
+
 def test_scatter_bit_exact(ctx, oracle, torch_cuda):
     """nova_b200_scatter (hit record + principled scatter + spawn) equals the oracle bit for bit on
     the hits of oracle paths through a mixed Lambert / GGX conductor / GGX dielectric scene."""
