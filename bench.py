@@ -898,12 +898,12 @@ def run_ours(args, rank, world, local_rank):
         extra["batched_over_plain"] = value / pval
         extra["autotune"] = {"tuning": tuning, "seconds": tune_s,
                              "note": "batched arm only; the plain arm uses the default tuning"}
-    if args.trace_mode is not None:
-        extra["trace_mode"] = args.trace_mode
         extra["films_identical"] = films_identical
         extra["equal_rmse"] = ("batched and plain films compared bit for bit after the timed steps; "
                                "rel_rmse_vs_cpu is the per-pixel relative RMSE of the film against the oracle "
                                "on the CPU sample's pixels")
+    if args.trace_mode is not None:
+        extra["trace_mode"] = args.trace_mode
     if check:
         extra["rel_rmse_vs_cpu"] = check["rel_rmse"]
         extra["rel_rmse_pixels"] = "every %dth pixel of every frame, all samples" % cpu_stride(args.workload)
