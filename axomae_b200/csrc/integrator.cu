@@ -609,8 +609,15 @@ __device__ __forceinline__ uint32_t lobe_class(const Queue &in, const float4 *hi
 #define NB_SHADE_SORT 0
 #endif
 
+/* Resident blocks of 128 per SM that k_shade is compiled for.  The kernel waits on its gathers, so
+ * more warps beat fewer spills up to a point: on the 32-job batch 7 blocks took 111.7 ms per step,
+ * 8 (64 registers) 108.6, 9 107.7, 10 (48 registers, more spills) 107.5, 12 108.4, 14 111.2. */
+#ifndef NB_SHADE_MIN_BLOCKS
+#define NB_SHADE_MIN_BLOCKS 10
+#endif
+
 template <class JS>
-__global__ void __launch_bounds__(128, 8) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
+__global__ void __launch_bounds__(128, NB_SHADE_MIN_BLOCKS) k_shade(Queue in, Queue out, WaveCounters *wcp, const float4 *hits,
                                                const uint2 *hit_slot, float4 *L, const __grid_constant__ JS js) {
   const uint32_t n = wcp->hit_count;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
