@@ -893,7 +893,7 @@ __device__ __forceinline__ uint32_t warp_take(unsigned *counter) {
 /* Resident blocks of 128 per SM that k_persist is compiled for.  It holds both the walk and the
  * shading state, so its register budget is the larger of the two phases': on the 32-job batch, 6
  * blocks (80 registers) took 379 ms per step, 5 (96) 408 ms and 4 (128, no spills) 465 ms, against
- * 316 ms for the per-wave kernels (40 resident warps for k_trace, 32 for k_shade). */
+ * 316 ms for the per-wave kernels (40 resident warps for k_trace, 32 for k_shade when measured). */
 #ifndef NB_PERSIST_MIN_BLOCKS
 #define NB_PERSIST_MIN_BLOCKS 6
 #endif
