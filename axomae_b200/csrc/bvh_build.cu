@@ -7,7 +7,7 @@
  *
  *   large nodes (> small_task primitives), one level per host iteration:
  *     k_init_level   reset per-node centroid bounds and bins
- *     k_cbounds      centroid bounds, one CTA per chunk of 4096 primitives, merged with atomics
+ *     k_cbounds      centroid bounds, one CTA per chunk of kChunk (1024) primitives, merged with atomics
  *     k_bin          centroid bins per axis in shared memory, merged into the node's global bins
  *     k_split        one CTA per node: SAH over bins*3 candidate planes, node allocation, children
  *     k_partition    primitive ids scattered to the children's ranges of the other id buffer
@@ -35,7 +35,14 @@ namespace {
 
 constexpr int kMaxBins = 32;
 constexpr uint32_t kSmallTaskDefault = 256;
-constexpr uint32_t kChunk = 4096;
+/* Primitives per CTA in the level kernels: the top levels of a scene have few large nodes, so
+ * smaller chunks put more CTAs on the GPU.  32 batch scenes: 4096 -> 57.5 ms build_batch, 116.6 ms
+ * one after another; 1024 -> 55.4 / 100.7 ms; 512 -> 54.6 / 99.1 ms; 256 -> 55.9 / 101.1 ms.  The
+ * tree does not depend on it. */
+#ifndef NB_BUILD_CHUNK
+#define NB_BUILD_CHUNK 1024
+#endif
+constexpr uint32_t kChunk = NB_BUILD_CHUNK;
 constexpr int kMedianDepth = 40;
 constexpr int kBlock = 256;
 constexpr int kSmallBlock = 64; /* a subtree of <= small_task primitives needs few threads per node */
