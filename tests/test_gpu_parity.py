@@ -212,6 +212,37 @@ def test_error_paths(ctx):
     assert e.value.status == 4  # INVALID_SCENE_TYPE
 
 
+def test_batch_calls_reject_bad_arguments(torch_cuda):
+    """The batch entry points check their arguments before any work: an empty batch, a null scene or
+    frame array, a frame with an invalid sample range, and two jobs on one context fail with
+    INVALID_ARGUMENT, and the contexts stay usable."""
+    import ctypes as C
+    from axomae_b200 import native, scenes
+    s = scenes.spheres_scene(16, 12, n_spheres=2, seed=9)
+    a, b = native.Context(0), native.Context(0)
+    try:
+        L = native.lib()
+        hs = (C.c_void_p * 2)(a.h, b.h)
+        opts = native.BvhOptions(0, 0, 0, 0)
+        assert L.nova_b200_upload_build_batch(hs, None, 2, C.byref(opts)) == 15
+        assert L.nova_b200_upload_build_render_batch(hs, None, None, 2, None, None, None, None) == 15
+        good = native.make_frame(s, 16, 12, 4, 3)
+        bad = native.make_frame(s, 16, 12, 4, 3, sample_begin=3, sample_count=2)
+        with pytest.raises(native.NovaError) as e:
+            native.upload_build_render_batch([a, b], [s, s], [good, bad])
+        assert e.value.status == 15
+        with pytest.raises(native.NovaError) as e:
+            native.upload_build_render_batch([a, a], [s, s], [good, good])
+        assert e.value.status == 15
+        native.upload_build_batch([a, b], [s, s])
+        fa, fb = np.zeros((12, 16, 4), np.float32), np.zeros((12, 16, 4), np.float32)
+        native.render_batch([a, b], [good, good], films_host=[fa, fb])
+        assert np.array_equal(fa, fb) and np.isfinite(fa).all()
+    finally:
+        a.close()
+        b.close()
+
+
 def test_upload_checks_indices_and_degenerate_triangles(ctx, oracle, torch_cuda):
     """The per-triangle scene tables are built on the device: an index past its mesh's vertices is
     rejected (INVALID_ARGUMENT), a scene of only degenerate triangles too (INVALID_SCENE_TYPE, as
