@@ -736,16 +736,31 @@ class B200Engine final : public Engine {
     return SUCCESS;
   }
 
-  /* api/engine.cpp:351-363 */
+  /* api/engine.cpp:351-363.  Every element is independent, so a large film is split over host
+   * threads (the same arithmetic per element: the result does not depend on the split). */
   void write_framebuffer(unsigned frame) {
     const HdrBufferStruct rb = buffers_->getRenderBuffers();
     const FloatView acc = buffers_->getAccumulator();
     const FloatView back = buffers_->backBuffer();
     const float denom = float(frame + 1);
-    for (size_t i = 0; i < acc.size(); i++) {
-      acc[i] += rb.partial_buffer[i];
-      back[i] = acc[i] / denom;
+    const float *partial = rb.partial_buffer;
+    auto range = [&](size_t b, size_t e) {
+      for (size_t i = b; i < e; i++) {
+        acc[i] += partial[i];
+        back[i] = acc[i] / denom;
+      }
+    };
+    const size_t n = acc.size();
+    const unsigned nt = n < (size_t)1 << 20 ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (nt == 1) {
+      range(0, n);
+      return;
     }
+    std::vector<std::thread> pool;
+    const size_t step = (n + nt - 1) / nt;
+    for (unsigned t = 1; t < nt; t++) pool.emplace_back(range, std::min(n, t * step), std::min(n, (t + 1) * step));
+    range(0, std::min(n, step));
+    for (auto &th : pool) th.join();
   }
 
   /* the exception bit of a failed frame's status */
