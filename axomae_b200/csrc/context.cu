@@ -861,6 +861,12 @@ nova_b200_status nova_b200_upload_scene(nova_b200_ctx *c, const nova_b200_scene_
     o.material = x.material;
     o.prim_offset = (uint32_t)offset;
     o.identity = is_identity(x.m) && is_identity(x.inv);
+    {
+      const nova_b200_material &mt = d->materials[x.material];
+      const bool eta = mt.eta[0] != 0.f || mt.eta[1] != 0.f || mt.eta[2] != 0.f;
+      const bool k = mt.k[0] != 0.f || mt.k[1] != 0.f || mt.k[2] != 0.f;
+      o.lobe_class = eta && !k ? 1u : 0u; /* NovaMaterials.h:118-121 */
+    }
     offset += d->meshes[x.mesh].n_tris;
   }
   if (offset >= (1ull << 27))

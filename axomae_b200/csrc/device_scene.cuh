@@ -54,6 +54,7 @@ struct DevInstance {
   uint32_t material;
   uint32_t prim_offset; /* global id of this instance's first triangle */
   int32_t identity;     /* m == inv == identity: the object-space ray is the world ray bit for bit */
+  uint32_t lobe_class;  /* 1: the material transmits (eta set, no absorption: the dielectric lobe) */
   const float4 *attr;   /* the mesh's interleaved vertex attributes, triangle indices and triangle */
   const uint32_t *idx;  /* count (copies of its DevMesh fields, so a hit record skips the mesh-table */
   uint32_t n_tris;      /* load) */
