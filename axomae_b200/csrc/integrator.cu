@@ -313,12 +313,6 @@ __device__ __forceinline__ unsigned warp_append(bool flag, unsigned *counter) {
 #define NB_HIT_CLASSES 1
 #endif
 
-/* The scene of queued ray i (valid when i < n). */
-template <class JS>
-__device__ __forceinline__ const DevScene &sc_of(const JS &js, const Queue &q, uint32_t i, uint32_t n) {
-  return js.at(i < n ? __float_as_uint(q.d[i].w) >> 8 : 0u).sc;
-}
-
 /* The closest-hit pass for one warp's lanes (ray i of n queued; the warp's lanes call together: the
  * hit append is a warp ballot). */
 template <int WIDTH, class JS, bool ADJ, bool COUNT, bool P>
@@ -326,7 +320,7 @@ __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, fl
                                            float4 *L, const JS &js, uint32_t i, uint32_t n,
                                            const uint32_t *order = nullptr) {
   {
-    bool is_hit = false;
+    bool is_hit = false, back = false;
     TraceResult r{-1, 0.f, 0.f, 0.f, 0u};
     uint64_t nv = 0, tt = 0;
     if (i < n) {
@@ -337,6 +331,7 @@ __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, fl
                                  COUNT ? &tt : nullptr);
       if (r.prim >= 0) {
         is_hit = true;
+        if constexpr (NB_HIT_CLASSES && !ADJ && !COUNT && !P) back = sc.instances[r.inst].lobe_class != 0u;
       } else if (!ADJ) { /* a replayed path's radiance is already known */
         const float4 b4 = ldq<P>(&q.beta[i]);
         const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
@@ -360,7 +355,6 @@ __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, fl
     if constexpr (NB_HIT_CLASSES && !ADJ && !COUNT && !P) {
       /* transmissive hits go to the end of the list, the others to the front, so the shading warps
        * mostly take one lobe family (BSDF.h:69-79) */
-      const bool back = is_hit && sc_of(js, q, i, n).instances[r.inst].lobe_class != 0u;
       const unsigned f = warp_append(is_hit && !back, &wcp->hit_count);
       const unsigned b = warp_append(back, &wcp->hit_back);
       slot = back ? wcp->cap - 1u - b : f;
@@ -638,11 +632,12 @@ __device__ __forceinline__ uint32_t lobe_class(const Queue &in, const float4 *hi
 #endif
 static_assert(!(NB_HIT_CLASSES && NB_SHADE_SORT), "one hit ordering at a time");
 
-/* Resident blocks of 128 per SM that k_shade is compiled for.  The kernel waits on its gathers, so
- * more warps beat fewer spills up to a point: on the 32-job batch 7 blocks took 111.7 ms per step,
- * 8 (64 registers) 108.6, 9 107.7, 10 (48 registers, more spills) 107.5, 12 108.4, 14 111.2. */
+/* Resident blocks of 128 per SM that k_shade is compiled for.  With hits of one lobe family per
+ * warp (NB_HIT_CLASSES), 8 blocks (64 registers) are best on the 32-job batch: 79.5 ms per step,
+ * against 79.9 at 9, 80.7 at 10 (48 registers, more spills) and 81.4 at 12; before the split 10
+ * blocks led (107.5 ms against 108.6 at 8), and 8 also suits the heightfield (11.7 against 12.1). */
 #ifndef NB_SHADE_MIN_BLOCKS
-#define NB_SHADE_MIN_BLOCKS 10
+#define NB_SHADE_MIN_BLOCKS 8
 #endif
 
 template <class JS>
