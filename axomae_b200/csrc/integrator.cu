@@ -331,7 +331,7 @@ __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, fl
                                  COUNT ? &tt : nullptr);
       if (r.prim >= 0) {
         is_hit = true;
-        if constexpr (NB_HIT_CLASSES && !ADJ && !COUNT && !P) back = sc.instances[r.inst].lobe_class != 0u;
+        if constexpr (NB_HIT_CLASSES && !COUNT && !P) back = sc.instances[r.inst].lobe_class != 0u;
       } else if (!ADJ) { /* a replayed path's radiance is already known */
         const float4 b4 = ldq<P>(&q.beta[i]);
         const V4 e = env_sample(sc, V3{d.x, d.y, d.z});
@@ -352,7 +352,7 @@ __device__ __forceinline__ void trace_warp(const Queue &q, WaveCounters *wcp, fl
       }
     }
     uint32_t slot;
-    if constexpr (NB_HIT_CLASSES && !ADJ && !COUNT && !P) {
+    if constexpr (NB_HIT_CLASSES && !COUNT && !P) {
       /* transmissive hits go to the end of the list, the others to the front, so the shading warps
        * mostly take one lobe family (BSDF.h:69-79) */
       const unsigned f = warp_append(is_hit && !back, &wcp->hit_count);
@@ -761,14 +761,24 @@ template <class JS>
 __global__ void __launch_bounds__(128, 8) k_shade_adj(Queue in, Queue out, AdjQueue ain, AdjQueue aout,
                                                       WaveCounters *wcp, const float4 *hits, const uint2 *hit_slot,
                                                       float *g_alb, float *g_rough, const __grid_constant__ JS js) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+#if NB_HIT_CLASSES
+  /* the front range of the hit list, then its back range counted from the end (see k_shade) */
+  const uint32_t nf = wcp->hit_count, nb = wcp->hit_back, cap = wcp->cap;
+  if ((t & ~31u) >= nf + nb) return;
+  const bool valid = t < nf + nb;
+  const uint32_t i = t < nf ? t : (valid ? cap - 1u - (t - nf) : 0u);
+#else
   const uint32_t n = wcp->hit_count;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if ((i & ~31u) >= n) return;
+  if ((t & ~31u) >= n) return;
+  const bool valid = t < n;
+  const uint32_t i = t;
+#endif
   bool enq = false, g_act = false;
   float4 no{}, nd{}, nbeta{}, nrem{}, ndl{};
   uint32_t g_prim = 0, g_mat = 0;
   float va[3] = {0.f, 0.f, 0.f}, vr[1] = {0.f};
-  if (i < n) {
+  if (valid) {
     const uint2 hs = hit_slot[i];
     const uint32_t slot_in = hs.x, inst = hs.y;
     const float4 o4 = in.o[slot_in], d4 = in.d[slot_in], b4 = in.beta[slot_in], h = hits[i];
