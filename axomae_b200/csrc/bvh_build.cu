@@ -503,13 +503,16 @@ constexpr int kWarpPrims = 32;
 constexpr int kWarpList = 256;   /* subtrees of <= kWarpPrims handed from the CTA loop to its warps */
 constexpr int kWarpStack = 40;   /* right siblings along one path: depth <= 31 below a 32-prim node */
 
-/* Sorts the lanes' (key, tie) pairs ascending over the warp and returns, for this lane's rank, the
- * lane that held it.  tie must be unique per lane (the primitive id, so equal centroids sort the
- * same way whatever order the ids arrive in; empty lanes use 0xffffffff - lane). */
-__device__ __forceinline__ int warp_sort_idx(float key, uint32_t tie) {
+/* Sorts the lanes' (key, tie) pairs ascending over each group of `span` lanes (a power of two,
+ * 2..32) and returns, for this lane's rank, the lane that held it.  tie must be unique per lane
+ * (the primitive id, so equal centroids sort the same way whatever order the ids arrive in; empty
+ * lanes use 0xffffffff - lane).  A node of n primitives sits in lanes 0..n-1 with empty lanes
+ * above, so the smallest power of two >= n sorts it: the bitonic stages above span only order the
+ * empty lanes. */
+__device__ __forceinline__ int warp_sort_idx(float key, uint32_t tie, int span) {
   const int lane = threadIdx.x & 31;
   int idx = lane;
-  for (int k = 2; k <= 32; k <<= 1)
+  for (int k = 2; k <= span; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
       const float ok = __shfl_xor_sync(0xffffffffu, key, j);
       const uint32_t ot = __shfl_xor_sync(0xffffffffu, tie, j);
@@ -521,12 +524,15 @@ __device__ __forceinline__ int warp_sort_idx(float key, uint32_t tie) {
   return idx;
 }
 
-/* Inclusive prefix (from lane 0) and suffix (from lane 31) bounds of the boxes held by the lanes. */
+/* Inclusive prefix (from lane 0) and suffix (towards lane 31) bounds of the boxes held by the
+ * lanes.  Each lane's scan reaches `span` lanes (a power of two): with the node's boxes in lanes
+ * 0..n-1, n <= span, and empty boxes above, the prefix of lane i < n and the suffix of lane i
+ * (over i..n-1) are exact, the same values as a scan over the whole warp (min and max are exact). */
 __device__ __forceinline__ void warp_scan_boxes(const float lo[3], const float hi[3], float pl[3], float ph[3],
-                                                float sl[3], float sh[3]) {
+                                                float sl[3], float sh[3], int span) {
   const int lane = threadIdx.x & 31;
   for (int k = 0; k < 3; k++) pl[k] = sl[k] = lo[k], ph[k] = sh[k] = hi[k];
-  for (int o = 1; o < 32; o <<= 1)
+  for (int o = 1; o < span; o <<= 1)
     for (int k = 0; k < 3; k++) {
       const float a = __shfl_up_sync(0xffffffffu, pl[k], o), b = __shfl_up_sync(0xffffffffu, ph[k], o);
       const float c = __shfl_down_sync(0xffffffffu, sl[k], o), d = __shfl_down_sync(0xffffffffu, sh[k], o);
@@ -564,13 +570,20 @@ __device__ void warp_build(const Shared &s, Task root, Task *wstack) {
     const float area = half_area(t.lo, t.hi);
     Best best{FLT_MAX, 0x7fffffff};
     float pl[3], ph[3], sl[3], sh[3];
+    /* sorts and scans reach the smallest power of two >= n lanes (warp-uniform: n is) */
+    const int span = n <= 2u ? 2 : 1 << (32 - __clz((int)n - 1));
+    int from_a[3] = {0, 0, 0}; /* per axis, the lane holding each sorted rank */
+    bool sorted = false;
     if (!make_leaf && area > 0.f && t.depth < kMedianDepth) {
+      sorted = true;
+#pragma unroll
       for (int a = 0; a < 3; a++) {
-        const int from = warp_sort_idx(act ? c[a] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane);
+        const int from = warp_sort_idx(act ? c[a] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane, span);
+        from_a[a] = from;
         float bl[3], bh[3];
         for (int k = 0; k < 3; k++)
           bl[k] = __shfl_sync(0xffffffffu, lo[k], from), bh[k] = __shfl_sync(0xffffffffu, hi[k], from);
-        warp_scan_boxes(bl, bh, pl, ph, sl, sh);
+        warp_scan_boxes(bl, bh, pl, ph, sl, sh, span);
         float rl[3], rh[3];
         for (int k = 0; k < 3; k++)
           rl[k] = __shfl_down_sync(0xffffffffu, sl[k], 1), rh[k] = __shfl_down_sync(0xffffffffu, sh[k], 1);
@@ -614,13 +627,15 @@ __device__ void warp_build(const Shared &s, Task root, Task *wstack) {
       axis = ext[1] > ext[0] ? (ext[2] > ext[1] ? 2 : 1) : (ext[2] > ext[0] ? 2 : 0);
       left_n = (int)n / 2;
     }
-    const int from = warp_sort_idx(act ? c[axis] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane);
+    /* the SAH pass already sorted every axis: reuse its order for the chosen one */
+    const int from = sorted ? (axis == 0 ? from_a[0] : (axis == 1 ? from_a[1] : from_a[2]))
+                            : warp_sort_idx(act ? c[axis] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane, span);
     const uint32_t sid = __shfl_sync(0xffffffffu, id, from);
     float bl[3], bh[3];
     for (int k = 0; k < 3; k++)
       bl[k] = __shfl_sync(0xffffffffu, lo[k], from), bh[k] = __shfl_sync(0xffffffffu, hi[k], from);
     if (act) dst[t.begin + lane] = sid;
-    warp_scan_boxes(bl, bh, pl, ph, sl, sh);
+    warp_scan_boxes(bl, bh, pl, ph, sl, sh, span);
     float cl[3], ch[3], dl[3], dh[3];
     for (int k = 0; k < 3; k++) {
       cl[k] = __shfl_sync(0xffffffffu, pl[k], left_n - 1), ch[k] = __shfl_sync(0xffffffffu, ph[k], left_n - 1);
