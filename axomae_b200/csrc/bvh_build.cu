@@ -496,27 +496,49 @@ __device__ unsigned block_exclusive_scan(unsigned v, unsigned *sh /* 32 */, unsi
  * barriers: per axis the lanes sort their centroids (bitonic, ties by primitive id), scan the sorted boxes
  * from both ends and evaluate the SAH of every split position (an exact sweep, where the larger
  * nodes use bins); the best (cost, axis, position) wins, the ids go to the other buffer in that
- * axis's sorted order and the left child continues on the warp while the right one waits on the
- * warp's stack.  Leaf rules, cost model and the median split below kMedianDepth are those of the
- * CTA path. */
+ * axis's sorted order.  Leaf rules, cost model and the median split below kMedianDepth are those of
+ * the CTA path.
+ *
+ * The work runs on lane segments: a segment of W lanes (W = 32 is the whole warp) builds a node of
+ * at most W primitives.  When both children of a split fit in W / 2 lanes the segment forks: its
+ * lower half builds the left subtree while its upper half builds the right one, each as a segment of
+ * W / 2 lanes, down to single lanes (one-primitive leaves); otherwise the left child continues on
+ * the segment and the right one waits on the segment's stack.  A half whose subtree is done waits
+ * for its sibling, and the two continue as their parent segment.  The splits do not depend on which
+ * lanes compute them or in which order, so the tree is the one a single warp building node after
+ * node produces. */
 constexpr int kWarpPrims = 32;
 constexpr int kWarpList = 256;   /* subtrees of <= kWarpPrims handed from the CTA loop to its warps */
-constexpr int kWarpStack = 40;   /* right siblings along one path: depth <= 31 below a 32-prim node */
+/* Right siblings a W-lane segment keeps: it pushes only at nodes of >= W / 2 + 2 primitives (smaller
+ * ones fork), nested with strictly decreasing sizes <= W, so at most W / 2 - 1 at once (none for
+ * W <= 2).  Per warp: one segment of 32 lanes (15 entries), 2 of 16 (7 each), 4 of 8 (3 each) and 8
+ * of 4 (1 each). */
+constexpr int kWarpStack = 15 + 2 * 7 + 4 * 3 + 8 * 1;
 
-/* Sorts the lanes' (key, tie) pairs ascending over each group of `span` lanes (a power of two,
- * 2..32) and returns, for this lane's rank, the lane that held it.  tie must be unique per lane
- * (the primitive id, so equal centroids sort the same way whatever order the ids arrive in; empty
- * lanes use 0xffffffff - lane).  A node of n primitives sits in lanes 0..n-1 with empty lanes
- * above, so the smallest power of two >= n sorts it: the bitonic stages above span only order the
- * empty lanes. */
-__device__ __forceinline__ int warp_sort_idx(float key, uint32_t tie, int span) {
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ unsigned seg_mask(int W) {
+  return W == 32 ? 0xffffffffu : ((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1));
+}
+
+/* The stack of the calling lane's W-lane segment, at level log2(32 / W) (W >= 4). */
+__device__ __forceinline__ Task *seg_stack(Task *stacks, int level, int W) {
+  const int base = level == 0 ? 0 : (level == 1 ? 15 : (level == 2 ? 29 : 41));
+  return stacks + base + ((threadIdx.x & 31) / W) * (W / 2 - 1);
+}
+
+/* Sorts the segment's (key, tie) pairs ascending over each group of `span` lanes (a power of two,
+ * 2..W) and returns, for this lane's rank, the segment lane that held it.  tie must be unique per
+ * lane (the primitive id, so equal centroids sort the same way whatever order the ids arrive in;
+ * empty lanes use 0xffffffff - lane).  A node of n primitives sits in segment lanes 0..n-1 with empty
+ * lanes above, so the smallest power of two >= n sorts it: the bitonic stages above span only order
+ * the empty lanes. */
+__device__ __forceinline__ int seg_sort_idx(float key, uint32_t tie, int span, int W, unsigned mask) {
+  const int lane = threadIdx.x & (W - 1);
   int idx = lane;
   for (int k = 2; k <= span; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
-      const float ok = __shfl_xor_sync(0xffffffffu, key, j);
-      const uint32_t ot = __shfl_xor_sync(0xffffffffu, tie, j);
-      const int oi = __shfl_xor_sync(0xffffffffu, idx, j);
+      const float ok = __shfl_xor_sync(mask, key, j, W);
+      const uint32_t ot = __shfl_xor_sync(mask, tie, j, W);
+      const int oi = __shfl_xor_sync(mask, idx, j, W);
       const bool other_less = ok < key || (ok == key && ot < tie);
       const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
       if (keep_min ? other_less : !other_less) key = ok, tie = ot, idx = oi;
@@ -524,37 +546,42 @@ __device__ __forceinline__ int warp_sort_idx(float key, uint32_t tie, int span) 
   return idx;
 }
 
-/* Inclusive prefix (from lane 0) and suffix (towards lane 31) bounds of the boxes held by the
- * lanes.  Each lane's scan reaches `span` lanes (a power of two): with the node's boxes in lanes
- * 0..n-1, n <= span, and empty boxes above, the prefix of lane i < n and the suffix of lane i
- * (over i..n-1) are exact, the same values as a scan over the whole warp (min and max are exact). */
-__device__ __forceinline__ void warp_scan_boxes(const float lo[3], const float hi[3], float pl[3], float ph[3],
-                                                float sl[3], float sh[3], int span) {
-  const int lane = threadIdx.x & 31;
+/* Inclusive prefix (from segment lane 0) and suffix (towards the segment's last lane) bounds of the
+ * boxes held by the segment's lanes.  Each lane's scan reaches `span` lanes (a power of two): with
+ * the node's boxes in lanes 0..n-1, n <= span, and empty boxes above, the prefix of lane i < n and
+ * the suffix of lane i (over i..n-1) are exact, the same values as a scan over the whole segment
+ * (min and max are exact). */
+__device__ __forceinline__ void seg_scan_boxes(const float lo[3], const float hi[3], float pl[3], float ph[3],
+                                               float sl[3], float sh[3], int span, int W, unsigned mask) {
+  const int lane = threadIdx.x & (W - 1);
   for (int k = 0; k < 3; k++) pl[k] = sl[k] = lo[k], ph[k] = sh[k] = hi[k];
   for (int o = 1; o < span; o <<= 1)
     for (int k = 0; k < 3; k++) {
-      const float a = __shfl_up_sync(0xffffffffu, pl[k], o), b = __shfl_up_sync(0xffffffffu, ph[k], o);
-      const float c = __shfl_down_sync(0xffffffffu, sl[k], o), d = __shfl_down_sync(0xffffffffu, sh[k], o);
+      const float a = __shfl_up_sync(mask, pl[k], o, W), b = __shfl_up_sync(mask, ph[k], o, W);
+      const float c = __shfl_down_sync(mask, sl[k], o, W), d = __shfl_down_sync(mask, sh[k], o, W);
       if (lane >= o) pl[k] = fminf(pl[k], a), ph[k] = fmaxf(ph[k], b);
-      if (lane + o < 32) sl[k] = fminf(sl[k], c), sh[k] = fmaxf(sh[k], d);
+      if (lane + o < W) sl[k] = fminf(sl[k], c), sh[k] = fmaxf(sh[k], d);
     }
 }
 
-__device__ __forceinline__ Best warp_best(Best b) {
-  for (int o = 16; o > 0; o >>= 1) {
-    Best q{__shfl_xor_sync(0xffffffffu, b.cost, o), __shfl_xor_sync(0xffffffffu, b.key, o)};
+__device__ __forceinline__ Best seg_best(Best b, int W, unsigned mask) {
+  for (int o = W / 2; o > 0; o >>= 1) {
+    Best q{__shfl_xor_sync(mask, b.cost, o, W), __shfl_xor_sync(mask, b.key, o, W)};
     if (better(q, b)) b = q;
   }
   return b;
 }
 
-/* Builds the subtree of `root` (<= 32 primitives) with the calling warp; all 32 lanes call it. */
-__device__ void warp_build(const Shared &s, Task root, Task *wstack) {
-  const int lane = threadIdx.x & 31;
-  int wsp = 0;
+/* Builds the subtree of `root` (<= 32 primitives) with the calling warp; all 32 lanes call it.
+ * stacks: the warp's kWarpStack entries. */
+__device__ void warp_build(const Shared &s, Task root, Task *stacks) {
+  int W = 32, level = 0; /* this lane's segment: width and log2(32 / W) */
+  uint32_t depth_sp = 0; /* per level (4 bits each, levels 0..3), the segment's stack depth */
+  bool failed = false;
   Task t = root;
-  for (int guard = 0; guard < 4 * kWarpPrims; guard++) {
+  for (int iter = 0;; iter++) {
+    const int lane = threadIdx.x & (W - 1);
+    unsigned mask = seg_mask(W);
     const uint32_t n = t.end - t.begin;
     const uint32_t *src = ids_of(s, t.buf);
     uint32_t *dst = ids_of(s, 1 - t.buf);
@@ -566,11 +593,19 @@ __device__ void warp_build(const Shared &s, Task root, Task *wstack) {
       lo[0] = a.x, lo[1] = a.y, lo[2] = a.z, hi[0] = b.x, hi[1] = b.y, hi[2] = b.z;
       c[0] = (a.x + b.x) * 0.5f, c[1] = (a.y + b.y) * 0.5f, c[2] = (a.z + b.z) * 0.5f;
     }
-    bool make_leaf = n <= 1;
+    /* a lane processes distinct nodes of a <= 32-primitive subtree, at most 63: past 2 * 63
+     * iterations something is broken, and every further node becomes a leaf, so the segments still
+     * drain their stacks and meet their siblings (no lane leaves while another waits for it).  The
+     * vote keeps the decision uniform over the segment (lanes of a joined segment count differently) */
+    if (__any_sync(mask, iter >= 2 * (2 * kWarpPrims - 1)) && !failed) {
+      failed = true;
+      if (lane == 0) atomicAdd(s.leaf_count + 1, 1u); /* reported as a build failure */
+    }
+    bool make_leaf = n <= 1 || failed;
     const float area = half_area(t.lo, t.hi);
     Best best{FLT_MAX, 0x7fffffff};
     float pl[3], ph[3], sl[3], sh[3];
-    /* sorts and scans reach the smallest power of two >= n lanes (warp-uniform: n is) */
+    /* sorts and scans reach the smallest power of two >= n lanes (uniform over the segment) */
     const int span = n <= 2u ? 2 : 1 << (32 - __clz((int)n - 1));
     int from_a[3] = {0, 0, 0}; /* per axis, the lane holding each sorted rank */
     bool sorted = false;
@@ -578,22 +613,22 @@ __device__ void warp_build(const Shared &s, Task root, Task *wstack) {
       sorted = true;
 #pragma unroll
       for (int a = 0; a < 3; a++) {
-        const int from = warp_sort_idx(act ? c[a] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane, span);
+        const int from = seg_sort_idx(act ? c[a] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane, span, W, mask);
         from_a[a] = from;
         float bl[3], bh[3];
         for (int k = 0; k < 3; k++)
-          bl[k] = __shfl_sync(0xffffffffu, lo[k], from), bh[k] = __shfl_sync(0xffffffffu, hi[k], from);
-        warp_scan_boxes(bl, bh, pl, ph, sl, sh, span);
+          bl[k] = __shfl_sync(mask, lo[k], from, W), bh[k] = __shfl_sync(mask, hi[k], from, W);
+        seg_scan_boxes(bl, bh, pl, ph, sl, sh, span, W, mask);
         float rl[3], rh[3];
         for (int k = 0; k < 3; k++)
-          rl[k] = __shfl_down_sync(0xffffffffu, sl[k], 1), rh[k] = __shfl_down_sync(0xffffffffu, sh[k], 1);
+          rl[k] = __shfl_down_sync(mask, sl[k], 1, W), rh[k] = __shfl_down_sync(mask, sh[k], 1, W);
         Best mine{FLT_MAX, 0x7fffffff};
         if ((uint32_t)lane + 1 < n) { /* split after sorted position lane: left = lane + 1 primitives */
           const float cost =
               s.cost_trav + (half_area(pl, ph) * (float)(lane + 1) + half_area(rl, rh) * (float)(n - 1 - lane)) / area;
           mine = Best{cost, a * 64 + lane};
         }
-        mine = warp_best(mine);
+        mine = seg_best(mine, W, mask);
         if (better(mine, best)) best = mine;
       }
     }
@@ -602,63 +637,89 @@ __device__ void warp_build(const Shared &s, Task root, Task *wstack) {
       if ((int)n <= s.max_leaf && (!has_split || (float)n <= best.cost)) make_leaf = true;
       if ((int)n <= s.hard_leaf && !has_split) make_leaf = true;
     }
-    if (make_leaf) {
-      if (act) s.order[t.begin + lane] = id;
-      if (lane == 0) finish_leaf(s, t);
-      if (wsp == 0) return;
-      __syncwarp();
-      t = wstack[--wsp];
-      __syncwarp();
+    if (!make_leaf) {
+      /* the split: best SAH position, or the median along the widest centroid extent */
+      int axis, left_n;
+      if (has_split) {
+        axis = best.key / 64;
+        left_n = best.key % 64 + 1;
+      } else {
+        float ext[3];
+        for (int k = 0; k < 3; k++) {
+          float mn = act ? c[k] : FLT_MAX, mx = act ? c[k] : -FLT_MAX;
+          for (int o = W / 2; o > 0; o >>= 1)
+            mn = fminf(mn, __shfl_xor_sync(mask, mn, o, W)), mx = fmaxf(mx, __shfl_xor_sync(mask, mx, o, W));
+          ext[k] = mx - mn;
+        }
+        axis = ext[1] > ext[0] ? (ext[2] > ext[1] ? 2 : 1) : (ext[2] > ext[0] ? 2 : 0);
+        left_n = (int)n / 2;
+      }
+      /* the SAH pass already sorted every axis: reuse its order for the chosen one */
+      const int from = sorted ? (axis == 0 ? from_a[0] : (axis == 1 ? from_a[1] : from_a[2]))
+                              : seg_sort_idx(act ? c[axis] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane, span,
+                                             W, mask);
+      const uint32_t sid = __shfl_sync(mask, id, from, W);
+      float bl[3], bh[3];
+      for (int k = 0; k < 3; k++)
+        bl[k] = __shfl_sync(mask, lo[k], from, W), bh[k] = __shfl_sync(mask, hi[k], from, W);
+      if (act) dst[t.begin + lane] = sid;
+      seg_scan_boxes(bl, bh, pl, ph, sl, sh, span, W, mask);
+      float cl[3], ch[3], dl[3], dh[3];
+      for (int k = 0; k < 3; k++) {
+        cl[k] = __shfl_sync(mask, pl[k], left_n - 1, W), ch[k] = __shfl_sync(mask, ph[k], left_n - 1, W);
+        dl[k] = __shfl_sync(mask, sl[k], left_n, W), dh[k] = __shfl_sync(mask, sh[k], left_n, W);
+      }
+      const uint32_t mid = t.begin + (uint32_t)left_n;
+      int node = 0;
+      if (lane == 0) {
+        node = (int)atomicAdd(s.node_counter, 1u);
+        if (t.parent >= 0) write_ref(s.nodes, t.parent, t.slot, node);
+        write_child(s.nodes, node, 0, cl, ch);
+        write_child(s.nodes, node, 1, dl, dh);
+      }
+      node = __shfl_sync(mask, node, 0, W);
+      __syncwarp(mask); /* the children read ids written by other lanes */
+      const Task L{t.begin, mid, node, 0, t.depth + 1, 1 - t.buf, {cl[0], cl[1], cl[2]}, {ch[0], ch[1], ch[2]}};
+      const Task R{mid, t.end, node, 1, t.depth + 1, 1 - t.buf, {dl[0], dl[1], dl[2]}, {dh[0], dh[1], dh[2]}};
+      if ((uint32_t)left_n <= (uint32_t)(W / 2) && n - (uint32_t)left_n <= (uint32_t)(W / 2)) {
+        /* fork: the lower half builds the left subtree, the upper half the right one */
+        t = lane < W / 2 ? L : R;
+        W >>= 1;
+        level++;
+        if (level < 4) depth_sp &= ~(15u << (4 * level));
+        continue;
+      }
+      const int sp = (int)((depth_sp >> (4 * level)) & 15u);
+      if (sp < W / 2 - 1) {
+        if (lane == 0) seg_stack(stacks, level, W)[sp] = R;
+        depth_sp += 1u << (4 * level);
+      } else if (lane == 0) {
+        atomicAdd(s.leaf_count + 1, 1u); /* cannot happen (see kWarpStack): reported as a build failure */
+      }
+      __syncwarp(mask);
+      t = L;
       continue;
     }
-    /* the split: best SAH position, or the median along the widest centroid extent */
-    int axis, left_n;
-    if (has_split) {
-      axis = best.key / 64;
-      left_n = best.key % 64 + 1;
-    } else {
-      float ext[3];
-      for (int k = 0; k < 3; k++) {
-        float mn = act ? c[k] : FLT_MAX, mx = act ? c[k] : -FLT_MAX;
-        for (int o = 16; o > 0; o >>= 1)
-          mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o)), mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        ext[k] = mx - mn;
+    if (act) s.order[t.begin + lane] = id;
+    if (lane == 0) finish_leaf(s, t);
+    /* next: the segment's pending sibling; a segment with none waits for its sibling half and the
+     * two continue as their parent */
+    for (;;) {
+      const int sp = level < 4 ? (int)((depth_sp >> (4 * level)) & 15u) : 0;
+      if (sp > 0) {
+        __syncwarp(mask);
+        t = seg_stack(stacks, level, W)[sp - 1];
+        depth_sp -= 1u << (4 * level);
+        __syncwarp(mask);
+        break;
       }
-      axis = ext[1] > ext[0] ? (ext[2] > ext[1] ? 2 : 1) : (ext[2] > ext[0] ? 2 : 0);
-      left_n = (int)n / 2;
+      if (level == 0) return;
+      W <<= 1;
+      level--;
+      mask = seg_mask(W);
+      __syncwarp(mask);
     }
-    /* the SAH pass already sorted every axis: reuse its order for the chosen one */
-    const int from = sorted ? (axis == 0 ? from_a[0] : (axis == 1 ? from_a[1] : from_a[2]))
-                            : warp_sort_idx(act ? c[axis] : FLT_MAX, act ? id : 0xffffffffu - (uint32_t)lane, span);
-    const uint32_t sid = __shfl_sync(0xffffffffu, id, from);
-    float bl[3], bh[3];
-    for (int k = 0; k < 3; k++)
-      bl[k] = __shfl_sync(0xffffffffu, lo[k], from), bh[k] = __shfl_sync(0xffffffffu, hi[k], from);
-    if (act) dst[t.begin + lane] = sid;
-    warp_scan_boxes(bl, bh, pl, ph, sl, sh, span);
-    float cl[3], ch[3], dl[3], dh[3];
-    for (int k = 0; k < 3; k++) {
-      cl[k] = __shfl_sync(0xffffffffu, pl[k], left_n - 1), ch[k] = __shfl_sync(0xffffffffu, ph[k], left_n - 1);
-      dl[k] = __shfl_sync(0xffffffffu, sl[k], left_n), dh[k] = __shfl_sync(0xffffffffu, sh[k], left_n);
-    }
-    const uint32_t mid = t.begin + (uint32_t)left_n;
-    int node = 0;
-    if (lane == 0) {
-      node = (int)atomicAdd(s.node_counter, 1u);
-      if (t.parent >= 0) write_ref(s.nodes, t.parent, t.slot, node);
-      write_child(s.nodes, node, 0, cl, ch);
-      write_child(s.nodes, node, 1, dl, dh);
-      if (wsp < kWarpStack)
-        wstack[wsp] = Task{mid, t.end, node, 1, t.depth + 1, 1 - t.buf, {dl[0], dl[1], dl[2]}, {dh[0], dh[1], dh[2]}};
-      else
-        atomicAdd(s.leaf_count + 1, 1u); /* cannot happen (depth <= 31): reported as a build failure */
-    }
-    node = __shfl_sync(0xffffffffu, node, 0);
-    if (wsp < kWarpStack) wsp++;
-    __syncwarp(); /* the children read ids written by other lanes */
-    t = Task{t.begin, mid, node, 0, t.depth + 1, 1 - t.buf, {cl[0], cl[1], cl[2]}, {ch[0], ch[1], ch[2]}};
   }
-  if (lane == 0) atomicAdd(s.leaf_count + 1, 1u); /* a subtree that did not finish: a build failure */
 }
 
 __global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Task *small_tasks) {
