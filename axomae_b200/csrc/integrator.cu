@@ -1453,6 +1453,18 @@ using WaitReady = std::function<nova_b200_status(size_t)>;
 
 /* Renders frames (one per job) as one wavefront on the executing context `x`.  Jobs are cut into
  * chunks whose per-path radiance fits the radiance buffer; a job's samples stay in order. */
+/* The order frames go into chunks: largest film first.  The films of the last chunk are copied
+ * out after its waves end (those of earlier chunks while later ones render), so it holds the
+ * smallest; a frame's film does not depend on the chunk it lands in. */
+std::vector<uint32_t> chunk_order(const std::vector<const nova_b200_frame *> &frames) {
+  std::vector<uint32_t> ord(frames.size());
+  for (uint32_t j = 0; j < (uint32_t)ord.size(); j++) ord[j] = j;
+  std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+    return (uint64_t)frames[a]->width * frames[a]->height > (uint64_t)frames[b]->width * frames[b]->height;
+  });
+  return ord;
+}
+
 nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *> &ctxs,
                              const std::vector<const nova_b200_frame *> &frames, float *const *films_host,
                              float *const *films_device, nova_b200_render_stats *stats,
@@ -1502,7 +1514,9 @@ nova_b200_status render_jobs(nova_b200_ctx *x, const std::vector<nova_b200_ctx *
   /* cut the work into chunks of at most `radiance` paths and kParamJobs frame pieces */
   std::vector<std::vector<Piece>> chunks(1);
   uint64_t in_chunk = 0;
-  for (size_t j = 0; j < nj; j++) {
+  const std::vector<uint32_t> ord = chunk_order(frames);
+  for (size_t q = 0; q < nj; q++) {
+    const size_t j = ord[q];
     const nova_b200_frame *f = frames[j];
     const uint64_t np = (uint64_t)f->width * f->height;
     uint32_t s = 0;
@@ -1703,8 +1717,13 @@ nova_b200_status nb_upload_build_render_batch(nova_b200_ctx *const *ctxs, const 
   std::vector<int> done(n, kPending);
   std::atomic<uint32_t> next{0};
   std::atomic<bool> stop{false};
+  /* scenes are built in the order chunks render them, the executing context's own first (its stream
+   * carries the render) */
+  std::vector<uint32_t> ord = chunk_order(fs);
+  std::rotate(ord.begin(), std::find(ord.begin(), ord.end(), 0u), std::find(ord.begin(), ord.end(), 0u) + 1);
   auto work = [&] {
-    for (uint32_t k; (k = next.fetch_add(1)) < n;) {
+    for (uint32_t q; (q = next.fetch_add(1)) < n;) {
+      const uint32_t k = ord[q];
       nova_b200_status st = stop.load() ? NOVA_B200_RENDERER_EXCEPTION : nova_b200_upload_scene(cs[k], &descs[k]);
       if (st == NOVA_B200_SUCCESS) st = nova_b200_build_bvh(cs[k], opts);
       {
