@@ -105,6 +105,34 @@ __device__ __forceinline__ void atomic_max_f(float *a, float v) {
     atomicMin(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
 }
 
+/* Adds each valid lane's primitive (box bl, bh) to bin b of one axis's shared bins.  When every lane
+ * of the warp falls in the same bin (neighbouring primitives of a large node often do) the warp
+ * reduces first and one lane adds, instead of 32 same-address atomics that execute one after the
+ * other.  Counts, minima and maxima are exact, so the bins are the same either way.  All 32 lanes
+ * call it. */
+__device__ __forceinline__ void bin_add(unsigned *cnt, float (*lo)[3], float (*hi)[3], int b, bool valid,
+                                        const float4 &bl, const float4 &bh) {
+  const unsigned same = __match_any_sync(0xffffffffu, valid ? b : -1);
+  if (same == 0xffffffffu) {
+    if (!valid) return; /* uniform: an invalid lane's -1 matches only other invalid lanes */
+    float l0 = bl.x, l1 = bl.y, l2 = bl.z, h0 = bh.x, h1 = bh.y, h2 = bh.z;
+    for (int o = 16; o > 0; o >>= 1) {
+      l0 = fminf(l0, __shfl_xor_sync(0xffffffffu, l0, o)), l1 = fminf(l1, __shfl_xor_sync(0xffffffffu, l1, o));
+      l2 = fminf(l2, __shfl_xor_sync(0xffffffffu, l2, o)), h0 = fmaxf(h0, __shfl_xor_sync(0xffffffffu, h0, o));
+      h1 = fmaxf(h1, __shfl_xor_sync(0xffffffffu, h1, o)), h2 = fmaxf(h2, __shfl_xor_sync(0xffffffffu, h2, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&cnt[b], 32u);
+      atomic_min_f(&lo[b][0], l0), atomic_min_f(&lo[b][1], l1), atomic_min_f(&lo[b][2], l2);
+      atomic_max_f(&hi[b][0], h0), atomic_max_f(&hi[b][1], h1), atomic_max_f(&hi[b][2], h2);
+    }
+  } else if (valid) {
+    atomicAdd(&cnt[b], 1u);
+    atomic_min_f(&lo[b][0], bl.x), atomic_min_f(&lo[b][1], bl.y), atomic_min_f(&lo[b][2], bl.z);
+    atomic_max_f(&hi[b][0], bh.x), atomic_max_f(&hi[b][1], bh.y), atomic_max_f(&hi[b][2], bh.z);
+  }
+}
+
 __device__ __forceinline__ float3 centroid(const Shared &s, uint32_t i) {
   float4 a = __ldg(s.lo + i), b = __ldg(s.hi + i);
   return make_float3((a.x + b.x) * 0.5f, (a.y + b.y) * 0.5f, (a.z + b.z) * 0.5f);
@@ -283,16 +311,17 @@ __global__ void k_bin(Shared s, const Task *tasks, const Chunk *chunks, const fl
     scale[a] = bin_scale(cmin[a], cb[6 * c.task + 3 + a], nb);
   }
   __syncthreads();
-  for (uint32_t i = c.begin + threadIdx.x; i < c.end; i += blockDim.x) {
-    const uint32_t id = src[i];
-    const float4 bl = __ldg(s.lo + id), bh = __ldg(s.hi + id);
-    const float3 p = make_float3((bl.x + bh.x) * 0.5f, (bl.y + bh.y) * 0.5f, (bl.z + bh.z) * 0.5f);
-    for (int a = 0; a < 3; a++) {
-      const int b = bin_of(comp(p, a), cmin[a], scale[a], nb);
-      atomicAdd(&scnt[a][b], 1u);
-      atomic_min_f(&slo[a][b][0], bl.x), atomic_min_f(&slo[a][b][1], bl.y), atomic_min_f(&slo[a][b][2], bl.z);
-      atomic_max_f(&shi[a][b][0], bh.x), atomic_max_f(&shi[a][b][1], bh.y), atomic_max_f(&shi[a][b][2], bh.z);
+  for (uint32_t r0 = c.begin; r0 < c.end; r0 += blockDim.x) { /* whole warps: bin_add votes */
+    const uint32_t i = r0 + threadIdx.x;
+    const bool valid = i < c.end;
+    float4 bl = make_float4(0.f, 0.f, 0.f, 0.f), bh = bl;
+    if (valid) {
+      const uint32_t id = src[i];
+      bl = __ldg(s.lo + id), bh = __ldg(s.hi + id);
     }
+    const float3 p = make_float3((bl.x + bh.x) * 0.5f, (bl.y + bh.y) * 0.5f, (bl.z + bh.z) * 0.5f);
+    for (int a = 0; a < 3; a++)
+      bin_add(scnt[a], slo[a], shi[a], bin_of(comp(p, a), cmin[a], scale[a], nb), valid, bl, bh);
   }
   __syncthreads();
   Bins &g = bins[c.task];
@@ -464,30 +493,35 @@ __global__ void k_partition(Shared s, const Task *tasks, const Chunk *chunks, Sp
 
 /* ------------------------------------------------------------------ small nodes */
 
-__device__ unsigned block_exclusive_scan(unsigned v, unsigned *sh /* 32 */, unsigned *total) {
+/* Sum of v over the block (every thread gets it).  sh: blockDim.x / 32 entries.  Two barriers. */
+__device__ __forceinline__ unsigned block_sum(unsigned v, unsigned *sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  unsigned x = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
+  v = __reduce_add_sync(0xffffffffu, v);
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  unsigned t = 0;
+  for (int j = 0; j < nw; j++) t += sh[j];
+  __syncthreads();
+  return t;
+}
+
+/* One round of a stable two-way partition over the block: this thread's rank among the round's
+ * valid left (or right) threads in thread order, and the round's left and right totals.
+ * sh: 2 * (blockDim.x / 32) entries.  Two barriers. */
+__device__ __forceinline__ unsigned round_rank(bool valid, bool left, unsigned *sh, unsigned &tl, unsigned &tr) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned ml = __ballot_sync(0xffffffffu, valid && left), mr = __ballot_sync(0xffffffffu, valid && !left);
+  if (lane == 0) sh[w] = __popc(ml), sh[nw + w] = __popc(mr);
+  __syncthreads();
+  unsigned bl = 0, br = 0;
+  tl = tr = 0;
+  for (int j = 0; j < nw; j++) {
+    if (j < w) bl += sh[j], br += sh[nw + j];
+    tl += sh[j], tr += sh[nw + j];
   }
   __syncthreads();
-  if (lane == 31) sh[w] = x;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned run = 0;
-    for (int j = 0; j < nw; j++) {
-      unsigned a = sh[j];
-      sh[j] = run;
-      run += a;
-    }
-    sh[31] = run;
-  }
-  __syncthreads();
-  const unsigned r = sh[w] + x - v;
-  *total = sh[31];
-  __syncthreads();
-  return r;
+  const unsigned below = (1u << lane) - 1u;
+  return left ? bl + __popc(ml & below) : br + __popc(mr & below);
 }
 
 /* ------------------------------------------------------------------ warp subtrees (<= 32 primitives)
@@ -779,16 +813,17 @@ __global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Tas
     Best best{FLT_MAX, 0x7fffffff};
     const float area = half_area(t.lo, t.hi);
     if (!make_leaf) {
-      for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
-        const uint32_t id = src[i];
-        const float4 bl = __ldg(s.lo + id), bh = __ldg(s.hi + id);
-        const float3 p = make_float3((bl.x + bh.x) * 0.5f, (bl.y + bh.y) * 0.5f, (bl.z + bh.z) * 0.5f);
-        for (int a = 0; a < 3; a++) {
-          const int b = bin_of(comp(p, a), cmin_s[a], scale_s[a], nb);
-          atomicAdd(&scnt[a][b], 1u);
-          atomic_min_f(&slo[a][b][0], bl.x), atomic_min_f(&slo[a][b][1], bl.y), atomic_min_f(&slo[a][b][2], bl.z);
-          atomic_max_f(&shi[a][b][0], bh.x), atomic_max_f(&shi[a][b][1], bh.y), atomic_max_f(&shi[a][b][2], bh.z);
+      for (uint32_t r0 = t.begin; r0 < t.end; r0 += blockDim.x) { /* whole warps: bin_add votes */
+        const uint32_t i = r0 + threadIdx.x;
+        const bool valid = i < t.end;
+        float4 bl = make_float4(0.f, 0.f, 0.f, 0.f), bh = bl;
+        if (valid) {
+          const uint32_t id = src[i];
+          bl = __ldg(s.lo + id), bh = __ldg(s.hi + id);
         }
+        const float3 p = make_float3((bl.x + bh.x) * 0.5f, (bl.y + bh.y) * 0.5f, (bl.z + bh.z) * 0.5f);
+        for (int a = 0; a < 3; a++)
+          bin_add(scnt[a], slo[a], shi[a], bin_of(comp(p, a), cmin_s[a], scale_s[a], nb), valid, bl, bh);
       }
       __syncthreads();
       if (area > 0.f && t.depth < kMedianDepth)
@@ -821,9 +856,7 @@ __global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Tas
                               : i < mid_med;
         cnt += left;
       }
-      unsigned tot;
-      block_exclusive_scan(cnt, scan_sh, &tot);
-      left_total = tot;
+      left_total = block_sum(cnt, scan_sh);
     }
     const uint32_t mid = t.begin + left_total;
     unsigned run_l = 0, run_r = 0;
@@ -838,10 +871,9 @@ __global__ void __launch_bounds__(kSmallBlock) k_build_small(Shared s, const Tas
                          : i < mid_med;
       }
       unsigned tl, tr;
-      const unsigned pl = block_exclusive_scan(valid && left, scan_sh, &tl);
-      const unsigned pr = block_exclusive_scan(valid && !left, scan_sh, &tr);
+      const unsigned rank = round_rank(valid, left, scan_sh, tl, tr);
       if (valid) {
-        const uint32_t pos = left ? t.begin + run_l + pl : mid + run_r + pr;
+        const uint32_t pos = left ? t.begin + run_l + rank : mid + run_r + rank;
         if (left ? (pos < mid) : (pos < t.end))
           dst[pos] = id;
         else
