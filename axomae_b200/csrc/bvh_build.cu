@@ -11,6 +11,7 @@
  *     k_bin          centroid bins per axis in shared memory, merged into the node's global bins
  *     k_split        one CTA per node: SAH over bins*3 candidate planes, node allocation, children
  *     k_partition    primitive ids scattered to the children's ranges of the other id buffer
+ *     k_make_chunks  the next level's chunk list (the host reads back only the task and chunk counts)
  *   small nodes (<= small_task): k_build_small, one CTA per node builds its whole subtree with a
  *     CTA-local task stack, shared-memory bins and a stable block-scan partition; nodes of at most
  *     32 primitives are handed to single warps (exact sweep SAH over sorted centroids, no barriers).
@@ -489,6 +490,52 @@ __global__ void k_partition(Shared s, const Task *tasks, const Chunk *chunks, Sp
     }
     __syncthreads();
   }
+}
+
+/* The next level's chunk list, on the device: every task's primitives cut into kChunk pieces, in
+ * task order (one block; an exclusive scan of the tasks' chunk counts, tile by tile).  The host
+ * then reads only the task and chunk counts. */
+__global__ void k_make_chunks(const Task *tasks, const unsigned *n_tasks, Chunk *chunks, unsigned max_chunks,
+                              unsigned *n_chunks, unsigned *errors) {
+  __shared__ unsigned warp_sum[32];
+  __shared__ unsigned base;
+  const unsigned nt = *n_tasks;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  for (unsigned t0 = 0; t0 < nt; t0 += blockDim.x) {
+    const unsigned t = t0 + threadIdx.x;
+    uint32_t b = 0, e = 0;
+    unsigned c = 0;
+    if (t < nt) {
+      b = tasks[t].begin;
+      e = tasks[t].end;
+      c = (e - b + kChunk - 1) / kChunk;
+    }
+    unsigned x = c; /* inclusive scan within the warp, then over the warps */
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[w] = x;
+    __syncthreads();
+    unsigned before = 0, tile = 0;
+    for (int j = 0; j < nw; j++) {
+      if (j < w) before += warp_sum[j];
+      tile += warp_sum[j];
+    }
+    const unsigned off = base + before + x - c;
+    for (unsigned k = 0; k < c; k++) {
+      if (off + k < max_chunks)
+        chunks[off + k] = Chunk{t, b + k * kChunk, min(e, b + (k + 1) * kChunk)};
+      else
+        atomicAdd(errors, 1u); /* cannot happen (the capacity bounds the chunks): a build failure */
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) base += tile;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_chunks = base;
 }
 
 /* ------------------------------------------------------------------ small nodes */
@@ -1071,7 +1118,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
   /* scratch */
   uint32_t *ids0 = nullptr, *ids1 = nullptr;
   Task *large_a = nullptr, *large_b = nullptr, *small = nullptr;
-  unsigned *counters = nullptr; /* node, large_next, small, leaf, partition errors */
+  unsigned *counters = nullptr; /* node, large_next, small, leaf, partition errors, next level's chunks */
   uint2 *leaves = nullptr;
   int *maxdepth = nullptr;
   float *scene = nullptr, *cb = nullptr;
@@ -1091,7 +1138,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     NB_TRY(cudaMallocAsync(&large_a, sizeof(Task) * max_large, stream));
     NB_TRY(cudaMallocAsync(&large_b, sizeof(Task) * max_large, stream));
     NB_TRY(cudaMallocAsync(&small, sizeof(Task) * max_small, stream));
-    NB_TRY(cudaMallocAsync(&counters, sizeof(unsigned) * 5, stream));
+    NB_TRY(cudaMallocAsync(&counters, sizeof(unsigned) * 6, stream));
     NB_TRY(cudaMallocAsync(&leaves, sizeof(uint2) * n, stream));
     NB_TRY(cudaMallocAsync(&maxdepth, sizeof(int), stream));
     NB_TRY(cudaMallocAsync(&scene, sizeof(float) * 6, stream));
@@ -1099,7 +1146,7 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     NB_TRY(cudaMallocAsync(&bins, sizeof(Bins) * max_large, stream));
     NB_TRY(cudaMallocAsync(&splits, sizeof(SplitInfo) * max_large, stream));
     NB_TRY(cudaMallocAsync(&chunks, sizeof(Chunk) * max_chunks, stream));
-    NB_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * 5, stream));
+    NB_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * 6, stream));
     NB_TRY(cudaMemsetAsync(maxdepth, 0, sizeof(int), stream));
     {
       const float init[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -1133,23 +1180,23 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
     sh.small_task = small_task;
 
     Task root{0u, n, -1, 0, 0, 0, {hscene[0], hscene[1], hscene[2]}, {hscene[3], hscene[4], hscene[5]}};
-    std::vector<Task> level;
+    Task *cur = large_a, *next = large_b;
+    uint32_t nt = 0, nc = 0; /* tasks and chunks of the current level */
     if (n > small_task) {
-      level.push_back(root);
+      std::vector<Chunk> ch;
+      for (uint32_t b = 0; b < n; b += kChunk) ch.push_back(Chunk{0u, b, std::min(n, b + kChunk)});
+      nt = 1;
+      nc = (uint32_t)ch.size();
+      NB_TRY(cudaMemcpyAsync(cur, &root, sizeof(Task), cudaMemcpyHostToDevice, stream));
+      NB_TRY(cudaMemcpyAsync(chunks, ch.data(), sizeof(Chunk) * nc, cudaMemcpyHostToDevice, stream));
     } else {
       NB_TRY(cudaMemcpyAsync(small, &root, sizeof(Task), cudaMemcpyHostToDevice, stream));
       const unsigned one = 1;
       NB_TRY(cudaMemcpyAsync(counters + 2, &one, sizeof(unsigned), cudaMemcpyHostToDevice, stream));
     }
-    Task *cur = large_a, *next = large_b;
-    while (!level.empty()) {
-      std::vector<Chunk> ch;
-      for (uint32_t ti = 0; ti < level.size(); ti++)
-        for (uint32_t b = level[ti].begin; b < level[ti].end; b += kChunk)
-          ch.push_back(Chunk{ti, b, std::min(level[ti].end, b + kChunk)});
-      const uint32_t nt = (uint32_t)level.size(), nc = (uint32_t)ch.size();
-      NB_TRY(cudaMemcpyAsync(cur, level.data(), sizeof(Task) * nt, cudaMemcpyHostToDevice, stream));
-      NB_TRY(cudaMemcpyAsync(chunks, ch.data(), sizeof(Chunk) * nc, cudaMemcpyHostToDevice, stream));
+    /* one level per iteration: the level's tasks and chunks stay on the device, the host reads their
+     * counts (one synchronisation per level) */
+    while (nt > 0) {
       NB_TRY(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned), stream));
       sh.large_next = next;
       k_init_level<<<nt, 128, 0, stream>>>(bins, cb, nt, nb);
@@ -1157,13 +1204,14 @@ cudaError_t build_bvh(const float4 *lo, const float4 *hi, uint32_t n, const BvhB
       k_bin<<<nc, kBlock, 0, stream>>>(sh, cur, chunks, cb, bins);
       k_split<<<nt, kBlock, 0, stream>>>(sh, cur, cb, bins, splits);
       k_partition<<<nc, kBlock, 0, stream>>>(sh, cur, chunks, splits);
+      k_make_chunks<<<1, 1024, 0, stream>>>(next, counters + 1, chunks, (unsigned)max_chunks, counters + 5,
+                                            counters + 4);
       NB_TRY(cudaGetLastError());
-      unsigned n_next = 0;
-      NB_TRY(cudaMemcpyAsync(&n_next, counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+      unsigned hn[5]; /* counters 1..5: next level's tasks, small tasks, leaves, errors, next level's chunks */
+      NB_TRY(cudaMemcpyAsync(hn, counters + 1, sizeof(hn), cudaMemcpyDeviceToHost, stream));
       NB_TRY(cudaStreamSynchronize(stream));
-      level.resize(n_next);
-      if (n_next) NB_TRY(cudaMemcpyAsync(level.data(), next, sizeof(Task) * n_next, cudaMemcpyDeviceToHost, stream));
-      NB_TRY(cudaStreamSynchronize(stream));
+      nt = hn[0];
+      nc = hn[4];
       std::swap(cur, next);
     }
     unsigned n_small = 0;
