@@ -90,7 +90,10 @@ bool is_identity(const float *m) {
  * bytes are read by a gather kernel when the caller's memory is pinned, else gathered in a pinned
  * host buffer and copied with one transfer; larger ones are copied directly from the caller's
  * memory. */
-constexpr size_t kSmallPiece = 1 << 16;
+/* 32 batch scenes (2,738 meshes, 444 MB, each array pinned on its own): with 64 KB the mesh arrays
+ * above it went one cudaMemcpyAsync each and the uploads took 24.7 ms (18 GB/s); with 256 KB they
+ * take 14.7 ms (30 GB/s), with 1 MB 16.6 ms. */
+constexpr size_t kSmallPiece = 1 << 18;
 
 struct Piece {
   const void *src;
