@@ -360,6 +360,31 @@ def test_upload_from_pinned_memory_equals_pageable(ctx, torch_cuda):
         other.close()
 
 
+def test_bvh_independent_of_subtree_threshold(ctx, torch_cuda):
+    """Nodes above the subtree threshold are split by the level kernels, smaller ones inside one CTA
+    (binned SAH, stable partition) and those of <= 32 primitives by warp lane segments (exact sweep).
+    The level kernels and the CTA path take the same binned decisions, so moving the threshold
+    gives the same tree: the same node and leaf counts, node visits per ray and film bit for bit."""
+    from axomae_b200 import native, scenes
+    s = scenes.mixed_scene(60000, 40, 32, seed=9)
+    fr = native.make_frame(s, 40, 32, 4, 6)
+    ctx.upload(s)
+    out = []
+    for small in (64, 256, 4096):
+        ctx.build(small_subtree=small)
+        info = {k: v for k, v in ctx.info().items() if k != "device_bytes"}
+        film = np.zeros((32, 40, 4), np.float32)
+        ctx.render(fr, film_host=film)
+        ctx.set_tuning(trace_mode=2)
+        st = ctx.render(fr, film_host=np.zeros_like(film))
+        ctx.set_tuning()
+        out.append((info, film, st.node_visits, st.tri_tests))
+    for info, film, nv, tt in out[1:]:
+        assert info == out[0][0]
+        assert np.array_equal(film.view(np.uint32), out[0][1].view(np.uint32))
+        assert (nv, tt) == (out[0][2], out[0][3])
+
+
 def test_batch_equals_individual_renders(torch_cuda):
     """nova_b200_render_batch: frames of different scenes, sizes, sample counts and depths rendered
     as one wavefront equal the same frames rendered one by one, bit for bit."""
