@@ -216,13 +216,15 @@ nova_b200_status nova_b200_render(nova_b200_ctx *ctx, const nova_b200_frame *fra
  * the batch takes several chunks (more than 104 frames, or more paths than one radiance buffer
  * holds), the films of frames finished in an earlier chunk are copied out on a second stream while
  * later chunks render, if they are device or pinned host buffers; pageable ones are written at the
- * end.  The call returns after every copy. */
+ * end.  Chunks take the frames largest film first (so the films left to copy after the last chunk
+ * are the smallest); a film does not depend on its chunk.  The call returns after every copy. */
 nova_b200_status nova_b200_render_batch(nova_b200_ctx *const *ctxs, const nova_b200_frame *frames, uint32_t n,
                                         float *const *films_host, float *const *films_device,
                                         nova_b200_render_stats *stats);
 
 /* Upload, build and render in one call (no counterpart in the reference): up to 16 host threads
- * upload each context's scene and build its BVH (opts may be NULL) in batch order, while the calling
+ * upload each context's scene and build its BVH (opts may be NULL) in the order the chunks render
+ * them (ctxs[0]'s scene first: its stream carries the render), while the calling
  * thread renders the frames as nova_b200_render_batch does, starting each chunk of the wavefront as
  * soon as the scenes of its frames are built; the later scenes' copies and builds overlap the first
  * chunks.  Scenes, BVHs and films equal those of nova_b200_upload_scene_batch,
